@@ -1,0 +1,386 @@
+"""Benchmark of the headline path: multi-seed LM IK with collision penalty.
+
+Workload (one "step"): 256 IK problems x 128 seeds of the 7-DOF revolute
+chain, 30 LM iterations (lambda 1e-2, x0.1 on accept, x10 on reject), 56
+robot spheres against 100 obstacle spheres plus 200 self-collision sphere
+pairs (hinge^2, margin 0.02 m, weight 1e4), then FP64 re-verification of
+every problem's winning seed (success = position < 1 mm and rotation
+< 0.01 rad).  Seeded synthetic data (pyroffi_b200.workloads.ik, seed 1002).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line.  ``value`` is problems solved per second over all
+ranks with the inputs resident in HBM; ``e2e`` is the same through the
+public solver API from pinned host buffers (H2D of seeds + targets, D2H of
+winners / errors / success flags inside the timed region).  ``--impl
+reference`` times the CPU port of the reference LM loop (oracle/cpu, FP32,
+OpenMP over all host threads) on a bounded sample of the same workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "IK solves/s @1mm/0.01rad (256 targets x 128 seeds, 30 LM iters, 100 obstacle spheres + 200 self pairs)"
+UNIT = "solves/s"
+P_PER_GPU, SEEDS, ITERS = 256, 128, 30
+# algorithmic FLOP per seed-iteration: 6 error evaluations of
+# (FK 130*7 + residual 60 + sphere transforms 33*56 + world pairs 12*56*100 + self pairs 12*200)
+# + Jacobian 45*7 + normal equations and Cholesky ~800
+FLOP_PER_SEED_ITER = 6 * (130 * 7 + 60 + 33 * 56 + 12 * 56 * 100 + 12 * 200) + 45 * 7 + 800
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-sample", type=int, default=8, help="problems per CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+# ---------------------------------------------------------------------------
+# CPU port (reference arm and cpu_baseline)
+# ---------------------------------------------------------------------------
+
+def cpu_port_lib():
+    import ctypes as C
+
+    so = ROOT / "oracle" / "_build" / "libpk_cpu.so"
+    if not so.exists():
+        subprocess.run(["make", "-C", str(ROOT / "oracle"), "cpu"], check=True, capture_output=True)
+    lib = C.CDLL(str(so))
+    lib.pk_cpu_max_threads.restype = C.c_int
+    return lib
+
+
+def cpu_solve(lib, w, p0, n_prob, n_threads):
+    """Run the CPU port on problems [p0, p0+n_prob); returns (seconds, cfgs, errs)."""
+    import ctypes as C
+
+    m = w.model
+    fp = lambda a: np.ascontiguousarray(a).ctypes.data_as(C.c_void_p)  # noqa: E731
+    keep = []
+
+    def arr(a, dt):
+        a = np.ascontiguousarray(a, dtype=dt)
+        keep.append(a)
+        return a.ctypes.data_as(C.c_void_p)
+
+    seeds = np.ascontiguousarray(w.seeds[p0:p0 + n_prob])
+    tgt = np.ascontiguousarray(w.target_T[p0:p0 + n_prob, None, :])
+    out_cfg = np.zeros_like(seeds)
+    out_err = np.zeros(seeds.shape[:2], np.float32)
+    tj = np.asarray([m.link_joint(w.target_link)], np.int32)
+    anc = m.ancestor_mask(w.target_link)[None]
+    f32, i32 = np.float32, np.int32
+    t0 = time.perf_counter()
+    st = lib.pk_cpu_ls_ik(
+        fp(seeds), arr(m.twists, f32), arr(m.parent_tf, f32), arr(m.parent_idx, i32), arr(m.act_idx, i32),
+        arr(m.mimic_mul, f32), arr(m.mimic_off, f32), arr(m.mimic_act_idx, i32), arr(m.topo_inv, i32),
+        arr(tj, i32), arr(anc, i32), fp(tgt), arr(w.spheres_local, f32), arr(w.sphere_joint, i32),
+        arr(w.world.spheres, f32), arr(w.self_pairs[:, 0], i32), arr(w.self_pairs[:, 1], i32),
+        arr(m.lower, f32), arr(m.upper, f32), arr(np.zeros(m.n_act), i32), fp(out_cfg), fp(out_err),
+        C.c_int(n_prob), C.c_int(seeds.shape[1]), C.c_int(m.n_act), C.c_int(m.n_joints), C.c_int(1),
+        C.c_int(len(w.spheres_local)), C.c_int(len(w.world.spheres)), C.c_int(len(w.self_pairs)),
+        C.c_int(w.max_iter), C.c_float(w.pos_weight), C.c_float(w.ori_weight), C.c_float(w.lambda_init),
+        C.c_float(w.lambda_down), C.c_float(w.lambda_up), C.c_float(1e-8), C.c_float(1e-8), C.c_int(1),
+        C.c_float(w.collision_weight), C.c_float(w.collision_margin), C.c_int(n_threads))
+    dt = time.perf_counter() - t0
+    if st != 0:
+        raise RuntimeError(f"pk_cpu_ls_ik failed ({st})")
+    return dt, out_cfg, out_err
+
+
+def cpu_success(w, p0, cfgs, errs):
+    from oracle import lm as olm
+
+    win, _ = olm.select_winner(cfgs.astype(np.float64), errs)
+    pe, re = olm.pose_errors(win, w.target_T[p0:p0 + len(cfgs)].astype(np.float64), w.model.as_dict(),
+                             w.model.link_joint(w.target_link))
+    return float(np.mean((pe < w.pos_tol) & (re < w.rot_tol)))
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    from pyroffi_b200 import workloads as W
+
+    w = W.ik(P=P_PER_GPU, Sd=SEEDS)
+    lib = cpu_port_lib()
+    threads = lib.pk_cpu_max_threads()
+    n = args.cpu_sample
+    for i in range(args.warmup):
+        cpu_solve(lib, w, (i * n) % P_PER_GPU, min(n, 2), threads)
+    times, succ = [], []
+    for i in range(args.steps):
+        p0 = (i * n) % P_PER_GPU
+        dt, cfgs, errs = cpu_solve(lib, w, p0, n, threads)
+        times.append(dt)
+        succ.append(cpu_success(w, p0, cfgs, errs))
+    total = sum(times)
+    value = n * args.steps / total
+    sample = f"{n} of the 256 problems per step (all 128 seeds, 30 iterations), problems rotated across steps"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "ik_lm_collision", "problems": P_PER_GPU, "seeds": SEEDS, "iters": ITERS,
+                   "robot": "7-DOF revolute chain", "obstacles": 100, "self_pairs": 200},
+        "success_rate": float(np.mean(succ)),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "reference CPU path is JAX (not installed); timed arm is the C port of the reference LM loop",
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.file = None
+
+    def __enter__(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or self.file is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.file.flush()
+        rows = [r.split(",") for r in Path(self.file.name).read_text().strip().splitlines() if r.strip()]
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            if len(r) < 9:
+                continue
+            for name, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def fp32_peak_tflops(torch, lib_call, stream_ptr):
+    """Measured FP32 FMA roof (TFLOP/s) on this GPU."""
+    out = torch.empty(148 * 8, dtype=torch.float32, device="cuda")
+    blocks, iters = 148 * 8, 20000
+    for _ in range(2):
+        lib_call("pk_fp32_fma_peak", stream_ptr(), out.data_ptr(), iters, blocks)
+    torch.cuda.synchronize()
+    best = None
+    for _ in range(5):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        lib_call("pk_fp32_fma_peak", stream_ptr(), out.data_ptr(), iters, blocks)
+        b.record()
+        b.synchronize()
+        ms = a.elapsed_time(b)
+        best = ms if best is None else min(best, ms)
+    return 4096.0 * iters * blocks / (best * 1e-3) / 1e12
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=120))
+
+    from pyroffi_b200 import _lib, workloads as W
+    from pyroffi_b200.ik import BatchIkSolver
+
+    _lib.load()
+    # each rank solves its own 256 problems (weak scaling; seed offset by rank)
+    w = W.ik(P=P_PER_GPU, Sd=SEEDS, seed=1002)
+    if rank > 0:
+        rng = np.random.default_rng(1002 + rank)
+        w.seeds = rng.uniform(w.model.lower, w.model.upper, size=w.seeds.shape).astype(np.float32)
+    solver = BatchIkSolver(w.model, w.target_link, spheres=w.spheres, world=w.world, self_pairs=w.self_pairs,
+                           max_iter=w.max_iter, lambda_init=w.lambda_init, lambda_down=w.lambda_down,
+                           lambda_up=w.lambda_up, pos_weight=w.pos_weight, ori_weight=w.ori_weight,
+                           collision_weight=w.collision_weight, collision_margin=w.collision_margin,
+                           pos_tol=w.pos_tol, rot_tol=w.rot_tol, device=dev)
+    seeds_d = torch.as_tensor(w.seeds, device=dev)
+    tgt_d = torch.as_tensor(w.target_T, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    # --- device-resident timing -------------------------------------------
+    for _ in range(args.warmup):
+        res = solver.solve(tgt_d, seeds_d)
+    barrier()
+    lm_ms, step_ms = [], []
+    with ClockSampler(local) as clocks:
+        barrier()
+        for _ in range(args.steps):
+            flush.fill_(1.0)                       # evict L2 between steps (outside the timed events)
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            e0.record(stream)
+            cfgs, errs = solver.run_lm(tgt_d, seeds_d)
+            e1.record(stream)
+            res_w = solver.verify_select(cfgs, errs, tgt_d)
+            e2.record(stream)
+            e2.synchronize()
+            lm_ms.append(e0.elapsed_time(e1))
+            step_ms.append(e0.elapsed_time(e2))
+        barrier()
+    clock_summary = clocks.summary()
+    success = float(res_w[3].float().mean().item())
+    t_local = sum(step_ms) / 1e3
+    t_max = t_local
+    if world > 1:
+        tt_ = torch.tensor([t_local], device=dev)
+        dist.all_reduce(tt_, op=dist.ReduceOp.MAX)
+        t_max = float(tt_.item())
+    value = world * P_PER_GPU * args.steps / t_max
+
+    # --- end to end through the public API, host buffers ------------------
+    seeds_h = torch.as_tensor(w.seeds).pin_memory()
+    tgt_h = torch.as_tensor(w.target_T).pin_memory()
+    win_h = torch.empty((P_PER_GPU, w.model.n_act), dtype=torch.float32).pin_memory()
+    ok_h = torch.empty(P_PER_GPU, dtype=torch.int32).pin_memory()
+    pos_h = torch.empty(P_PER_GPU, dtype=torch.float64).pin_memory()
+    rot_h = torch.empty(P_PER_GPU, dtype=torch.float64).pin_memory()
+    h2d = seeds_h.numel() * 4 + tgt_h.numel() * 4
+    d2h = win_h.numel() * 4 + ok_h.numel() * 4 + pos_h.numel() * 8 + rot_h.numel() * 8
+
+    def e2e_step():
+        s = seeds_h.to(dev, non_blocking=True)
+        t = tgt_h.to(dev, non_blocking=True)
+        r = solver.solve(t, s)
+        win_h.copy_(r.winner_cfg, non_blocking=True)
+        ok_h.copy_(r.success, non_blocking=True)
+        pos_h.copy_(r.pos_err, non_blocking=True)
+        rot_h.copy_(r.rot_err, non_blocking=True)
+
+    for _ in range(args.warmup):
+        e2e_step()
+    barrier()
+    e2e_ms = []
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        e2e_step()
+        b.record(stream)
+        b.synchronize()
+        e2e_ms.append(a.elapsed_time(b))
+    barrier()
+    t_e2e = sum(e2e_ms) / 1e3
+    if world > 1:
+        tt_ = torch.tensor([t_e2e], device=dev)
+        dist.all_reduce(tt_, op=dist.ReduceOp.MAX)
+        t_e2e = float(tt_.item())
+    e2e_value = world * P_PER_GPU * args.steps / t_e2e
+
+    line = None
+    if rank == 0:
+        lm_avg_s = statistics.mean(lm_ms) / 1e3
+        flops = FLOP_PER_SEED_ITER * P_PER_GPU * SEEDS * ITERS
+        achieved = flops / lm_avg_s / 1e12
+        peak = fp32_peak_tflops(torch, _lib.call, lambda: stream.cuda_stream)
+        cpu = None
+        if not args.no_cpu_baseline:
+            lib = cpu_port_lib()
+            threads = lib.pk_cpu_max_threads()
+            cpu_solve(lib, w, 0, 1, threads)
+            dt, cfgs_c, errs_c = cpu_solve(lib, w, 0, args.cpu_sample, threads)
+            cpu = {"value": args.cpu_sample / dt, "unit": UNIT, "cores": threads, "kind": "port",
+                   "sample": f"{args.cpu_sample} problems x 128 seeds x 30 iterations (C port, OpenMP)",
+                   "success_rate": cpu_success(w, 0, cfgs_c, errs_c)}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "ik_lm_collision", "problems_per_gpu": P_PER_GPU, "seeds": SEEDS,
+                       "iters": ITERS, "robot": "7-DOF revolute chain, 56 spheres", "obstacles": 100,
+                       "self_pairs": 200, "lambda": "1e-2, x0.1 accept / x10 reject",
+                       "l2": "flushed (256 MB write) between timed steps"},
+            "success_rate": success,
+            "gpu_launches": 2 * args.steps,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": None, "kernel": "lm_kernel<8,1,4>",
+                         "peak_source": "measured FP32 FMA microbenchmark (pk_fp32_fma_peak), this run",
+                         "flop_per_seed_iter": FLOP_PER_SEED_ITER},
+            "kernel_ms": {"lm": statistics.mean(lm_ms), "verify_select": statistics.mean(step_ms) - statistics.mean(lm_ms)},
+            "clocks": clock_summary,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

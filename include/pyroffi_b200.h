@@ -1,0 +1,222 @@
+/*
+ * pyroffi_b200 -- C-ABI of the B200 (sm_100a) kinematics hot path.
+ *
+ * Every entry point takes plain device pointers, sizes and a CUDA stream
+ * (passed as void*, a cudaStream_t), launches on that stream and returns an
+ * int status (PK_OK or a PK_ERR_* code; pk_last_error() gives the message of
+ * the calling thread's last failure).  No entry point keeps a caller's
+ * pointer after it returns, synchronises the stream, or allocates device
+ * memory.  All arrays are row-major, float32 / int32, device-resident.
+ *
+ * The drop-in entry points mirror, argument for argument and in the same
+ * order, the XLA FFI handlers of the reference (CoMMALab/pyroffi,
+ * src/pyroffi/cuda_kernels/); the extents that an XLA buffer carries are
+ * passed explicitly after the buffers.
+ */
+#ifndef PYROFFI_B200_H_
+#define PYROFFI_B200_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define PK_OK 0
+#define PK_ERR_INVALID 1   /* bad shape / index / argument (reference: kInvalidArgument) */
+#define PK_ERR_CAPACITY 2  /* exceeds a compile-time capacity (joints, DOF, EEs, smem) */
+#define PK_ERR_CUDA 3      /* a CUDA runtime call failed (reference: kInternal) */
+#define PK_ERR_TIMEOUT 4   /* a bounded device-side wait ran out */
+
+/* capacities */
+#define PK_MAX_JOINTS_ABI 64
+#define PK_MAX_ACT_ABI 32
+#define PK_MAX_EE_ABI 4
+
+const char* pk_version(void);
+const char* pk_last_error(void);
+const char* pk_status_string(int status);
+
+/*
+ * Forward kinematics: world pose of every joint, out[B, n_joints, 7] wxyz_xyz.
+ * Replaces the XLA FFI target "fk_cuda" (FkCudaFfi,
+ * src/pyroffi/cuda_kernels/_fk_cuda_kernel.cu:236-471); argument order as in
+ * its Bind() (:456-471): cfg[B,n_act], twists[n_j,6], parent_tf[n_j,7],
+ * parent_idx, act_idx, mimic_mul, mimic_off, mimic_act_idx, topo_inv [n_j],
+ * fk_level_starts[n_levels+1], fk_level_joints[n_j].
+ */
+int pk_fk_cuda(void* stream, const float* cfg, const float* twists, const float* parent_tf,
+               const int32_t* parent_idx, const int32_t* act_idx, const float* mimic_mul,
+               const float* mimic_off, const int32_t* mimic_act_idx, const int32_t* topo_inv,
+               const int32_t* fk_level_starts, const int32_t* fk_level_joints, float* out,
+               int64_t batch, int32_t n_act, int32_t n_joints, int32_t n_levels);
+
+/*
+ * World distances of robot spheres, out[B, K, M], M = Ms+Mc+Mb+Mh (spheres,
+ * capsules, boxes, halfspaces in that order); spheres with radius < 0 give
+ * 1e9.  Replaces "collision_world_sphere" (CollisionWorldSphereFfi,
+ * src/pyroffi/cuda_kernels/_collision_cuda_kernel.cu:507-671).
+ * centers[3,B,K] SoA, radii[B,K], ws[Ms,4], wc[Mc,7], wb[Mb,15], wh[Mh,6].
+ */
+int pk_collision_world_sphere(void* stream, const float* centers, const float* radii,
+                              const float* world_spheres, const float* world_capsules,
+                              const float* world_boxes, const float* world_halfspaces, float* out,
+                              int64_t B, int32_t K, int32_t Ms, int32_t Mc, int32_t Mb, int32_t Mh);
+
+/*
+ * Per-link minimum over its S spheres (sphere k = s*N + n), out[B, N, M].
+ * Replaces "collision_world_sphere_reduced" (CollisionWorldSphereReducedFfi,
+ * _collision_cuda_kernel.cu:673-839); n = the int64 attribute "n".
+ */
+int pk_collision_world_sphere_reduced(void* stream, const float* centers, const float* radii,
+                                      const float* world_spheres, const float* world_capsules,
+                                      const float* world_boxes, const float* world_halfspaces,
+                                      float* out, int64_t B, int32_t K, int32_t Ms, int32_t Mc,
+                                      int32_t Mb, int32_t Mh, int64_t n);
+
+/*
+ * Capsule robot vs world, out[B, N, M]; caps[7,B,N] SoA (p1, p2, r).
+ * Replaces "collision_world_capsule" (CollisionWorldCapsuleFfi,
+ * _collision_cuda_kernel.cu:843-1004).
+ */
+int pk_collision_world_capsule(void* stream, const float* caps, const float* world_spheres,
+                               const float* world_capsules, const float* world_boxes,
+                               const float* world_halfspaces, float* out, int64_t B, int32_t N,
+                               int32_t Ms, int32_t Mc, int32_t Mb, int32_t Mh);
+
+/*
+ * Self distances, out[B, P] = min over all S x S sphere pairs of links
+ * (pair_i[p], pair_j[p]); centers[B,S,N,3] AoS, radii[B,S,N]; padding
+ * (radius < 0) skipped.  Replaces "collision_self_sphere"
+ * (CollisionSelfSphereFfi, _collision_cuda_kernel.cu:1006-1111).
+ */
+int pk_collision_self_sphere(void* stream, const float* centers, const float* radii,
+                             const int32_t* pair_i, const int32_t* pair_j, float* out, int64_t B,
+                             int32_t S, int32_t N, int32_t P);
+
+/*
+ * Capsule self distances, out[B, P]; caps[B,N,7] AoS.  Replaces
+ * "collision_self_capsule" (CollisionSelfCapsuleFfi,
+ * _collision_cuda_kernel.cu:1114-1214).
+ */
+int pk_collision_self_capsule(void* stream, const float* caps, const int32_t* pair_i,
+                              const int32_t* pair_j, float* out, int64_t B, int32_t N, int32_t P);
+
+/*
+ * Multi-seed Levenberg-Marquardt IK, out_cfg[P, Sd, n_act] (best config per
+ * seed) and out_err[P, Sd] (its weighted squared error incl. the collision
+ * penalty).  Replaces "ls_ik_cuda" (LsIkCudaFfi,
+ * src/pyroffi/cuda_kernels/_ls_ik_cuda_kernel.cu:400-529): arguments in the
+ * order of its Bind() (:493-529), attributes max_iter .. collision_margin
+ * after the buffers, then the extents.  Damping factors are the reference's
+ * x0.5 on accept, x3 on reject.
+ */
+int pk_ls_ik_cuda(void* stream, const float* seeds, const float* twists, const float* parent_tf,
+                  const int32_t* parent_idx, const int32_t* act_idx, const float* mimic_mul,
+                  const float* mimic_off, const int32_t* mimic_act_idx, const int32_t* topo_inv,
+                  const int32_t* target_jnts, const int32_t* ancestor_masks, const float* target_Ts,
+                  const float* robot_spheres_local, const int32_t* robot_sphere_joint_idx,
+                  const float* world_spheres, const float* world_capsules, const float* world_boxes,
+                  const float* world_halfspaces, const float* lower, const float* upper,
+                  const int32_t* fixed_mask, int64_t max_iter, float pos_weight, float ori_weight,
+                  float lambda_init, float eps_pos, float eps_ori, int64_t enable_collision,
+                  float collision_weight, float collision_margin, float* out_cfg, float* out_err,
+                  int32_t n_problems, int32_t n_seeds, int32_t n_act, int32_t n_joints,
+                  int32_t n_ee, int32_t n_robot_spheres, int32_t Ms, int32_t Mc, int32_t Mb,
+                  int32_t Mh);
+
+/* Options of the extended LM entry point (no reference counterpart). */
+typedef struct pk_lm_options {
+  int32_t max_iter;
+  float pos_weight;
+  float ori_weight;
+  float lambda_init;
+  float lambda_down;      /* multiply lambda on accept (reference 0.5) */
+  float lambda_up;        /* multiply lambda on reject (reference 3.0) */
+  float eps_pos;
+  float eps_ori;
+  int32_t enable_collision;
+  float collision_weight;
+  float collision_margin;
+  int32_t threads_per_seed; /* 0 = choose automatically; else 1, 2, 4 or 8 */
+  int32_t seeds_per_block;  /* 0 = choose automatically */
+} pk_lm_options;
+
+/*
+ * Extended LM IK (a new target, not a drop-in): as pk_ls_ik_cuda plus
+ * explicit robot-sphere self-collision pairs (self_i, self_j index
+ * robot_spheres_local, hinge-squared with the same margin and weight),
+ * configurable damping factors and launch shape.  target_Ts[P, n_ee, 7].
+ */
+int pk_ls_ik_ex(void* stream, const pk_lm_options* opt, const float* seeds, const float* twists,
+                const float* parent_tf, const int32_t* parent_idx, const int32_t* act_idx,
+                const float* mimic_mul, const float* mimic_off, const int32_t* mimic_act_idx,
+                const int32_t* topo_inv, const int32_t* target_jnts, const int32_t* ancestor_masks,
+                const float* target_Ts, const float* robot_spheres_local,
+                const int32_t* robot_sphere_joint_idx, const float* world_spheres,
+                const float* world_capsules, const float* world_boxes,
+                const float* world_halfspaces, const int32_t* self_i, const int32_t* self_j,
+                const float* lower, const float* upper, const int32_t* fixed_mask, float* out_cfg,
+                float* out_err, int32_t n_problems, int32_t n_seeds, int32_t n_act,
+                int32_t n_joints, int32_t n_ee, int32_t n_robot_spheres, int32_t Ms, int32_t Mc,
+                int32_t Mb, int32_t Mh, int32_t n_self_pairs);
+
+/*
+ * FP64 re-verification and winner selection (no reference counterpart; it
+ * replaces the argmin of _ls_ik_solve_cuda_batch_jit,
+ * src/pyroffi/optimization_engines/_ls_ik.py:974-999, and the FP64 check of
+ * tests/bench_ik.py:341-353).  For every problem p: the winner seed is
+ * argmin_s err[p,s] + continuity_weight * ||cfg[p,s] - prev[p]||^2 (prev may
+ * be NULL); its configuration goes to winner_cfg[P, n_act]; FK of the
+ * winner's configuration in FP64 gives, for EE 0, pos_err[P] (m) and
+ * rot_err[P] (rad, ||log(R_tgt^-1 R)||), and success[P] = pos_err < pos_tol
+ * && rot_err < rot_tol.  Any of pos_err / rot_err / success may be NULL.
+ */
+int pk_ik_verify_select(void* stream, const float* cfgs, const float* errs, const float* prev,
+                        float continuity_weight, const float* twists, const float* parent_tf,
+                        const int32_t* parent_idx, const int32_t* act_idx, const float* mimic_mul,
+                        const float* mimic_off, const int32_t* mimic_act_idx,
+                        const int32_t* topo_inv, const int32_t* target_jnts,
+                        const float* target_Ts, float pos_tol, float rot_tol, float* winner_cfg,
+                        double* pos_err, double* rot_err, int32_t* success, int32_t n_problems,
+                        int32_t n_seeds, int32_t n_act, int32_t n_joints, int32_t n_ee);
+
+/*
+ * Fused FK -> link poses -> sphere world centres -> world distances (no
+ * reference counterpart; it fuses Robot.forward_kinematics,
+ * src/pyroffi/_robot.py:66-109, RobotCollisionSpherized.at_config,
+ * src/pyroffi/collision/_robot_collision.py:744-794, and the world-distance
+ * kernels).  Spheres are given per link in link frames: link_spheres[N, S, 4]
+ * (x, y, z, r; r < 0 = padding), parent_joint_indices[N] (-1 = base link,
+ * identity pose).  Outputs (each may be NULL):
+ *   min_dist[B]          min over all spheres and obstacles (1e9 if none),
+ *   link_poses[B, N, 7]  link poses,
+ *   dist_bkm[B, K, M]    per-sphere distances with K = S*N, k = s*N + n, in
+ *                        the layout of pk_collision_world_sphere.
+ */
+int pk_fk_sphere_collision(void* stream, const float* cfg, const float* twists,
+                           const float* parent_tf, const int32_t* parent_idx,
+                           const int32_t* act_idx, const float* mimic_mul, const float* mimic_off,
+                           const int32_t* mimic_act_idx, const int32_t* topo_inv,
+                           const int32_t* parent_joint_indices, const float* link_spheres,
+                           const float* world_spheres, const float* world_capsules,
+                           const float* world_boxes, const float* world_halfspaces,
+                           float* min_dist, float* link_poses, float* dist_bkm, int64_t batch,
+                           int32_t n_act, int32_t n_joints, int32_t n_links, int32_t S, int32_t Ms,
+                           int32_t Mc, int32_t Mb, int32_t Mh);
+
+/*
+ * FP32 FMA-pipe microbenchmark (no reference counterpart): `blocks` blocks of
+ * 256 threads, each thread 8 independent FMA chains of `iters` steps, i.e.
+ * 4096 * iters * blocks FLOPs.  Time it with events on `stream`; it gives
+ * the measured SIMT roof the kinematics kernels are compared against.
+ * `out` must hold `blocks` floats (normally left untouched).
+ */
+int pk_fp32_fma_peak(void* stream, float* out, int32_t iters, int32_t blocks);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PYROFFI_B200_H_ */

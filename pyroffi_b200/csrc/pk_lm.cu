@@ -1,0 +1,852 @@
+// Multi-seed Levenberg-Marquardt IK with a collision hinge penalty, FP64
+// winner re-verification.
+//
+// pk_ls_ik_cuda replaces the reference's "ls_ik_cuda" XLA FFI target
+// (src/pyroffi/cuda_kernels/_ls_ik_cuda_kernel.cu:65-529).  The iteration is
+// the reference's: residual = world position difference + rotation vector of
+// q_ee * conj(q_tgt); stacked geometric Jacobian; row weights; Jacobi column
+// scaling; FP64 damped normal equations with fixed-joint masking and a
+// Cholesky solve; trust-region clip; 5-point line search on clamped trials;
+// accept/reject of the damping step; all-time best tracking.
+//
+// B200 mapping:
+//  * a group of TPS adjacent lanes owns one seed.  Every lane of the group
+//    runs the (cheap) FK / Jacobian / normal-equation math redundantly, so
+//    the group's decisions are bit-identical without broadcasts, and the
+//    (dominant) collision penalty is split: lane t transforms robot spheres
+//    t, t+TPS, ... and tests them against every obstacle; partial sums meet
+//    in a butterfly shuffle.
+//  * robot description, obstacle set, sphere list, limits and this block's
+//    targets are staged once per block in shared memory; joint poses of
+//    each lane live in a bank-strided shared slot array; configuration,
+//    Jacobian and damping state stay in registers (all loops over the DOF
+//    are unrolled to the compile-time bucket MAXA, padded dimensions are
+//    masked like fixed joints).
+//  * sphere-sphere hinge terms are tested on squared distance first:
+//    d - margin < 0  <=>  |c - o|^2 < (r_s + r_o + margin)^2 for a positive
+//    sum, so the square root runs only for the rare active pairs.
+#include <float.h>
+
+#include "pk_obstacles.cuh"
+
+namespace pk {
+
+struct LmArgs {
+  ModelArgs m;
+  WorldArgs w;
+  const float* seeds;
+  const int* target_jnts;
+  const int* ancestor_masks;
+  const float* target_Ts;
+  const float* spheres_local;
+  const int* sphere_joint;
+  const int* self_i;
+  const int* self_j;
+  const float* lower;
+  const float* upper;
+  const int* fixed_mask;
+  float* out_cfg;
+  float* out_err;
+  int P, Sd, n_act, n_ee, n_rs, n_self;
+  int max_iter;
+  float pos_w, ori_w, lam0, lam_down, lam_up, eps_pos, eps_ori;
+  int coll;
+  float coll_w, margin;
+  int spb;
+};
+
+// Shared-memory layout of one LM block.
+struct LmShared {
+  JointTable jt;
+  unsigned long long anc[PK_MAX_EE];  // ancestor bits by original joint index
+  float tgt[PK_MAX_EE][7];
+  int tsorted[PK_MAX_EE];
+  float lo[PK_MAX_ACT], hi[PK_MAX_ACT];
+  int fixed[PK_MAX_ACT];
+};
+
+template <int N>
+__device__ __forceinline__ float reg_get(const float (&a)[N], int i) {
+  float v = 0.f;
+#pragma unroll
+  for (int k = 0; k < N; ++k) v = (k == i) ? a[k] : v;
+  return v;
+}
+
+// Line-search step sizes {1, 0.5, 0.25, 0.1, 0.025} (_ls_ik_cuda_kernel.cu:339).
+__device__ __forceinline__ float line_alpha(int i) {
+  return i == 0 ? 1.0f : i == 1 ? 0.5f : i == 2 ? 0.25f : i == 3 ? 0.1f : 0.025f;
+}
+
+template <int TPS>
+__device__ __forceinline__ float group_sum(float v, unsigned gmask) {
+#pragma unroll
+  for (int o = TPS / 2; o > 0; o >>= 1) v += __shfl_xor_sync(gmask, v, o);
+  return v;
+}
+
+struct PenaltyCtx {
+  const float4* rs;     // robot spheres (x, y, z, r), joint frame
+  const int* rsj;       // sorted joint position (-1: skip)
+  const float4* ws;     // world spheres (x, y, z, r + margin)
+  const float* wc;
+  const float* wb;
+  const float* wh;
+  const int2* pairs;    // self pairs
+  float* pos;           // [n_rs*3][spb] sphere world positions (self pairs)
+  int n_rs, Ms, Mc, Mb, Mh, n_self, spb;
+  float margin;
+};
+
+// Partial hinge penalty of lane t of a TPS-group (not weighted, not summed).
+template <int TPS>
+__device__ float penalty_share(const PenaltyCtx& c, const PoseSlots& ps, int t, int g, unsigned gmask) {
+  constexpr int CH = 4;
+  float pen = 0.f;
+  for (int k0 = t; k0 < c.n_rs; k0 += TPS * CH) {
+    float cx[CH], cy[CH], cz[CH], cr[CH];
+#pragma unroll
+    for (int u = 0; u < CH; ++u) {
+      const int k = k0 + u * TPS;
+      cx[u] = 1e18f; cy[u] = 1e18f; cz[u] = 1e18f; cr[u] = 0.f;
+      if (k < c.n_rs) {
+        const int js = c.rsj[k];
+        if (js >= 0) {
+          const float4 s = c.rs[k];
+          const float3 w = pose_apply(ps.load(js), make_float3(s.x, s.y, s.z));
+          cx[u] = w.x; cy[u] = w.y; cz[u] = w.z; cr[u] = s.w;
+          if (c.n_self > 0) {
+            c.pos[(k * 3 + 0) * c.spb + g] = w.x;
+            c.pos[(k * 3 + 1) * c.spb + g] = w.y;
+            c.pos[(k * 3 + 2) * c.spb + g] = w.z;
+          }
+        }
+      }
+    }
+    for (int m = 0; m < c.Ms; ++m) {
+      const float4 o = c.ws[m];
+#pragma unroll
+      for (int u = 0; u < CH; ++u) {
+        const float rr = cr[u] + o.w;
+        const float dx = cx[u] - o.x, dy = cy[u] - o.y, dz = cz[u] - o.z;
+        const float d2 = dx * dx + dy * dy + dz * dz;
+        if (d2 < rr * fabsf(rr)) {
+          const float e = sqrtf(d2) - rr;
+          pen += e * e;
+        }
+      }
+    }
+    if (c.Mc + c.Mb + c.Mh > 0) {
+#pragma unroll
+      for (int u = 0; u < CH; ++u) {
+        if (cx[u] == 1e18f) continue;
+        const float3 p = make_float3(cx[u], cy[u], cz[u]);
+        for (int m = 0; m < c.Mc; ++m) {
+          const float d = d_sphere_capsule(p, cr[u], c.wc + 7 * m);
+          if (d < c.margin) { const float e = d - c.margin; pen += e * e; }
+        }
+        for (int m = 0; m < c.Mb; ++m) {
+          const float d = d_sphere_box(p, cr[u], c.wb + 15 * m);
+          if (d < c.margin) { const float e = d - c.margin; pen += e * e; }
+        }
+        for (int m = 0; m < c.Mh; ++m) {
+          const float d = d_sphere_halfspace(p, cr[u], c.wh + 6 * m);
+          if (d < c.margin) { const float e = d - c.margin; pen += e * e; }
+        }
+      }
+    }
+  }
+  if (c.n_self > 0) {
+    __syncwarp(gmask);
+    for (int q = t; q < c.n_self; q += TPS) {
+      const int2 pr = c.pairs[q];
+      if (pr.x < 0 || pr.y < 0 || pr.x >= c.n_rs || pr.y >= c.n_rs) continue;
+      if (c.rsj[pr.x] < 0 || c.rsj[pr.y] < 0) continue;
+      const float rr = c.rs[pr.x].w + c.rs[pr.y].w + c.margin;
+      const float dx = c.pos[(pr.x * 3 + 0) * c.spb + g] - c.pos[(pr.y * 3 + 0) * c.spb + g];
+      const float dy = c.pos[(pr.x * 3 + 1) * c.spb + g] - c.pos[(pr.y * 3 + 1) * c.spb + g];
+      const float dz = c.pos[(pr.x * 3 + 2) * c.spb + g] - c.pos[(pr.y * 3 + 2) * c.spb + g];
+      const float d2 = dx * dx + dy * dy + dz * dz;
+      if (d2 < rr * fabsf(rr)) {
+        const float e = sqrtf(d2) - rr;
+        pen += e * e;
+      }
+    }
+    __syncwarp(gmask);
+  }
+  return pen;
+}
+
+// Residual of every EE (reference helper _ik_cuda_helpers.cuh:472-499).
+template <int MAXEE>
+__device__ __forceinline__ void ee_residual(const LmShared& sh, const PoseSlots& ps, int n_ee,
+                                            float (&r)[6 * MAXEE], float (&pee)[3 * MAXEE]) {
+#pragma unroll
+  for (int e = 0; e < MAXEE; ++e) {
+    if (e >= n_ee) {
+#pragma unroll
+      for (int c = 0; c < 6; ++c) r[6 * e + c] = 0.f;
+      pee[3 * e] = pee[3 * e + 1] = pee[3 * e + 2] = 0.f;
+      continue;
+    }
+    const Pose T = ps.load(sh.tsorted[e]);
+    const float* g = sh.tgt[e];
+    r[6 * e + 0] = T.tx - g[4];
+    r[6 * e + 1] = T.ty - g[5];
+    r[6 * e + 2] = T.tz - g[6];
+    // q_err = q_ee * conj(q_tgt)
+    const float bw = g[0], bx = -g[1], by = -g[2], bz = -g[3];
+    float qw = T.w * bw - T.x * bx - T.y * by - T.z * bz;
+    float qx = T.w * bx + T.x * bw + T.y * bz - T.z * by;
+    float qy = T.w * by - T.x * bz + T.y * bw + T.z * bx;
+    float qz = T.w * bz + T.x * by - T.y * bx + T.z * bw;
+    if (qw < 0.f) { qw = -qw; qx = -qx; qy = -qy; qz = -qz; }
+    const float s = sqrtf(qx * qx + qy * qy + qz * qz);
+    float f;
+    if (s > 1e-6f) f = 2.f * atan2f(s, qw) / s;
+    else f = 2.f;
+    r[6 * e + 3] = qx * f;
+    r[6 * e + 4] = qy * f;
+    r[6 * e + 5] = qz * f;
+    pee[3 * e] = T.tx; pee[3 * e + 1] = T.ty; pee[3 * e + 2] = T.tz;
+  }
+}
+
+template <int MAXA, int MAXEE, int TPS>
+__global__ void __launch_bounds__(128, (MAXA <= 8 ? 4 : 2)) lm_kernel(LmArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  LmShared& sh = *reinterpret_cast<LmShared*>(smem_raw);
+  unsigned char* p = smem_raw + ((sizeof(LmShared) + 15) & ~size_t(15));
+  float4* rs4 = reinterpret_cast<float4*>(p); p += sizeof(float4) * a.n_rs;
+  float4* ws4 = reinterpret_cast<float4*>(p); p += sizeof(float4) * a.w.Ms;
+  int2* pairs = reinterpret_cast<int2*>(p); p += sizeof(int2) * ((a.n_self + 1) & ~1);
+  int* rsj = reinterpret_cast<int*>(p); p += sizeof(int) * ((a.n_rs + 3) & ~3);
+  float* wc = reinterpret_cast<float*>(p); p += sizeof(float) * a.w.Mc * 7;
+  float* wb = reinterpret_cast<float*>(p); p += sizeof(float) * a.w.Mb * 15;
+  float* wh = reinterpret_cast<float*>(p); p += sizeof(float) * a.w.Mh * 6;
+  p = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15));
+  float* slots = reinterpret_cast<float*>(p); p += sizeof(float) * a.m.n_joints * 7 * blockDim.x;
+  float* pos = reinterpret_cast<float*>(p);
+
+  const int pb = blockIdx.y;  // problem
+  load_joint_table(sh.jt, a.m);
+  const int tid = threadIdx.x;
+  if (tid < a.n_ee) {
+    const int tj = a.target_jnts[tid];
+    sh.tsorted[tid] = (tj >= 0 && tj < a.m.n_joints) ? sh.jt.sorted_of[tj] : 0;
+    unsigned long long bits = 0ull;
+    for (int j = 0; j < a.m.n_joints; ++j)
+      if (a.ancestor_masks[tid * a.m.n_joints + j]) bits |= 1ull << j;
+    sh.anc[tid] = bits;
+    for (int c = 0; c < 7; ++c) sh.tgt[tid][c] = a.target_Ts[((size_t)pb * a.n_ee + tid) * 7 + c];
+  }
+  for (int i = tid; i < MAXA; i += blockDim.x) {
+    const bool real = i < a.n_act;
+    sh.lo[i] = real ? a.lower[i] : 0.f;
+    sh.hi[i] = real ? a.upper[i] : 0.f;
+    sh.fixed[i] = real ? (a.fixed_mask[i] != 0) : 1;
+  }
+  for (int i = tid; i < a.n_rs; i += blockDim.x) {
+    rs4[i] = make_float4(a.spheres_local[4 * i], a.spheres_local[4 * i + 1], a.spheres_local[4 * i + 2],
+                         a.spheres_local[4 * i + 3]);
+    const int j = a.sphere_joint[i];
+    rsj[i] = (j >= 0 && j < a.m.n_joints) ? sh.jt.sorted_of[j] : -1;
+  }
+  for (int i = tid; i < a.w.Ms; i += blockDim.x)
+    ws4[i] = make_float4(a.w.spheres[4 * i], a.w.spheres[4 * i + 1], a.w.spheres[4 * i + 2],
+                         a.w.spheres[4 * i + 3] + a.margin);
+  for (int i = tid; i < a.w.Mc * 7; i += blockDim.x) wc[i] = a.w.capsules[i];
+  for (int i = tid; i < a.w.Mb * 15; i += blockDim.x) wb[i] = a.w.boxes[i];
+  for (int i = tid; i < a.w.Mh * 6; i += blockDim.x) wh[i] = a.w.halfspaces[i];
+  for (int i = tid; i < a.n_self; i += blockDim.x) pairs[i] = make_int2(a.self_i[i], a.self_j[i]);
+  __syncthreads();
+
+  const int g = tid / TPS, t = tid - g * TPS;
+  const int lane = tid & 31;
+  const unsigned gmask = (TPS == 32) ? 0xffffffffu : (((1u << TPS) - 1u) << (lane & ~(TPS - 1)));
+  const int s = blockIdx.x * a.spb + g;
+  if (s >= a.Sd) return;
+  const size_t gs = (size_t)pb * a.Sd + s;
+
+  const JointTable& jt = sh.jt;
+  const PoseSlots ps{slots + tid, (int)blockDim.x};
+  const bool use_coll = a.coll && (a.n_rs > 0);
+  PenaltyCtx pc;
+  pc.rs = rs4; pc.rsj = rsj; pc.ws = ws4; pc.wc = wc; pc.wb = wb; pc.wh = wh; pc.pairs = pairs;
+  pc.pos = pos; pc.n_rs = a.n_rs; pc.Ms = a.w.Ms; pc.Mc = a.w.Mc; pc.Mb = a.w.Mb; pc.Mh = a.w.Mh;
+  pc.n_self = a.n_self; pc.spb = a.spb; pc.margin = a.margin;
+
+  float W[6] = {a.pos_w, a.pos_w, a.pos_w, a.ori_w, a.ori_w, a.ori_w};
+
+  float cfg[MAXA], best[MAXA];
+#pragma unroll
+  for (int i = 0; i < MAXA; ++i) {
+    cfg[i] = (i < a.n_act) ? a.seeds[gs * a.n_act + i] : 0.f;
+    best[i] = cfg[i];
+  }
+
+  auto penalty = [&]() -> float {
+    if (!use_coll) return 0.f;
+    const float share = penalty_share<TPS>(pc, ps, t, g, gmask);
+    return a.coll_w * group_sum<TPS>(share, gmask);
+  };
+  auto run_fk = [&](const float (&q)[MAXA]) {
+    fk_thread(jt, [&](int i) { return reg_get<MAXA>(q, i); }, ps);
+  };
+  auto weighted_sq = [&](const float (&r)[6 * MAXEE]) {
+    float e = 0.f;
+#pragma unroll
+    for (int k = 0; k < 6 * MAXEE; ++k) {
+      const float rw = r[k] * W[k % 6];
+      e += rw * rw;
+    }
+    return e;
+  };
+
+  float r[6 * MAXEE], pee[3 * MAXEE];
+  run_fk(cfg);
+  ee_residual<MAXEE>(sh, ps, a.n_ee, r, pee);
+  float best_err = weighted_sq(r) + penalty();
+  float lam = a.lam0;
+
+  for (int it = 0; it < a.max_iter; ++it) {
+    run_fk(cfg);
+    ee_residual<MAXEE>(sh, ps, a.n_ee, r, pee);
+    bool all_conv = true;
+    float max_p = 0.f, max_o = 0.f;
+#pragma unroll
+    for (int e = 0; e < MAXEE; ++e) {
+      if (e < a.n_ee) {
+        const float np = sqrtf(r[6 * e] * r[6 * e] + r[6 * e + 1] * r[6 * e + 1] + r[6 * e + 2] * r[6 * e + 2]);
+        const float no = sqrtf(r[6 * e + 3] * r[6 * e + 3] + r[6 * e + 4] * r[6 * e + 4] + r[6 * e + 5] * r[6 * e + 5]);
+        if (np >= a.eps_pos || no >= a.eps_ori) all_conv = false;
+        max_p = fmaxf(max_p, np);
+        max_o = fmaxf(max_o, no);
+      }
+    }
+    if (all_conv) break;
+
+    // weighted stacked Jacobian J[k][c]
+    float J[6 * MAXEE][MAXA];
+#pragma unroll
+    for (int k = 0; k < 6 * MAXEE; ++k)
+#pragma unroll
+      for (int c = 0; c < MAXA; ++c) J[k][c] = 0.f;
+    for (int i = 0; i < jt.n; ++i) {
+      const int jk = jt.jkind[i];
+      const int a1 = jt.a1[i], a2 = jt.a2[i];
+      if (jk == 0 || (a1 < 0 && a2 < 0)) continue;
+      const Pose Tj = ps.load(i);
+      const float3 z = quat_rotate(Tj.w, Tj.x, Tj.y, Tj.z,
+                                   make_float3(jt.axis[i][0], jt.axis[i][1], jt.axis[i][2]));
+      const float sm = jt.mul[i];
+      const int orig = jt.orig[i];
+#pragma unroll
+      for (int e = 0; e < MAXEE; ++e) {
+        if (e >= a.n_ee || !((sh.anc[e] >> orig) & 1ull)) continue;
+        float col[6];
+        if (jk == 1) {
+          const float ax = pee[3 * e] - Tj.tx, ay = pee[3 * e + 1] - Tj.ty, az = pee[3 * e + 2] - Tj.tz;
+          col[0] = z.y * az - z.z * ay; col[1] = z.z * ax - z.x * az; col[2] = z.x * ay - z.y * ax;
+          col[3] = z.x; col[4] = z.y; col[5] = z.z;
+        } else {
+          col[0] = z.x; col[1] = z.y; col[2] = z.z; col[3] = col[4] = col[5] = 0.f;
+        }
+#pragma unroll
+        for (int c = 0; c < MAXA; ++c) {
+          const float wsel = ((c == a1) ? sm : 0.f) + ((c == a2) ? sm : 0.f);
+#pragma unroll
+          for (int k = 0; k < 6; ++k) J[6 * e + k][c] += wsel * col[k];
+        }
+      }
+    }
+    float fw[6 * MAXEE];
+#pragma unroll
+    for (int k = 0; k < 6 * MAXEE; ++k) {
+      fw[k] = r[k] * W[k % 6];
+#pragma unroll
+      for (int c = 0; c < MAXA; ++c) J[k][c] *= W[k % 6];
+    }
+    float curr = 0.f;
+#pragma unroll
+    for (int k = 0; k < 6 * MAXEE; ++k) curr += fw[k] * fw[k];
+    curr += penalty();
+
+    // Jacobi column scaling
+    float col_s[MAXA];
+#pragma unroll
+    for (int c = 0; c < MAXA; ++c) {
+      float sq = 0.f;
+#pragma unroll
+      for (int k = 0; k < 6 * MAXEE; ++k) sq += J[k][c] * J[k][c];
+      col_s[c] = sqrtf(sq) + 1e-8f;
+    }
+#pragma unroll
+    for (int k = 0; k < 6 * MAXEE; ++k)
+#pragma unroll
+      for (int c = 0; c < MAXA; ++c) J[k][c] = J[k][c] / col_s[c];
+
+    // FP64 normal equations (lower triangle, packed) + masking
+    double A[MAXA * (MAXA + 1) / 2];
+    double rhs[MAXA];
+#pragma unroll
+    for (int i = 0; i < MAXA; ++i) {
+      const bool fi = sh.fixed[i];
+#pragma unroll
+      for (int j = 0; j <= i; ++j) {
+        double acc = 0.0;
+#pragma unroll
+        for (int k = 0; k < 6 * MAXEE; ++k) acc += (double)J[k][i] * (double)J[k][j];
+        if (i == j) acc += (double)lam;
+        const bool fj = sh.fixed[j];
+        A[i * (i + 1) / 2 + j] = (fi || fj) ? ((i == j) ? 1.0 : 0.0) : acc;
+      }
+      double rb = 0.0;
+#pragma unroll
+      for (int k = 0; k < 6 * MAXEE; ++k) rb += (double)J[k][i] * (double)fw[k];
+      rhs[i] = fi ? 0.0 : -rb;
+    }
+    // Cholesky A = L L^T in place; a non-positive pivot zeroes the step
+    bool ok = true;
+#pragma unroll
+    for (int k = 0; k < MAXA; ++k) {
+      double s2 = A[k * (k + 1) / 2 + k];
+#pragma unroll
+      for (int q = 0; q < k; ++q) s2 -= A[k * (k + 1) / 2 + q] * A[k * (k + 1) / 2 + q];
+      if (!(s2 > 0.0)) ok = false;
+      const double lkk = sqrt(ok ? s2 : 1.0);
+      const double inv = 1.0 / lkk;
+      A[k * (k + 1) / 2 + k] = lkk;
+#pragma unroll
+      for (int i = k + 1; i < MAXA; ++i) {
+        double tt = A[i * (i + 1) / 2 + k];
+#pragma unroll
+        for (int q = 0; q < k; ++q) tt -= A[i * (i + 1) / 2 + q] * A[k * (k + 1) / 2 + q];
+        A[i * (i + 1) / 2 + k] = tt * inv;
+      }
+    }
+    // forward / backward substitution
+#pragma unroll
+    for (int i = 0; i < MAXA; ++i) {
+      double s2 = rhs[i];
+#pragma unroll
+      for (int q = 0; q < i; ++q) s2 -= A[i * (i + 1) / 2 + q] * rhs[q];
+      rhs[i] = s2 / A[i * (i + 1) / 2 + i];
+    }
+#pragma unroll
+    for (int i = MAXA - 1; i >= 0; --i) {
+      double s2 = rhs[i];
+#pragma unroll
+      for (int q = i + 1; q < MAXA; ++q) s2 -= A[q * (q + 1) / 2 + i] * rhs[q];
+      rhs[i] = s2 / A[i * (i + 1) / 2 + i];
+    }
+    float delta[MAXA];
+    float dn2 = 0.f;
+#pragma unroll
+    for (int c = 0; c < MAXA; ++c) {
+      delta[c] = ok ? (float)rhs[c] / col_s[c] : 0.f;
+      dn2 += delta[c] * delta[c];
+    }
+    // trust region
+    float R;
+    if (max_p > 1e-2f || max_o > 0.6f) R = 0.38f;
+    else if (max_p > 1e-3f || max_o > 0.25f) R = 0.22f;
+    else if (max_p > 2e-4f || max_o > 0.08f) R = 0.12f;
+    else R = 0.05f;
+    const float dn = sqrtf(dn2);
+    if (dn > R) {
+      const float sc = R / (dn + 1e-18f);
+#pragma unroll
+      for (int c = 0; c < MAXA; ++c) delta[c] *= sc;
+    }
+
+    // line search
+    float best_a_err = 1e30f;
+    int best_a = 0;
+#pragma unroll 1
+    for (int ai = 0; ai < 5; ++ai) {
+      float trial[MAXA];
+#pragma unroll
+      for (int c = 0; c < MAXA; ++c) trial[c] = fmaxf(sh.lo[c], fminf(sh.hi[c], cfg[c] + line_alpha(ai) * delta[c]));
+      run_fk(trial);
+      float rt[6 * MAXEE], pt[3 * MAXEE];
+      ee_residual<MAXEE>(sh, ps, a.n_ee, rt, pt);
+      const float et = weighted_sq(rt) + penalty();
+      if (et < best_a_err) { best_a_err = et; best_a = ai; }
+    }
+    const float alpha = line_alpha(best_a);
+    float trial[MAXA];
+#pragma unroll
+    for (int c = 0; c < MAXA; ++c) trial[c] = fmaxf(sh.lo[c], fminf(sh.hi[c], cfg[c] + alpha * delta[c]));
+    if (best_a_err < curr * (1.0f - 1e-4f)) {
+#pragma unroll
+      for (int c = 0; c < MAXA; ++c) cfg[c] = trial[c];
+      lam = fmaxf(lam * a.lam_down, 1e-10f);
+    } else {
+      lam = fminf(lam * a.lam_up, 1e6f);
+    }
+    if (best_a_err < best_err) {
+      best_err = best_a_err;
+#pragma unroll
+      for (int c = 0; c < MAXA; ++c) best[c] = trial[c];
+    }
+  }
+
+  if (t == 0) {
+#pragma unroll
+    for (int c = 0; c < MAXA; ++c)
+      if (c < a.n_act) a.out_cfg[gs * a.n_act + c] = best[c];
+    a.out_err[gs] = best_err;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FP64 re-verification + winner selection, one block per problem
+// ---------------------------------------------------------------------------
+
+struct PoseD {
+  double w, x, y, z, tx, ty, tz;
+};
+
+__device__ __forceinline__ void qrot_d(double w, double x, double y, double z, double vx, double vy,
+                                       double vz, double& ox, double& oy, double& oz) {
+  const double tx = 2.0 * (y * vz - z * vy), ty = 2.0 * (z * vx - x * vz), tz = 2.0 * (x * vy - y * vx);
+  ox = vx + w * tx + (y * tz - z * ty);
+  oy = vy + w * ty + (z * tx - x * tz);
+  oz = vz + w * tz + (x * ty - y * tx);
+}
+
+__device__ __forceinline__ PoseD compose_d(const PoseD& a, const PoseD& b) {
+  PoseD o;
+  o.w = a.w * b.w - a.x * b.x - a.y * b.y - a.z * b.z;
+  o.x = a.w * b.x + a.x * b.w + a.y * b.z - a.z * b.y;
+  o.y = a.w * b.y - a.x * b.z + a.y * b.w + a.z * b.x;
+  o.z = a.w * b.z + a.x * b.y - a.y * b.x + a.z * b.w;
+  double rx, ry, rz;
+  qrot_d(a.w, a.x, a.y, a.z, b.tx, b.ty, b.tz, rx, ry, rz);
+  o.tx = rx + a.tx; o.ty = ry + a.ty; o.tz = rz + a.tz;
+  return o;
+}
+
+// exp(twist * q) in FP64 (full SE(3) exponential; series below 1e-8 rad^2).
+__device__ PoseD motion_d(const float* tw, double q) {
+  const double vx = tw[0] * q, vy = tw[1] * q, vz = tw[2] * q;
+  const double ox = tw[3] * q, oy = tw[4] * q, oz = tw[5] * q;
+  const double t2 = ox * ox + oy * oy + oz * oz;
+  double sh_t, ch, B, C;
+  if (t2 < 1e-8) {
+    sh_t = 0.5 - t2 / 48.0;
+    ch = 1.0 - t2 / 8.0;
+    B = 0.5 - t2 / 24.0;
+    C = 1.0 / 6.0 - t2 / 120.0;
+  } else {
+    const double th = sqrt(t2);
+    double sh, st, ct;
+    sincos(0.5 * th, &sh, &ch);
+    sincos(th, &st, &ct);
+    sh_t = sh / th;
+    B = (1.0 - ct) / t2;
+    C = (th - st) / (t2 * th);
+  }
+  PoseD d;
+  d.w = ch; d.x = sh_t * ox; d.y = sh_t * oy; d.z = sh_t * oz;
+  const double cx = oy * vz - oz * vy, cy = oz * vx - ox * vz, cz = ox * vy - oy * vx;
+  const double ccx = oy * cz - oz * cy, ccy = oz * cx - ox * cz, ccz = ox * cy - oy * cx;
+  d.tx = vx + B * cx + C * ccx;
+  d.ty = vy + B * cy + C * ccy;
+  d.tz = vz + B * cz + C * ccz;
+  return d;
+}
+
+struct VerifyArgs {
+  ModelArgs m;
+  const float* cfgs;
+  const float* errs;
+  const float* prev;
+  float cw;
+  const int* target_jnts;
+  const float* target_Ts;
+  float pos_tol, rot_tol;
+  float* winner_cfg;
+  double* pos_err;
+  double* rot_err;
+  int* success;
+  int P, Sd, n_act, n_ee;
+};
+
+__global__ void __launch_bounds__(128) verify_select_kernel(VerifyArgs a) {
+  __shared__ JointTable jt;
+  __shared__ double Tw[PK_MAX_JOINTS][7];
+  __shared__ float sbest[32];
+  __shared__ int sidx[32];
+  __shared__ int winner;
+  load_joint_table(jt, a.m);
+  const int p = blockIdx.x;
+  float bv = FLT_MAX;
+  int bi = 0x7fffffff;
+  for (int s = threadIdx.x; s < a.Sd; s += blockDim.x) {
+    const size_t gs = (size_t)p * a.Sd + s;
+    float v = a.errs[gs];
+    if (a.prev && a.cw != 0.f) {
+      float d2 = 0.f;
+      for (int c = 0; c < a.n_act; ++c) {
+        const float d = a.cfgs[gs * a.n_act + c] - a.prev[(size_t)p * a.n_act + c];
+        d2 += d * d;
+      }
+      v += a.cw * d2;
+    }
+    if (v < bv || (v == bv && s < bi) || (bi == 0x7fffffff && !(v == v))) { bv = v; bi = s; }
+  }
+  // block argmin, ties -> smallest seed index
+  for (int o = 16; o > 0; o >>= 1) {
+    const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+    if (ov < bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+  }
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) { sbest[wid] = bv; sidx[wid] = bi; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float v = sbest[0];
+    int i = sidx[0];
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
+      if (sbest[w] < v || (sbest[w] == v && sidx[w] < i)) { v = sbest[w]; i = sidx[w]; }
+    winner = (i == 0x7fffffff) ? 0 : i;
+  }
+  __syncthreads();
+  const size_t gw = (size_t)p * a.Sd + winner;
+  for (int c = threadIdx.x; c < a.n_act; c += blockDim.x)
+    a.winner_cfg[(size_t)p * a.n_act + c] = a.cfgs[gw * a.n_act + c];
+  if (threadIdx.x != 0) return;
+  // FP64 FK of the winner
+  const float* q = a.cfgs + gw * a.n_act;
+  for (int i = 0; i < jt.n; ++i) {
+    const int src = jt.src[i];
+    const double qv = ((src < 0) ? 0.0 : (double)q[src]) * (double)jt.mul[i] + (double)jt.off[i];
+    PoseD Tpc{jt.ptf[i][0], jt.ptf[i][1], jt.ptf[i][2], jt.ptf[i][3], jt.ptf[i][4], jt.ptf[i][5], jt.ptf[i][6]};
+    if (jt.kind[i] != kFixed) Tpc = compose_d(Tpc, motion_d(jt.tw[i], qv));
+    const int ps = jt.psorted[i];
+    PoseD T = Tpc;
+    if (ps >= 0) {
+      const PoseD Pp{Tw[ps][0], Tw[ps][1], Tw[ps][2], Tw[ps][3], Tw[ps][4], Tw[ps][5], Tw[ps][6]};
+      T = compose_d(Pp, Tpc);
+    }
+    Tw[i][0] = T.w; Tw[i][1] = T.x; Tw[i][2] = T.y; Tw[i][3] = T.z;
+    Tw[i][4] = T.tx; Tw[i][5] = T.ty; Tw[i][6] = T.tz;
+  }
+  double pe = 0.0, re = 0.0;
+  for (int e = 0; e < a.n_ee; ++e) {
+    const int tj = a.target_jnts[e];
+    const int i = (tj >= 0 && tj < jt.n) ? jt.sorted_of[tj] : 0;
+    const float* g = a.target_Ts + ((size_t)p * a.n_ee + e) * 7;
+    const double dx = Tw[i][4] - g[4], dy = Tw[i][5] - g[5], dz = Tw[i][6] - g[6];
+    pe = fmax(pe, sqrt(dx * dx + dy * dy + dz * dz));
+    // conj(q_tgt) * q
+    const double aw = g[0], ax = -g[1], ay = -g[2], az = -g[3];
+    const double bw = Tw[i][0], bx = Tw[i][1], by = Tw[i][2], bz = Tw[i][3];
+    const double rw = aw * bw - ax * bx - ay * by - az * bz;
+    const double rx = aw * bx + ax * bw + ay * bz - az * by;
+    const double ry = aw * by - ax * bz + ay * bw + az * bx;
+    const double rz = aw * bz + ax * by - ay * bx + az * bw;
+    const double nv = sqrt(rx * rx + ry * ry + rz * rz);
+    re = fmax(re, 2.0 * atan2(nv, fabs(rw)));
+  }
+  if (a.pos_err) a.pos_err[p] = pe;
+  if (a.rot_err) a.rot_err[p] = re;
+  if (a.success) a.success[p] = (pe < (double)a.pos_tol && re < (double)a.rot_tol) ? 1 : 0;
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+
+static size_t lm_smem_bytes(const LmArgs& a, int threads) {
+  size_t b = (sizeof(LmShared) + 15) & ~size_t(15);
+  b += sizeof(float4) * a.n_rs + sizeof(float4) * a.w.Ms + sizeof(int2) * ((a.n_self + 1) & ~1) +
+       sizeof(int) * ((a.n_rs + 3) & ~3) + sizeof(float) * (a.w.Mc * 7 + a.w.Mb * 15 + a.w.Mh * 6);
+  b = (b + 15) & ~size_t(15);
+  b += sizeof(float) * (size_t)a.m.n_joints * 7 * threads;
+  if (a.n_self > 0) b += sizeof(float) * (size_t)a.n_rs * 3 * a.spb;
+  return b;
+}
+
+template <int MAXA, int MAXEE, int TPS>
+static int launch_lm_t(const LmArgs& a0, cudaStream_t st) {
+  LmArgs a = a0;
+  const int threads = a.spb * TPS;
+  const size_t smem = lm_smem_bytes(a, threads);
+  PK_CHECK_CAP(smem <= 220 * 1024, "LM working set (%zu B of shared memory) too large", smem);
+  auto kern = lm_kernel<MAXA, MAXEE, TPS>;
+  if (int s = set_smem_limit((const void*)kern, smem)) return s;
+  dim3 grid((a.Sd + a.spb - 1) / a.spb, a.P);
+  kern<<<grid, threads, smem, st>>>(a);
+  return cuda_status(cudaGetLastError(), "lm_kernel launch");
+}
+
+template <int MAXA, int MAXEE>
+static int launch_lm_tps(const LmArgs& a, int tps, cudaStream_t st) {
+  switch (tps) {
+    case 1: return launch_lm_t<MAXA, MAXEE, 1>(a, st);
+    case 2: return launch_lm_t<MAXA, MAXEE, 2>(a, st);
+    case 4: return launch_lm_t<MAXA, MAXEE, 4>(a, st);
+    default: return launch_lm_t<MAXA, MAXEE, 8>(a, st);
+  }
+}
+
+static int launch_lm(LmArgs a, int tps, int spb, cudaStream_t st) {
+  if (tps <= 0) tps = (a.coll && a.n_rs > 0) ? 4 : 1;
+  PK_CHECK_ARG(tps == 1 || tps == 2 || tps == 4 || tps == 8, "threads_per_seed must be 1, 2, 4 or 8");
+  if (spb <= 0) spb = 128 / tps;
+  PK_CHECK_ARG(spb * tps <= 128 && (spb * tps) % 32 == 0,
+               "seeds_per_block * threads_per_seed must be a multiple of 32 and at most 128");
+  a.spb = spb;
+  if (a.n_act <= 8 && a.n_ee <= 1) return launch_lm_tps<8, 1>(a, tps, st);
+  if (a.n_act <= 16 && a.n_ee <= 2) return launch_lm_tps<16, 2>(a, tps, st);
+  set_error("the LM kernel supports n_act <= 16 with n_ee <= 2 (got n_act=%d, n_ee=%d)", a.n_act, a.n_ee);
+  return PK_ERR_CAPACITY;
+}
+
+static int validate_lm(const LmArgs& a) {
+  PK_CHECK_ARG(a.P >= 0 && a.Sd >= 0 && a.n_act >= 0 && a.n_ee >= 0 && a.n_rs >= 0 && a.n_self >= 0,
+               "negative extent");
+  PK_CHECK_CAP(a.m.n_joints <= PK_MAX_JOINTS, "n_joints=%d exceeds %d", a.m.n_joints, PK_MAX_JOINTS);
+  PK_CHECK_CAP(a.n_act <= PK_MAX_ACT, "n_act=%d exceeds %d (the reference kernel silently overflows "
+               "its per-thread arrays here)", a.n_act, PK_MAX_ACT);
+  PK_CHECK_CAP(a.n_ee <= PK_MAX_EE, "n_ee=%d exceeds %d", a.n_ee, PK_MAX_EE);
+  PK_CHECK_ARG(a.n_ee >= 1, "at least one end-effector target is required");
+  PK_CHECK_ARG(a.max_iter >= 0 && a.max_iter <= 1000000, "max_iter out of range");
+  return PK_OK;
+}
+
+}  // namespace pk
+
+using namespace pk;
+
+static int lm_common(void* stream, const pk_lm_options& o, const float* seeds, const float* twists,
+                     const float* parent_tf, const int32_t* parent_idx, const int32_t* act_idx,
+                     const float* mimic_mul, const float* mimic_off, const int32_t* mimic_act_idx,
+                     const int32_t* topo_inv, const int32_t* target_jnts,
+                     const int32_t* ancestor_masks, const float* target_Ts,
+                     const float* robot_spheres_local, const int32_t* robot_sphere_joint_idx,
+                     const float* ws, const float* wc, const float* wb, const float* wh,
+                     const int32_t* self_i, const int32_t* self_j, const float* lower,
+                     const float* upper, const int32_t* fixed_mask, float* out_cfg,
+                     float* out_err, int32_t P, int32_t Sd, int32_t n_act, int32_t n_joints,
+                     int32_t n_ee, int32_t n_rs, int32_t Ms, int32_t Mc, int32_t Mb, int32_t Mh,
+                     int32_t n_self) {
+  LmArgs a{};
+  a.m = ModelArgs{twists, parent_tf, parent_idx, act_idx, mimic_mul, mimic_off, mimic_act_idx,
+                  topo_inv, n_joints, n_act};
+  a.w = WorldArgs{ws, wc, wb, wh, Ms, Mc, Mb, Mh};
+  a.seeds = seeds; a.target_jnts = target_jnts; a.ancestor_masks = ancestor_masks;
+  a.target_Ts = target_Ts; a.spheres_local = robot_spheres_local;
+  a.sphere_joint = robot_sphere_joint_idx; a.self_i = self_i; a.self_j = self_j;
+  a.lower = lower; a.upper = upper; a.fixed_mask = fixed_mask;
+  a.out_cfg = out_cfg; a.out_err = out_err;
+  a.P = P; a.Sd = Sd; a.n_act = n_act; a.n_ee = n_ee; a.n_rs = n_rs; a.n_self = n_self;
+  a.max_iter = o.max_iter; a.pos_w = o.pos_weight; a.ori_w = o.ori_weight;
+  a.lam0 = o.lambda_init; a.lam_down = o.lambda_down; a.lam_up = o.lambda_up;
+  a.eps_pos = o.eps_pos; a.eps_ori = o.eps_ori;
+  a.coll = o.enable_collision ? 1 : 0; a.coll_w = o.collision_weight; a.margin = o.collision_margin;
+  if (int s = validate_lm(a)) return s;
+  if (P == 0 || Sd == 0) return PK_OK;
+  PK_CHECK_ARG(seeds && twists && parent_tf && parent_idx && act_idx && mimic_mul && mimic_off &&
+                   mimic_act_idx && topo_inv && target_jnts && ancestor_masks && target_Ts &&
+                   lower && upper && fixed_mask && out_cfg && out_err,
+               "null buffer");
+  PK_CHECK_ARG(n_rs == 0 || (robot_spheres_local && robot_sphere_joint_idx), "null robot spheres");
+  PK_CHECK_ARG((Ms == 0 || ws) && (Mc == 0 || wc) && (Mb == 0 || wb) && (Mh == 0 || wh),
+               "null world buffer");
+  PK_CHECK_ARG(n_self == 0 || (self_i && self_j), "null self pairs");
+  if (!a.coll) { a.n_self = 0; }
+  return launch_lm(a, o.threads_per_seed, o.seeds_per_block, (cudaStream_t)stream);
+}
+
+extern "C" int pk_ls_ik_cuda(void* stream, const float* seeds, const float* twists,
+                             const float* parent_tf, const int32_t* parent_idx,
+                             const int32_t* act_idx, const float* mimic_mul, const float* mimic_off,
+                             const int32_t* mimic_act_idx, const int32_t* topo_inv,
+                             const int32_t* target_jnts, const int32_t* ancestor_masks,
+                             const float* target_Ts, const float* robot_spheres_local,
+                             const int32_t* robot_sphere_joint_idx, const float* world_spheres,
+                             const float* world_capsules, const float* world_boxes,
+                             const float* world_halfspaces, const float* lower, const float* upper,
+                             const int32_t* fixed_mask, int64_t max_iter, float pos_weight,
+                             float ori_weight, float lambda_init, float eps_pos, float eps_ori,
+                             int64_t enable_collision, float collision_weight,
+                             float collision_margin, float* out_cfg, float* out_err,
+                             int32_t n_problems, int32_t n_seeds, int32_t n_act, int32_t n_joints,
+                             int32_t n_ee, int32_t n_robot_spheres, int32_t Ms, int32_t Mc,
+                             int32_t Mb, int32_t Mh) {
+  PK_CHECK_ARG(max_iter >= 0 && max_iter <= 1000000, "max_iter out of range");
+  pk_lm_options o{};
+  o.max_iter = (int32_t)max_iter;
+  o.pos_weight = pos_weight;
+  o.ori_weight = ori_weight;
+  o.lambda_init = lambda_init;
+  o.lambda_down = 0.5f;
+  o.lambda_up = 3.0f;
+  o.eps_pos = eps_pos;
+  o.eps_ori = eps_ori;
+  o.enable_collision = enable_collision ? 1 : 0;
+  o.collision_weight = collision_weight;
+  o.collision_margin = collision_margin;
+  return lm_common(stream, o, seeds, twists, parent_tf, parent_idx, act_idx, mimic_mul, mimic_off,
+                   mimic_act_idx, topo_inv, target_jnts, ancestor_masks, target_Ts,
+                   robot_spheres_local, robot_sphere_joint_idx, world_spheres, world_capsules,
+                   world_boxes, world_halfspaces, nullptr, nullptr, lower, upper, fixed_mask,
+                   out_cfg, out_err, n_problems, n_seeds, n_act, n_joints, n_ee, n_robot_spheres,
+                   Ms, Mc, Mb, Mh, 0);
+}
+
+extern "C" int pk_ls_ik_ex(void* stream, const pk_lm_options* opt, const float* seeds,
+                           const float* twists, const float* parent_tf, const int32_t* parent_idx,
+                           const int32_t* act_idx, const float* mimic_mul, const float* mimic_off,
+                           const int32_t* mimic_act_idx, const int32_t* topo_inv,
+                           const int32_t* target_jnts, const int32_t* ancestor_masks,
+                           const float* target_Ts, const float* robot_spheres_local,
+                           const int32_t* robot_sphere_joint_idx, const float* world_spheres,
+                           const float* world_capsules, const float* world_boxes,
+                           const float* world_halfspaces, const int32_t* self_i,
+                           const int32_t* self_j, const float* lower, const float* upper,
+                           const int32_t* fixed_mask, float* out_cfg, float* out_err,
+                           int32_t n_problems, int32_t n_seeds, int32_t n_act, int32_t n_joints,
+                           int32_t n_ee, int32_t n_robot_spheres, int32_t Ms, int32_t Mc,
+                           int32_t Mb, int32_t Mh, int32_t n_self_pairs) {
+  PK_CHECK_ARG(opt != nullptr, "null options");
+  return lm_common(stream, *opt, seeds, twists, parent_tf, parent_idx, act_idx, mimic_mul,
+                   mimic_off, mimic_act_idx, topo_inv, target_jnts, ancestor_masks, target_Ts,
+                   robot_spheres_local, robot_sphere_joint_idx, world_spheres, world_capsules,
+                   world_boxes, world_halfspaces, self_i, self_j, lower, upper, fixed_mask,
+                   out_cfg, out_err, n_problems, n_seeds, n_act, n_joints, n_ee, n_robot_spheres,
+                   Ms, Mc, Mb, Mh, n_self_pairs);
+}
+
+extern "C" int pk_ik_verify_select(void* stream, const float* cfgs, const float* errs,
+                                   const float* prev, float continuity_weight,
+                                   const float* twists, const float* parent_tf,
+                                   const int32_t* parent_idx, const int32_t* act_idx,
+                                   const float* mimic_mul, const float* mimic_off,
+                                   const int32_t* mimic_act_idx, const int32_t* topo_inv,
+                                   const int32_t* target_jnts, const float* target_Ts,
+                                   float pos_tol, float rot_tol, float* winner_cfg,
+                                   double* pos_err, double* rot_err, int32_t* success,
+                                   int32_t n_problems, int32_t n_seeds, int32_t n_act,
+                                   int32_t n_joints, int32_t n_ee) {
+  PK_CHECK_ARG(n_problems >= 0 && n_seeds >= 0 && n_act >= 0 && n_ee >= 1, "bad extent");
+  PK_CHECK_CAP(n_joints <= PK_MAX_JOINTS, "n_joints=%d exceeds %d", n_joints, PK_MAX_JOINTS);
+  if (n_problems == 0) return PK_OK;
+  PK_CHECK_ARG(n_seeds >= 1, "need at least one seed per problem");
+  PK_CHECK_ARG(cfgs && errs && twists && parent_tf && parent_idx && act_idx && mimic_mul &&
+                   mimic_off && mimic_act_idx && topo_inv && target_jnts && target_Ts && winner_cfg,
+               "null buffer");
+  VerifyArgs a{};
+  a.m = ModelArgs{twists, parent_tf, parent_idx, act_idx, mimic_mul, mimic_off, mimic_act_idx,
+                  topo_inv, n_joints, n_act};
+  a.cfgs = cfgs; a.errs = errs; a.prev = prev; a.cw = continuity_weight;
+  a.target_jnts = target_jnts; a.target_Ts = target_Ts; a.pos_tol = pos_tol; a.rot_tol = rot_tol;
+  a.winner_cfg = winner_cfg; a.pos_err = pos_err; a.rot_err = rot_err; a.success = success;
+  a.P = n_problems; a.Sd = n_seeds; a.n_act = n_act; a.n_ee = n_ee;
+  verify_select_kernel<<<n_problems, 128, 0, (cudaStream_t)stream>>>(a);
+  return cuda_status(cudaGetLastError(), "verify_select_kernel launch");
+}
