@@ -159,6 +159,10 @@ __global__ void __launch_bounds__(256) self_sphere_kernel(const float* __restric
     const int li = __ldg(pair_i + p), lj = __ldg(pair_j + p);
     const float4* base = sph + c * SN;
     float dmin = 1e9f;
+    if (li < 0 || li >= N || lj < 0 || lj >= N) {  // invalid link index: no pair
+      out[(b0 + c) * P + p] = dmin;
+      continue;
+    }
     for (int si = 0; si < S; ++si) {
       const float4 A = base[si * N + li];
       if (A.w < 0.f) continue;
@@ -182,6 +186,10 @@ __global__ void __launch_bounds__(256) self_capsule_kernel(const float* __restri
   const long long b = idx / P;
   const int p = (int)(idx - b * P);
   const int li = __ldg(pair_i + p), lj = __ldg(pair_j + p);
+  if (li < 0 || li >= N || lj < 0 || lj >= N) {  // invalid link index: no pair
+    out[idx] = 1e9f;
+    return;
+  }
   float A[7], Bc[7];
 #pragma unroll
   for (int c = 0; c < 7; ++c) {

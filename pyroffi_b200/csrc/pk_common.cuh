@@ -122,7 +122,8 @@ struct ModelArgs {
   int n_act;
 };
 
-struct JointTable {
+// 16-byte aligned so float4 arrays can follow it in shared memory.
+struct __align__(16) JointTable {
   float ptf[PK_MAX_JOINTS][7];  // parent_tf, by sorted position
   float tw[PK_MAX_JOINTS][6];   // twist
   float mul[PK_MAX_JOINTS];

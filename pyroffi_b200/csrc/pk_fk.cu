@@ -105,7 +105,7 @@ __global__ void __launch_bounds__(256) fk_sphere_collision_kernel(FusedArgs a) {
     fk_thread(jt, [&](int i) { return __ldg(c + i); }, ps);
     for (int n = 0; n < N; ++n) {
       const int pj = a.parent_joint[n];
-      Pose T_l = (pj < 0) ? pose_identity() : ps.load(jt.sorted_of[pj]);
+      Pose T_l = (pj < 0 || pj >= jt.n) ? pose_identity() : ps.load(jt.sorted_of[pj]);
       float* d = lp + ((size_t)tid * N + n) * 7;
       d[0] = T_l.w; d[1] = T_l.x; d[2] = T_l.y; d[3] = T_l.z;
       d[4] = T_l.tx; d[5] = T_l.ty; d[6] = T_l.tz;

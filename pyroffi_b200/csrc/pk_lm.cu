@@ -63,6 +63,11 @@ struct LmShared {
   int tsorted[PK_MAX_EE];
   float lo[PK_MAX_ACT], hi[PK_MAX_ACT];
   int fixed[PK_MAX_ACT];
+  float4 jb[PK_MAX_JOINTS];        // bounding sphere of each sphere-carrying joint (joint frame)
+  int jstart[PK_MAX_JOINTS + 1];   // sphere range per sphere-carrying joint
+  int jlist[PK_MAX_JOINTS];        // sorted joint position per sphere-carrying joint
+  int n_js;
+  int n_rs;                        // valid robot spheres after staging
 };
 
 template <int N>
@@ -86,94 +91,112 @@ __device__ __forceinline__ float group_sum(float v, unsigned gmask) {
 }
 
 struct PenaltyCtx {
-  const float4* rs;     // robot spheres (x, y, z, r), joint frame
-  const int* rsj;       // sorted joint position (-1: skip)
-  const float4* ws;     // world spheres (x, y, z, r + margin)
+  const float4* rs;      // robot spheres (x, y, z, r) in their joint frame, grouped by joint
+  const int* rsj;        // sorted joint position of each sphere
+  const float4* jb;      // per sphere-carrying joint: bounding sphere (x, y, z, R) in its frame
+  const int* jstart;     // [n_js + 1] sphere range of each sphere-carrying joint
+  const int* jlist;      // [n_js] sorted joint position of each sphere-carrying joint
+  const float4* ws;      // world spheres (x, y, z, r + margin)
   const float* wc;
   const float* wb;
   const float* wh;
-  const int2* pairs;    // self pairs
-  float* pos;           // [n_rs*3][spb] sphere world positions (self pairs)
-  int n_rs, Ms, Mc, Mb, Mh, n_self, spb;
+  const int2* pairs;     // self pairs (grouped sphere positions; -1 = invalid)
+  float* pos;            // [n_rs*3][spb] world positions of the seed's spheres
+  int n_rs, n_js, Ms, Mc, Mb, Mh, n_self, spb;
   float margin;
 };
 
+// Hinge term of a sphere pair given squared centre distance d2 and
+// rr = r_a + r_b + margin: (d - margin)^2 when d < margin.  Tested on d2
+// first (for rr > 0, d < margin <=> d2 < rr^2; rr <= 0 never hits).
+__device__ __forceinline__ void hinge_sq(float d2, float rr, float& pen) {
+  if (d2 < rr * fabsf(rr)) {
+    const float e = sqrtf(d2) - rr;
+    pen += e * e;
+  }
+}
+
 // Partial hinge penalty of lane t of a TPS-group (not weighted, not summed).
+//  1. lane t places spheres t, t+TPS, ... in world coordinates (shared slots);
+//  2. world spheres: for each sphere-carrying joint, lane t tests the joint's
+//     bounding sphere against obstacles t, t+TPS, ... (a conservative cull:
+//     |B - o| >= R + r_o + margin implies every sphere of the joint clears
+//     o), collects the survivors in a bit mask and tests the joint's
+//     spheres against those only;
+//  3. capsules / boxes / halfspaces: exact test of lane t's spheres;
+//  4. self pairs t, t+TPS, ...
 template <int TPS>
 __device__ float penalty_share(const PenaltyCtx& c, const PoseSlots& ps, int t, int g, unsigned gmask) {
-  constexpr int CH = 4;
   float pen = 0.f;
-  for (int k0 = t; k0 < c.n_rs; k0 += TPS * CH) {
-    float cx[CH], cy[CH], cz[CH], cr[CH];
-#pragma unroll
-    for (int u = 0; u < CH; ++u) {
-      const int k = k0 + u * TPS;
-      cx[u] = 1e18f; cy[u] = 1e18f; cz[u] = 1e18f; cr[u] = 0.f;
-      if (k < c.n_rs) {
-        const int js = c.rsj[k];
-        if (js >= 0) {
-          const float4 s = c.rs[k];
-          const float3 w = pose_apply(ps.load(js), make_float3(s.x, s.y, s.z));
-          cx[u] = w.x; cy[u] = w.y; cz[u] = w.z; cr[u] = s.w;
-          if (c.n_self > 0) {
-            c.pos[(k * 3 + 0) * c.spb + g] = w.x;
-            c.pos[(k * 3 + 1) * c.spb + g] = w.y;
-            c.pos[(k * 3 + 2) * c.spb + g] = w.z;
-          }
+  float* const px = c.pos;
+  const int sp = c.spb;
+  for (int k = t; k < c.n_rs; k += TPS) {
+    const float4 s = c.rs[k];
+    const float3 w = pose_apply(ps.load(c.rsj[k]), make_float3(s.x, s.y, s.z));
+    px[(k * 3 + 0) * sp + g] = w.x;
+    px[(k * 3 + 1) * sp + g] = w.y;
+    px[(k * 3 + 2) * sp + g] = w.z;
+  }
+  __syncwarp(gmask);
+
+  for (int j = 0; j < c.n_js && c.Ms > 0; ++j) {
+    const float4 bl = c.jb[j];
+    const float3 B = pose_apply(ps.load(c.jlist[j]), make_float3(bl.x, bl.y, bl.z));
+    const int k0 = c.jstart[j], k1 = c.jstart[j + 1];
+    for (int ob = 0; ob < c.Ms; ob += 32 * TPS) {
+      unsigned mask = 0u;
+#pragma unroll 8
+      for (int i = 0; i < 32; ++i) {
+        const int o = ob + t + i * TPS;
+        if (o < c.Ms) {
+          const float4 O = c.ws[o];
+          const float rr = bl.w + O.w;
+          const float dx = B.x - O.x, dy = B.y - O.y, dz = B.z - O.z;
+          if (dx * dx + dy * dy + dz * dz < rr * fabsf(rr)) mask |= 1u << i;
         }
       }
-    }
-    for (int m = 0; m < c.Ms; ++m) {
-      const float4 o = c.ws[m];
-#pragma unroll
-      for (int u = 0; u < CH; ++u) {
-        const float rr = cr[u] + o.w;
-        const float dx = cx[u] - o.x, dy = cy[u] - o.y, dz = cz[u] - o.z;
-        const float d2 = dx * dx + dy * dy + dz * dz;
-        if (d2 < rr * fabsf(rr)) {
-          const float e = sqrtf(d2) - rr;
-          pen += e * e;
-        }
-      }
-    }
-    if (c.Mc + c.Mb + c.Mh > 0) {
-#pragma unroll
-      for (int u = 0; u < CH; ++u) {
-        if (cx[u] == 1e18f) continue;
-        const float3 p = make_float3(cx[u], cy[u], cz[u]);
-        for (int m = 0; m < c.Mc; ++m) {
-          const float d = d_sphere_capsule(p, cr[u], c.wc + 7 * m);
-          if (d < c.margin) { const float e = d - c.margin; pen += e * e; }
-        }
-        for (int m = 0; m < c.Mb; ++m) {
-          const float d = d_sphere_box(p, cr[u], c.wb + 15 * m);
-          if (d < c.margin) { const float e = d - c.margin; pen += e * e; }
-        }
-        for (int m = 0; m < c.Mh; ++m) {
-          const float d = d_sphere_halfspace(p, cr[u], c.wh + 6 * m);
-          if (d < c.margin) { const float e = d - c.margin; pen += e * e; }
+      while (mask) {
+        const int i = __ffs(mask) - 1;
+        mask &= mask - 1u;
+        const float4 O = c.ws[ob + t + i * TPS];
+        for (int k = k0; k < k1; ++k) {
+          const float dx = px[(k * 3 + 0) * sp + g] - O.x;
+          const float dy = px[(k * 3 + 1) * sp + g] - O.y;
+          const float dz = px[(k * 3 + 2) * sp + g] - O.z;
+          hinge_sq(dx * dx + dy * dy + dz * dz, c.rs[k].w + O.w, pen);
         }
       }
     }
   }
-  if (c.n_self > 0) {
-    __syncwarp(gmask);
-    for (int q = t; q < c.n_self; q += TPS) {
-      const int2 pr = c.pairs[q];
-      if (pr.x < 0 || pr.y < 0 || pr.x >= c.n_rs || pr.y >= c.n_rs) continue;
-      if (c.rsj[pr.x] < 0 || c.rsj[pr.y] < 0) continue;
-      const float rr = c.rs[pr.x].w + c.rs[pr.y].w + c.margin;
-      const float dx = c.pos[(pr.x * 3 + 0) * c.spb + g] - c.pos[(pr.y * 3 + 0) * c.spb + g];
-      const float dy = c.pos[(pr.x * 3 + 1) * c.spb + g] - c.pos[(pr.y * 3 + 1) * c.spb + g];
-      const float dz = c.pos[(pr.x * 3 + 2) * c.spb + g] - c.pos[(pr.y * 3 + 2) * c.spb + g];
-      const float d2 = dx * dx + dy * dy + dz * dz;
-      if (d2 < rr * fabsf(rr)) {
-        const float e = sqrtf(d2) - rr;
-        pen += e * e;
+
+  if (c.Mc + c.Mb + c.Mh > 0) {
+    for (int k = t; k < c.n_rs; k += TPS) {
+      const float3 p = make_float3(px[(k * 3 + 0) * sp + g], px[(k * 3 + 1) * sp + g], px[(k * 3 + 2) * sp + g]);
+      const float r = c.rs[k].w;
+      for (int m = 0; m < c.Mc; ++m) {
+        const float d = d_sphere_capsule(p, r, c.wc + 7 * m);
+        if (d < c.margin) { const float e = d - c.margin; pen += e * e; }
+      }
+      for (int m = 0; m < c.Mb; ++m) {
+        const float d = d_sphere_box(p, r, c.wb + 15 * m);
+        if (d < c.margin) { const float e = d - c.margin; pen += e * e; }
+      }
+      for (int m = 0; m < c.Mh; ++m) {
+        const float d = d_sphere_halfspace(p, r, c.wh + 6 * m);
+        if (d < c.margin) { const float e = d - c.margin; pen += e * e; }
       }
     }
-    __syncwarp(gmask);
   }
+
+  for (int q = t; q < c.n_self; q += TPS) {
+    const int2 pr = c.pairs[q];
+    if (pr.x < 0) continue;
+    const float dx = px[(pr.x * 3 + 0) * sp + g] - px[(pr.y * 3 + 0) * sp + g];
+    const float dy = px[(pr.x * 3 + 1) * sp + g] - px[(pr.y * 3 + 1) * sp + g];
+    const float dz = px[(pr.x * 3 + 2) * sp + g] - px[(pr.y * 3 + 2) * sp + g];
+    hinge_sq(dx * dx + dy * dy + dz * dz, c.rs[pr.x].w + c.rs[pr.y].w + c.margin, pen);
+  }
+  __syncwarp(gmask);
   return pen;
 }
 
@@ -221,6 +244,7 @@ __global__ void __launch_bounds__(128, (MAXA <= 8 ? 4 : 2)) lm_kernel(LmArgs a) 
   float4* ws4 = reinterpret_cast<float4*>(p); p += sizeof(float4) * a.w.Ms;
   int2* pairs = reinterpret_cast<int2*>(p); p += sizeof(int2) * ((a.n_self + 1) & ~1);
   int* rsj = reinterpret_cast<int*>(p); p += sizeof(int) * ((a.n_rs + 3) & ~3);
+  int* rsk = reinterpret_cast<int*>(p); p += sizeof(int) * ((a.n_rs + 3) & ~3);  // input sphere -> grouped slot
   float* wc = reinterpret_cast<float*>(p); p += sizeof(float) * a.w.Mc * 7;
   float* wb = reinterpret_cast<float*>(p); p += sizeof(float) * a.w.Mb * 15;
   float* wh = reinterpret_cast<float*>(p); p += sizeof(float) * a.w.Mh * 6;
@@ -246,11 +270,59 @@ __global__ void __launch_bounds__(128, (MAXA <= 8 ? 4 : 2)) lm_kernel(LmArgs a) 
     sh.hi[i] = real ? a.upper[i] : 0.f;
     sh.fixed[i] = real ? (a.fixed_mask[i] != 0) : 1;
   }
-  for (int i = tid; i < a.n_rs; i += blockDim.x) {
-    rs4[i] = make_float4(a.spheres_local[4 * i], a.spheres_local[4 * i + 1], a.spheres_local[4 * i + 2],
-                         a.spheres_local[4 * i + 3]);
-    const int j = a.sphere_joint[i];
-    rsj[i] = (j >= 0 && j < a.m.n_joints) ? sh.jt.sorted_of[j] : -1;
+  // Robot spheres grouped by joint (in topological order), invalid joint
+  // indices dropped (the reference skips them too, _ls_ik_cuda_kernel.cu:171),
+  // plus one bounding sphere per sphere-carrying joint.  Built by thread 0:
+  // a few dozen entries, once per block.
+  if (tid == 0) {
+    const int nj = a.m.n_joints;
+    int cnt[PK_MAX_JOINTS];
+    for (int j = 0; j < nj; ++j) cnt[j] = 0;
+    for (int k = 0; k < a.n_rs; ++k) {
+      const int j = a.sphere_joint[k];
+      if (j >= 0 && j < nj) cnt[sh.jt.sorted_of[j]]++;
+    }
+    int n_js = 0, total = 0;
+    int slot_of[PK_MAX_JOINTS];
+    for (int js = 0; js < nj; ++js) {
+      slot_of[js] = -1;
+      if (cnt[js] == 0) continue;
+      slot_of[js] = n_js;
+      sh.jlist[n_js] = js;
+      sh.jstart[n_js] = total;
+      total += cnt[js];
+      cnt[js] = sh.jstart[n_js];  // running insert position
+      ++n_js;
+    }
+    sh.jstart[n_js] = total;
+    sh.n_js = n_js;
+    sh.n_rs = total;
+    for (int k = 0; k < a.n_rs; ++k) {
+      const int j = a.sphere_joint[k];
+      if (j < 0 || j >= nj) { rsk[k] = -1; continue; }
+      const int js = sh.jt.sorted_of[j];
+      const int at = cnt[js]++;
+      rsk[k] = at;
+      rs4[at] = make_float4(a.spheres_local[4 * k], a.spheres_local[4 * k + 1], a.spheres_local[4 * k + 2],
+                            a.spheres_local[4 * k + 3]);
+      rsj[at] = js;
+    }
+    for (int q = 0; q < n_js; ++q) {
+      float lo[3] = {3e38f, 3e38f, 3e38f}, hi[3] = {-3e38f, -3e38f, -3e38f};
+      for (int k = sh.jstart[q]; k < sh.jstart[q + 1]; ++k) {
+        const float v[3] = {rs4[k].x, rs4[k].y, rs4[k].z};
+        for (int d = 0; d < 3; ++d) { lo[d] = fminf(lo[d], v[d]); hi[d] = fmaxf(hi[d], v[d]); }
+      }
+      const float cx = 0.5f * (lo[0] + hi[0]), cy = 0.5f * (lo[1] + hi[1]), cz = 0.5f * (lo[2] + hi[2]);
+      float R = -3e38f;
+      for (int k = sh.jstart[q]; k < sh.jstart[q + 1]; ++k) {
+        const float dx = rs4[k].x - cx, dy = rs4[k].y - cy, dz = rs4[k].z - cz;
+        R = fmaxf(R, sqrtf(dx * dx + dy * dy + dz * dz) + rs4[k].w);
+      }
+      // slack keeps the cull conservative under FP32 rounding
+      sh.jb[q] = make_float4(cx, cy, cz, R + 1e-5f + 1e-6f * fabsf(R));
+    }
+    (void)slot_of;
   }
   for (int i = tid; i < a.w.Ms; i += blockDim.x)
     ws4[i] = make_float4(a.w.spheres[4 * i], a.w.spheres[4 * i + 1], a.w.spheres[4 * i + 2],
@@ -258,7 +330,12 @@ __global__ void __launch_bounds__(128, (MAXA <= 8 ? 4 : 2)) lm_kernel(LmArgs a) 
   for (int i = tid; i < a.w.Mc * 7; i += blockDim.x) wc[i] = a.w.capsules[i];
   for (int i = tid; i < a.w.Mb * 15; i += blockDim.x) wb[i] = a.w.boxes[i];
   for (int i = tid; i < a.w.Mh * 6; i += blockDim.x) wh[i] = a.w.halfspaces[i];
-  for (int i = tid; i < a.n_self; i += blockDim.x) pairs[i] = make_int2(a.self_i[i], a.self_j[i]);
+  __syncthreads();
+  for (int i = tid; i < a.n_self; i += blockDim.x) {
+    const int x = a.self_i[i], y = a.self_j[i];
+    const bool ok = x >= 0 && y >= 0 && x < a.n_rs && y < a.n_rs && rsk[x] >= 0 && rsk[y] >= 0;
+    pairs[i] = ok ? make_int2(rsk[x], rsk[y]) : make_int2(-1, -1);
+  }
   __syncthreads();
 
   const int g = tid / TPS, t = tid - g * TPS;
@@ -270,11 +347,12 @@ __global__ void __launch_bounds__(128, (MAXA <= 8 ? 4 : 2)) lm_kernel(LmArgs a) 
 
   const JointTable& jt = sh.jt;
   const PoseSlots ps{slots + tid, (int)blockDim.x};
-  const bool use_coll = a.coll && (a.n_rs > 0);
+  const bool use_coll = a.coll && (sh.n_rs > 0);
   PenaltyCtx pc;
-  pc.rs = rs4; pc.rsj = rsj; pc.ws = ws4; pc.wc = wc; pc.wb = wb; pc.wh = wh; pc.pairs = pairs;
-  pc.pos = pos; pc.n_rs = a.n_rs; pc.Ms = a.w.Ms; pc.Mc = a.w.Mc; pc.Mb = a.w.Mb; pc.Mh = a.w.Mh;
-  pc.n_self = a.n_self; pc.spb = a.spb; pc.margin = a.margin;
+  pc.rs = rs4; pc.rsj = rsj; pc.jb = sh.jb; pc.jstart = sh.jstart; pc.jlist = sh.jlist;
+  pc.ws = ws4; pc.wc = wc; pc.wb = wb; pc.wh = wh; pc.pairs = pairs;
+  pc.pos = pos; pc.n_rs = sh.n_rs; pc.n_js = sh.n_js; pc.Ms = a.w.Ms; pc.Mc = a.w.Mc; pc.Mb = a.w.Mb;
+  pc.Mh = a.w.Mh; pc.n_self = a.n_self; pc.spb = a.spb; pc.margin = a.margin;
 
   float W[6] = {a.pos_w, a.pos_w, a.pos_w, a.ori_w, a.ori_w, a.ori_w};
 
@@ -306,7 +384,12 @@ __global__ void __launch_bounds__(128, (MAXA <= 8 ? 4 : 2)) lm_kernel(LmArgs a) 
   float r[6 * MAXEE], pee[3 * MAXEE];
   run_fk(cfg);
   ee_residual<MAXEE>(sh, ps, a.n_ee, r, pee);
-  float best_err = weighted_sq(r) + penalty();
+  // penalty at the current configuration: the reference re-evaluates it at
+  // the top of every iteration; it only changes when a trial is accepted, and
+  // then equals that trial's penalty bit for bit (same configuration, same
+  // code), so it is carried instead of recomputed.
+  float pen_cur = penalty();
+  float best_err = weighted_sq(r) + pen_cur;
   float lam = a.lam0;
 
   for (int it = 0; it < a.max_iter; ++it) {
@@ -370,7 +453,7 @@ __global__ void __launch_bounds__(128, (MAXA <= 8 ? 4 : 2)) lm_kernel(LmArgs a) 
     float curr = 0.f;
 #pragma unroll
     for (int k = 0; k < 6 * MAXEE; ++k) curr += fw[k] * fw[k];
-    curr += penalty();
+    curr += pen_cur;
 
     // Jacobi column scaling
     float col_s[MAXA];
@@ -462,6 +545,7 @@ __global__ void __launch_bounds__(128, (MAXA <= 8 ? 4 : 2)) lm_kernel(LmArgs a) 
 
     // line search
     float best_a_err = 1e30f;
+    float best_a_pen = pen_cur;
     int best_a = 0;
 #pragma unroll 1
     for (int ai = 0; ai < 5; ++ai) {
@@ -471,8 +555,9 @@ __global__ void __launch_bounds__(128, (MAXA <= 8 ? 4 : 2)) lm_kernel(LmArgs a) 
       run_fk(trial);
       float rt[6 * MAXEE], pt[3 * MAXEE];
       ee_residual<MAXEE>(sh, ps, a.n_ee, rt, pt);
-      const float et = weighted_sq(rt) + penalty();
-      if (et < best_a_err) { best_a_err = et; best_a = ai; }
+      const float pt_pen = penalty();
+      const float et = weighted_sq(rt) + pt_pen;
+      if (et < best_a_err) { best_a_err = et; best_a = ai; best_a_pen = pt_pen; }
     }
     const float alpha = line_alpha(best_a);
     float trial[MAXA];
@@ -481,6 +566,7 @@ __global__ void __launch_bounds__(128, (MAXA <= 8 ? 4 : 2)) lm_kernel(LmArgs a) 
     if (best_a_err < curr * (1.0f - 1e-4f)) {
 #pragma unroll
       for (int c = 0; c < MAXA; ++c) cfg[c] = trial[c];
+      pen_cur = best_a_pen;
       lam = fmaxf(lam * a.lam_down, 1e-10f);
     } else {
       lam = fminf(lam * a.lam_up, 1e6f);
@@ -663,10 +749,10 @@ __global__ void __launch_bounds__(128) verify_select_kernel(VerifyArgs a) {
 static size_t lm_smem_bytes(const LmArgs& a, int threads) {
   size_t b = (sizeof(LmShared) + 15) & ~size_t(15);
   b += sizeof(float4) * a.n_rs + sizeof(float4) * a.w.Ms + sizeof(int2) * ((a.n_self + 1) & ~1) +
-       sizeof(int) * ((a.n_rs + 3) & ~3) + sizeof(float) * (a.w.Mc * 7 + a.w.Mb * 15 + a.w.Mh * 6);
+       2 * sizeof(int) * ((a.n_rs + 3) & ~3) + sizeof(float) * (a.w.Mc * 7 + a.w.Mb * 15 + a.w.Mh * 6);
   b = (b + 15) & ~size_t(15);
   b += sizeof(float) * (size_t)a.m.n_joints * 7 * threads;
-  if (a.n_self > 0) b += sizeof(float) * (size_t)a.n_rs * 3 * a.spb;
+  if (a.coll) b += sizeof(float) * (size_t)a.n_rs * 3 * a.spb;
   return b;
 }
 
