@@ -129,6 +129,7 @@ struct __align__(16) JointTable {
   float mul[PK_MAX_JOINTS];
   float off[PK_MAX_JOINTS];
   float axis[PK_MAX_JOINTS][3]; // unit Jacobian axis in the joint frame
+  float ru[PK_MAX_JOINTS][4];   // revolute motion: unit omega axis and |omega|
   int src[PK_MAX_JOINTS];       // actuated source index (-1: none)
   int psorted[PK_MAX_JOINTS];   // sorted position of the parent (-1: root)
   int orig[PK_MAX_JOINTS];      // original joint index
@@ -183,6 +184,11 @@ __device__ inline void load_joint_table(JointTable& jt, const ModelArgs& m) {
     else if (ang2 == 0.f) kind = kPrismatic;
     else kind = kScrew;
     jt.kind[i] = kind;
+    {
+      const float n_w = sqrtf(ang2);
+      const float inv = (n_w > 0.f) ? 1.f / n_w : 0.f;
+      jt.ru[i][0] = tw[3] * inv; jt.ru[i][1] = tw[4] * inv; jt.ru[i][2] = tw[5] * inv; jt.ru[i][3] = n_w;
+    }
     // Jacobian column kind as in the reference helper: revolute when
     // |omega|^2 > 1e-6, else prismatic when |v|^2 > 1e-6.
     if (ang2 > 1e-6f) {
@@ -214,6 +220,30 @@ __device__ __forceinline__ Pose load_ptf(const JointTable& jt, int i) {
               jt.ptf[i][4], jt.ptf[i][5], jt.ptf[i][6]};
 }
 
+// T_parent_child = parent_tf o exp(twist * q) of sorted joint i.  For a
+// revolute twist (0, w) with w = n u, |u| = 1, exp is the pure rotation
+// (cos(q n / 2), sin(q n / 2) u) -- the same quaternion as
+// (cos(t/2), sin(t/2)/t * w q) with t = |q| n, without the square root and
+// division -- so T_pc keeps parent_tf's translation.
+__device__ __forceinline__ Pose joint_local(const JointTable& jt, int i, float q) {
+  Pose P = load_ptf(jt, i);
+  const int kind = jt.kind[i];
+  if (kind == kFixed) return P;
+  if (kind == kRevolute) {
+    float s, c;
+    sincosf(0.5f * q * jt.ru[i][3], &s, &c);
+    const float bx = s * jt.ru[i][0], by = s * jt.ru[i][1], bz = s * jt.ru[i][2];
+    Pose o;
+    o.w = P.w * c - P.x * bx - P.y * by - P.z * bz;
+    o.x = P.w * bx + P.x * c + P.y * bz - P.z * by;
+    o.y = P.w * by - P.x * bz + P.y * c + P.z * bx;
+    o.z = P.w * bz + P.x * by - P.y * bx + P.z * c;
+    o.tx = P.tx; o.ty = P.ty; o.tz = P.tz;
+    return o;
+  }
+  return pose_compose(P, joint_motion(kind, jt.tw[i], q));
+}
+
 // Per-thread pose storage in shared memory, strided by `stride` floats
 // between consecutive components so consecutive threads hit consecutive
 // banks.  Component c of sorted joint i lives at base[(i*7+c)*stride].
@@ -241,9 +271,7 @@ __device__ __forceinline__ void fk_thread(const JointTable& jt, CfgFn cfg_at, co
     const int src = jt.src[i];
     const float qref = (src < 0) ? 0.f : cfg_at(src);
     const float q = qref * jt.mul[i] + jt.off[i];
-    const int kind = jt.kind[i];
-    Pose Tpc = load_ptf(jt, i);
-    if (kind != kFixed) Tpc = pose_compose(Tpc, joint_motion(kind, jt.tw[i], q));
+    const Pose Tpc = joint_local(jt, i, q);
     const int ps = jt.psorted[i];
     Pose Tw;
     if (ps < 0) Tw = Tpc;

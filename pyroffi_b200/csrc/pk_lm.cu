@@ -22,9 +22,18 @@
 //    Jacobian and damping state stay in registers (all loops over the DOF
 //    are unrolled to the compile-time bucket MAXA, padded dimensions are
 //    masked like fixed joints).
-//  * sphere-sphere hinge terms are tested on squared distance first:
+//  * the collision penalty never touches most (sphere, obstacle) pairs:
+//    every sphere-carrying joint gets a bounding sphere; a per-block
+//    uniform grid over the world spheres hands each joint only the obstacles
+//    whose (inflated) ball covers the joint's cell; self pairs are grouped
+//    by joint pair and a group is skipped when the two bounding spheres are
+//    margin apart.  All culls are conservative (exact in real arithmetic,
+//    with slack for FP32), so the penalty equals the brute-force sum.
+//  * hinge terms are tested on squared distance first:
 //    d - margin < 0  <=>  |c - o|^2 < (r_s + r_o + margin)^2 for a positive
 //    sum, so the square root runs only for the rare active pairs.
+//  * the penalty at the current configuration is carried from the accepted
+//    trial instead of being recomputed (it is the same value).
 #include <float.h>
 
 #include "pk_obstacles.cuh"
@@ -68,6 +77,10 @@ struct LmShared {
   int jlist[PK_MAX_JOINTS];        // sorted joint position per sphere-carrying joint
   int n_js;
   int n_rs;                        // valid robot spheres after staging
+  int n_groups;                    // self-pair groups
+  int grid_on;
+  float3 glo, ginv;                // obstacle grid origin, inverse cell size
+  float rmax;                      // largest joint bounding radius
 };
 
 template <int N>
@@ -83,6 +96,81 @@ __device__ __forceinline__ float line_alpha(int i) {
   return i == 0 ? 1.0f : i == 1 ? 0.5f : i == 2 ? 0.25f : i == 3 ? 0.1f : 0.025f;
 }
 
+// World spheres are padded to whole 32*TPS chunks so the culling loop needs no bounds test.
+__host__ __device__ __forceinline__ int lm_ms_pad(int Ms, int tps) {
+  const int chunk = 32 * tps;
+  return ((Ms + chunk - 1) / chunk) * chunk;
+}
+
+// Per-seed stride (floats) of the sphere position slots: odd, so the seeds
+// of a warp reading the same sphere hit distinct banks.
+__host__ __device__ __forceinline__ int lm_pos_stride(int n_rs, int n_joints) {
+  return (3 * n_rs + 3 * n_joints) | 1;  // sphere positions, then joint bounding centres
+}
+
+// Obstacle grid resolution per axis (cells = PK_LM_GRID^3, indices packed in 4 bits).
+#define PK_LM_GRID 8
+
+// Byte offsets of the LM block's dynamic shared memory.
+struct LmLayout {
+  size_t rs, ws, pairs, gjoint, gstart, rsj, rsk, cells, cell_obs, wc, wb, wh, slots, pos, total;
+  int ms_pad, grid, max_entries, scratch_ints;
+};
+
+__host__ __device__ inline size_t lm_align16(size_t x) { return (x + 15) & ~size_t(15); }
+
+__host__ __device__ inline LmLayout lm_layout(const LmArgs& a, int tps) {
+  LmLayout L;
+  size_t o = lm_align16(sizeof(LmShared));
+  const int n_rs = a.n_rs, n_self = a.coll ? a.n_self : 0;
+  L.ms_pad = lm_ms_pad(a.w.Ms, tps);
+  const int PS = lm_pos_stride(n_rs, a.m.n_joints);
+  L.scratch_ints = a.coll ? PS * a.spb : 0;
+  L.grid = (a.coll && a.w.Ms >= 32 && a.w.Ms <= 65535 && a.w.Ms <= L.scratch_ints) ? 1 : 0;
+  L.max_entries = L.grid ? min(max(48 * a.w.Ms, 1024), 16384) : 0;
+  L.rs = o; o = lm_align16(o + 16 * (size_t)n_rs);
+  L.ws = o; o = lm_align16(o + 16 * (size_t)L.ms_pad);
+  L.pairs = o; o = lm_align16(o + 8 * (size_t)n_self);
+  L.gjoint = o; o = lm_align16(o + 8 * (size_t)(n_self + 1));
+  L.gstart = o; o = lm_align16(o + 4 * (size_t)(n_self + 2));
+  L.rsj = o; o = lm_align16(o + 4 * (size_t)n_rs);
+  L.rsk = o; o = lm_align16(o + 4 * (size_t)n_rs);
+  L.cells = o; o = lm_align16(o + (L.grid ? 4 * (size_t)(PK_LM_GRID * PK_LM_GRID * PK_LM_GRID + 1) : 0));
+  L.cell_obs = o; o = lm_align16(o + 2 * (size_t)L.max_entries);
+  L.wc = o; o = lm_align16(o + 28 * (size_t)a.w.Mc);
+  L.wb = o; o = lm_align16(o + 60 * (size_t)a.w.Mb);
+  L.wh = o; o = lm_align16(o + 24 * (size_t)a.w.Mh);
+  L.slots = o; o = lm_align16(o + 28 * (size_t)a.m.n_joints * a.spb);
+  L.pos = o; o = lm_align16(o + 4 * (size_t)L.scratch_ints);
+  L.total = o;
+  return L;
+}
+
+// FK of one configuration computed by every lane of a seed group (identical
+// values) and stored by the leader only.  A non-chain parent is read back
+// from the shared slots, so a tree needs the group to sync after each store.
+template <typename CfgFn>
+__device__ __forceinline__ void fk_group(const JointTable& jt, CfgFn cfg_at, const PoseSlots& out, bool leader,
+                                         unsigned gmask) {
+  Pose prev = pose_identity();
+  const int n = jt.n;
+  const bool chain = jt.chain != 0;
+  for (int i = 0; i < n; ++i) {
+    const int src = jt.src[i];
+    const float qref = (src < 0) ? 0.f : cfg_at(src);
+    const float q = qref * jt.mul[i] + jt.off[i];
+    const Pose Tpc = joint_local(jt, i, q);
+    const int ps = jt.psorted[i];
+    Pose Tw;
+    if (ps < 0) Tw = Tpc;
+    else if (ps == i - 1) Tw = pose_compose(prev, Tpc);
+    else Tw = pose_compose(out.load(ps), Tpc);
+    if (leader) out.store(i, Tw);
+    if (!chain) __syncwarp(gmask);
+    prev = Tw;
+  }
+}
+
 template <int TPS>
 __device__ __forceinline__ float group_sum(float v, unsigned gmask) {
 #pragma unroll
@@ -92,17 +180,22 @@ __device__ __forceinline__ float group_sum(float v, unsigned gmask) {
 
 struct PenaltyCtx {
   const float4* rs;      // robot spheres (x, y, z, r) in their joint frame, grouped by joint
-  const int* rsj;        // sorted joint position of each sphere
-  const float4* jb;      // per sphere-carrying joint: bounding sphere (x, y, z, R) in its frame
-  const int* jstart;     // [n_js + 1] sphere range of each sphere-carrying joint
-  const int* jlist;      // [n_js] sorted joint position of each sphere-carrying joint
-  const float4* ws;      // world spheres (x, y, z, r + margin)
+  const float4* jb;      // per sphere-carrying joint slot: bounding sphere (x, y, z, R) in its frame
+  const int* jstart;     // [n_js + 1] sphere range of each joint slot
+  const int* jlist;      // [n_js] sorted joint position of each joint slot
+  const float4* ws;      // world spheres (x, y, z, r + margin), padded to a multiple of 32*TPS
   const float* wc;
   const float* wb;
   const float* wh;
-  const int2* pairs;     // self pairs (grouped sphere positions; -1 = invalid)
-  float* pos;            // [n_rs*3][spb] world positions of the seed's spheres
-  int n_rs, n_js, Ms, Mc, Mb, Mh, n_self, spb;
+  const int2* pairs;     // self pairs in sphere slots, grouped by joint-slot pair
+  const int2* gjoint;    // [n_groups] joint slots (a, b) of each self-pair group
+  const int* gstart;     // [n_groups + 1]
+  const int* cell_start; // [G^3 + 1] obstacle grid (null: no grid, scan every obstacle)
+  const unsigned short* cell_obs;
+  float* pos;            // this seed: sphere world positions [n_rs][3], then bounding centres [n_js][3]
+  float3 glo, ginv;      // grid origin and inverse cell size
+  int G;
+  int n_rs, n_js, n_groups, Ms_pad, Mc, Mb, Mh;
   float margin;
 };
 
@@ -116,54 +209,81 @@ __device__ __forceinline__ void hinge_sq(float d2, float rr, float& pen) {
   }
 }
 
+// Exact hinge terms of the spheres [k0, k1) of one joint against world sphere O.
+__device__ __forceinline__ void narrow_world(const PenaltyCtx& c, int k0, int k1, float4 O, float& pen) {
+  const float* px = c.pos;
+  for (int k = k0; k < k1; ++k) {
+    const float dx = px[3 * k] - O.x, dy = px[3 * k + 1] - O.y, dz = px[3 * k + 2] - O.z;
+    hinge_sq(dx * dx + dy * dy + dz * dz, c.rs[k].w + O.w, pen);
+  }
+}
+
 // Partial hinge penalty of lane t of a TPS-group (not weighted, not summed).
-//  1. lane t places spheres t, t+TPS, ... in world coordinates (shared slots);
-//  2. world spheres: for each sphere-carrying joint, lane t tests the joint's
-//     bounding sphere against obstacles t, t+TPS, ... (a conservative cull:
-//     |B - o| >= R + r_o + margin implies every sphere of the joint clears
-//     o), collects the survivors in a bit mask and tests the joint's
-//     spheres against those only;
+//  1. per sphere-carrying joint, the joint's bounding-sphere centre (lane 0)
+//     and lane t's share of its spheres go to this seed's shared slots;
+//  2. world spheres: conservative culls before any sphere-level test.  The
+//     joint's bounding sphere (centre B, radius R) can only reach obstacle o
+//     if |B - o| < R + r_o + margin.  With the obstacle grid, only the
+//     obstacles registered in B's cell (every obstacle whose ball of radius
+//     r_o + margin + max R covers part of that cell) are candidates; lane t
+//     takes candidates t, t+TPS, ...  Without it, lane t scans obstacles
+//     t, t+TPS, ... into a 32-bit survivor mask.
 //  3. capsules / boxes / halfspaces: exact test of lane t's spheres;
-//  4. self pairs t, t+TPS, ...
+//  4. self pairs by joint-slot group: a group is skipped when the two
+//     joints' bounding spheres are margin apart; otherwise lane t tests
+//     its pairs t, t+TPS, ... of the group.
 template <int TPS>
-__device__ float penalty_share(const PenaltyCtx& c, const PoseSlots& ps, int t, int g, unsigned gmask) {
+__device__ float penalty_share(const PenaltyCtx& c, const PoseSlots& ps, int t, unsigned gmask) {
   float pen = 0.f;
   float* const px = c.pos;
-  const int sp = c.spb;
-  for (int k = t; k < c.n_rs; k += TPS) {
-    const float4 s = c.rs[k];
-    const float3 w = pose_apply(ps.load(c.rsj[k]), make_float3(s.x, s.y, s.z));
-    px[(k * 3 + 0) * sp + g] = w.x;
-    px[(k * 3 + 1) * sp + g] = w.y;
-    px[(k * 3 + 2) * sp + g] = w.z;
+  float* const pb = c.pos + 3 * c.n_rs;
+  for (int j = 0; j < c.n_js; ++j) {
+    const Pose T = ps.load(c.jlist[j]);
+    if (t == 0) {
+      const float4 bl = c.jb[j];
+      const float3 B = pose_apply(T, make_float3(bl.x, bl.y, bl.z));
+      pb[3 * j] = B.x; pb[3 * j + 1] = B.y; pb[3 * j + 2] = B.z;
+    }
+    for (int k = c.jstart[j] + t; k < c.jstart[j + 1]; k += TPS) {
+      const float4 s = c.rs[k];
+      const float3 w = pose_apply(T, make_float3(s.x, s.y, s.z));
+      px[3 * k] = w.x; px[3 * k + 1] = w.y; px[3 * k + 2] = w.z;
+    }
   }
   __syncwarp(gmask);
 
-  for (int j = 0; j < c.n_js && c.Ms > 0; ++j) {
-    const float4 bl = c.jb[j];
-    const float3 B = pose_apply(ps.load(c.jlist[j]), make_float3(bl.x, bl.y, bl.z));
+  for (int j = 0; j < c.n_js && c.Ms_pad > 0; ++j) {
+    const float R = c.jb[j].w;
+    const float Bx = pb[3 * j], By = pb[3 * j + 1], Bz = pb[3 * j + 2];
     const int k0 = c.jstart[j], k1 = c.jstart[j + 1];
-    for (int ob = 0; ob < c.Ms; ob += 32 * TPS) {
-      unsigned mask = 0u;
-#pragma unroll 8
-      for (int i = 0; i < 32; ++i) {
-        const int o = ob + t + i * TPS;
-        if (o < c.Ms) {
-          const float4 O = c.ws[o];
-          const float rr = bl.w + O.w;
-          const float dx = B.x - O.x, dy = B.y - O.y, dz = B.z - O.z;
+    if (c.cell_start) {
+      const int ix = __float2int_rd((Bx - c.glo.x) * c.ginv.x);
+      const int iy = __float2int_rd((By - c.glo.y) * c.ginv.y);
+      const int iz = __float2int_rd((Bz - c.glo.z) * c.ginv.z);
+      // outside the grid no obstacle is within reach of this joint
+      if ((unsigned)ix >= (unsigned)c.G || (unsigned)iy >= (unsigned)c.G || (unsigned)iz >= (unsigned)c.G) continue;
+      const int cell = (ix * c.G + iy) * c.G + iz;
+      const int e1 = c.cell_start[cell + 1];
+      for (int e = c.cell_start[cell] + t; e < e1; e += TPS) {
+        const float4 O = c.ws[c.cell_obs[e]];
+        const float rr = R + O.w;
+        const float dx = Bx - O.x, dy = By - O.y, dz = Bz - O.z;
+        if (dx * dx + dy * dy + dz * dz < rr * fabsf(rr)) narrow_world(c, k0, k1, O, pen);
+      }
+    } else {
+      for (int ob = t; ob < c.Ms_pad; ob += 32 * TPS) {
+        unsigned mask = 0u;
+#pragma unroll
+        for (int i = 0; i < 32; ++i) {
+          const float4 O = c.ws[ob + i * TPS];
+          const float rr = R + O.w;
+          const float dx = Bx - O.x, dy = By - O.y, dz = Bz - O.z;
           if (dx * dx + dy * dy + dz * dz < rr * fabsf(rr)) mask |= 1u << i;
         }
-      }
-      while (mask) {
-        const int i = __ffs(mask) - 1;
-        mask &= mask - 1u;
-        const float4 O = c.ws[ob + t + i * TPS];
-        for (int k = k0; k < k1; ++k) {
-          const float dx = px[(k * 3 + 0) * sp + g] - O.x;
-          const float dy = px[(k * 3 + 1) * sp + g] - O.y;
-          const float dz = px[(k * 3 + 2) * sp + g] - O.z;
-          hinge_sq(dx * dx + dy * dy + dz * dz, c.rs[k].w + O.w, pen);
+        while (mask) {
+          const int i = __ffs(mask) - 1;
+          mask &= mask - 1u;
+          narrow_world(c, k0, k1, c.ws[ob + i * TPS], pen);
         }
       }
     }
@@ -171,7 +291,7 @@ __device__ float penalty_share(const PenaltyCtx& c, const PoseSlots& ps, int t, 
 
   if (c.Mc + c.Mb + c.Mh > 0) {
     for (int k = t; k < c.n_rs; k += TPS) {
-      const float3 p = make_float3(px[(k * 3 + 0) * sp + g], px[(k * 3 + 1) * sp + g], px[(k * 3 + 2) * sp + g]);
+      const float3 p = make_float3(px[3 * k], px[3 * k + 1], px[3 * k + 2]);
       const float r = c.rs[k].w;
       for (int m = 0; m < c.Mc; ++m) {
         const float d = d_sphere_capsule(p, r, c.wc + 7 * m);
@@ -188,13 +308,20 @@ __device__ float penalty_share(const PenaltyCtx& c, const PoseSlots& ps, int t, 
     }
   }
 
-  for (int q = t; q < c.n_self; q += TPS) {
-    const int2 pr = c.pairs[q];
-    if (pr.x < 0) continue;
-    const float dx = px[(pr.x * 3 + 0) * sp + g] - px[(pr.y * 3 + 0) * sp + g];
-    const float dy = px[(pr.x * 3 + 1) * sp + g] - px[(pr.y * 3 + 1) * sp + g];
-    const float dz = px[(pr.x * 3 + 2) * sp + g] - px[(pr.y * 3 + 2) * sp + g];
-    hinge_sq(dx * dx + dy * dy + dz * dz, c.rs[pr.x].w + c.rs[pr.y].w + c.margin, pen);
+  for (int gi = 0; gi < c.n_groups; ++gi) {
+    const int2 ja = c.gjoint[gi];
+    const float dx = pb[3 * ja.x] - pb[3 * ja.y];
+    const float dy = pb[3 * ja.x + 1] - pb[3 * ja.y + 1];
+    const float dz = pb[3 * ja.x + 2] - pb[3 * ja.y + 2];
+    const float rr = c.jb[ja.x].w + c.jb[ja.y].w + c.margin;
+    if (!(dx * dx + dy * dy + dz * dz < rr * fabsf(rr))) continue;
+    for (int q = c.gstart[gi] + t; q < c.gstart[gi + 1]; q += TPS) {
+      const int2 pr = c.pairs[q];
+      const float ex = px[3 * pr.x] - px[3 * pr.y];
+      const float ey = px[3 * pr.x + 1] - px[3 * pr.y + 1];
+      const float ez = px[3 * pr.x + 2] - px[3 * pr.y + 2];
+      hinge_sq(ex * ex + ey * ey + ez * ez, c.rs[pr.x].w + c.rs[pr.y].w + c.margin, pen);
+    }
   }
   __syncwarp(gmask);
   return pen;
@@ -235,22 +362,172 @@ __device__ __forceinline__ void ee_residual(const LmShared& sh, const PoseSlots&
   }
 }
 
+// Damped Gauss-Newton step of the current point (_ls_ik_cuda_kernel.cu:257-335):
+// weighted stacked Jacobian from the joint poses in `ps`, Jacobi column
+// scaling, FP64 normal equations (Js^T Js + lam I) p = -Js^T fw with fixed
+// and padded joints masked, Cholesky solve (p = 0 on a non-positive pivot),
+// unscaling and the trust-region clip.  Writes `delta`, returns ||fw||^2.
+template <int MAXA, int MAXEE>
+__device__ __forceinline__ float lm_direction(const LmShared& sh, const PoseSlots& ps, int n_ee, const float (&W)[6],
+                                              const float (&r)[6 * MAXEE], const float (&pee)[3 * MAXEE],
+                                              float lam, float max_p, float max_o, float (&delta)[MAXA]) {
+  const JointTable& jt = sh.jt;
+  // weighted stacked Jacobian J[k][c]
+  float J[6 * MAXEE][MAXA];
+#pragma unroll
+  for (int k = 0; k < 6 * MAXEE; ++k)
+#pragma unroll
+    for (int c = 0; c < MAXA; ++c) J[k][c] = 0.f;
+  for (int i = 0; i < jt.n; ++i) {
+    const int jk = jt.jkind[i];
+    const int a1 = jt.a1[i], a2 = jt.a2[i];
+    if (jk == 0 || (a1 < 0 && a2 < 0)) continue;
+    const Pose Tj = ps.load(i);
+    const float3 z = quat_rotate(Tj.w, Tj.x, Tj.y, Tj.z,
+                                 make_float3(jt.axis[i][0], jt.axis[i][1], jt.axis[i][2]));
+    const float sm = jt.mul[i];
+    const int orig = jt.orig[i];
+#pragma unroll
+    for (int e = 0; e < MAXEE; ++e) {
+      if (e >= n_ee || !((sh.anc[e] >> orig) & 1ull)) continue;
+      float col[6];
+      if (jk == 1) {
+        const float ax = pee[3 * e] - Tj.tx, ay = pee[3 * e + 1] - Tj.ty, az = pee[3 * e + 2] - Tj.tz;
+        col[0] = z.y * az - z.z * ay; col[1] = z.z * ax - z.x * az; col[2] = z.x * ay - z.y * ax;
+        col[3] = z.x; col[4] = z.y; col[5] = z.z;
+      } else {
+        col[0] = z.x; col[1] = z.y; col[2] = z.z; col[3] = col[4] = col[5] = 0.f;
+      }
+#pragma unroll
+      for (int c = 0; c < MAXA; ++c) {
+        const float wsel = ((c == a1) ? sm : 0.f) + ((c == a2) ? sm : 0.f);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) J[6 * e + k][c] += wsel * col[k];
+      }
+    }
+  }
+  float fw[6 * MAXEE];
+#pragma unroll
+  for (int k = 0; k < 6 * MAXEE; ++k) {
+    fw[k] = r[k] * W[k % 6];
+#pragma unroll
+    for (int c = 0; c < MAXA; ++c) J[k][c] *= W[k % 6];
+  }
+  float fw2 = 0.f;
+#pragma unroll
+  for (int k = 0; k < 6 * MAXEE; ++k) fw2 += fw[k] * fw[k];
+
+  // Jacobi column scaling
+  float col_s[MAXA];
+#pragma unroll
+  for (int c = 0; c < MAXA; ++c) {
+    float sq = 0.f;
+#pragma unroll
+    for (int k = 0; k < 6 * MAXEE; ++k) sq += J[k][c] * J[k][c];
+    col_s[c] = sqrtf(sq) + 1e-8f;
+  }
+#pragma unroll
+  for (int k = 0; k < 6 * MAXEE; ++k)
+#pragma unroll
+    for (int c = 0; c < MAXA; ++c) J[k][c] = J[k][c] / col_s[c];
+
+  // FP64 normal equations (lower triangle, packed) + masking
+  double A[MAXA * (MAXA + 1) / 2];
+  double rhs[MAXA];
+#pragma unroll
+  for (int i = 0; i < MAXA; ++i) {
+    const bool fi = sh.fixed[i];
+#pragma unroll
+    for (int j = 0; j <= i; ++j) {
+      double acc = 0.0;
+#pragma unroll
+      for (int k = 0; k < 6 * MAXEE; ++k) acc += (double)J[k][i] * (double)J[k][j];
+      if (i == j) acc += (double)lam;
+      const bool fj = sh.fixed[j];
+      A[i * (i + 1) / 2 + j] = (fi || fj) ? ((i == j) ? 1.0 : 0.0) : acc;
+    }
+    double rb = 0.0;
+#pragma unroll
+    for (int k = 0; k < 6 * MAXEE; ++k) rb += (double)J[k][i] * (double)fw[k];
+    rhs[i] = fi ? 0.0 : -rb;
+  }
+  // Cholesky A = L L^T in place; a non-positive pivot zeroes the step
+  bool ok = true;
+#pragma unroll
+  for (int k = 0; k < MAXA; ++k) {
+    double s2 = A[k * (k + 1) / 2 + k];
+#pragma unroll
+    for (int q = 0; q < k; ++q) s2 -= A[k * (k + 1) / 2 + q] * A[k * (k + 1) / 2 + q];
+    if (!(s2 > 0.0)) ok = false;
+    const double lkk = sqrt(ok ? s2 : 1.0);
+    const double inv = 1.0 / lkk;
+    A[k * (k + 1) / 2 + k] = lkk;
+#pragma unroll
+    for (int i = k + 1; i < MAXA; ++i) {
+      double tt = A[i * (i + 1) / 2 + k];
+#pragma unroll
+      for (int q = 0; q < k; ++q) tt -= A[i * (i + 1) / 2 + q] * A[k * (k + 1) / 2 + q];
+      A[i * (i + 1) / 2 + k] = tt * inv;
+    }
+  }
+  // forward / backward substitution
+#pragma unroll
+  for (int i = 0; i < MAXA; ++i) {
+    double s2 = rhs[i];
+#pragma unroll
+    for (int q = 0; q < i; ++q) s2 -= A[i * (i + 1) / 2 + q] * rhs[q];
+    rhs[i] = s2 / A[i * (i + 1) / 2 + i];
+  }
+#pragma unroll
+  for (int i = MAXA - 1; i >= 0; --i) {
+    double s2 = rhs[i];
+#pragma unroll
+    for (int q = i + 1; q < MAXA; ++q) s2 -= A[q * (q + 1) / 2 + i] * rhs[q];
+    rhs[i] = s2 / A[i * (i + 1) / 2 + i];
+  }
+  float dn2 = 0.f;
+#pragma unroll
+  for (int c = 0; c < MAXA; ++c) {
+    delta[c] = ok ? (float)rhs[c] / col_s[c] : 0.f;
+    dn2 += delta[c] * delta[c];
+  }
+  // trust region
+  float R;
+  if (max_p > 1e-2f || max_o > 0.6f) R = 0.38f;
+  else if (max_p > 1e-3f || max_o > 0.25f) R = 0.22f;
+  else if (max_p > 2e-4f || max_o > 0.08f) R = 0.12f;
+  else R = 0.05f;
+  const float dn = sqrtf(dn2);
+  if (dn > R) {
+    const float sc = R / (dn + 1e-18f);
+#pragma unroll
+    for (int c = 0; c < MAXA; ++c) delta[c] *= sc;
+  }
+
+  return fw2;
+}
+
 template <int MAXA, int MAXEE, int TPS>
 __global__ void __launch_bounds__(128, (MAXA <= 8 ? 4 : 2)) lm_kernel(LmArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   LmShared& sh = *reinterpret_cast<LmShared*>(smem_raw);
-  unsigned char* p = smem_raw + ((sizeof(LmShared) + 15) & ~size_t(15));
-  float4* rs4 = reinterpret_cast<float4*>(p); p += sizeof(float4) * a.n_rs;
-  float4* ws4 = reinterpret_cast<float4*>(p); p += sizeof(float4) * a.w.Ms;
-  int2* pairs = reinterpret_cast<int2*>(p); p += sizeof(int2) * ((a.n_self + 1) & ~1);
-  int* rsj = reinterpret_cast<int*>(p); p += sizeof(int) * ((a.n_rs + 3) & ~3);
-  int* rsk = reinterpret_cast<int*>(p); p += sizeof(int) * ((a.n_rs + 3) & ~3);  // input sphere -> grouped slot
-  float* wc = reinterpret_cast<float*>(p); p += sizeof(float) * a.w.Mc * 7;
-  float* wb = reinterpret_cast<float*>(p); p += sizeof(float) * a.w.Mb * 15;
-  float* wh = reinterpret_cast<float*>(p); p += sizeof(float) * a.w.Mh * 6;
-  p = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15));
-  float* slots = reinterpret_cast<float*>(p); p += sizeof(float) * a.m.n_joints * 7 * blockDim.x;
-  float* pos = reinterpret_cast<float*>(p);
+  const LmLayout L = lm_layout(a, TPS);
+  float4* rs4 = reinterpret_cast<float4*>(smem_raw + L.rs);
+  float4* ws4 = reinterpret_cast<float4*>(smem_raw + L.ws);
+  int2* pairs = reinterpret_cast<int2*>(smem_raw + L.pairs);
+  int2* gjoint = reinterpret_cast<int2*>(smem_raw + L.gjoint);
+  int* gstart = reinterpret_cast<int*>(smem_raw + L.gstart);
+  int* rsj = reinterpret_cast<int*>(smem_raw + L.rsj);
+  int* rsk = reinterpret_cast<int*>(smem_raw + L.rsk);
+  int* cell_start = reinterpret_cast<int*>(smem_raw + L.cells);
+  unsigned short* cell_obs = reinterpret_cast<unsigned short*>(smem_raw + L.cell_obs);
+  float* wc = reinterpret_cast<float*>(smem_raw + L.wc);
+  float* wb = reinterpret_cast<float*>(smem_raw + L.wb);
+  float* wh = reinterpret_cast<float*>(smem_raw + L.wh);
+  float* slots = reinterpret_cast<float*>(smem_raw + L.slots);
+  float* pos = reinterpret_cast<float*>(smem_raw + L.pos);  // [spb][PS]; staging scratch before use
+  int* scratch = reinterpret_cast<int*>(smem_raw + L.pos);
+  const int PS = lm_pos_stride(a.n_rs, a.m.n_joints);
 
   const int pb = blockIdx.y;  // problem
   load_joint_table(sh.jt, a.m);
@@ -270,20 +547,28 @@ __global__ void __launch_bounds__(128, (MAXA <= 8 ? 4 : 2)) lm_kernel(LmArgs a) 
     sh.hi[i] = real ? a.upper[i] : 0.f;
     sh.fixed[i] = real ? (a.fixed_mask[i] != 0) : 1;
   }
-  // Robot spheres grouped by joint (in topological order), invalid joint
-  // indices dropped (the reference skips them too, _ls_ik_cuda_kernel.cu:171),
-  // plus one bounding sphere per sphere-carrying joint.  Built by thread 0:
-  // a few dozen entries, once per block.
+  for (int i = tid; i < L.ms_pad; i += blockDim.x)
+    ws4[i] = (i < a.w.Ms) ? make_float4(a.w.spheres[4 * i], a.w.spheres[4 * i + 1], a.w.spheres[4 * i + 2],
+                                        a.w.spheres[4 * i + 3] + a.margin)
+                          : make_float4(1e18f, 1e18f, 1e18f, 0.f);  // padding: never within reach
+  for (int i = tid; i < a.w.Mc * 7; i += blockDim.x) wc[i] = a.w.capsules[i];
+  for (int i = tid; i < a.w.Mb * 15; i += blockDim.x) wb[i] = a.w.boxes[i];
+  for (int i = tid; i < a.w.Mh * 6; i += blockDim.x) wh[i] = a.w.halfspaces[i];
+
+  // Thread 0 (a few hundred serial steps, once per block): robot spheres
+  // grouped by joint in topological order (invalid joint indices dropped, as
+  // the reference skips them, _ls_ik_cuda_kernel.cu:171); one bounding sphere
+  // per sphere-carrying joint; self pairs remapped to grouped sphere slots
+  // and grouped by joint-slot pair; the obstacle-grid bounds.
   if (tid == 0) {
     const int nj = a.m.n_joints;
-    int cnt[PK_MAX_JOINTS];
+    int cnt[PK_MAX_JOINTS], slot_of[PK_MAX_JOINTS];
     for (int j = 0; j < nj; ++j) cnt[j] = 0;
     for (int k = 0; k < a.n_rs; ++k) {
       const int j = a.sphere_joint[k];
       if (j >= 0 && j < nj) cnt[sh.jt.sorted_of[j]]++;
     }
     int n_js = 0, total = 0;
-    int slot_of[PK_MAX_JOINTS];
     for (int js = 0; js < nj; ++js) {
       slot_of[js] = -1;
       if (cnt[js] == 0) continue;
@@ -305,8 +590,9 @@ __global__ void __launch_bounds__(128, (MAXA <= 8 ? 4 : 2)) lm_kernel(LmArgs a) 
       rsk[k] = at;
       rs4[at] = make_float4(a.spheres_local[4 * k], a.spheres_local[4 * k + 1], a.spheres_local[4 * k + 2],
                             a.spheres_local[4 * k + 3]);
-      rsj[at] = js;
+      rsj[at] = slot_of[js];
     }
+    float rmax = 0.f;
     for (int q = 0; q < n_js; ++q) {
       float lo[3] = {3e38f, 3e38f, 3e38f}, hi[3] = {-3e38f, -3e38f, -3e38f};
       for (int k = sh.jstart[q]; k < sh.jstart[q + 1]; ++k) {
@@ -319,24 +605,136 @@ __global__ void __launch_bounds__(128, (MAXA <= 8 ? 4 : 2)) lm_kernel(LmArgs a) 
         const float dx = rs4[k].x - cx, dy = rs4[k].y - cy, dz = rs4[k].z - cz;
         R = fmaxf(R, sqrtf(dx * dx + dy * dy + dz * dz) + rs4[k].w);
       }
-      // slack keeps the cull conservative under FP32 rounding
-      sh.jb[q] = make_float4(cx, cy, cz, R + 1e-5f + 1e-6f * fabsf(R));
+      // slack keeps the culls conservative under FP32 rounding
+      R = R + 1e-4f + 1e-5f * fabsf(R);
+      sh.jb[q] = make_float4(cx, cy, cz, R);
+      rmax = fmaxf(rmax, R);
     }
-    (void)slot_of;
+    // self pairs in grouped sphere slots, grouped by (joint slot, joint slot)
+    int n_groups = 0;
+    if (a.coll && a.n_self > 0 && n_js > 0) {
+      const int NK = n_js * n_js;
+      const bool by_key = NK <= L.scratch_ints;
+      int* kc = scratch;
+      if (by_key)
+        for (int i = 0; i < NK; ++i) kc[i] = 0;
+      int n_valid = 0;
+      for (int pass = 0; pass < 2; ++pass) {
+        for (int q = 0; q < a.n_self; ++q) {
+          int x = a.self_i[q], y = a.self_j[q];
+          if (x < 0 || y < 0 || x >= a.n_rs || y >= a.n_rs) continue;
+          x = rsk[x]; y = rsk[y];
+          if (x < 0 || y < 0) continue;
+          if (rsj[x] > rsj[y]) { const int tmp = x; x = y; y = tmp; }
+          const int key = by_key ? rsj[x] * n_js + rsj[y] : 0;
+          if (pass == 0) {
+            if (by_key) kc[key]++;
+            ++n_valid;
+          } else {
+            pairs[by_key ? kc[key]++ : n_valid++] = make_int2(x, y);
+          }
+        }
+        if (pass == 0) {
+          if (by_key) {
+            int run = 0;
+            for (int key = 0; key < NK; ++key) {
+              if (kc[key] == 0) continue;
+              gjoint[n_groups] = make_int2(key / n_js, key % n_js);
+              gstart[n_groups] = run;
+              const int c0 = kc[key];
+              kc[key] = run;
+              run += c0;
+              ++n_groups;
+            }
+            gstart[n_groups] = run;
+          } else if (n_valid > 0) {
+            // too many joint slots for the key table: one group that is never culled
+            gjoint[0] = make_int2(0, 0);
+            gstart[0] = 0;
+            gstart[1] = n_valid;
+            n_groups = 1;
+          }
+          n_valid = 0;
+        }
+      }
+    }
+    sh.n_groups = n_groups;
+    // obstacle-grid bounds: the union of every world sphere's ball of radius
+    // r + margin + (largest joint bounding radius), slightly inflated
+    sh.grid_on = 0;
+    if (L.grid && n_js > 0) {
+      float lo[3] = {3e38f, 3e38f, 3e38f}, hi[3] = {-3e38f, -3e38f, -3e38f};
+      for (int o = 0; o < a.w.Ms; ++o) {
+        const float4 O = ws4[o];
+        const float rho = O.w + rmax + 1e-3f;
+        lo[0] = fminf(lo[0], O.x - rho); hi[0] = fmaxf(hi[0], O.x + rho);
+        lo[1] = fminf(lo[1], O.y - rho); hi[1] = fmaxf(hi[1], O.y + rho);
+        lo[2] = fminf(lo[2], O.z - rho); hi[2] = fmaxf(hi[2], O.z + rho);
+      }
+      sh.glo = make_float3(lo[0], lo[1], lo[2]);
+      sh.ginv = make_float3(PK_LM_GRID / fmaxf(hi[0] - lo[0], 1e-6f), PK_LM_GRID / fmaxf(hi[1] - lo[1], 1e-6f),
+                            PK_LM_GRID / fmaxf(hi[2] - lo[2], 1e-6f));
+      sh.rmax = rmax;
+      sh.grid_on = 1;
+    }
   }
-  for (int i = tid; i < a.w.Ms; i += blockDim.x)
-    ws4[i] = make_float4(a.w.spheres[4 * i], a.w.spheres[4 * i + 1], a.w.spheres[4 * i + 2],
-                         a.w.spheres[4 * i + 3] + a.margin);
-  for (int i = tid; i < a.w.Mc * 7; i += blockDim.x) wc[i] = a.w.capsules[i];
-  for (int i = tid; i < a.w.Mb * 15; i += blockDim.x) wb[i] = a.w.boxes[i];
-  for (int i = tid; i < a.w.Mh * 6; i += blockDim.x) wh[i] = a.w.halfspaces[i];
   __syncthreads();
-  for (int i = tid; i < a.n_self; i += blockDim.x) {
-    const int x = a.self_i[i], y = a.self_j[i];
-    const bool ok = x >= 0 && y >= 0 && x < a.n_rs && y < a.n_rs && rsk[x] >= 0 && rsk[y] >= 0;
-    pairs[i] = ok ? make_int2(rsk[x], rsk[y]) : make_int2(-1, -1);
+
+  // Obstacle grid: PK_LM_GRID^3 cells over those bounds; obstacle o is listed
+  // in every cell its inflated ball's bounding box touches, in increasing o
+  // (each cell's list is built by one thread, so the order is deterministic).
+  if (sh.grid_on) {
+    constexpr int G = PK_LM_GRID, NC = G * G * G;
+    int* obox = scratch;
+    for (int o = tid; o < a.w.Ms; o += blockDim.x) {
+      const float4 O = ws4[o];
+      const float rho = O.w + sh.rmax + 1e-3f;
+      const float c3[3] = {O.x, O.y, O.z}, l3[3] = {sh.glo.x, sh.glo.y, sh.glo.z}, i3[3] = {sh.ginv.x, sh.ginv.y, sh.ginv.z};
+      int packed = 0;
+      for (int d = 0; d < 3; ++d) {
+        const int i0 = min(max(__float2int_rd((c3[d] - rho - l3[d]) * i3[d]), 0), G - 1);
+        const int i1 = min(max(__float2int_rd((c3[d] + rho - l3[d]) * i3[d]), 0), G - 1);
+        packed |= (i0 | (i1 << 4)) << (8 * d);
+      }
+      obox[o] = packed;
+    }
+    __syncthreads();
+    for (int cell = tid; cell < NC; cell += blockDim.x) {
+      const int ix = cell / (G * G), iy = (cell / G) % G, iz = cell % G;
+      int n = 0;
+      for (int o = 0; o < a.w.Ms; ++o) {
+        const int b = obox[o];
+        n += (ix >= (b & 15)) & (ix <= ((b >> 4) & 15)) & (iy >= ((b >> 8) & 15)) & (iy <= ((b >> 12) & 15)) &
+             (iz >= ((b >> 16) & 15)) & (iz <= ((b >> 20) & 15));
+      }
+      cell_start[cell] = n;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      int run = 0;
+      for (int cell = 0; cell < NC; ++cell) {
+        const int n = cell_start[cell];
+        cell_start[cell] = run;
+        run += n;
+      }
+      cell_start[NC] = run;
+      if (run > L.max_entries) sh.grid_on = 0;  // does not fit: scan all obstacles instead
+    }
+    __syncthreads();
+    if (sh.grid_on) {
+      for (int cell = tid; cell < NC; cell += blockDim.x) {
+        const int ix = cell / (G * G), iy = (cell / G) % G, iz = cell % G;
+        int at = cell_start[cell];
+        for (int o = 0; o < a.w.Ms; ++o) {
+          const int b = obox[o];
+          if ((ix >= (b & 15)) & (ix <= ((b >> 4) & 15)) & (iy >= ((b >> 8) & 15)) & (iy <= ((b >> 12) & 15)) &
+              (iz >= ((b >> 16) & 15)) & (iz <= ((b >> 20) & 15)))
+            cell_obs[at++] = (unsigned short)o;
+        }
+      }
+    }
+    __syncthreads();
   }
-  __syncthreads();
 
   const int g = tid / TPS, t = tid - g * TPS;
   const int lane = tid & 31;
@@ -346,13 +744,17 @@ __global__ void __launch_bounds__(128, (MAXA <= 8 ? 4 : 2)) lm_kernel(LmArgs a) 
   const size_t gs = (size_t)pb * a.Sd + s;
 
   const JointTable& jt = sh.jt;
-  const PoseSlots ps{slots + tid, (int)blockDim.x};
+  // one pose-slot set per seed (written by lane 0 of the group, read by all)
+  const PoseSlots ps{slots + g, a.spb};
+  const bool leader = (t == 0);
   const bool use_coll = a.coll && (sh.n_rs > 0);
   PenaltyCtx pc;
-  pc.rs = rs4; pc.rsj = rsj; pc.jb = sh.jb; pc.jstart = sh.jstart; pc.jlist = sh.jlist;
-  pc.ws = ws4; pc.wc = wc; pc.wb = wb; pc.wh = wh; pc.pairs = pairs;
-  pc.pos = pos; pc.n_rs = sh.n_rs; pc.n_js = sh.n_js; pc.Ms = a.w.Ms; pc.Mc = a.w.Mc; pc.Mb = a.w.Mb;
-  pc.Mh = a.w.Mh; pc.n_self = a.n_self; pc.spb = a.spb; pc.margin = a.margin;
+  pc.rs = rs4; pc.jb = sh.jb; pc.jstart = sh.jstart; pc.jlist = sh.jlist;
+  pc.ws = ws4; pc.wc = wc; pc.wb = wb; pc.wh = wh; pc.pairs = pairs; pc.gjoint = gjoint; pc.gstart = gstart;
+  pc.cell_start = sh.grid_on ? cell_start : nullptr; pc.cell_obs = cell_obs;
+  pc.pos = pos + (size_t)g * PS; pc.glo = sh.glo; pc.ginv = sh.ginv; pc.G = PK_LM_GRID;
+  pc.n_rs = sh.n_rs; pc.n_js = sh.n_js; pc.n_groups = sh.n_groups; pc.Ms_pad = L.ms_pad;
+  pc.Mc = a.w.Mc; pc.Mb = a.w.Mb; pc.Mh = a.w.Mh; pc.margin = a.margin;
 
   float W[6] = {a.pos_w, a.pos_w, a.pos_w, a.ori_w, a.ori_w, a.ori_w};
 
@@ -365,11 +767,15 @@ __global__ void __launch_bounds__(128, (MAXA <= 8 ? 4 : 2)) lm_kernel(LmArgs a) 
 
   auto penalty = [&]() -> float {
     if (!use_coll) return 0.f;
-    const float share = penalty_share<TPS>(pc, ps, t, g, gmask);
+    const float share = penalty_share<TPS>(pc, ps, t, gmask);
     return a.coll_w * group_sum<TPS>(share, gmask);
   };
+  // Every lane of the group computes the FK (same values); lane 0 stores it.
+  // The syncs keep lane 0 from overwriting poses another lane still reads.
   auto run_fk = [&](const float (&q)[MAXA]) {
-    fk_thread(jt, [&](int i) { return reg_get<MAXA>(q, i); }, ps);
+    __syncwarp(gmask);
+    fk_group(jt, [&](int i) { return reg_get<MAXA>(q, i); }, ps, leader, gmask);
+    __syncwarp(gmask);
   };
   auto weighted_sq = [&](const float (&r)[6 * MAXEE]) {
     float e = 0.f;
@@ -381,184 +787,62 @@ __global__ void __launch_bounds__(128, (MAXA <= 8 ? 4 : 2)) lm_kernel(LmArgs a) 
     return e;
   };
 
+  // Evaluation schedule: ev = -1 the initial point, then per iteration ev = 0
+  // (current point: residual, Jacobian, damped step) and ev = 1..5 (the
+  // line-search trials).  A single call site each for FK, residual and
+  // penalty keeps the kernel small enough for the instruction cache.
   float r[6 * MAXEE], pee[3 * MAXEE];
-  run_fk(cfg);
-  ee_residual<MAXEE>(sh, ps, a.n_ee, r, pee);
-  // penalty at the current configuration: the reference re-evaluates it at
-  // the top of every iteration; it only changes when a trial is accepted, and
-  // then equals that trial's penalty bit for bit (same configuration, same
-  // code), so it is carried instead of recomputed.
-  float pen_cur = penalty();
-  float best_err = weighted_sq(r) + pen_cur;
+  float delta[MAXA];
   float lam = a.lam0;
-
-  for (int it = 0; it < a.max_iter; ++it) {
-    run_fk(cfg);
+  float pen_cur = 0.f, best_err = 0.f, curr = 0.f;
+  float best_a_err = 1e30f, best_a_pen = 0.f;
+  int best_a = 0;
+  int it = 0, ev = -1;
+#pragma unroll
+  for (int c = 0; c < MAXA; ++c) delta[c] = 0.f;
+  while (true) {
+    float q[MAXA];
+#pragma unroll
+    for (int c = 0; c < MAXA; ++c)
+      q[c] = (ev <= 0) ? cfg[c] : fmaxf(sh.lo[c], fminf(sh.hi[c], cfg[c] + line_alpha(ev - 1) * delta[c]));
+    run_fk(q);
     ee_residual<MAXEE>(sh, ps, a.n_ee, r, pee);
-    bool all_conv = true;
-    float max_p = 0.f, max_o = 0.f;
-#pragma unroll
-    for (int e = 0; e < MAXEE; ++e) {
-      if (e < a.n_ee) {
-        const float np = sqrtf(r[6 * e] * r[6 * e] + r[6 * e + 1] * r[6 * e + 1] + r[6 * e + 2] * r[6 * e + 2]);
-        const float no = sqrtf(r[6 * e + 3] * r[6 * e + 3] + r[6 * e + 4] * r[6 * e + 4] + r[6 * e + 5] * r[6 * e + 5]);
-        if (np >= a.eps_pos || no >= a.eps_ori) all_conv = false;
-        max_p = fmaxf(max_p, np);
-        max_o = fmaxf(max_o, no);
-      }
-    }
-    if (all_conv) break;
 
-    // weighted stacked Jacobian J[k][c]
-    float J[6 * MAXEE][MAXA];
-#pragma unroll
-    for (int k = 0; k < 6 * MAXEE; ++k)
-#pragma unroll
-      for (int c = 0; c < MAXA; ++c) J[k][c] = 0.f;
-    for (int i = 0; i < jt.n; ++i) {
-      const int jk = jt.jkind[i];
-      const int a1 = jt.a1[i], a2 = jt.a2[i];
-      if (jk == 0 || (a1 < 0 && a2 < 0)) continue;
-      const Pose Tj = ps.load(i);
-      const float3 z = quat_rotate(Tj.w, Tj.x, Tj.y, Tj.z,
-                                   make_float3(jt.axis[i][0], jt.axis[i][1], jt.axis[i][2]));
-      const float sm = jt.mul[i];
-      const int orig = jt.orig[i];
+    if (ev == 0) {
+      bool all_conv = true;
+      float max_p = 0.f, max_o = 0.f;
 #pragma unroll
       for (int e = 0; e < MAXEE; ++e) {
-        if (e >= a.n_ee || !((sh.anc[e] >> orig) & 1ull)) continue;
-        float col[6];
-        if (jk == 1) {
-          const float ax = pee[3 * e] - Tj.tx, ay = pee[3 * e + 1] - Tj.ty, az = pee[3 * e + 2] - Tj.tz;
-          col[0] = z.y * az - z.z * ay; col[1] = z.z * ax - z.x * az; col[2] = z.x * ay - z.y * ax;
-          col[3] = z.x; col[4] = z.y; col[5] = z.z;
-        } else {
-          col[0] = z.x; col[1] = z.y; col[2] = z.z; col[3] = col[4] = col[5] = 0.f;
-        }
-#pragma unroll
-        for (int c = 0; c < MAXA; ++c) {
-          const float wsel = ((c == a1) ? sm : 0.f) + ((c == a2) ? sm : 0.f);
-#pragma unroll
-          for (int k = 0; k < 6; ++k) J[6 * e + k][c] += wsel * col[k];
+        if (e < a.n_ee) {
+          const float np = sqrtf(r[6 * e] * r[6 * e] + r[6 * e + 1] * r[6 * e + 1] + r[6 * e + 2] * r[6 * e + 2]);
+          const float no = sqrtf(r[6 * e + 3] * r[6 * e + 3] + r[6 * e + 4] * r[6 * e + 4] + r[6 * e + 5] * r[6 * e + 5]);
+          if (np >= a.eps_pos || no >= a.eps_ori) all_conv = false;
+          max_p = fmaxf(max_p, np);
+          max_o = fmaxf(max_o, no);
         }
       }
-    }
-    float fw[6 * MAXEE];
-#pragma unroll
-    for (int k = 0; k < 6 * MAXEE; ++k) {
-      fw[k] = r[k] * W[k % 6];
-#pragma unroll
-      for (int c = 0; c < MAXA; ++c) J[k][c] *= W[k % 6];
-    }
-    float curr = 0.f;
-#pragma unroll
-    for (int k = 0; k < 6 * MAXEE; ++k) curr += fw[k] * fw[k];
-    curr += pen_cur;
-
-    // Jacobi column scaling
-    float col_s[MAXA];
-#pragma unroll
-    for (int c = 0; c < MAXA; ++c) {
-      float sq = 0.f;
-#pragma unroll
-      for (int k = 0; k < 6 * MAXEE; ++k) sq += J[k][c] * J[k][c];
-      col_s[c] = sqrtf(sq) + 1e-8f;
-    }
-#pragma unroll
-    for (int k = 0; k < 6 * MAXEE; ++k)
-#pragma unroll
-      for (int c = 0; c < MAXA; ++c) J[k][c] = J[k][c] / col_s[c];
-
-    // FP64 normal equations (lower triangle, packed) + masking
-    double A[MAXA * (MAXA + 1) / 2];
-    double rhs[MAXA];
-#pragma unroll
-    for (int i = 0; i < MAXA; ++i) {
-      const bool fi = sh.fixed[i];
-#pragma unroll
-      for (int j = 0; j <= i; ++j) {
-        double acc = 0.0;
-#pragma unroll
-        for (int k = 0; k < 6 * MAXEE; ++k) acc += (double)J[k][i] * (double)J[k][j];
-        if (i == j) acc += (double)lam;
-        const bool fj = sh.fixed[j];
-        A[i * (i + 1) / 2 + j] = (fi || fj) ? ((i == j) ? 1.0 : 0.0) : acc;
-      }
-      double rb = 0.0;
-#pragma unroll
-      for (int k = 0; k < 6 * MAXEE; ++k) rb += (double)J[k][i] * (double)fw[k];
-      rhs[i] = fi ? 0.0 : -rb;
-    }
-    // Cholesky A = L L^T in place; a non-positive pivot zeroes the step
-    bool ok = true;
-#pragma unroll
-    for (int k = 0; k < MAXA; ++k) {
-      double s2 = A[k * (k + 1) / 2 + k];
-#pragma unroll
-      for (int q = 0; q < k; ++q) s2 -= A[k * (k + 1) / 2 + q] * A[k * (k + 1) / 2 + q];
-      if (!(s2 > 0.0)) ok = false;
-      const double lkk = sqrt(ok ? s2 : 1.0);
-      const double inv = 1.0 / lkk;
-      A[k * (k + 1) / 2 + k] = lkk;
-#pragma unroll
-      for (int i = k + 1; i < MAXA; ++i) {
-        double tt = A[i * (i + 1) / 2 + k];
-#pragma unroll
-        for (int q = 0; q < k; ++q) tt -= A[i * (i + 1) / 2 + q] * A[k * (k + 1) / 2 + q];
-        A[i * (i + 1) / 2 + k] = tt * inv;
-      }
-    }
-    // forward / backward substitution
-#pragma unroll
-    for (int i = 0; i < MAXA; ++i) {
-      double s2 = rhs[i];
-#pragma unroll
-      for (int q = 0; q < i; ++q) s2 -= A[i * (i + 1) / 2 + q] * rhs[q];
-      rhs[i] = s2 / A[i * (i + 1) / 2 + i];
-    }
-#pragma unroll
-    for (int i = MAXA - 1; i >= 0; --i) {
-      double s2 = rhs[i];
-#pragma unroll
-      for (int q = i + 1; q < MAXA; ++q) s2 -= A[q * (q + 1) / 2 + i] * rhs[q];
-      rhs[i] = s2 / A[i * (i + 1) / 2 + i];
-    }
-    float delta[MAXA];
-    float dn2 = 0.f;
-#pragma unroll
-    for (int c = 0; c < MAXA; ++c) {
-      delta[c] = ok ? (float)rhs[c] / col_s[c] : 0.f;
-      dn2 += delta[c] * delta[c];
-    }
-    // trust region
-    float R;
-    if (max_p > 1e-2f || max_o > 0.6f) R = 0.38f;
-    else if (max_p > 1e-3f || max_o > 0.25f) R = 0.22f;
-    else if (max_p > 2e-4f || max_o > 0.08f) R = 0.12f;
-    else R = 0.05f;
-    const float dn = sqrtf(dn2);
-    if (dn > R) {
-      const float sc = R / (dn + 1e-18f);
-#pragma unroll
-      for (int c = 0; c < MAXA; ++c) delta[c] *= sc;
+      if (all_conv) break;
+      curr = lm_direction<MAXA, MAXEE>(sh, ps, a.n_ee, W, r, pee, lam, max_p, max_o, delta) + pen_cur;
+      best_a_err = 1e30f;
+      best_a_pen = pen_cur;
+      best_a = 0;
+      ev = 1;
+      continue;
     }
 
-    // line search
-    float best_a_err = 1e30f;
-    float best_a_pen = pen_cur;
-    int best_a = 0;
-#pragma unroll 1
-    for (int ai = 0; ai < 5; ++ai) {
-      float trial[MAXA];
-#pragma unroll
-      for (int c = 0; c < MAXA; ++c) trial[c] = fmaxf(sh.lo[c], fminf(sh.hi[c], cfg[c] + line_alpha(ai) * delta[c]));
-      run_fk(trial);
-      float rt[6 * MAXEE], pt[3 * MAXEE];
-      ee_residual<MAXEE>(sh, ps, a.n_ee, rt, pt);
-      const float pt_pen = penalty();
-      const float et = weighted_sq(rt) + pt_pen;
-      if (et < best_a_err) { best_a_err = et; best_a = ai; best_a_pen = pt_pen; }
+    const float pen = penalty();
+    const float err = weighted_sq(r) + pen;
+    if (ev < 0) {
+      pen_cur = pen;
+      best_err = err;
+      if (a.max_iter <= 0) break;
+      ev = 0;
+      continue;
     }
+    if (err < best_a_err) { best_a_err = err; best_a = ev - 1; best_a_pen = pen; }
+    if (ev < 5) { ++ev; continue; }
+
+    // accept / reject the damped step, track the all-time best
     const float alpha = line_alpha(best_a);
     float trial[MAXA];
 #pragma unroll
@@ -576,6 +860,8 @@ __global__ void __launch_bounds__(128, (MAXA <= 8 ? 4 : 2)) lm_kernel(LmArgs a) 
 #pragma unroll
       for (int c = 0; c < MAXA; ++c) best[c] = trial[c];
     }
+    if (++it >= a.max_iter) break;
+    ev = 0;
   }
 
   if (t == 0) {
@@ -746,21 +1032,13 @@ __global__ void __launch_bounds__(128) verify_select_kernel(VerifyArgs a) {
 // host side
 // ---------------------------------------------------------------------------
 
-static size_t lm_smem_bytes(const LmArgs& a, int threads) {
-  size_t b = (sizeof(LmShared) + 15) & ~size_t(15);
-  b += sizeof(float4) * a.n_rs + sizeof(float4) * a.w.Ms + sizeof(int2) * ((a.n_self + 1) & ~1) +
-       2 * sizeof(int) * ((a.n_rs + 3) & ~3) + sizeof(float) * (a.w.Mc * 7 + a.w.Mb * 15 + a.w.Mh * 6);
-  b = (b + 15) & ~size_t(15);
-  b += sizeof(float) * (size_t)a.m.n_joints * 7 * threads;
-  if (a.coll) b += sizeof(float) * (size_t)a.n_rs * 3 * a.spb;
-  return b;
-}
+static size_t lm_smem_bytes(const LmArgs& a, int tps) { return lm_layout(a, tps).total; }
 
 template <int MAXA, int MAXEE, int TPS>
 static int launch_lm_t(const LmArgs& a0, cudaStream_t st) {
   LmArgs a = a0;
   const int threads = a.spb * TPS;
-  const size_t smem = lm_smem_bytes(a, threads);
+  const size_t smem = lm_smem_bytes(a, TPS);
   PK_CHECK_CAP(smem <= 220 * 1024, "LM working set (%zu B of shared memory) too large", smem);
   auto kern = lm_kernel<MAXA, MAXEE, TPS>;
   if (int s = set_smem_limit((const void*)kern, smem)) return s;
