@@ -104,6 +104,10 @@ __host__ __device__ __forceinline__ int lm_ms_pad(int Ms, int tps) {
 
 // Per-seed stride (floats) of the sphere position slots: odd, so the seeds
 // of a warp reading the same sphere hit distinct banks.
+// Trial-lane kernel: float4 positions per seed, padded by one float4 so the
+// 6 seeds of a warp reading the same sphere use different bank groups.
+__host__ __device__ __forceinline__ int lm_pos4_stride(int n_rs) { return n_rs + 1; }
+
 __host__ __device__ __forceinline__ int lm_pos_stride(int n_rs, int n_joints) {
   return (3 * n_rs + 3 * n_joints) | 1;  // sphere positions, then joint bounding centres
 }
@@ -113,24 +117,32 @@ __host__ __device__ __forceinline__ int lm_pos_stride(int n_rs, int n_joints) {
 
 // Byte offsets of the LM block's dynamic shared memory.
 struct LmLayout {
-  size_t rs, ws, pairs, gjoint, gstart, rsj, rsk, cells, cell_obs, wc, wb, wh, slots, pos, total;
+  size_t rs, ws, pairs, pair4, gjoint, gstart, rsj, rsk, cells, cell_obs, wc, wb, wh, slots, pos, scratch, total;
   int ms_pad, grid, max_entries, scratch_ints;
 };
 
 __host__ __device__ inline size_t lm_align16(size_t x) { return (x + 15) & ~size_t(15); }
 
-__host__ __device__ inline LmLayout lm_layout(const LmArgs& a, int tps) {
+// threads == 0: seed-group kernel (per-seed pose slots and positions);
+// threads > 0: trial-lane kernel (per-lane pose slots for `threads` lanes,
+// per-seed sphere positions).
+__host__ __device__ inline LmLayout lm_layout(const LmArgs& a, int tps, int threads = 0) {
   LmLayout L;
   size_t o = lm_align16(sizeof(LmShared));
   const int n_rs = a.n_rs, n_self = a.coll ? a.n_self : 0;
   L.ms_pad = lm_ms_pad(a.w.Ms, tps);
   const int PS = lm_pos_stride(n_rs, a.m.n_joints);
-  L.scratch_ints = a.coll ? PS * a.spb : 0;
+  if (threads == 0) {
+    L.scratch_ints = a.coll ? PS * a.spb : 0;
+  } else {
+    L.scratch_ints = 7 * a.m.n_joints * threads;  // the pose slots double as staging scratch
+  }
   L.grid = (a.coll && a.w.Ms >= 32 && a.w.Ms <= 65535 && a.w.Ms <= L.scratch_ints) ? 1 : 0;
   L.max_entries = L.grid ? min(max(48 * a.w.Ms, 1024), 16384) : 0;
   L.rs = o; o = lm_align16(o + 16 * (size_t)n_rs);
   L.ws = o; o = lm_align16(o + 16 * (size_t)L.ms_pad);
   L.pairs = o; o = lm_align16(o + 8 * (size_t)n_self);
+  L.pair4 = o; o = lm_align16(o + (threads > 0 ? 16 * (size_t)n_self : 0));
   L.gjoint = o; o = lm_align16(o + 8 * (size_t)(n_self + 1));
   L.gstart = o; o = lm_align16(o + 4 * (size_t)(n_self + 2));
   L.rsj = o; o = lm_align16(o + 4 * (size_t)n_rs);
@@ -140,8 +152,15 @@ __host__ __device__ inline LmLayout lm_layout(const LmArgs& a, int tps) {
   L.wc = o; o = lm_align16(o + 28 * (size_t)a.w.Mc);
   L.wb = o; o = lm_align16(o + 60 * (size_t)a.w.Mb);
   L.wh = o; o = lm_align16(o + 24 * (size_t)a.w.Mh);
-  L.slots = o; o = lm_align16(o + 28 * (size_t)a.m.n_joints * a.spb);
-  L.pos = o; o = lm_align16(o + 4 * (size_t)L.scratch_ints);
+  if (threads == 0) {
+    L.slots = o; o = lm_align16(o + 28 * (size_t)a.m.n_joints * a.spb);
+    L.pos = o; o = lm_align16(o + 4 * (size_t)L.scratch_ints);
+    L.scratch = L.pos;
+  } else {
+    L.slots = o; o = lm_align16(o + 28 * (size_t)a.m.n_joints * threads);
+    L.pos = o; o = lm_align16(o + 16 * (size_t)lm_pos4_stride(n_rs) * a.spb);
+    L.scratch = L.slots;
+  }
   L.total = o;
   return L;
 }
@@ -507,11 +526,13 @@ __device__ __forceinline__ float lm_direction(const LmShared& sh, const PoseSlot
   return fw2;
 }
 
-template <int MAXA, int MAXEE, int TPS>
-__global__ void __launch_bounds__(128, (MAXA <= 8 ? 4 : 2)) lm_kernel(LmArgs a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+// Block prologue shared by both LM kernels: robot description, targets of
+// problem blockIdx.y, limits, world, grouped robot spheres and joint bounding
+// spheres, grouped self pairs and the obstacle grid, all in shared memory.
+// Ends with __syncthreads().
+template <int MAXA>
+__device__ void lm_stage(const LmArgs& a, unsigned char* smem_raw, const LmLayout& L) {
   LmShared& sh = *reinterpret_cast<LmShared*>(smem_raw);
-  const LmLayout L = lm_layout(a, TPS);
   float4* rs4 = reinterpret_cast<float4*>(smem_raw + L.rs);
   float4* ws4 = reinterpret_cast<float4*>(smem_raw + L.ws);
   int2* pairs = reinterpret_cast<int2*>(smem_raw + L.pairs);
@@ -524,10 +545,7 @@ __global__ void __launch_bounds__(128, (MAXA <= 8 ? 4 : 2)) lm_kernel(LmArgs a) 
   float* wc = reinterpret_cast<float*>(smem_raw + L.wc);
   float* wb = reinterpret_cast<float*>(smem_raw + L.wb);
   float* wh = reinterpret_cast<float*>(smem_raw + L.wh);
-  float* slots = reinterpret_cast<float*>(smem_raw + L.slots);
-  float* pos = reinterpret_cast<float*>(smem_raw + L.pos);  // [spb][PS]; staging scratch before use
-  int* scratch = reinterpret_cast<int*>(smem_raw + L.pos);
-  const int PS = lm_pos_stride(a.n_rs, a.m.n_joints);
+  int* scratch = reinterpret_cast<int*>(smem_raw + L.scratch);  // reused by the kernel after staging
 
   const int pb = blockIdx.y;  // problem
   load_joint_table(sh.jt, a.m);
@@ -736,6 +754,29 @@ __global__ void __launch_bounds__(128, (MAXA <= 8 ? 4 : 2)) lm_kernel(LmArgs a) 
     __syncthreads();
   }
 
+}
+
+template <int MAXA, int MAXEE, int TPS>
+__global__ void __launch_bounds__(128, (MAXA <= 8 ? 4 : 2)) lm_kernel(LmArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const LmLayout L = lm_layout(a, TPS);
+  lm_stage<MAXA>(a, smem_raw, L);
+  LmShared& sh = *reinterpret_cast<LmShared*>(smem_raw);
+  float4* rs4 = reinterpret_cast<float4*>(smem_raw + L.rs);
+  float4* ws4 = reinterpret_cast<float4*>(smem_raw + L.ws);
+  int2* pairs = reinterpret_cast<int2*>(smem_raw + L.pairs);
+  int2* gjoint = reinterpret_cast<int2*>(smem_raw + L.gjoint);
+  int* gstart = reinterpret_cast<int*>(smem_raw + L.gstart);
+  int* cell_start = reinterpret_cast<int*>(smem_raw + L.cells);
+  unsigned short* cell_obs = reinterpret_cast<unsigned short*>(smem_raw + L.cell_obs);
+  float* wc = reinterpret_cast<float*>(smem_raw + L.wc);
+  float* wb = reinterpret_cast<float*>(smem_raw + L.wb);
+  float* wh = reinterpret_cast<float*>(smem_raw + L.wh);
+  float* slots = reinterpret_cast<float*>(smem_raw + L.slots);
+  float* pos = reinterpret_cast<float*>(smem_raw + L.pos);
+  const int PS = lm_pos_stride(a.n_rs, a.m.n_joints);
+  const int tid = threadIdx.x;
+  const int pb = blockIdx.y;
   const int g = tid / TPS, t = tid - g * TPS;
   const int lane = tid & 31;
   const unsigned gmask = (TPS == 32) ? 0xffffffffu : (((1u << TPS) - 1u) << (lane & ~(TPS - 1)));
@@ -864,6 +905,284 @@ __global__ void __launch_bounds__(128, (MAXA <= 8 ? 4 : 2)) lm_kernel(LmArgs a) 
     ev = 0;
   }
 
+  if (t == 0) {
+#pragma unroll
+    for (int c = 0; c < MAXA; ++c)
+      if (c < a.n_act) a.out_cfg[gs * a.n_act + c] = best[c];
+    a.out_err[gs] = best_err;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Trial-lane LM kernel: a group of 5 lanes owns one seed; per iteration all 5
+// compute the current point's residual, Jacobian and damped step (identical
+// values), lane t computes the FK and residual of line-search trial t, then
+// the 5 lanes evaluate the collision penalty of each trial together and the
+// 5 errors meet by shuffle.  FK, the step computation and the penalty all
+// run with one instruction stream per warp of 6 seeds.
+// ---------------------------------------------------------------------------
+
+// Cooperative penalty of one configuration by the 5 lanes of a seed group.
+// Work items are striped over the lanes (lane t takes items t, t+5, ...):
+// sphere transforms into the seed's float4 position buffer (x, y, z, r),
+// then per-joint grid queries (bounding-sphere cull, exact tests of the
+// joint's spheres against the surviving obstacles), capsule / box /
+// halfspace tests and the self pairs (pre-resolved to byte offsets into the
+// position buffer and r_a + r_b + margin).  Every lane runs the same loops,
+// so a warp (6 seeds) does not diverge on the culling outcome of one seed.
+// Returns lane t's partial sum.
+struct CoopCtx {
+  const float4* rs;      // robot spheres grouped by joint slot (joint frame)
+  const float4* jb;      // bounding sphere per joint slot
+  const int* jstart;
+  const int* jlist;
+  const float4* ws;      // world spheres (x, y, z, r + margin)
+  const float* wc;
+  const float* wb;
+  const float* wh;
+  const int4* pair4;     // self pairs: (byte offset a, byte offset b, rr bits, 0)
+  int n_pairs;
+  const int* cell_start; // null: scan every obstacle
+  const unsigned short* cell_obs;
+  float4* pos;           // this seed's sphere world positions and radii [n_rs]
+  float3 glo, ginv;
+  int n_rs, n_js, Ms, Mc, Mb, Mh;
+  float margin;
+};
+
+__device__ float coop_penalty(const CoopCtx& c, const PoseSlots& psk, int t, unsigned gmask) {
+  constexpr int GL = 5;
+  float part = 0.f;
+  float4* const px = c.pos;
+  for (int j = 0; j < c.n_js; ++j) {
+    const int k0 = c.jstart[j], k1 = c.jstart[j + 1];
+    int k = k0 + ((t - k0) % GL + GL) % GL;  // first grouped sphere of this joint with k % 5 == t
+    if (k >= k1) continue;
+    const Pose T = psk.load(c.jlist[j]);
+    for (; k < k1; k += GL) {
+      const float4 s = c.rs[k];
+      const float3 w = pose_apply(T, make_float3(s.x, s.y, s.z));
+      px[k] = make_float4(w.x, w.y, w.z, s.w);
+    }
+  }
+  __syncwarp(gmask);
+
+  for (int j = t; j < c.n_js && c.Ms > 0; j += GL) {
+    const float4 bl = c.jb[j];
+    const float3 B = pose_apply(psk.load(c.jlist[j]), make_float3(bl.x, bl.y, bl.z));
+    int e0 = 0, e1 = c.Ms;
+    const unsigned short* list = nullptr;
+    if (c.cell_start) {
+      const int ix = __float2int_rd((B.x - c.glo.x) * c.ginv.x);
+      const int iy = __float2int_rd((B.y - c.glo.y) * c.ginv.y);
+      const int iz = __float2int_rd((B.z - c.glo.z) * c.ginv.z);
+      if ((unsigned)ix >= PK_LM_GRID || (unsigned)iy >= PK_LM_GRID || (unsigned)iz >= PK_LM_GRID) continue;
+      const int cell = (ix * PK_LM_GRID + iy) * PK_LM_GRID + iz;
+      e0 = c.cell_start[cell];
+      e1 = c.cell_start[cell + 1];
+      list = c.cell_obs;
+    }
+    const int k0 = c.jstart[j], k1 = c.jstart[j + 1];
+    for (int e = e0; e < e1; ++e) {
+      const float4 O = c.ws[list ? (int)list[e] : e];
+      const float rr = bl.w + O.w;
+      const float dx = B.x - O.x, dy = B.y - O.y, dz = B.z - O.z;
+      if (dx * dx + dy * dy + dz * dz < rr * fabsf(rr)) {
+        for (int k = k0; k < k1; ++k) {
+          const float4 P = px[k];
+          const float ex = P.x - O.x, ey = P.y - O.y, ez = P.z - O.z;
+          hinge_sq(ex * ex + ey * ey + ez * ez, P.w + O.w, part);
+        }
+      }
+    }
+  }
+
+  if (c.Mc + c.Mb + c.Mh > 0) {
+    for (int k = t; k < c.n_rs; k += GL) {
+      const float4 P = px[k];
+      const float3 p = make_float3(P.x, P.y, P.z);
+      for (int m = 0; m < c.Mc; ++m) {
+        const float d = d_sphere_capsule(p, P.w, c.wc + 7 * m);
+        if (d < c.margin) { const float e = d - c.margin; part += e * e; }
+      }
+      for (int m = 0; m < c.Mb; ++m) {
+        const float d = d_sphere_box(p, P.w, c.wb + 15 * m);
+        if (d < c.margin) { const float e = d - c.margin; part += e * e; }
+      }
+      for (int m = 0; m < c.Mh; ++m) {
+        const float d = d_sphere_halfspace(p, P.w, c.wh + 6 * m);
+        if (d < c.margin) { const float e = d - c.margin; part += e * e; }
+      }
+    }
+  }
+
+  const char* const pbytes = reinterpret_cast<const char*>(px);
+#pragma unroll 4
+  for (int q = t; q < c.n_pairs; q += GL) {
+    const int4 pr = c.pair4[q];
+    const float4 A = *reinterpret_cast<const float4*>(pbytes + pr.x);
+    const float4 Bq = *reinterpret_cast<const float4*>(pbytes + pr.y);
+    const float dx = A.x - Bq.x, dy = A.y - Bq.y, dz = A.z - Bq.z;
+    hinge_sq(dx * dx + dy * dy + dz * dz, __int_as_float(pr.z), part);
+  }
+  __syncwarp(gmask);
+  return part;
+}
+
+// Sum of the group's 5 partial sums in lane order (the same value, bit for
+// bit, on every lane of the group).
+__device__ __forceinline__ float group5_sum(float v, unsigned gmask, int base) {
+  float s = 0.f;
+#pragma unroll
+  for (int k = 0; k < 5; ++k) s += __shfl_sync(gmask, v, base + k);
+  return s;
+}
+
+template <int MAXA, int MAXEE>
+__global__ void __launch_bounds__(128, 4) lm_trial_kernel(LmArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const LmLayout L = lm_layout(a, 1, blockDim.x);
+  lm_stage<MAXA>(a, smem_raw, L);
+  LmShared& sh = *reinterpret_cast<LmShared*>(smem_raw);
+  const int tid = threadIdx.x;
+  const int pb = blockIdx.y;
+  {
+    // self pairs as byte offsets into a seed's float4 position buffer plus
+    // r_a + r_b + margin, so a pair test is three shared loads and a compare
+    const int2* pairs = reinterpret_cast<const int2*>(smem_raw + L.pairs);
+    const float4* rs4 = reinterpret_cast<const float4*>(smem_raw + L.rs);
+    int4* pair4 = reinterpret_cast<int4*>(smem_raw + L.pair4);
+    const int np = sh.n_groups > 0 ? reinterpret_cast<const int*>(smem_raw + L.gstart)[sh.n_groups] : 0;
+    for (int q = tid; q < np; q += blockDim.x) {
+      const int2 pr = pairs[q];
+      pair4[q] = make_int4(16 * pr.x, 16 * pr.y, __float_as_int(rs4[pr.x].w + rs4[pr.y].w + a.margin), 0);
+    }
+    __syncthreads();
+  }
+  const int lane = tid & 31, wid = tid >> 5;
+  const int gw = lane / 5, t = lane - 5 * gw;
+  if (gw >= 6) return;  // lanes 30, 31
+  const int s = blockIdx.x * a.spb + wid * 6 + gw;
+  if (s >= a.Sd) return;
+  const size_t gs = (size_t)pb * a.Sd + s;
+  const unsigned gmask = 0x1Fu << (5 * gw);
+  const int base = 5 * gw;
+
+  CoopCtx cc;
+  cc.rs = reinterpret_cast<const float4*>(smem_raw + L.rs);
+  cc.jb = sh.jb; cc.jstart = sh.jstart; cc.jlist = sh.jlist;
+  cc.ws = reinterpret_cast<const float4*>(smem_raw + L.ws);
+  cc.wc = reinterpret_cast<const float*>(smem_raw + L.wc);
+  cc.wb = reinterpret_cast<const float*>(smem_raw + L.wb);
+  cc.wh = reinterpret_cast<const float*>(smem_raw + L.wh);
+  cc.pair4 = reinterpret_cast<const int4*>(smem_raw + L.pair4);
+  cc.n_pairs = sh.n_groups > 0 ? reinterpret_cast<const int*>(smem_raw + L.gstart)[sh.n_groups] : 0;
+  cc.cell_start = sh.grid_on ? reinterpret_cast<const int*>(smem_raw + L.cells) : nullptr;
+  cc.cell_obs = reinterpret_cast<const unsigned short*>(smem_raw + L.cell_obs);
+  cc.pos = reinterpret_cast<float4*>(smem_raw + L.pos) + (size_t)(wid * 6 + gw) * lm_pos4_stride(a.n_rs);
+  cc.glo = sh.glo; cc.ginv = sh.ginv;
+  cc.n_rs = sh.n_rs; cc.n_js = sh.n_js; cc.Ms = a.w.Ms;
+  cc.Mc = a.w.Mc; cc.Mb = a.w.Mb; cc.Mh = a.w.Mh; cc.margin = a.margin;
+  const bool use_coll = a.coll && (sh.n_rs > 0);
+
+  const JointTable& jt = sh.jt;
+  const PoseSlots ps{reinterpret_cast<float*>(smem_raw + L.slots) + tid, (int)blockDim.x};
+  float W[6] = {a.pos_w, a.pos_w, a.pos_w, a.ori_w, a.ori_w, a.ori_w};
+  float cfg[MAXA], best[MAXA], delta[MAXA];
+#pragma unroll
+  for (int i = 0; i < MAXA; ++i) {
+    cfg[i] = (i < a.n_act) ? a.seeds[gs * a.n_act + i] : 0.f;
+    best[i] = cfg[i];
+    delta[i] = 0.f;
+  }
+  auto run_fk = [&](const float (&q)[MAXA]) { fk_thread(jt, [&](int i) { return reg_get<MAXA>(q, i); }, ps); };
+  auto weighted_sq = [&](const float (&r)[6 * MAXEE]) {
+    float e = 0.f;
+#pragma unroll
+    for (int k = 0; k < 6 * MAXEE; ++k) {
+      const float rw = r[k] * W[k % 6];
+      e += rw * rw;
+    }
+    return e;
+  };
+
+  float r[6 * MAXEE], pee[3 * MAXEE];
+  // ev = -1: the initial point; ev = 0: current point (step); ev = 1: this lane's trial
+  float lam = a.lam0, pen_cur = 0.f, best_err = 0.f, curr = 0.f;
+  int it = 0, ev = -1;
+  while (true) {
+    float q[MAXA];
+#pragma unroll
+    for (int c = 0; c < MAXA; ++c)
+      q[c] = (ev <= 0) ? cfg[c] : fmaxf(sh.lo[c], fminf(sh.hi[c], cfg[c] + line_alpha(t) * delta[c]));
+    run_fk(q);
+    ee_residual<MAXEE>(sh, ps, a.n_ee, r, pee);
+    if (ev == 0) {
+      bool all_conv = true;
+      float max_p = 0.f, max_o = 0.f;
+#pragma unroll
+      for (int e = 0; e < MAXEE; ++e) {
+        if (e < a.n_ee) {
+          const float np = sqrtf(r[6 * e] * r[6 * e] + r[6 * e + 1] * r[6 * e + 1] + r[6 * e + 2] * r[6 * e + 2]);
+          const float no = sqrtf(r[6 * e + 3] * r[6 * e + 3] + r[6 * e + 4] * r[6 * e + 4] + r[6 * e + 5] * r[6 * e + 5]);
+          if (np >= a.eps_pos || no >= a.eps_ori) all_conv = false;
+          max_p = fmaxf(max_p, np);
+          max_o = fmaxf(max_o, no);
+        }
+      }
+      if (all_conv) break;
+      curr = lm_direction<MAXA, MAXEE>(sh, ps, a.n_ee, W, r, pee, lam, max_p, max_o, delta) + pen_cur;
+      ev = 1;
+      continue;
+    }
+    // penalty of every trial (lane k's poses), the 5 lanes together
+    __syncwarp(gmask);
+    float pen = 0.f;
+    if (use_coll) {
+      float* const slot_base = reinterpret_cast<float*>(smem_raw + L.slots) + (tid - t);
+      for (int k = 0; k < (ev < 0 ? 1 : 5); ++k) {
+        const PoseSlots psk{slot_base + k, (int)blockDim.x};
+        const float pk = a.coll_w * group5_sum(coop_penalty(cc, psk, t, gmask), gmask, base);
+        if (k == t || ev < 0) pen = pk;
+      }
+    }
+    const float err = weighted_sq(r) + pen;
+    if (ev < 0) {
+      pen_cur = pen;
+      best_err = err;
+      if (a.max_iter <= 0) break;
+      ev = 0;
+      continue;
+    }
+    // the 5 trial errors meet; the first minimum wins (_ls_ik_cuda_kernel.cu:361-366)
+    float best_a_err = 1e30f, best_a_pen = pen_cur;
+    int best_a = 0;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      const float ek = __shfl_sync(gmask, err, base + k);
+      const float pk = __shfl_sync(gmask, pen, base + k);
+      if (ek < best_a_err) { best_a_err = ek; best_a = k; best_a_pen = pk; }
+    }
+    const float alpha = line_alpha(best_a);
+    float trial[MAXA];
+#pragma unroll
+    for (int c = 0; c < MAXA; ++c) trial[c] = fmaxf(sh.lo[c], fminf(sh.hi[c], cfg[c] + alpha * delta[c]));
+    if (best_a_err < curr * (1.0f - 1e-4f)) {
+#pragma unroll
+      for (int c = 0; c < MAXA; ++c) cfg[c] = trial[c];
+      pen_cur = best_a_pen;
+      lam = fmaxf(lam * a.lam_down, 1e-10f);
+    } else {
+      lam = fminf(lam * a.lam_up, 1e6f);
+    }
+    if (best_a_err < best_err) {
+      best_err = best_a_err;
+#pragma unroll
+      for (int c = 0; c < MAXA; ++c) best[c] = trial[c];
+    }
+    if (++it >= a.max_iter) break;
+    ev = 0;
+  }
   if (t == 0) {
 #pragma unroll
     for (int c = 0; c < MAXA; ++c)
@@ -1057,9 +1376,30 @@ static int launch_lm_tps(const LmArgs& a, int tps, cudaStream_t st) {
   }
 }
 
+template <int MAXA, int MAXEE>
+static int launch_lm_trial(LmArgs a, cudaStream_t st) {
+  const int threads = 128;
+  a.spb = 6 * (threads / 32);  // 6 groups of 5 lanes per warp
+  const size_t smem = lm_layout(a, 1, threads).total;
+  PK_CHECK_CAP(smem <= 220 * 1024, "LM working set (%zu B of shared memory) too large", smem);
+  auto kern = lm_trial_kernel<MAXA, MAXEE>;
+  if (int s = set_smem_limit((const void*)kern, smem)) return s;
+  dim3 grid((a.Sd + a.spb - 1) / a.spb, a.P);
+  kern<<<grid, threads, smem, st>>>(a);
+  return cuda_status(cudaGetLastError(), "lm_trial_kernel launch");
+}
+
 static int launch_lm(LmArgs a, int tps, int spb, cudaStream_t st) {
-  if (tps <= 0) tps = (a.coll && a.n_rs > 0) ? 4 : 1;
-  PK_CHECK_ARG(tps == 1 || tps == 2 || tps == 4 || tps == 8, "threads_per_seed must be 1, 2, 4 or 8");
+  // threads_per_seed 0 or 5: the trial-lane kernel (5 lanes per seed, one
+  // line-search trial each); 1, 2, 4, 8: the seed-group kernel with the
+  // collision penalty split across that many lanes.
+  if (tps <= 0 || tps == 5) {
+    if (a.n_act <= 8 && a.n_ee <= 1) return launch_lm_trial<8, 1>(a, st);
+    if (a.n_act <= 16 && a.n_ee <= 2) return launch_lm_trial<16, 2>(a, st);
+    set_error("the LM kernel supports n_act <= 16 with n_ee <= 2 (got n_act=%d, n_ee=%d)", a.n_act, a.n_ee);
+    return PK_ERR_CAPACITY;
+  }
+  PK_CHECK_ARG(tps == 1 || tps == 2 || tps == 4 || tps == 8, "threads_per_seed must be 0, 1, 2, 4, 5 or 8");
   if (spb <= 0) spb = 128 / tps;
   PK_CHECK_ARG(spb * tps <= 128 && (spb * tps) % 32 == 0,
                "seeds_per_block * threads_per_seed must be a multiple of 32 and at most 128");

@@ -53,7 +53,7 @@ def oracle_run(w, p, max_iter, seeds=None, lam_down=None, lam_up=None, self_pair
                      self_j=w.self_pairs[:, 1] if self_pairs else None)
 
 
-@pytest.mark.parametrize("tps", [1, 2, 4, 8])
+@pytest.mark.parametrize("tps", [0, 1, 2, 4, 5, 8])
 @pytest.mark.parametrize("max_iter", [0, 1, 2])
 def test_lm_few_iterations_seed_by_seed(tps, max_iter):
     w = small_ik(P=3, Sd=40)
