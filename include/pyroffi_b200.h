@@ -206,6 +206,41 @@ int pk_fk_sphere_collision(void* stream, const float* cfg, const float* twists,
                            int32_t n_act, int32_t n_joints, int32_t n_links, int32_t S, int32_t Ms,
                            int32_t Mc, int32_t Mb, int32_t Mh);
 
+/* Weights of the trajectory cost (no reference counterpart; the defaults of
+ * ChompTrajOptConfig, src/pyroffi/optimization_engines/_chomp_optimization.py:31-91,
+ * are margin 0.01, w_smooth 1, w_acc 0.5, w_jerk 0.1, w_limits 1, w_coll 3). */
+typedef struct pk_traj_options {
+  float margin;
+  float w_smooth;
+  float w_acc;
+  float w_jerk;
+  float w_limits;
+  float w_coll;
+} pk_traj_options;
+
+/*
+ * CHOMP trajectory cost and its gradient (hand-written adjoint; no
+ * reference counterpart -- it replaces jax.value_and_grad of cost_fn,
+ * _chomp_optimization.py:243-263, and the finite-difference gradients of
+ * _chomp_trajopt_cuda_kernel.cu:719-784).  traj[B, T, n_act]; robot
+ * spheres per link in link frames link_spheres[N, S, 4] (r < 0 padding),
+ * parent_joint_indices[N]; active self link pairs (pair_i, pair_j)[P];
+ * world obstacles as elsewhere; lower/upper[n_act].  Outputs (each may be
+ * NULL, not all): cost[B]; grad[B, T, n_act] = dJ/dtraj (the collision
+ * part recomputes the link poses, nothing is kept from a forward call);
+ * wp_coll[B, T] the unweighted collision hinge per waypoint.
+ */
+int pk_traj_cost_grad(void* stream, const pk_traj_options* opt, const float* traj, const float* twists,
+                      const float* parent_tf, const int32_t* parent_idx, const int32_t* act_idx,
+                      const float* mimic_mul, const float* mimic_off, const int32_t* mimic_act_idx,
+                      const int32_t* topo_inv, const int32_t* parent_joint_indices,
+                      const float* link_spheres, const int32_t* pair_i, const int32_t* pair_j,
+                      const float* world_spheres, const float* world_capsules, const float* world_boxes,
+                      const float* world_halfspaces, const float* lower, const float* upper, float* cost,
+                      float* grad, float* wp_coll, int64_t B, int32_t T, int32_t n_act, int32_t n_joints,
+                      int32_t n_links, int32_t S, int32_t P, int32_t Ms, int32_t Mc, int32_t Mb,
+                      int32_t Mh);
+
 /*
  * FP32 FMA-pipe microbenchmark (no reference counterpart): `blocks` blocks of
  * 256 threads, each thread 8 independent FMA chains of `iters` steps, i.e.

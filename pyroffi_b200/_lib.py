@@ -62,7 +62,15 @@ SIGNATURES: dict[str, list] = {
     "pk_ik_verify_select": [_p] * 4 + [_f32] + [_p] * 10 + [_f32, _f32] + [_p] * 4 + [_i32] * 5,
     "pk_fk_sphere_collision": [_p] * 19 + [_i64] + [_i32] * 8,
     "pk_fp32_fma_peak": [_p, _p, _i32, _i32],
+    "pk_traj_cost_grad": [_p, C.c_void_p] + [_p] * 22 + [_i64] + [_i32] * 10,
 }
+
+
+class TrajOptions(C.Structure):
+    """``pk_traj_options`` of the C-ABI."""
+
+    _fields_ = [("margin", _f32), ("w_smooth", _f32), ("w_acc", _f32), ("w_jerk", _f32),
+                ("w_limits", _f32), ("w_coll", _f32)]
 
 _lock = threading.Lock()
 _lib: C.CDLL | None = None
