@@ -193,7 +193,9 @@ int pk_ik_verify_select(void* stream, const float* cfgs, const float* errs, cons
  *   min_dist[B]          min over all spheres and obstacles (1e9 if none),
  *   link_poses[B, N, 7]  link poses,
  *   dist_bkm[B, K, M]    per-sphere distances with K = S*N, k = s*N + n, in
- *                        the layout of pk_collision_world_sphere.
+ *                        the layout of pk_collision_world_sphere,
+ *   dist_bnm[B, N, M]    per-link minimum over the link's spheres, in the
+ *                        layout of pk_collision_world_sphere_reduced.
  */
 int pk_fk_sphere_collision(void* stream, const float* cfg, const float* twists,
                            const float* parent_tf, const int32_t* parent_idx,
@@ -202,7 +204,8 @@ int pk_fk_sphere_collision(void* stream, const float* cfg, const float* twists,
                            const int32_t* parent_joint_indices, const float* link_spheres,
                            const float* world_spheres, const float* world_capsules,
                            const float* world_boxes, const float* world_halfspaces,
-                           float* min_dist, float* link_poses, float* dist_bkm, int64_t batch,
+                           float* min_dist, float* link_poses, float* dist_bkm, float* dist_bnm,
+                           int64_t batch,
                            int32_t n_act, int32_t n_joints, int32_t n_links, int32_t S, int32_t Ms,
                            int32_t Mc, int32_t Mb, int32_t Mh);
 

@@ -62,6 +62,7 @@ struct FusedArgs {
   float* min_dist;          // [B] or null
   float* link_poses;        // [B, N, 7] or null
   float* dist_bkm;          // [B, K, M] or null
+  float* dist_bnm;          // [B, N, M] or null (min over each link's spheres)
   long long batch;
   int N, S;
   int cpb;                  // configurations per block
@@ -138,7 +139,9 @@ __global__ void __launch_bounds__(256) fk_sphere_collision_kernel(FusedArgs a) {
   const int warp = tid >> 5, lane = tid & 31, nwarps = T >> 5;
   const bool vec4 = a.dist_bkm && ((M & 3) == 0) &&
                     ((reinterpret_cast<uintptr_t>(a.dist_bkm) & 15) == 0);
-  for (int c = 0; c < nc; ++c) {
+  // (with only the per-link output requested, its pass below also gives the minimum)
+  const bool sphere_pass = a.dist_bkm || !a.dist_bnm;
+  for (int c = 0; c < nc && sphere_pass; ++c) {
     float vmin = 1e9f;
     float* orow_base = a.dist_bkm ? a.dist_bkm + (b0 + c) * (long long)K * M : nullptr;
     for (int k = warp; k < K; k += nwarps) {
@@ -168,6 +171,28 @@ __global__ void __launch_bounds__(256) fk_sphere_collision_kernel(FusedArgs a) {
     }
     vmin = warp_min(vmin);
     if (lane == 0) atomicMin(&cmin[c], float_to_ordered(vmin));
+  }
+  // per-link rows [B, N, M]: min over the link's spheres, padding skipped
+  if (a.dist_bnm) {
+    for (int row = warp; row < nc * N; row += nwarps) {
+      const int c = row / N, nl = row - c * N;
+      float* orow = a.dist_bnm + ((b0 + c) * (long long)N + nl) * M;
+      float vmin = 1e9f;
+      for (int m0 = lane; m0 < M; m0 += 32) {
+        float d = 1e9f;
+        for (int s = 0; s < S; ++s) {
+          const float4 ce = centres[c * K + s * N + nl];
+          if (ce.w < 0.f) continue;
+          d = fminf(d, obstacle_dist(ob, m0, make_float3(ce.x, ce.y, ce.z), ce.w));
+        }
+        orow[m0] = d;
+        vmin = fminf(vmin, d);
+      }
+      if (!sphere_pass) {
+        vmin = warp_min(vmin);
+        if (lane == 0) atomicMin(&cmin[c], float_to_ordered(vmin));
+      }
+    }
   }
   __syncthreads();
   if (a.min_dist)
@@ -223,7 +248,7 @@ extern "C" int pk_fk_sphere_collision(
     const float* mimic_off, const int32_t* mimic_act_idx, const int32_t* topo_inv,
     const int32_t* parent_joint_indices, const float* link_spheres, const float* world_spheres,
     const float* world_capsules, const float* world_boxes, const float* world_halfspaces,
-    float* min_dist, float* link_poses, float* dist_bkm, int64_t batch, int32_t n_act,
+    float* min_dist, float* link_poses, float* dist_bkm, float* dist_bnm, int64_t batch, int32_t n_act,
     int32_t n_joints, int32_t n_links, int32_t S, int32_t Ms, int32_t Mc, int32_t Mb,
     int32_t Mh) {
   PK_CHECK_ARG(batch >= 0 && n_links >= 0 && S >= 0 && Ms >= 0 && Mc >= 0 && Mb >= 0 && Mh >= 0,
@@ -267,6 +292,7 @@ extern "C" int pk_fk_sphere_collision(
   a.min_dist = min_dist;
   a.link_poses = link_poses;
   a.dist_bkm = dist_bkm;
+  a.dist_bnm = dist_bnm;
   a.batch = batch;
   a.N = n_links;
   a.S = S;

@@ -219,3 +219,30 @@ def test_fused_large_batch_min_only():
     idx = np.random.default_rng(0).choice(len(w.cfg), 512, replace=False)
     _, _, dmin = fused_reference(w.model, w.spheres, w.world, w.cfg[idx])
     np.testing.assert_allclose(res.min_dist.cpu().numpy()[idx], dmin, atol=2e-5)
+
+
+@pytest.mark.parametrize("both", [False, True])
+@pytest.mark.parametrize("case", ["sweep", "padded"])
+def test_fused_per_link_rows(case, both):
+    """[B, N, M] per-link rows (the reduced layout) from the fused kernel, alone or with [B, K, M]."""
+    if case == "sweep":
+        w = W.sweep(B=24)     # 16 spheres per link, 4096 spheres + 256 boxes
+        model, spheres, world, cfg = w.model, w.spheres, w.world, w.cfg
+    else:
+        rng = np.random.default_rng(5)
+        model = R.bimanual_tree(rng)
+        spheres = R.random_spheres(model, rng, per_link_range=(0, 5))
+        world = W.empty_world()
+        world.spheres, world.capsules, world.boxes, world.halfspaces = mixed_world(rng, Ms=9, Mc=5, Mb=3, Mh=1)
+        cfg = model.random_cfgs(rng, 45)
+    res = fk_sphere_collision(DeviceRobot.upload(model, DEV), DeviceSpheres.upload(spheres, DEV),
+                              DeviceWorld.upload(world, DEV), tt(cfg), per_sphere=both, per_link=True)
+    links, bkm, dmin = fused_reference(model, spheres, world, cfg)
+    B, N, S = len(cfg), spheres.n_links, spheres.S
+    r_k = np.broadcast_to(spheres.radii.T.reshape(-1), (B, S * N))
+    d = np.where(r_k[..., None] < 0, np.inf, bkm).reshape(B, S, N, -1).min(axis=1)
+    bnm = np.where(np.isinf(d), 1e9, d)
+    np.testing.assert_allclose(res.dist_bnm.cpu().numpy(), bnm, atol=2e-5, rtol=1e-6)
+    np.testing.assert_allclose(res.min_dist.cpu().numpy(), dmin, atol=2e-5)
+    if both:
+        np.testing.assert_allclose(res.dist_bkm.cpu().numpy(), bkm, atol=2e-5, rtol=1e-6)
