@@ -243,6 +243,7 @@ def run_ours(args):
         dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=120))
 
     from pyroffi_b200 import _lib, workloads as W
+    from pyroffi_b200.dist import max_over_ranks
     from pyroffi_b200.ik import BatchIkSolver
 
     _lib.load()
@@ -288,11 +289,7 @@ def run_ours(args):
     clock_summary = clocks.summary()
     success = float(res_w[3].float().mean().item())
     t_local = sum(step_ms) / 1e3
-    t_max = t_local
-    if world > 1:
-        tt_ = torch.tensor([t_local], device=dev)
-        dist.all_reduce(tt_, op=dist.ReduceOp.MAX)
-        t_max = float(tt_.item())
+    t_max = max_over_ranks(t_local, dev)
     value = world * P_PER_GPU * args.steps / t_max
 
     # --- end to end through the public API, host buffers ------------------
@@ -327,11 +324,7 @@ def run_ours(args):
         b.synchronize()
         e2e_ms.append(a.elapsed_time(b))
     barrier()
-    t_e2e = sum(e2e_ms) / 1e3
-    if world > 1:
-        tt_ = torch.tensor([t_e2e], device=dev)
-        dist.all_reduce(tt_, op=dist.ReduceOp.MAX)
-        t_e2e = float(tt_.item())
+    t_e2e = max_over_ranks(sum(e2e_ms) / 1e3, dev)
     e2e_value = world * P_PER_GPU * args.steps / t_e2e
 
     line = None

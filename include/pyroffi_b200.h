@@ -139,7 +139,7 @@ typedef struct pk_lm_options {
   int32_t enable_collision;
   float collision_weight;
   float collision_margin;
-  int32_t threads_per_seed; /* 0 = choose automatically; else 1, 2, 4 or 8 */
+  int32_t threads_per_seed; /* 0 = default (2); 1, 2, 4, 8 = lanes sharing one seed; 5 = one lane per line-search trial */
   int32_t seeds_per_block;  /* 0 = choose automatically */
 } pk_lm_options;
 

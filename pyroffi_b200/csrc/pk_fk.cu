@@ -69,6 +69,113 @@ struct FusedArgs {
   int stage_world;          // obstacles in shared memory
 };
 
+// Signed gap between robot sphere (c, r) and obstacle sphere o, with
+// sqrt(x) = x * rsqrt(x) (relative error a few ulp, under 1e-6 m at the
+// distances of a workspace); d2 = 0 gives 0.
+__device__ __forceinline__ float sphere_gap(float3 c, float r, float4 o) {
+  const float dx = c.x - o.x, dy = c.y - o.y, dz = c.z - o.z;
+  const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+  return d2 * rsqrtf(fmaxf(d2, 1e-30f)) - (r + o.w);
+}
+
+// Distance rows of one block.  Block row r is configuration c = r / R and
+// robot sphere k (R = K, output [B, K, M]) or link n (R = N, PER_LINK,
+// output [B, N, M] = min over the link's S spheres); the M columns are the
+// obstacles.  A lane owns a quad of 4 consecutive columns for a whole chunk
+// of rows: four sphere obstacles stay in registers while the rows stream
+// past (robot spheres are shared-memory broadcasts), other obstacle types go
+// through obstacle_dist.  lpr lanes cover one row (lpr * 4 >= M when M is
+// small, so short rows pack 32 / lpr rows per warp); work units (column
+// tile, row chunk) are spread over the warps.  Each lane folds its running
+// minimum into cmin[c] (shared atomics) whenever its configuration changes.
+// Padding spheres (radius < 0) give 1e9 in [B, K, M] and are skipped in the
+// per-link minimum.
+template <bool PER_LINK>
+__device__ __forceinline__ void distance_rows(const FusedArgs& a, const ObsView& ob,
+                                              const float4* centres, int* cmin, long long b0,
+                                              int nc, float* out, bool do_min = true) {
+  const int N = a.N, S = a.S, K = N * S;
+  const int M = ob.Ms + ob.Mc + ob.Mb + ob.Mh;
+  const int R = PER_LINK ? N : K;
+  const int nrows = nc * R;
+  if (M == 0 || nrows == 0) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int cols4 = (M + 3) >> 2;
+  int lpr = 1;
+  while (lpr < 32 && lpr < cols4) lpr <<= 1;
+  const int rpw = 32 / lpr;
+  const int sub = lane / lpr, sl = lane - sub * lpr;
+  const int ntile = (cols4 + lpr - 1) / lpr;
+  int rc = max(1, (16 * nwarps + ntile - 1) / ntile);
+  const int crow = ((nrows + rc - 1) / rc + rpw - 1) / rpw * rpw;
+  rc = (nrows + crow - 1) / crow;
+  const bool vec = out && ((M & 3) == 0) && ((reinterpret_cast<uintptr_t>(out) & 15) == 0);
+  const long long row_step = (long long)rpw * M;
+
+  for (int u = warp; u < ntile * rc; u += nwarps) {
+    const int tile = u % ntile, chunk = u / ntile;
+    const int m0 = 4 * (tile * lpr + sl);
+    const bool active = m0 < M;
+    const bool sph4 = m0 + 3 < ob.Ms;
+    float4 o0 = make_float4(0.f, 0.f, 0.f, 0.f), o1 = o0, o2 = o0, o3 = o0;
+    if (sph4) { o0 = ob.sph[m0]; o1 = ob.sph[m0 + 1]; o2 = ob.sph[m0 + 2]; o3 = ob.sph[m0 + 3]; }
+    const int r0 = chunk * crow + sub, r1 = min(nrows, chunk * crow + crow);
+    int c = r0 / R, k = r0 - c * R;
+    int cur = c;
+    float vmin = 1e9f;
+    float* orow = (out && active) ? out + (b0 * R + r0) * (long long)M + m0 : nullptr;
+    for (int r = r0; r < r1; r += rpw) {
+      if (c != cur) {
+        if (do_min) atomicMin(&cmin[cur], float_to_ordered(vmin));
+        cur = c;
+        vmin = 1e9f;
+      }
+      if (active) {
+        float d0 = 1e9f, d1 = 1e9f, d2 = 1e9f, d3 = 1e9f;
+        auto add = [&](const float4 ce) {
+          const float3 cc = make_float3(ce.x, ce.y, ce.z);
+          if (sph4) {
+            d0 = fminf(d0, sphere_gap(cc, ce.w, o0));
+            d1 = fminf(d1, sphere_gap(cc, ce.w, o1));
+            d2 = fminf(d2, sphere_gap(cc, ce.w, o2));
+            d3 = fminf(d3, sphere_gap(cc, ce.w, o3));
+          } else {
+            d0 = fminf(d0, obstacle_dist(ob, m0, cc, ce.w));
+            if (m0 + 1 < M) d1 = fminf(d1, obstacle_dist(ob, m0 + 1, cc, ce.w));
+            if (m0 + 2 < M) d2 = fminf(d2, obstacle_dist(ob, m0 + 2, cc, ce.w));
+            if (m0 + 3 < M) d3 = fminf(d3, obstacle_dist(ob, m0 + 3, cc, ce.w));
+          }
+        };
+        if (PER_LINK) {
+          const float4* cl = centres + c * K + k;  // sphere s of link k at cl[s * N]
+          for (int s = 0; s < S; ++s) {
+            const float4 ce = cl[s * N];
+            if (ce.w >= 0.f) add(ce);
+          }
+        } else {
+          const float4 ce = centres[r];
+          if (ce.w >= 0.f) add(ce);
+        }
+        vmin = fminf(vmin, fminf(fminf(d0, d1), fminf(d2, d3)));
+        if (orow) {
+          if (vec) {
+            __stcs(reinterpret_cast<float4*>(orow), make_float4(d0, d1, d2, d3));
+          } else {
+            orow[0] = d0;
+            if (m0 + 1 < M) orow[1] = d1;
+            if (m0 + 2 < M) orow[2] = d2;
+            if (m0 + 3 < M) orow[3] = d3;
+          }
+        }
+      }
+      if (orow) orow += row_step;
+      k += rpw;
+      while (k >= R) { k -= R; ++c; }
+    }
+    if (do_min && r0 < r1) atomicMin(&cmin[cur], float_to_ordered(vmin));
+  }
+}
+
 __global__ void __launch_bounds__(256) fk_sphere_collision_kernel(FusedArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   JointTable& jt = *reinterpret_cast<JointTable*>(smem_raw);
@@ -134,66 +241,10 @@ __global__ void __launch_bounds__(256) fk_sphere_collision_kernel(FusedArgs a) {
   }
   __syncthreads();
 
-  // phase 3: distances; each warp takes rows k = warp, warp + nwarps, ... of
-  // one configuration at a time, lanes run over obstacles.
-  const int warp = tid >> 5, lane = tid & 31, nwarps = T >> 5;
-  const bool vec4 = a.dist_bkm && ((M & 3) == 0) &&
-                    ((reinterpret_cast<uintptr_t>(a.dist_bkm) & 15) == 0);
-  // (with only the per-link output requested, its pass below also gives the minimum)
-  const bool sphere_pass = a.dist_bkm || !a.dist_bnm;
-  for (int c = 0; c < nc && sphere_pass; ++c) {
-    float vmin = 1e9f;
-    float* orow_base = a.dist_bkm ? a.dist_bkm + (b0 + c) * (long long)K * M : nullptr;
-    for (int k = warp; k < K; k += nwarps) {
-      const float4 ce = centres[c * K + k];
-      const float3 cc = make_float3(ce.x, ce.y, ce.z);
-      const bool pad = ce.w < 0.f;
-      float* orow = orow_base ? orow_base + (long long)k * M : nullptr;
-      if (vec4) {
-        for (int m0 = lane * 4; m0 < M; m0 += 128) {
-          float4 d;
-          d.x = pad ? 1e9f : obstacle_dist(ob, m0 + 0, cc, ce.w);
-          d.y = pad ? 1e9f : obstacle_dist(ob, m0 + 1, cc, ce.w);
-          d.z = pad ? 1e9f : obstacle_dist(ob, m0 + 2, cc, ce.w);
-          d.w = pad ? 1e9f : obstacle_dist(ob, m0 + 3, cc, ce.w);
-          vmin = fminf(vmin, fminf(fminf(d.x, d.y), fminf(d.z, d.w)));
-          __stcs(reinterpret_cast<float4*>(orow + m0), d);
-        }
-      } else if (!pad) {
-        for (int m0 = lane; m0 < M; m0 += 32) {
-          const float d = obstacle_dist(ob, m0, cc, ce.w);
-          vmin = fminf(vmin, d);
-          if (orow) orow[m0] = d;
-        }
-      } else if (orow) {
-        for (int m0 = lane; m0 < M; m0 += 32) orow[m0] = 1e9f;
-      }
-    }
-    vmin = warp_min(vmin);
-    if (lane == 0) atomicMin(&cmin[c], float_to_ordered(vmin));
-  }
-  // per-link rows [B, N, M]: min over the link's spheres, padding skipped
-  if (a.dist_bnm) {
-    for (int row = warp; row < nc * N; row += nwarps) {
-      const int c = row / N, nl = row - c * N;
-      float* orow = a.dist_bnm + ((b0 + c) * (long long)N + nl) * M;
-      float vmin = 1e9f;
-      for (int m0 = lane; m0 < M; m0 += 32) {
-        float d = 1e9f;
-        for (int s = 0; s < S; ++s) {
-          const float4 ce = centres[c * K + s * N + nl];
-          if (ce.w < 0.f) continue;
-          d = fminf(d, obstacle_dist(ob, m0, make_float3(ce.x, ce.y, ce.z), ce.w));
-        }
-        orow[m0] = d;
-        vmin = fminf(vmin, d);
-      }
-      if (!sphere_pass) {
-        vmin = warp_min(vmin);
-        if (lane == 0) atomicMin(&cmin[c], float_to_ordered(vmin));
-      }
-    }
-  }
+  // phase 3: distances (per-sphere rows, per-link rows, or the minimum only)
+  const bool want_bkm = a.dist_bkm != nullptr, want_bnm = a.dist_bnm != nullptr;
+  if (want_bkm || !want_bnm) distance_rows<false>(a, ob, centres, cmin, b0, nc, a.dist_bkm);
+  if (want_bnm) distance_rows<true>(a, ob, centres, cmin, b0, nc, a.dist_bnm, !want_bkm);
   __syncthreads();
   if (a.min_dist)
     for (int c = tid; c < nc; c += T) a.min_dist[b0 + c] = ordered_to_float(cmin[c]);
@@ -275,10 +326,16 @@ extern "C" int pk_fk_sphere_collision(
     return b;
   };
   const size_t limit = 200 * 1024;
-  bool stage = smem_for(1, true) <= limit && sizeof(float) * w.smem_floats() <= 128 * 1024;
+  // Sphere obstacles are read once per work unit into registers, so only a
+  // small world is worth a shared-memory copy; a large one is read through L1.
+  bool stage = smem_for(1, true) <= limit && sizeof(float) * w.smem_floats() <= 48 * 1024;
   PK_CHECK_ARG(stage || world_spheres == nullptr || (reinterpret_cast<uintptr_t>(world_spheres) & 15) == 0,
                "world_spheres must be 16-byte aligned");
   while (cpb > 1 && smem_for(cpb, stage) > limit) cpb >>= 1;
+  // enough blocks to fill every SM a few times over
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  while (cpb > 1 && (batch + cpb - 1) / cpb < 4LL * sms) cpb >>= 1;
   PK_CHECK_CAP(smem_for(cpb, stage) <= limit, "robot too large for the fused kernel");
   const size_t smem = smem_for(cpb, stage);
   if (int st = set_smem_limit((const void*)fk_sphere_collision_kernel, smem)) return st;

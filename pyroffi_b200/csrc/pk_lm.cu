@@ -1390,10 +1390,15 @@ static int launch_lm_trial(LmArgs a, cudaStream_t st) {
 }
 
 static int launch_lm(LmArgs a, int tps, int spb, cudaStream_t st) {
-  // threads_per_seed 0 or 5: the trial-lane kernel (5 lanes per seed, one
+  // threads_per_seed 5: the trial-lane kernel (5 lanes per seed, one
   // line-search trial each); 1, 2, 4, 8: the seed-group kernel with the
-  // collision penalty split across that many lanes.
-  if (tps <= 0 || tps == 5) {
+  // collision penalty split across that many lanes; 0: the fastest measured
+  // default, 2 lanes x 64 seeds per block.
+  if (tps <= 0) {
+    tps = 2;
+    if (spb <= 0) spb = 64;
+  }
+  if (tps == 5) {
     if (a.n_act <= 8 && a.n_ee <= 1) return launch_lm_trial<8, 1>(a, st);
     if (a.n_act <= 16 && a.n_ee <= 2) return launch_lm_trial<16, 2>(a, st);
     set_error("the LM kernel supports n_act <= 16 with n_ee <= 2 (got n_act=%d, n_ee=%d)", a.n_act, a.n_ee);
