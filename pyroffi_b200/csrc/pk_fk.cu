@@ -69,114 +69,230 @@ struct FusedArgs {
   int stage_world;          // obstacles in shared memory
 };
 
-// Signed gap between robot sphere (c, r) and obstacle sphere o, with
-// sqrt(x) = x * rsqrt(x) (relative error a few ulp, under 1e-6 m at the
-// distances of a workspace); d2 = 0 gives 0.
-__device__ __forceinline__ float sphere_gap(float3 c, float r, float4 o) {
-  const float dx = c.x - o.x, dy = c.y - o.y, dz = c.z - o.z;
-  const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-  return d2 * rsqrtf(fmaxf(d2, 1e-30f)) - (r + o.w);
+// 1/sqrt(x) by the PTX approximate reciprocal square root (MUFU; a few ulp).
+__device__ __forceinline__ float rsqrt_approx(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
 }
 
-// Distance rows of one block.  Block row r is configuration c = r / R and
-// robot sphere k (R = K, output [B, K, M]) or link n (R = N, PER_LINK,
-// output [B, N, M] = min over the link's S spheres); the M columns are the
-// obstacles.  A lane owns a quad of 4 consecutive columns for a whole chunk
-// of rows: four sphere obstacles stay in registers while the rows stream
-// past (robot spheres are shared-memory broadcasts), other obstacle types go
-// through obstacle_dist.  lpr lanes cover one row (lpr * 4 >= M when M is
-// small, so short rows pack 32 / lpr rows per warp); work units (column
-// tile, row chunk) are spread over the warps.  Each lane folds its running
-// minimum into cmin[c] (shared atomics) whenever its configuration changes.
-// Padding spheres (radius < 0) give 1e9 in [B, K, M] and are skipped in the
-// per-link minimum.
-template <bool PER_LINK>
-__device__ __forceinline__ void distance_rows(const FusedArgs& a, const ObsView& ob,
-                                              const float4* centres, int* cmin, long long b0,
-                                              int nc, float* out, bool do_min = true) {
-  const int N = a.N, S = a.S, K = N * S;
-  const int M = ob.Ms + ob.Mc + ob.Mb + ob.Mh;
-  const int R = PER_LINK ? N : K;
-  const int nrows = nc * R;
-  if (M == 0 || nrows == 0) return;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  const int cols4 = (M + 3) >> 2;
-  int lpr = 1;
-  while (lpr < 32 && lpr < cols4) lpr <<= 1;
-  const int rpw = 32 / lpr;
-  const int sub = lane / lpr, sl = lane - sub * lpr;
-  const int ntile = (cols4 + lpr - 1) / lpr;
-  int rc = max(1, (16 * nwarps + ntile - 1) / ntile);
-  const int crow = ((nrows + rc - 1) / rc + rpw - 1) / rpw * rpw;
-  rc = (nrows + crow - 1) / crow;
-  const bool vec = out && ((M & 3) == 0) && ((reinterpret_cast<uintptr_t>(out) & 15) == 0);
-  const long long row_step = (long long)rpw * M;
+// sqrt(x) for x >= 0 as x * rsqrt(x + 1e-30): the 1e-30 keeps x = 0 finite
+// (giving 0) and is below FP32 resolution for any x above 1e-23.
+__device__ __forceinline__ float sqrt_fast(float x) { return x * rsqrt_approx(x + 1e-30f); }
 
-  for (int u = warp; u < ntile * rc; u += nwarps) {
-    const int tile = u % ntile, chunk = u / ntile;
-    const int m0 = 4 * (tile * lpr + sl);
-    const bool active = m0 < M;
-    const bool sph4 = m0 + 3 < ob.Ms;
-    float4 o0 = make_float4(0.f, 0.f, 0.f, 0.f), o1 = o0, o2 = o0, o3 = o0;
-    if (sph4) { o0 = ob.sph[m0]; o1 = ob.sph[m0 + 1]; o2 = ob.sph[m0 + 2]; o3 = ob.sph[m0 + 3]; }
-    const int r0 = chunk * crow + sub, r1 = min(nrows, chunk * crow + crow);
-    int c = r0 / R, k = r0 - c * R;
-    int cur = c;
-    float vmin = 1e9f;
-    float* orow = (out && active) ? out + (b0 * R + r0) * (long long)M + m0 : nullptr;
-    for (int r = r0; r < r1; r += rpw) {
-      if (c != cur) {
-        if (do_min) atomicMin(&cmin[cur], float_to_ordered(vmin));
-        cur = c;
-        vmin = 1e9f;
-      }
-      if (active) {
-        float d0 = 1e9f, d1 = 1e9f, d2 = 1e9f, d3 = 1e9f;
-        auto add = [&](const float4 ce) {
-          const float3 cc = make_float3(ce.x, ce.y, ce.z);
-          if (sph4) {
-            d0 = fminf(d0, sphere_gap(cc, ce.w, o0));
-            d1 = fminf(d1, sphere_gap(cc, ce.w, o1));
-            d2 = fminf(d2, sphere_gap(cc, ce.w, o2));
-            d3 = fminf(d3, sphere_gap(cc, ce.w, o3));
-          } else {
-            d0 = fminf(d0, obstacle_dist(ob, m0, cc, ce.w));
-            if (m0 + 1 < M) d1 = fminf(d1, obstacle_dist(ob, m0 + 1, cc, ce.w));
-            if (m0 + 2 < M) d2 = fminf(d2, obstacle_dist(ob, m0 + 2, cc, ce.w));
-            if (m0 + 3 < M) d3 = fminf(d3, obstacle_dist(ob, m0 + 3, cc, ce.w));
-          }
-        };
-        if (PER_LINK) {
-          const float4* cl = centres + c * K + k;  // sphere s of link k at cl[s * N]
-          for (int s = 0; s < S; ++s) {
-            const float4 ce = cl[s * N];
-            if (ce.w >= 0.f) add(ce);
-          }
-        } else {
-          const float4 ce = centres[r];
-          if (ce.w >= 0.f) add(ce);
-        }
-        vmin = fminf(vmin, fminf(fminf(d0, d1), fminf(d2, d3)));
-        if (orow) {
-          if (vec) {
-            __stcs(reinterpret_cast<float4*>(orow), make_float4(d0, d1, d2, d3));
-          } else {
-            orow[0] = d0;
-            if (m0 + 1 < M) orow[1] = d1;
-            if (m0 + 2 < M) orow[2] = d2;
-            if (m0 + 3 < M) orow[3] = d3;
-          }
-        }
-      }
-      if (orow) orow += row_step;
-      k += rpw;
-      while (k >= R) { k -= R; ++c; }
-    }
-    if (do_min && r0 < r1) atomicMin(&cmin[cur], float_to_ordered(vmin));
+// |c - o| for a robot sphere centre c and obstacle sphere o.
+__device__ __forceinline__ float centre_dist(float4 c, float4 o) {
+  const float dx = c.x - o.x, dy = c.y - o.y, dz = c.z - o.z;
+  const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, 1e-30f)));
+  return d2 * rsqrt_approx(d2);
+}
+
+// One obstacle held in registers by a lane: kind 0 sphere (x, y, z, r),
+// 1 capsule (p1, p2, r, 1/|p2 - p1|^2 or 0), 2 box (centre, axis columns,
+// half-lengths), 3 halfspace (n, n . p0).
+struct ObsReg {
+  int kind;
+  float p[15];
+};
+
+__device__ __forceinline__ ObsReg load_obstacle(const ObsView& ob, int m) {
+  ObsReg o;
+#pragma unroll
+  for (int i = 0; i < 15; ++i) o.p[i] = 0.f;
+  if (m < ob.Ms) {
+    o.kind = 0;
+    const float4 s = ob.sph[m];
+    o.p[0] = s.x; o.p[1] = s.y; o.p[2] = s.z; o.p[3] = s.w;
+    return o;
+  }
+  m -= ob.Ms;
+  if (m < ob.Mc) {
+    o.kind = 1;
+#pragma unroll
+    for (int i = 0; i < 7; ++i) o.p[i] = ob.cap[7 * m + i];
+    const float vx = o.p[3] - o.p[0], vy = o.p[4] - o.p[1], vz = o.p[5] - o.p[2];
+    const float len2 = vx * vx + vy * vy + vz * vz;
+    o.p[7] = (len2 > 1e-12f) ? 1.f / len2 : 0.f;
+    return o;
+  }
+  m -= ob.Mc;
+  if (m < ob.Mb) {
+    o.kind = 2;
+#pragma unroll
+    for (int i = 0; i < 15; ++i) o.p[i] = ob.box[15 * m + i];
+    return o;
+  }
+  m -= ob.Mb;
+  o.kind = 3;
+  const float* h = ob.hs + 6 * m;
+  o.p[0] = h[0]; o.p[1] = h[1]; o.p[2] = h[2];
+  o.p[3] = h[3] * h[0] + h[4] * h[1] + h[5] * h[2];
+  return o;
+}
+
+// Signed distance from sphere (c, r) to a register obstacle of a known kind.
+template <int KIND>
+__device__ __forceinline__ float reg_dist(const ObsReg& o, float4 c) {
+  if (KIND == 0) {
+    return centre_dist(c, make_float4(o.p[0], o.p[1], o.p[2], 0.f)) - (c.w + o.p[3]);
+  } else if (KIND == 1) {
+    const float vx = o.p[3] - o.p[0], vy = o.p[4] - o.p[1], vz = o.p[5] - o.p[2];
+    float t = ((c.x - o.p[0]) * vx + (c.y - o.p[1]) * vy + (c.z - o.p[2]) * vz) * o.p[7];
+    t = fmaxf(0.f, fminf(1.f, t));
+    const float px = fmaf(t, vx, o.p[0]) - c.x, py = fmaf(t, vy, o.p[1]) - c.y, pz = fmaf(t, vz, o.p[2]) - c.z;
+    return sqrt_fast(px * px + py * py + pz * pz) - (c.w + o.p[6]);
+  } else if (KIND == 2) {
+    const float dx = c.x - o.p[0], dy = c.y - o.p[1], dz = c.z - o.p[2];
+    const float q1 = fabsf(dx * o.p[3] + dy * o.p[4] + dz * o.p[5]) - o.p[12];
+    const float q2 = fabsf(dx * o.p[6] + dy * o.p[7] + dz * o.p[8]) - o.p[13];
+    const float q3 = fabsf(dx * o.p[9] + dy * o.p[10] + dz * o.p[11]) - o.p[14];
+    const float m1 = fmaxf(q1, 0.f), m2 = fmaxf(q2, 0.f), m3 = fmaxf(q3, 0.f);
+    return sqrt_fast(m1 * m1 + m2 * m2 + m3 * m3) + fminf(fmaxf(fmaxf(q1, q2), q3), 0.f) - c.w;
+  } else {
+    return c.x * o.p[0] + c.y * o.p[1] + c.z * o.p[2] - o.p[3] - c.w;
   }
 }
 
-__global__ void __launch_bounds__(256) fk_sphere_collision_kernel(FusedArgs a) {
+// Rows of one configuration against one register obstacle (a single column
+// m per lane): per-sphere rows (R = K) or per-link minima (R = N).  Returns
+// the lane's minimum; stores go to o, o + M, ... when `store`.
+template <bool PER_LINK, int KIND>
+__device__ __forceinline__ float single_rows(const ObsReg& ob, const float4* cc, int N, int S, int R,
+                                             float* o, int M, bool store) {
+  float vmin = 1e9f;
+  for (int k = 0; k < R; ++k) {
+    float d = 1e9f;
+    if (PER_LINK) {
+      for (int s = 0; s < S; ++s) {
+        const float4 ce = cc[s * N + k];
+        if (ce.w >= 0.f) d = fminf(d, reg_dist<KIND>(ob, ce));
+      }
+    } else {
+      const float4 ce = cc[k];
+      if (ce.w >= 0.f) d = reg_dist<KIND>(ob, ce);
+    }
+    vmin = fminf(vmin, d);
+    if (store) o[(long long)k * M] = d;
+  }
+  return vmin;
+}
+
+// Distance rows of one block.  Block row (c, k) is configuration c and
+// robot sphere k (R = K, output [B, K, M]) or link k (R = N, PER_LINK,
+// output [B, N, M] = min over the link's S spheres); the M columns are the
+// obstacles.  Columns come in two kinds of tile:
+//  * sphere quads: the first Ms4 = 4 * floor(Ms / 4) columns; a lane owns
+//    4 consecutive sphere obstacles in registers, lpr lanes cover a row
+//    (lpr * 4 >= Ms4 when that is small, so short rows pack 32 / lpr rows per
+//    warp) and rows stream past as shared-memory broadcasts; 16-byte
+//    streaming stores;
+//  * singles: the remaining columns (sphere tail, capsules, boxes,
+//    halfspaces), one obstacle per lane in registers, 32 consecutive columns
+//    per tile, coalesced 4-byte stores.
+// Work units (tile, chunk of configurations) are spread over the warps.
+// After each configuration the warp reduces its minimum by shuffles and
+// folds it into cmin[c] with one atomic.  Padding spheres (radius < 0) give
+// 1e9 in [B, K, M] and are skipped in the per-link minimum (a link without
+// spheres gives 1e9).
+template <bool PER_LINK>
+__device__ __forceinline__ void distance_rows(const FusedArgs& a, const ObsView& ob,
+                                              const float4* centres, int* cmin, long long b0,
+                                              int nc, float* out, bool do_min) {
+  const int N = a.N, S = a.S, K = N * S;
+  const int M = ob.Ms + ob.Mc + ob.Mb + ob.Mh;
+  const int R = PER_LINK ? N : K;
+  if (M == 0 || R == 0 || nc == 0) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int Ms4 = ob.Ms & ~3;
+  const int quads = Ms4 >> 2;
+  int lpr = 1;
+  while (lpr < 32 && lpr < quads) lpr <<= 1;
+  const int rpw = 32 / lpr;
+  const int sub = lane / lpr, sl = lane - sub * lpr;
+  const int ntq = (quads + lpr - 1) / lpr;
+  const int nts = (M - Ms4 + 31) / 32;
+  const int nt = ntq + nts;
+  int nchunk = min(nc, max(1, (16 * nwarps + nt - 1) / nt));
+  const int cchunk = (nc + nchunk - 1) / nchunk;
+  nchunk = (nc + cchunk - 1) / cchunk;
+  const bool vec = out && ((M & 3) == 0) && ((reinterpret_cast<uintptr_t>(out) & 15) == 0);
+
+  for (int u = warp; u < nt * nchunk; u += nwarps) {
+    const int tile = u % nt, chunk = u / nt;
+    const bool is_quad = tile < ntq;
+    const int m0 = is_quad ? 4 * (tile * lpr + sl) : Ms4 + 32 * (tile - ntq) + lane;
+    const bool active = is_quad ? (m0 < Ms4) : (m0 < M);
+    const bool store = out != nullptr && active;
+    float4 o0 = make_float4(0.f, 0.f, 0.f, 0.f), o1 = o0, o2 = o0, o3 = o0;
+    ObsReg single;
+    single.kind = -1;
+    if (is_quad && active) {
+      o0 = ob.sph[m0]; o1 = ob.sph[m0 + 1]; o2 = ob.sph[m0 + 2]; o3 = ob.sph[m0 + 3];
+    } else if (!is_quad && active) {
+      single = load_obstacle(ob, m0);
+    }
+    const int c1 = min(nc, (chunk + 1) * cchunk);
+    for (int c = chunk * cchunk; c < c1; ++c) {
+      float vmin = 1e9f;
+      const float4* cc = centres + c * K;
+      if (is_quad && active) {
+        // quad rows k = sub, sub + rpw, ...; output pointer advanced only when storing
+        float* o = store ? out + ((b0 + c) * R + sub) * (long long)M + m0 : nullptr;
+        const long long ostep = store ? (long long)rpw * M : 0;
+        for (int k = sub; k < R; k += rpw, o += ostep) {
+          float4 d;
+          if (PER_LINK) {
+            d = make_float4(1e9f, 1e9f, 1e9f, 1e9f);
+            bool any = false;
+#pragma unroll 2
+            for (int s = 0; s < S; ++s) {
+              const float4 ce = cc[s * N + k];
+              if (ce.w < 0.f) continue;
+              any = true;
+              d.x = fminf(d.x, centre_dist(ce, o0) - ce.w);
+              d.y = fminf(d.y, centre_dist(ce, o1) - ce.w);
+              d.z = fminf(d.z, centre_dist(ce, o2) - ce.w);
+              d.w = fminf(d.w, centre_dist(ce, o3) - ce.w);
+            }
+            if (any) { d.x -= o0.w; d.y -= o1.w; d.z -= o2.w; d.w -= o3.w; }
+          } else {
+            const float4 ce = cc[k];
+            if (ce.w >= 0.f) {
+              d.x = centre_dist(ce, o0) - (ce.w + o0.w);
+              d.y = centre_dist(ce, o1) - (ce.w + o1.w);
+              d.z = centre_dist(ce, o2) - (ce.w + o2.w);
+              d.w = centre_dist(ce, o3) - (ce.w + o3.w);
+            } else {
+              d = make_float4(1e9f, 1e9f, 1e9f, 1e9f);
+            }
+          }
+          vmin = fminf(vmin, fminf(fminf(d.x, d.y), fminf(d.z, d.w)));
+          if (store) {
+            if (vec) {
+              __stcs(reinterpret_cast<float4*>(o), d);
+            } else {
+              o[0] = d.x; o[1] = d.y; o[2] = d.z; o[3] = d.w;
+            }
+          }
+        }
+      } else if (active) {
+        float* o = store ? out + (b0 + c) * R * (long long)M + m0 : nullptr;
+        switch (single.kind) {
+          case 0: vmin = single_rows<PER_LINK, 0>(single, cc, N, S, R, o, M, store); break;
+          case 1: vmin = single_rows<PER_LINK, 1>(single, cc, N, S, R, o, M, store); break;
+          case 2: vmin = single_rows<PER_LINK, 2>(single, cc, N, S, R, o, M, store); break;
+          default: vmin = single_rows<PER_LINK, 3>(single, cc, N, S, R, o, M, store); break;
+        }
+      }
+      if (do_min) {
+        vmin = warp_min(vmin);
+        if (lane == 0) atomicMin(&cmin[c], float_to_ordered(vmin));
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256, 3) fk_sphere_collision_kernel(FusedArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   JointTable& jt = *reinterpret_cast<JointTable*>(smem_raw);
   unsigned char* p = smem_raw + sizeof(JointTable);
@@ -242,9 +358,9 @@ __global__ void __launch_bounds__(256) fk_sphere_collision_kernel(FusedArgs a) {
   __syncthreads();
 
   // phase 3: distances (per-sphere rows, per-link rows, or the minimum only)
-  const bool want_bkm = a.dist_bkm != nullptr, want_bnm = a.dist_bnm != nullptr;
-  if (want_bkm || !want_bnm) distance_rows<false>(a, ob, centres, cmin, b0, nc, a.dist_bkm);
-  if (want_bnm) distance_rows<true>(a, ob, centres, cmin, b0, nc, a.dist_bnm, !want_bkm);
+  // (the per-link pass gives the minimum when only that, or nothing, is requested)
+  if (a.dist_bkm) distance_rows<false>(a, ob, centres, cmin, b0, nc, a.dist_bkm, true);
+  if (a.dist_bnm || !a.dist_bkm) distance_rows<true>(a, ob, centres, cmin, b0, nc, a.dist_bnm, !a.dist_bkm);
   __syncthreads();
   if (a.min_dist)
     for (int c = tid; c < nc; c += T) a.min_dist[b0 + c] = ordered_to_float(cmin[c]);
