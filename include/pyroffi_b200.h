@@ -163,6 +163,66 @@ int pk_ls_ik_ex(void* stream, const pk_lm_options* opt, const float* seeds, cons
                 int32_t Mb, int32_t Mh, int32_t n_self_pairs);
 
 /*
+ * One robot class of a batched IK call (no reference counterpart).  The
+ * model, target and sphere arrays are those of pk_ls_ik_ex for this robot;
+ * seeds and outputs are laid out [n_problems, seed_stride, n_act] and
+ * [n_problems, seed_stride], so problems may use fewer seeds than the
+ * stride (unused slots are neither read nor written).
+ *   body 0: seed-group kernel (n_act <= 8, n_ee == 1; lanes per seed and
+ *           seeds per block from pk_lm_options);
+ *   body 1: one warp per seed with its state in shared memory
+ *           (n_act <= 32, n_ee <= 4).
+ */
+typedef struct pk_ik_class {
+  const float* twists;
+  const float* parent_tf;
+  const int32_t* parent_idx;
+  const int32_t* act_idx;
+  const float* mimic_mul;
+  const float* mimic_off;
+  const int32_t* mimic_act_idx;
+  const int32_t* topo_inv;
+  int32_t n_joints;
+  int32_t n_act;
+  const int32_t* target_jnts;     /* [n_ee] */
+  const int32_t* ancestor_masks;  /* [n_ee, n_joints] */
+  const float* target_Ts;         /* [n_problems, n_ee, 7] */
+  int32_t n_ee;
+  const float* robot_spheres_local;       /* [n_robot_spheres, 4] */
+  const int32_t* robot_sphere_joint_idx;  /* [n_robot_spheres] */
+  int32_t n_robot_spheres;
+  const int32_t* self_i;          /* [n_self] robot-sphere index pairs, or null */
+  const int32_t* self_j;
+  int32_t n_self;
+  const float* lower;             /* [n_act] */
+  const float* upper;
+  const int32_t* fixed_mask;
+  const float* seeds;             /* [n_problems, seed_stride, n_act] */
+  float* out_cfg;                 /* [n_problems, seed_stride, n_act] */
+  float* out_err;                 /* [n_problems, seed_stride] */
+  int32_t n_problems;
+  int32_t seed_stride;
+  int32_t body;
+} pk_ik_class;
+
+/*
+ * Batched LM IK over several robot classes sharing one world (no reference
+ * counterpart): the persistent form of pk_ls_ik_ex.  items[n_items][4] =
+ * (class, problem, first seed, seed count) in device memory, in the order
+ * blocks should take them (longest first balances the tail); a body-0 item
+ * holds at most seeds_per_block seeds.  Each body runs one persistent kernel
+ * whose blocks take items from a device counter in queue[2] (caller-owned
+ * device memory; cleared here with an async memset on `stream` before the
+ * launch, so one queue serves one call in flight at a time).  blocks = 0
+ * sizes each grid to one full wave on the current device.  Same per-seed
+ * iteration and outputs as pk_ls_ik_ex with opt.
+ */
+int pk_ik_batch(void* stream, const pk_lm_options* opt, const pk_ik_class* classes, int32_t n_classes,
+                const float* world_spheres, const float* world_capsules, const float* world_boxes,
+                const float* world_halfspaces, int32_t Ms, int32_t Mc, int32_t Mb, int32_t Mh,
+                const int32_t* items, int32_t n_items, int32_t* queue, int32_t blocks);
+
+/*
  * FP64 re-verification and winner selection (no reference counterpart; it
  * replaces the argmin of _ls_ik_solve_cuda_batch_jit,
  * src/pyroffi/optimization_engines/_ls_ik.py:974-999, and the FP64 check of

@@ -61,9 +61,25 @@ SIGNATURES: dict[str, list] = {
     "pk_ls_ik_ex": [_p, C.POINTER(LmOptions)] + [_p] * 25 + [_i32] * 11,
     "pk_ik_verify_select": [_p] * 4 + [_f32] + [_p] * 10 + [_f32, _f32] + [_p] * 4 + [_i32] * 5,
     "pk_fk_sphere_collision": [_p] * 20 + [_i64] + [_i32] * 8,
+    "pk_ik_batch": [_p, C.POINTER(LmOptions), C.c_void_p, _i32] + [_p] * 4 + [_i32] * 4 + [_p, _i32, _p, _i32],
     "pk_fp32_fma_peak": [_p, _p, _i32, _i32],
     "pk_traj_cost_grad": [_p, C.c_void_p] + [_p] * 22 + [_i64] + [_i32] * 10,
 }
+
+
+class IkClass(C.Structure):
+    """``pk_ik_class`` of the C-ABI (one robot class of a batched IK call)."""
+
+    _fields_ = [
+        ("twists", _p), ("parent_tf", _p), ("parent_idx", _p), ("act_idx", _p), ("mimic_mul", _p),
+        ("mimic_off", _p), ("mimic_act_idx", _p), ("topo_inv", _p), ("n_joints", _i32), ("n_act", _i32),
+        ("target_jnts", _p), ("ancestor_masks", _p), ("target_Ts", _p), ("n_ee", _i32),
+        ("robot_spheres_local", _p), ("robot_sphere_joint_idx", _p), ("n_robot_spheres", _i32),
+        ("self_i", _p), ("self_j", _p), ("n_self", _i32),
+        ("lower", _p), ("upper", _p), ("fixed_mask", _p),
+        ("seeds", _p), ("out_cfg", _p), ("out_err", _p), ("n_problems", _i32), ("seed_stride", _i32),
+        ("body", _i32),
+    ]
 
 
 class TrajOptions(C.Structure):

@@ -36,7 +36,9 @@
 //    trial instead of being recomputed (it is the same value).
 #include <float.h>
 
-#include "pk_obstacles.cuh"
+#include <algorithm>
+
+#include "pk_batch.cuh"
 
 namespace pk {
 
@@ -531,7 +533,7 @@ __device__ __forceinline__ float lm_direction(const LmShared& sh, const PoseSlot
 // spheres, grouped self pairs and the obstacle grid, all in shared memory.
 // Ends with __syncthreads().
 template <int MAXA>
-__device__ void lm_stage(const LmArgs& a, unsigned char* smem_raw, const LmLayout& L) {
+__device__ void lm_stage(const LmArgs& a, unsigned char* smem_raw, const LmLayout& L, int pb) {
   LmShared& sh = *reinterpret_cast<LmShared*>(smem_raw);
   float4* rs4 = reinterpret_cast<float4*>(smem_raw + L.rs);
   float4* ws4 = reinterpret_cast<float4*>(smem_raw + L.ws);
@@ -547,7 +549,6 @@ __device__ void lm_stage(const LmArgs& a, unsigned char* smem_raw, const LmLayou
   float* wh = reinterpret_cast<float*>(smem_raw + L.wh);
   int* scratch = reinterpret_cast<int*>(smem_raw + L.scratch);  // reused by the kernel after staging
 
-  const int pb = blockIdx.y;  // problem
   load_joint_table(sh.jt, a.m);
   const int tid = threadIdx.x;
   if (tid < a.n_ee) {
@@ -756,11 +757,13 @@ __device__ void lm_stage(const LmArgs& a, unsigned char* smem_raw, const LmLayou
 
 }
 
+// `count` seeds of problem pb, with the block's shared memory already
+// staged for (a, pb) by lm_stage; seed group g reads and writes flat seed
+// index gs_base + g.  A group past `count` does nothing
+// (the body has no block-wide barrier).
 template <int MAXA, int MAXEE, int TPS>
-__global__ void __launch_bounds__(128, (MAXA <= 8 ? 4 : 2)) lm_kernel(LmArgs a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const LmLayout L = lm_layout(a, TPS);
-  lm_stage<MAXA>(a, smem_raw, L);
+__device__ __forceinline__ void lm_seed_groups(const LmArgs& a, unsigned char* smem_raw, const LmLayout& L, int pb,
+                                               int count, size_t gs_base) {
   LmShared& sh = *reinterpret_cast<LmShared*>(smem_raw);
   float4* rs4 = reinterpret_cast<float4*>(smem_raw + L.rs);
   float4* ws4 = reinterpret_cast<float4*>(smem_raw + L.ws);
@@ -776,13 +779,12 @@ __global__ void __launch_bounds__(128, (MAXA <= 8 ? 4 : 2)) lm_kernel(LmArgs a) 
   float* pos = reinterpret_cast<float*>(smem_raw + L.pos);
   const int PS = lm_pos_stride(a.n_rs, a.m.n_joints);
   const int tid = threadIdx.x;
-  const int pb = blockIdx.y;
   const int g = tid / TPS, t = tid - g * TPS;
   const int lane = tid & 31;
   const unsigned gmask = (TPS == 32) ? 0xffffffffu : (((1u << TPS) - 1u) << (lane & ~(TPS - 1)));
-  const int s = blockIdx.x * a.spb + g;
-  if (s >= a.Sd) return;
-  const size_t gs = (size_t)pb * a.Sd + s;
+  if (g >= count) return;
+  const size_t gs = gs_base + g;
+  (void)pb;
 
   const JointTable& jt = sh.jt;
   // one pose-slot set per seed (written by lane 0 of the group, read by all)
@@ -910,6 +912,58 @@ __global__ void __launch_bounds__(128, (MAXA <= 8 ? 4 : 2)) lm_kernel(LmArgs a) 
     for (int c = 0; c < MAXA; ++c)
       if (c < a.n_act) a.out_cfg[gs * a.n_act + c] = best[c];
     a.out_err[gs] = best_err;
+  }
+}
+
+template <int MAXA, int MAXEE, int TPS>
+__global__ void __launch_bounds__(128, (MAXA <= 8 ? 4 : 2)) lm_kernel(LmArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const LmLayout L = lm_layout(a, TPS);
+  const int pb = blockIdx.y;
+  lm_stage<MAXA>(a, smem_raw, L, pb);
+  const int s_first = blockIdx.x * a.spb;
+  const int count = min(a.spb, a.Sd - s_first);
+  lm_seed_groups<MAXA, MAXEE, TPS>(a, smem_raw, L, pb, count, (size_t)pb * a.Sd + s_first);
+}
+
+// Persistent seed-group kernel of pk_ik_batch: blocks take items (class,
+// problem, first seed, count) from the list through the counter queue[0]
+// until it runs out, skipping items of classes that use the warp body, and
+// stage each item's class and problem before running its seeds.
+struct SeedGroupBatch {
+  LmArgs cls[PK_MAX_CLASSES];
+  int body[PK_MAX_CLASSES];
+  int n_classes;
+  const int4* items;
+  int n_items;
+  int* queue;
+};
+
+template <int TPS>
+__global__ void __launch_bounds__(128, 4) lm_batch_kernel(const __grid_constant__ SeedGroupBatch B) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int s_item;
+  __shared__ LmArgs s_args;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(B.queue, 1);
+    __syncthreads();
+    const int it = s_item;
+    __syncthreads();
+    if (it >= B.n_items) break;
+    const int4 item = B.items[it];
+    if (item.x < 0 || item.x >= B.n_classes) continue;
+    int body;
+    pick_class(B.body, item.x, body);
+    if (body != kBodySeedGroup) continue;
+    if (threadIdx.x == 0) pick_class(B.cls, item.x, s_args);
+    __syncthreads();
+    const LmArgs& a = s_args;
+    if (item.y < 0 || item.y >= a.P || item.z < 0 || item.w <= 0 || item.z + item.w > a.Sd || item.w > a.spb)
+      continue;  // malformed item: nothing is read or written for it
+    const LmLayout L = lm_layout(a, TPS);
+    lm_stage<8>(a, smem_raw, L, item.y);
+    lm_seed_groups<8, 1, TPS>(a, smem_raw, L, item.y, item.w, (size_t)item.y * a.Sd + item.z);
+    __syncthreads();
   }
 }
 
@@ -1042,7 +1096,7 @@ template <int MAXA, int MAXEE>
 __global__ void __launch_bounds__(128, 4) lm_trial_kernel(LmArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const LmLayout L = lm_layout(a, 1, blockDim.x);
-  lm_stage<MAXA>(a, smem_raw, L);
+  lm_stage<MAXA>(a, smem_raw, L, blockIdx.y);
   LmShared& sh = *reinterpret_cast<LmShared*>(smem_raw);
   const int tid = threadIdx.x;
   const int pb = blockIdx.y;
@@ -1389,11 +1443,36 @@ static int launch_lm_trial(LmArgs a, cudaStream_t st) {
   return cuda_status(cudaGetLastError(), "lm_trial_kernel launch");
 }
 
+static pk_ik_class class_of(const LmArgs& a) {
+  pk_ik_class c{};
+  c.twists = a.m.twists; c.parent_tf = a.m.parent_tf; c.parent_idx = a.m.parent_idx; c.act_idx = a.m.act_idx;
+  c.mimic_mul = a.m.mimic_mul; c.mimic_off = a.m.mimic_off; c.mimic_act_idx = a.m.mimic_act_idx;
+  c.topo_inv = a.m.topo_inv; c.n_joints = a.m.n_joints; c.n_act = a.n_act;
+  c.target_jnts = a.target_jnts; c.ancestor_masks = a.ancestor_masks; c.target_Ts = a.target_Ts; c.n_ee = a.n_ee;
+  c.robot_spheres_local = a.spheres_local; c.robot_sphere_joint_idx = a.sphere_joint; c.n_robot_spheres = a.n_rs;
+  c.self_i = a.self_i; c.self_j = a.self_j; c.n_self = a.n_self;
+  c.lower = a.lower; c.upper = a.upper; c.fixed_mask = a.fixed_mask;
+  c.seeds = a.seeds; c.out_cfg = a.out_cfg; c.out_err = a.out_err;
+  c.n_problems = a.P; c.seed_stride = a.Sd; c.body = kBodyWarp;
+  return c;
+}
+
+static pk_lm_options options_of(const LmArgs& a) {
+  pk_lm_options o{};
+  o.max_iter = a.max_iter; o.pos_weight = a.pos_w; o.ori_weight = a.ori_w; o.lambda_init = a.lam0;
+  o.lambda_down = a.lam_down; o.lambda_up = a.lam_up; o.eps_pos = a.eps_pos; o.eps_ori = a.eps_ori;
+  o.enable_collision = a.coll; o.collision_weight = a.coll_w; o.collision_margin = a.margin;
+  return o;
+}
+
 static int launch_lm(LmArgs a, int tps, int spb, cudaStream_t st) {
   // threads_per_seed 5: the trial-lane kernel (5 lanes per seed, one
   // line-search trial each); 1, 2, 4, 8: the seed-group kernel with the
-  // collision penalty split across that many lanes; 0: the fastest measured
-  // default, 2 lanes x 64 seeds per block.
+  // collision penalty split across that many lanes; 32: one warp per seed
+  // (pk_lm_wide.cu), also taken for robots beyond the seed-group buckets
+  // (n_act > 16 or n_ee > 2); 0: the fastest measured default, 2 lanes x
+  // 64 seeds per block.
+  if (tps == 32 || a.n_act > 16 || a.n_ee > 2) return launch_warp_grid(class_of(a), a.w, options_of(a), st);
   if (tps <= 0) {
     tps = 2;
     if (spb <= 0) spb = 64;
@@ -1404,7 +1483,7 @@ static int launch_lm(LmArgs a, int tps, int spb, cudaStream_t st) {
     set_error("the LM kernel supports n_act <= 16 with n_ee <= 2 (got n_act=%d, n_ee=%d)", a.n_act, a.n_ee);
     return PK_ERR_CAPACITY;
   }
-  PK_CHECK_ARG(tps == 1 || tps == 2 || tps == 4 || tps == 8, "threads_per_seed must be 0, 1, 2, 4, 5 or 8");
+  PK_CHECK_ARG(tps == 1 || tps == 2 || tps == 4 || tps == 8, "threads_per_seed must be 0, 1, 2, 4, 5, 8 or 32");
   if (spb <= 0) spb = 128 / tps;
   PK_CHECK_ARG(spb * tps <= 128 && (spb * tps) % 32 == 0,
                "seeds_per_block * threads_per_seed must be a multiple of 32 and at most 128");
@@ -1558,4 +1637,107 @@ extern "C" int pk_ik_verify_select(void* stream, const float* cfgs, const float*
   a.P = n_problems; a.Sd = n_seeds; a.n_act = n_act; a.n_ee = n_ee;
   verify_select_kernel<<<n_problems, 128, 0, (cudaStream_t)stream>>>(a);
   return cuda_status(cudaGetLastError(), "verify_select_kernel launch");
+}
+
+namespace pk {
+
+template <int TPS>
+static int launch_batch_t(const SeedGroupBatch& B, size_t smem, int threads, int blocks, cudaStream_t st) {
+  auto kern = lm_batch_kernel<TPS>;
+  if (int s = set_smem_limit((const void*)kern, smem)) return s;
+  if (blocks <= 0) {
+    int dev = 0, sms = 0, per_sm = 0;
+    if (int s = cuda_status(cudaGetDevice(&dev), "cudaGetDevice")) return s;
+    if (int s = cuda_status(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attribute")) return s;
+    if (int s = cuda_status(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem), "occupancy"))
+      return s;
+    blocks = std::max(1, sms * std::max(per_sm, 1));
+  }
+  kern<<<blocks, threads, smem, st>>>(B);
+  return cuda_status(cudaGetLastError(), "lm_batch_kernel launch");
+}
+
+int launch_seed_group_batch(const BatchCall& b, cudaStream_t st, int* launched) {
+  int tps = b.opt.threads_per_seed, spb = b.opt.seeds_per_block;
+  if (tps <= 0) { tps = 2; if (spb <= 0) spb = 64; }
+  if (spb <= 0) spb = 128 / tps;
+  SeedGroupBatch B{};
+  bool any = false;
+  size_t smem = 0;
+  for (int c = 0; c < b.n_classes; ++c) {
+    const pk_ik_class& k = b.cls[c];
+    B.body[c] = k.body;
+    if (k.body != kBodySeedGroup) continue;
+    PK_CHECK_ARG(tps == 1 || tps == 2 || tps == 4 || tps == 8,
+                 "seed-group classes take threads_per_seed 0, 1, 2, 4 or 8 (got %d)", tps);
+    PK_CHECK_ARG(spb * tps <= 128 && (spb * tps) % 32 == 0,
+                 "seeds_per_block * threads_per_seed must be a multiple of 32 and at most 128");
+    PK_CHECK_CAP(k.n_act <= 8 && k.n_ee == 1, "seed-group classes need n_act <= 8 and one EE (class %d: %d, %d)",
+                 c, k.n_act, k.n_ee);
+    LmArgs a{};
+    a.m = ModelArgs{k.twists, k.parent_tf, k.parent_idx, k.act_idx, k.mimic_mul, k.mimic_off, k.mimic_act_idx,
+                    k.topo_inv, k.n_joints, k.n_act};
+    a.w = b.w;
+    a.seeds = k.seeds; a.target_jnts = k.target_jnts; a.ancestor_masks = k.ancestor_masks; a.target_Ts = k.target_Ts;
+    a.spheres_local = k.robot_spheres_local; a.sphere_joint = k.robot_sphere_joint_idx;
+    a.self_i = k.self_i; a.self_j = k.self_j; a.lower = k.lower; a.upper = k.upper; a.fixed_mask = k.fixed_mask;
+    a.out_cfg = k.out_cfg; a.out_err = k.out_err;
+    a.P = k.n_problems; a.Sd = k.seed_stride; a.n_act = k.n_act; a.n_ee = k.n_ee; a.n_rs = k.n_robot_spheres;
+    a.n_self = k.n_self;
+    const pk_lm_options& o = b.opt;
+    a.max_iter = o.max_iter; a.pos_w = o.pos_weight; a.ori_w = o.ori_weight; a.lam0 = o.lambda_init;
+    a.lam_down = o.lambda_down; a.lam_up = o.lambda_up; a.eps_pos = o.eps_pos; a.eps_ori = o.eps_ori;
+    a.coll = o.enable_collision ? 1 : 0; a.coll_w = o.collision_weight; a.margin = o.collision_margin;
+    if (!a.coll) a.n_self = 0;
+    a.spb = spb;
+    if (int s = validate_lm(a)) return s;
+    PK_CHECK_ARG(k.seeds && k.out_cfg && k.out_err && k.target_Ts && k.lower && k.upper && k.fixed_mask,
+                 "null buffer in class %d", c);
+    B.cls[c] = a;
+    smem = std::max(smem, lm_layout(a, tps).total);
+    any = true;
+  }
+  if (!any || b.n_items == 0) return PK_OK;
+  PK_CHECK_CAP(smem <= 220 * 1024, "LM working set (%zu B of shared memory) too large", smem);
+  B.n_classes = b.n_classes;
+  B.items = b.items;
+  B.n_items = b.n_items;
+  B.queue = b.queue;
+  const int threads = spb * tps;
+  int s;
+  switch (tps) {
+    case 1: s = launch_batch_t<1>(B, smem, threads, b.blocks, st); break;
+    case 2: s = launch_batch_t<2>(B, smem, threads, b.blocks, st); break;
+    case 4: s = launch_batch_t<4>(B, smem, threads, b.blocks, st); break;
+    default: s = launch_batch_t<8>(B, smem, threads, b.blocks, st); break;
+  }
+  if (s == PK_OK && launched) ++*launched;
+  return s;
+}
+
+}  // namespace pk
+
+extern "C" int pk_ik_batch(void* stream, const pk_lm_options* opt, const pk_ik_class* classes, int32_t n_classes,
+                           const float* world_spheres, const float* world_capsules, const float* world_boxes,
+                           const float* world_halfspaces, int32_t Ms, int32_t Mc, int32_t Mb, int32_t Mh,
+                           const int32_t* items, int32_t n_items, int32_t* queue, int32_t blocks) {
+  PK_CHECK_ARG(opt != nullptr && classes != nullptr, "null options or classes");
+  PK_CHECK_ARG(n_classes >= 1, "at least one class is required");
+  PK_CHECK_CAP(n_classes <= PK_MAX_CLASSES, "n_classes=%d exceeds %d", n_classes, PK_MAX_CLASSES);
+  PK_CHECK_ARG(n_items >= 0 && Ms >= 0 && Mc >= 0 && Mb >= 0 && Mh >= 0, "negative extent");
+  PK_CHECK_ARG((Ms == 0 || world_spheres) && (Mc == 0 || world_capsules) && (Mb == 0 || world_boxes) &&
+                   (Mh == 0 || world_halfspaces),
+               "null world buffer");
+  if (n_items == 0) return PK_OK;
+  PK_CHECK_ARG(items && queue, "null items or queue");
+  PK_CHECK_ARG((reinterpret_cast<uintptr_t>(items) & 15) == 0, "items must be 16-byte aligned");
+  for (int c = 0; c < n_classes; ++c)
+    PK_CHECK_ARG(classes[c].body == kBodySeedGroup || classes[c].body == kBodyWarp, "class %d: body must be 0 or 1", c);
+  const cudaStream_t st = (cudaStream_t)stream;
+  if (int s = cuda_status(cudaMemsetAsync(queue, 0, 2 * sizeof(int32_t), st), "queue reset")) return s;
+  BatchCall b{classes, n_classes, WorldArgs{world_spheres, world_capsules, world_boxes, world_halfspaces, Ms, Mc, Mb, Mh},
+              *opt, reinterpret_cast<const int4*>(items), n_items, queue, blocks};
+  int launched = 0;
+  if (int s = launch_warp_batch(b, st, &launched)) return s;
+  return launch_seed_group_batch(b, st, &launched);
 }

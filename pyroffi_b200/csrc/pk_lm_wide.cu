@@ -1,0 +1,951 @@
+// Warp-per-seed Levenberg-Marquardt IK: the body for wide robots (trees,
+// up to 32 actuated DOF, up to 4 end effectors), the grid launch that
+// pk_ls_ik_ex uses for them, and its persistent work-queue kernel for
+// pk_ik_batch.
+//
+// The per-seed iteration is the one of the seed-group kernel (pk_lm.cu),
+// which restates ls_ik_lm_kernel (src/pyroffi/cuda_kernels/
+// _ls_ik_cuda_kernel.cu:65-394): residual, weighted stacked Jacobian, Jacobi
+// column scaling, FP64 damped normal equations, Cholesky (step 0 on a
+// non-positive pivot), trust-region clip, 5-point line search on clamped
+// trials, accept/reject of the damping, all-time best.
+//
+// B200 mapping: one warp owns one seed and keeps the seed's state in
+// shared memory, so no per-thread array grows with the DOF count:
+//  * FK runs level by level over the joint tree (joints of one depth level
+//    on different lanes);
+//  * lane c builds Jacobian column c.  Only the active columns are formed:
+//    an actuated joint that is fixed, or moves no end effector, has an
+//    all-zero column whose damped step is exactly 0, so dropping it changes
+//    nothing but the size of the solve;
+//  * the FP64 normal equations are formed by rows (lane j computes A[i][j])
+//    and factored by the left-looking Cholesky of the seed-group kernel,
+//    parallel over the rows below the pivot with the same arithmetic per
+//    entry; the two triangular solves run column by column;
+//  * the collision penalty is split over the lanes: sphere transforms by
+//    sphere, world spheres by sphere-carrying joint (bounding-sphere cull
+//    and a per-block obstacle grid, as in the seed-group kernel), other
+//    obstacle types by sphere, self pairs by pair, then a warp sum.
+// The robot class, world and grid are staged per block in shared memory and
+// re-staged only when a block moves to another class (targets: another
+// problem).
+#include <float.h>
+
+#include <algorithm>
+
+#include "pk_batch.cuh"
+
+namespace pk {
+
+constexpr int WG = 8;                  // obstacle grid cells per axis (coordinates packed in 4 bits)
+constexpr int W_MAXROWS = 6 * PK_MAX_EE;
+
+struct WideArgs {
+  ModelArgs m;
+  const float* seeds;
+  const int* target_jnts;
+  const int* ancestor_masks;
+  const float* target_Ts;
+  const float* spheres_local;
+  const int* sphere_joint;
+  const int* self_i;
+  const int* self_j;
+  const float* lower;
+  const float* upper;
+  const int* fixed_mask;
+  float* out_cfg;
+  float* out_err;
+  int n_act, n_ee, n_rs, n_self, seed_stride, n_problems;
+};
+
+// Byte offsets of the dynamic shared memory, sized for the largest class.
+struct WideLayout {
+  size_t rs, rsj, rsk, pairs, ws, wc, wb, wh, cells, cell_obs, obox, warps, warp_bytes, total;
+  size_t w_cfg, w_best, w_dact, w_trial, w_dcol, w_cs, w_r, w_fw, w_pee, w_T, w_J, w_A, w_y, w_pos;
+  int max_rs, max_self, max_joints, max_act, max_rows, max_entries, nwarps;
+};
+
+struct WideLaunch {
+  WideArgs cls[PK_MAX_CLASSES];
+  int body[PK_MAX_CLASSES];
+  int n_classes;
+  WorldArgs w;
+  int max_iter;
+  float pos_w, ori_w, lam0, lam_down, lam_up, eps_pos, eps_ori;
+  int coll;
+  float coll_w, margin;
+  const int4* items;  // persistent: the item list
+  int n_items;
+  int* queue;         // persistent: item counter; null: grid launch (problem blockIdx.y, seed block blockIdx.x)
+  int grid_chunk;     // grid launch: seeds per block
+  WideLayout L;
+};
+
+struct WideShared {
+  JointTable jt;
+  unsigned long long anc[PK_MAX_EE];
+  float tgt[PK_MAX_EE][7];
+  int tsorted[PK_MAX_EE];
+  float lo[PK_MAX_ACT], hi[PK_MAX_ACT];
+  int ncol;
+  int col_act[PK_MAX_ACT];
+  int col_start[PK_MAX_ACT + 1];
+  int col_joint[2 * PK_MAX_JOINTS];
+  float col_w[2 * PK_MAX_JOINTS];
+  int n_lvl;
+  int lvl_start[PK_MAX_JOINTS + 1];
+  int lvl_joint[PK_MAX_JOINTS];
+  int n_js;
+  int js_joint[PK_MAX_JOINTS];     // sorted joint of each sphere-carrying slot
+  int jstart[PK_MAX_JOINTS + 1];   // grouped sphere range per slot
+  float4 jb[PK_MAX_JOINTS];        // bounding sphere per slot (joint frame)
+  int n_rs, n_pairs;
+  int grid_on;
+  float3 glo, ginv;
+  float rmax;
+};
+
+__host__ __device__ inline size_t w_align16(size_t x) { return (x + 15) & ~size_t(15); }
+
+__host__ inline WideLayout wide_layout(int max_rs, int max_self, int max_joints, int max_act, int max_ee,
+                                       const WorldArgs& w, int nwarps) {
+  WideLayout L{};
+  L.max_rs = max_rs; L.max_self = max_self; L.max_joints = max_joints; L.max_act = max_act;
+  L.max_rows = 6 * max_ee; L.nwarps = nwarps;
+  L.max_entries = (w.Ms >= 32 && w.Ms <= 65535) ? std::min(std::max(16 * w.Ms, 1024), 8192) : 0;
+  size_t o = w_align16(sizeof(WideShared));
+  L.rs = o; o = w_align16(o + 16 * (size_t)max_rs);
+  L.rsj = o; o = w_align16(o + 4 * (size_t)max_rs);
+  L.rsk = o; o = w_align16(o + 4 * (size_t)max_rs);
+  L.pairs = o; o = w_align16(o + 8 * (size_t)max_self);
+  L.ws = o; o = w_align16(o + 16 * (size_t)w.Ms);
+  L.wc = o; o = w_align16(o + 28 * (size_t)w.Mc);
+  L.wb = o; o = w_align16(o + 60 * (size_t)w.Mb);
+  L.wh = o; o = w_align16(o + 24 * (size_t)w.Mh);
+  L.cells = o; o = w_align16(o + (L.max_entries ? 4 * (size_t)(WG * WG * WG + 1) : 0));
+  L.cell_obs = o; o = w_align16(o + 2 * (size_t)L.max_entries);
+  L.obox = o; o = w_align16(o + (L.max_entries ? 4 * (size_t)w.Ms : 0));
+  // one warp's area
+  size_t q = 0;
+  L.w_cfg = q; q += 4 * PK_MAX_ACT;
+  L.w_best = q; q += 4 * PK_MAX_ACT;
+  L.w_dact = q; q += 4 * PK_MAX_ACT;
+  L.w_trial = q; q += 4 * PK_MAX_ACT;
+  L.w_dcol = q; q += 4 * PK_MAX_ACT;
+  L.w_cs = q; q += 4 * PK_MAX_ACT;
+  L.w_r = q; q += 4 * W_MAXROWS;
+  L.w_fw = q; q += 4 * W_MAXROWS;
+  L.w_pee = q; q += 4 * 3 * PK_MAX_EE;
+  q = w_align16(q);
+  L.w_T = q; q = w_align16(q + 28 * (size_t)max_joints);
+  L.w_J = q; q = w_align16(q + 4 * (size_t)L.max_rows * max_act);
+  L.w_A = q; q = w_align16(q + 8 * (size_t)max_act * (max_act + 1) / 2);
+  L.w_y = q; q = w_align16(q + 8 * (size_t)PK_MAX_ACT);
+  L.w_pos = q; q = w_align16(q + 16 * (size_t)max_rs);
+  L.warp_bytes = q;
+  L.warps = o;
+  L.total = o + q * nwarps;
+  return L;
+}
+
+// ---------------------------------------------------------------------------
+// staging
+// ---------------------------------------------------------------------------
+
+// Robot class c and the world, by all threads of the block; ends with __syncthreads().
+__device__ void wide_stage_class(const WideLaunch& P, const WideArgs& A, unsigned char* smem) {
+  const WideLayout& L = P.L;
+  WideShared& sh = *reinterpret_cast<WideShared*>(smem);
+  float4* rs4 = reinterpret_cast<float4*>(smem + L.rs);
+  int* rsj = reinterpret_cast<int*>(smem + L.rsj);
+  int* rsk = reinterpret_cast<int*>(smem + L.rsk);
+  int2* pairs = reinterpret_cast<int2*>(smem + L.pairs);
+  float4* ws4 = reinterpret_cast<float4*>(smem + L.ws);
+  float* wc = reinterpret_cast<float*>(smem + L.wc);
+  float* wb = reinterpret_cast<float*>(smem + L.wb);
+  float* wh = reinterpret_cast<float*>(smem + L.wh);
+  int* cell_start = reinterpret_cast<int*>(smem + L.cells);
+  unsigned short* cell_obs = reinterpret_cast<unsigned short*>(smem + L.cell_obs);
+  int* obox = reinterpret_cast<int*>(smem + L.obox);
+  const int tid = threadIdx.x;
+  const WorldArgs& w = P.w;
+
+  load_joint_table(sh.jt, A.m);  // ends with __syncthreads()
+  const int nj = A.m.n_joints;
+  if (tid < A.n_ee) {
+    unsigned long long bits = 0ull;
+    for (int j = 0; j < nj; ++j)
+      if (A.ancestor_masks[tid * nj + j]) bits |= 1ull << j;
+    sh.anc[tid] = bits;
+    const int tj = A.target_jnts[tid];
+    sh.tsorted[tid] = (tj >= 0 && tj < nj) ? sh.jt.sorted_of[tj] : 0;
+  }
+  for (int i = tid; i < PK_MAX_ACT; i += blockDim.x) {
+    const bool real = i < A.n_act;
+    sh.lo[i] = real ? A.lower[i] : 0.f;
+    sh.hi[i] = real ? A.upper[i] : 0.f;
+  }
+  for (int i = tid; i < w.Ms; i += blockDim.x)
+    ws4[i] = make_float4(w.spheres[4 * i], w.spheres[4 * i + 1], w.spheres[4 * i + 2], w.spheres[4 * i + 3] + P.margin);
+  for (int i = tid; i < w.Mc * 7; i += blockDim.x) wc[i] = w.capsules[i];
+  for (int i = tid; i < w.Mb * 15; i += blockDim.x) wb[i] = w.boxes[i];
+  for (int i = tid; i < w.Mh * 6; i += blockDim.x) wh[i] = w.halfspaces[i];
+  __syncthreads();
+
+  // Thread 0: active columns and their joint lists, FK levels, spheres
+  // grouped by joint (invalid joint indices dropped, as the reference skips
+  // them), bounding spheres, self pairs in grouped indices, grid bounds.
+  if (tid == 0) {
+    const JointTable& jt = sh.jt;
+    const int n = jt.n;
+    // active columns
+    int ncol = 0, t = 0;
+    for (int act = 0; act < A.n_act; ++act) {
+      if (A.fixed_mask[act] != 0) continue;
+      const int t0 = t;
+      for (int i = 0; i < n; ++i) {
+        if (jt.jkind[i] == 0) continue;
+        const int hits = (jt.a1[i] == act) + (jt.a2[i] == act);
+        if (hits == 0) continue;
+        bool moves = false;
+        for (int e = 0; e < A.n_ee; ++e) moves |= ((sh.anc[e] >> jt.orig[i]) & 1ull) != 0;
+        if (!moves) continue;
+        sh.col_joint[t] = i;
+        sh.col_w[t] = jt.mul[i] * (float)hits;
+        ++t;
+      }
+      if (t == t0) continue;
+      sh.col_act[ncol] = act;
+      sh.col_start[ncol] = t0;
+      ++ncol;
+    }
+    sh.col_start[ncol] = t;
+    sh.ncol = ncol;
+    // levels
+    int lvl[PK_MAX_JOINTS], cnt[PK_MAX_JOINTS + 1];
+    int n_lvl = 0;
+    for (int i = 0; i < n; ++i) {
+      const int p = jt.psorted[i];
+      lvl[i] = (p < 0 || p >= i) ? 0 : lvl[p] + 1;
+      n_lvl = max(n_lvl, lvl[i] + 1);
+    }
+    for (int l = 0; l <= n_lvl; ++l) cnt[l] = 0;
+    for (int i = 0; i < n; ++i) cnt[lvl[i]]++;
+    int run = 0;
+    for (int l = 0; l < n_lvl; ++l) { sh.lvl_start[l] = run; run += cnt[l]; cnt[l] = sh.lvl_start[l]; }
+    sh.lvl_start[n_lvl] = run;
+    for (int i = 0; i < n; ++i) sh.lvl_joint[cnt[lvl[i]]++] = i;
+    sh.n_lvl = n_lvl;
+    // spheres grouped by sphere-carrying joint, in sorted joint order
+    int scnt[PK_MAX_JOINTS], slot_of[PK_MAX_JOINTS];
+    for (int j = 0; j < n; ++j) scnt[j] = 0;
+    for (int k = 0; k < A.n_rs; ++k) {
+      const int j = A.sphere_joint[k];
+      if (j >= 0 && j < nj) scnt[jt.sorted_of[j]]++;
+    }
+    int n_js = 0, total = 0;
+    for (int js = 0; js < n; ++js) {
+      slot_of[js] = -1;
+      if (scnt[js] == 0) continue;
+      slot_of[js] = n_js;
+      sh.js_joint[n_js] = js;
+      sh.jstart[n_js] = total;
+      total += scnt[js];
+      scnt[js] = sh.jstart[n_js];
+      ++n_js;
+    }
+    sh.jstart[n_js] = total;
+    sh.n_js = n_js;
+    sh.n_rs = total;
+    for (int k = 0; k < A.n_rs; ++k) {
+      const int j = A.sphere_joint[k];
+      if (j < 0 || j >= nj) { rsk[k] = -1; continue; }
+      const int js = jt.sorted_of[j];
+      const int at = scnt[js]++;
+      rsk[k] = at;
+      rs4[at] = make_float4(A.spheres_local[4 * k], A.spheres_local[4 * k + 1], A.spheres_local[4 * k + 2],
+                            A.spheres_local[4 * k + 3]);
+      rsj[at] = slot_of[js];
+    }
+    float rmax = 0.f;
+    for (int q = 0; q < n_js; ++q) {
+      float lo3[3] = {3e38f, 3e38f, 3e38f}, hi3[3] = {-3e38f, -3e38f, -3e38f};
+      for (int k = sh.jstart[q]; k < sh.jstart[q + 1]; ++k) {
+        const float v[3] = {rs4[k].x, rs4[k].y, rs4[k].z};
+        for (int d = 0; d < 3; ++d) { lo3[d] = fminf(lo3[d], v[d]); hi3[d] = fmaxf(hi3[d], v[d]); }
+      }
+      const float cx = 0.5f * (lo3[0] + hi3[0]), cy = 0.5f * (lo3[1] + hi3[1]), cz = 0.5f * (lo3[2] + hi3[2]);
+      float R = -3e38f;
+      for (int k = sh.jstart[q]; k < sh.jstart[q + 1]; ++k) {
+        const float dx = rs4[k].x - cx, dy = rs4[k].y - cy, dz = rs4[k].z - cz;
+        R = fmaxf(R, sqrtf(dx * dx + dy * dy + dz * dz) + rs4[k].w);
+      }
+      R = R + 1e-4f + 1e-5f * fabsf(R);  // slack keeps the cull conservative under FP32 rounding
+      sh.jb[q] = make_float4(cx, cy, cz, R);
+      rmax = fmaxf(rmax, R);
+    }
+    sh.rmax = rmax;
+    // self pairs in grouped sphere positions (pairs with an invalid sphere are dropped)
+    int n_pairs = 0;
+    if (P.coll && A.n_self > 0) {
+      for (int q = 0; q < A.n_self; ++q) {
+        const int x = A.self_i[q], y = A.self_j[q];
+        if (x < 0 || y < 0 || x >= A.n_rs || y >= A.n_rs) continue;
+        if (rsk[x] < 0 || rsk[y] < 0) continue;
+        pairs[n_pairs++] = make_int2(rsk[x], rsk[y]);
+      }
+    }
+    sh.n_pairs = n_pairs;
+    // grid bounds: union of every world sphere's ball of radius r + margin + rmax
+    sh.grid_on = 0;
+    if (L.max_entries > 0 && n_js > 0 && P.coll) {
+      float lo3[3] = {3e38f, 3e38f, 3e38f}, hi3[3] = {-3e38f, -3e38f, -3e38f};
+      for (int o = 0; o < w.Ms; ++o) {
+        const float4 O = ws4[o];
+        const float rho = O.w + rmax + 1e-3f;
+        lo3[0] = fminf(lo3[0], O.x - rho); hi3[0] = fmaxf(hi3[0], O.x + rho);
+        lo3[1] = fminf(lo3[1], O.y - rho); hi3[1] = fmaxf(hi3[1], O.y + rho);
+        lo3[2] = fminf(lo3[2], O.z - rho); hi3[2] = fmaxf(hi3[2], O.z + rho);
+      }
+      sh.glo = make_float3(lo3[0], lo3[1], lo3[2]);
+      sh.ginv = make_float3(WG / fmaxf(hi3[0] - lo3[0], 1e-6f), WG / fmaxf(hi3[1] - lo3[1], 1e-6f),
+                            WG / fmaxf(hi3[2] - lo3[2], 1e-6f));
+      sh.grid_on = 1;
+    }
+  }
+  __syncthreads();
+
+  // obstacle grid: obstacle o is listed in every cell its inflated ball's
+  // bounding box touches, in increasing o (one thread per cell)
+  if (sh.grid_on) {
+    constexpr int NC = WG * WG * WG;
+    for (int o = tid; o < w.Ms; o += blockDim.x) {
+      const float4 O = ws4[o];
+      const float rho = O.w + sh.rmax + 1e-3f;
+      const float c3[3] = {O.x, O.y, O.z}, l3[3] = {sh.glo.x, sh.glo.y, sh.glo.z},
+                  i3[3] = {sh.ginv.x, sh.ginv.y, sh.ginv.z};
+      int packed = 0;
+      for (int d = 0; d < 3; ++d) {
+        const int i0 = min(max(__float2int_rd((c3[d] - rho - l3[d]) * i3[d]), 0), WG - 1);
+        const int i1 = min(max(__float2int_rd((c3[d] + rho - l3[d]) * i3[d]), 0), WG - 1);
+        packed |= (i0 | (i1 << 4)) << (8 * d);
+      }
+      obox[o] = packed;
+    }
+    __syncthreads();
+    auto inside = [&](int b, int ix, int iy, int iz) {
+      return (ix >= (b & 15)) & (ix <= ((b >> 4) & 15)) & (iy >= ((b >> 8) & 15)) & (iy <= ((b >> 12) & 15)) &
+             (iz >= ((b >> 16) & 15)) & (iz <= ((b >> 20) & 15));
+    };
+    for (int cell = tid; cell < NC; cell += blockDim.x) {
+      const int ix = cell / (WG * WG), iy = (cell / WG) % WG, iz = cell % WG;
+      int cnt = 0;
+      for (int o = 0; o < w.Ms; ++o) cnt += inside(obox[o], ix, iy, iz);
+      cell_start[cell] = cnt;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      int run = 0;
+      for (int cell = 0; cell < NC; ++cell) {
+        const int c = cell_start[cell];
+        cell_start[cell] = run;
+        run += c;
+      }
+      cell_start[NC] = run;
+      if (run > L.max_entries) sh.grid_on = 0;  // does not fit: scan every obstacle instead
+    }
+    __syncthreads();
+    if (sh.grid_on) {
+      for (int cell = tid; cell < NC; cell += blockDim.x) {
+        const int ix = cell / (WG * WG), iy = (cell / WG) % WG, iz = cell % WG;
+        int at = cell_start[cell];
+        for (int o = 0; o < w.Ms; ++o)
+          if (inside(obox[o], ix, iy, iz)) cell_obs[at++] = (unsigned short)o;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Targets of problem pb (threads < n_ee); the caller synchronises.
+__device__ inline void wide_stage_targets(const WideArgs& A, int pb, WideShared& sh) {
+  const int t = threadIdx.x;
+  if (t < A.n_ee)
+    for (int c = 0; c < 7; ++c) sh.tgt[t][c] = A.target_Ts[((size_t)pb * A.n_ee + t) * 7 + c];
+}
+
+// ---------------------------------------------------------------------------
+// per-seed body (one warp)
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ float w_warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ void w_hinge(float d2, float rr, float& pen) {
+  if (d2 < rr * fabsf(rr)) {
+    const float e = sqrtf(d2) - rr;
+    pen += e * e;
+  }
+}
+
+struct WideWarp {
+  float *cfg, *best, *dact, *trial, *dcol, *cs, *r, *fw, *pee, *T, *J;
+  double *A, *y;
+  float4* pos;
+};
+
+__device__ __forceinline__ Pose w_load(const float* T, int i) {
+  const float* p = T + 7 * i;
+  return Pose{p[0], p[1], p[2], p[3], p[4], p[5], p[6]};
+}
+__device__ __forceinline__ void w_store(float* T, int i, const Pose& P) {
+  float* p = T + 7 * i;
+  p[0] = P.w; p[1] = P.x; p[2] = P.y; p[3] = P.z; p[4] = P.tx; p[5] = P.ty; p[6] = P.tz;
+}
+
+// FK of configuration q (shared, n_act floats) into W.T, level by level.
+__device__ __forceinline__ void w_fk(const WideShared& sh, const float* q, const WideWarp& W, int lane) {
+  const JointTable& jt = sh.jt;
+  for (int lv = 0; lv < sh.n_lvl; ++lv) {
+    for (int idx = sh.lvl_start[lv] + lane; idx < sh.lvl_start[lv + 1]; idx += 32) {
+      const int i = sh.lvl_joint[idx];
+      const int src = jt.src[i];
+      const float qq = ((src < 0) ? 0.f : q[src]) * jt.mul[i] + jt.off[i];
+      const Pose Tpc = joint_local(jt, i, qq);
+      const int p = jt.psorted[i];
+      w_store(W.T, i, (p < 0) ? Tpc : pose_compose(w_load(W.T, p), Tpc));
+    }
+    __syncwarp();
+  }
+}
+
+// Residual of every EE into W.r / W.pee (lane e), as the seed-group kernel's ee_residual.
+__device__ __forceinline__ void w_residual(const WideShared& sh, int n_ee, const WideWarp& W, int lane) {
+  if (lane < n_ee) {
+    const int e = lane;
+    const Pose T = w_load(W.T, sh.tsorted[e]);
+    const float* g = sh.tgt[e];
+    float* r = W.r + 6 * e;
+    r[0] = T.tx - g[4];
+    r[1] = T.ty - g[5];
+    r[2] = T.tz - g[6];
+    const float bw = g[0], bx = -g[1], by = -g[2], bz = -g[3];
+    float qw = T.w * bw - T.x * bx - T.y * by - T.z * bz;
+    float qx = T.w * bx + T.x * bw + T.y * bz - T.z * by;
+    float qy = T.w * by - T.x * bz + T.y * bw + T.z * bx;
+    float qz = T.w * bz + T.x * by - T.y * bx + T.z * bw;
+    if (qw < 0.f) { qw = -qw; qx = -qx; qy = -qy; qz = -qz; }
+    const float s = sqrtf(qx * qx + qy * qy + qz * qz);
+    const float f = (s > 1e-6f) ? 2.f * atan2f(s, qw) / s : 2.f;
+    r[3] = qx * f;
+    r[4] = qy * f;
+    r[5] = qz * f;
+    W.pee[3 * e] = T.tx; W.pee[3 * e + 1] = T.ty; W.pee[3 * e + 2] = T.tz;
+  }
+  __syncwarp();
+}
+
+// Collision penalty (before the weight) of the configuration whose poses are in W.T.
+__device__ float w_penalty(const WideLaunch& P, const WideShared& sh, const unsigned char* smem,
+                           const WideWarp& W, int lane) {
+  const WideLayout& L = P.L;
+  const float4* rs4 = reinterpret_cast<const float4*>(smem + L.rs);
+  const int* rsj = reinterpret_cast<const int*>(smem + L.rsj);
+  const int2* pairs = reinterpret_cast<const int2*>(smem + L.pairs);
+  const float4* ws4 = reinterpret_cast<const float4*>(smem + L.ws);
+  const float* wc = reinterpret_cast<const float*>(smem + L.wc);
+  const float* wb = reinterpret_cast<const float*>(smem + L.wb);
+  const float* wh = reinterpret_cast<const float*>(smem + L.wh);
+  const int* cell_start = reinterpret_cast<const int*>(smem + L.cells);
+  const unsigned short* cell_obs = reinterpret_cast<const unsigned short*>(smem + L.cell_obs);
+  const int n_rs = sh.n_rs;
+  for (int k = lane; k < n_rs; k += 32) {
+    const float4 s = rs4[k];
+    const float3 p = pose_apply(w_load(W.T, sh.js_joint[rsj[k]]), make_float3(s.x, s.y, s.z));
+    W.pos[k] = make_float4(p.x, p.y, p.z, s.w);
+  }
+  __syncwarp();
+  float pen = 0.f;
+  const int Ms = P.w.Ms;
+  if (Ms > 0) {
+    for (int j = lane; j < sh.n_js; j += 32) {
+      const float4 bl = sh.jb[j];
+      const float3 B = pose_apply(w_load(W.T, sh.js_joint[j]), make_float3(bl.x, bl.y, bl.z));
+      const int k0 = sh.jstart[j], k1 = sh.jstart[j + 1];
+      int e0 = 0, e1 = Ms;
+      const unsigned short* list = nullptr;
+      if (sh.grid_on) {
+        const int ix = __float2int_rd((B.x - sh.glo.x) * sh.ginv.x);
+        const int iy = __float2int_rd((B.y - sh.glo.y) * sh.ginv.y);
+        const int iz = __float2int_rd((B.z - sh.glo.z) * sh.ginv.z);
+        // outside the grid no obstacle is within reach of this joint
+        if ((unsigned)ix >= (unsigned)WG || (unsigned)iy >= (unsigned)WG || (unsigned)iz >= (unsigned)WG) continue;
+        const int cell = (ix * WG + iy) * WG + iz;
+        e0 = cell_start[cell];
+        e1 = cell_start[cell + 1];
+        list = cell_obs;
+      }
+      for (int e = e0; e < e1; ++e) {
+        const float4 O = ws4[list ? (int)list[e] : e];
+        const float rr = bl.w + O.w;
+        const float dx = B.x - O.x, dy = B.y - O.y, dz = B.z - O.z;
+        if (dx * dx + dy * dy + dz * dz < rr * fabsf(rr)) {
+          for (int k = k0; k < k1; ++k) {
+            const float4 p = W.pos[k];
+            const float ex = p.x - O.x, ey = p.y - O.y, ez = p.z - O.z;
+            w_hinge(ex * ex + ey * ey + ez * ez, p.w + O.w, pen);
+          }
+        }
+      }
+    }
+  }
+  const float margin = P.margin;
+  if (P.w.Mc + P.w.Mb + P.w.Mh > 0) {
+    for (int k = lane; k < n_rs; k += 32) {
+      const float4 q = W.pos[k];
+      const float3 p = make_float3(q.x, q.y, q.z);
+      for (int m = 0; m < P.w.Mc; ++m) {
+        const float d = d_sphere_capsule(p, q.w, wc + 7 * m);
+        if (d < margin) { const float e = d - margin; pen += e * e; }
+      }
+      for (int m = 0; m < P.w.Mb; ++m) {
+        const float d = d_sphere_box(p, q.w, wb + 15 * m);
+        if (d < margin) { const float e = d - margin; pen += e * e; }
+      }
+      for (int m = 0; m < P.w.Mh; ++m) {
+        const float d = d_sphere_halfspace(p, q.w, wh + 6 * m);
+        if (d < margin) { const float e = d - margin; pen += e * e; }
+      }
+    }
+  }
+  for (int q = lane; q < sh.n_pairs; q += 32) {
+    const int2 pr = pairs[q];
+    const float4 a = W.pos[pr.x], b = W.pos[pr.y];
+    const float ex = a.x - b.x, ey = a.y - b.y, ez = a.z - b.z;
+    w_hinge(ex * ex + ey * ey + ez * ez, a.w + b.w + margin, pen);
+  }
+  pen = w_warp_sum(pen);
+  __syncwarp();
+  return pen;
+}
+
+// Weighted squared residual sum, the same on every lane (sequential order).
+__device__ __forceinline__ float w_weighted_sq(const WideWarp& W, int n_ee, const float (&Wt)[6]) {
+  float e = 0.f;
+  for (int k = 0; k < 6 * n_ee; ++k) {
+    const float rw = W.r[k] * Wt[k % 6];
+    e += rw * rw;
+  }
+  return e;
+}
+
+// Damped step of the current point into W.dact (all actuated entries);
+// returns ||fw||^2.  Poses of the current point are in W.T, its residual in W.r.
+__device__ float w_direction(const WideShared& sh, int n_act, int n_ee, const float (&Wt)[6], float lam,
+                             float max_p, float max_o, const WideWarp& W, int lane) {
+  const JointTable& jt = sh.jt;
+  const int ncol = sh.ncol, rows = 6 * n_ee;
+  // Jacobian column `lane`: weighted, Jacobi-scaled, stored column-major
+  if (lane < ncol) {
+    float Jc[W_MAXROWS];
+#pragma unroll
+    for (int k = 0; k < W_MAXROWS; ++k) Jc[k] = 0.f;
+    for (int t = sh.col_start[lane]; t < sh.col_start[lane + 1]; ++t) {
+      const int i = sh.col_joint[t];
+      const float wt = sh.col_w[t];
+      const Pose Tj = w_load(W.T, i);
+      const float3 z = quat_rotate(Tj.w, Tj.x, Tj.y, Tj.z, make_float3(jt.axis[i][0], jt.axis[i][1], jt.axis[i][2]));
+      const int orig = jt.orig[i];
+      const bool rev = jt.jkind[i] == 1;
+#pragma unroll
+      for (int e = 0; e < PK_MAX_EE; ++e) {
+        if (e >= n_ee || !((sh.anc[e] >> orig) & 1ull)) continue;
+        float col[6];
+        if (rev) {
+          const float ax = W.pee[3 * e] - Tj.tx, ay = W.pee[3 * e + 1] - Tj.ty, az = W.pee[3 * e + 2] - Tj.tz;
+          col[0] = z.y * az - z.z * ay; col[1] = z.z * ax - z.x * az; col[2] = z.x * ay - z.y * ax;
+          col[3] = z.x; col[4] = z.y; col[5] = z.z;
+        } else {
+          col[0] = z.x; col[1] = z.y; col[2] = z.z; col[3] = col[4] = col[5] = 0.f;
+        }
+#pragma unroll
+        for (int k = 0; k < 6; ++k) Jc[6 * e + k] += wt * col[k];
+      }
+    }
+    float sq = 0.f;
+#pragma unroll
+    for (int k = 0; k < W_MAXROWS; ++k) {
+      if (k < rows) {
+        Jc[k] *= Wt[k % 6];
+        sq += Jc[k] * Jc[k];
+      }
+    }
+    const float s = sqrtf(sq) + 1e-8f;
+    W.cs[lane] = s;
+#pragma unroll
+    for (int k = 0; k < W_MAXROWS; ++k)
+      if (k < rows) W.J[lane * rows + k] = Jc[k] / s;
+  }
+  if (lane < rows) W.fw[lane] = W.r[lane] * Wt[lane % 6];
+  __syncwarp();
+  float fw2 = 0.f;
+  for (int k = 0; k < rows; ++k) fw2 += W.fw[k] * W.fw[k];
+
+  // FP64 normal equations, packed lower triangle: lane j computes A[i][j]
+  for (int i = 0; i < ncol; ++i) {
+    const int j = lane;
+    if (j <= i) {
+      double acc = 0.0;
+      for (int k = 0; k < rows; ++k) acc += (double)W.J[i * rows + k] * (double)W.J[j * rows + k];
+      if (i == j) acc += (double)lam;
+      W.A[i * (i + 1) / 2 + j] = acc;
+    }
+  }
+  if (lane < ncol) {
+    double rb = 0.0;
+    for (int k = 0; k < rows; ++k) rb += (double)W.J[lane * rows + k] * (double)W.fw[k];
+    W.y[lane] = -rb;
+  }
+  __syncwarp();
+
+  // Cholesky A = L L^T, left-looking; a non-positive pivot zeroes the step
+  bool ok = true;
+  for (int k = 0; k < ncol; ++k) {
+    const int kk = k * (k + 1) / 2;
+    double s2 = W.A[kk + k];
+    for (int q = 0; q < k; ++q) s2 -= W.A[kk + q] * W.A[kk + q];
+    if (!(s2 > 0.0)) ok = false;
+    const double lkk = sqrt(ok ? s2 : 1.0);
+    const double inv = 1.0 / lkk;
+    for (int i = k + 1 + lane; i < ncol; i += 32) {
+      const int ii = i * (i + 1) / 2;
+      double tt = W.A[ii + k];
+      for (int q = 0; q < k; ++q) tt -= W.A[ii + q] * W.A[kk + q];
+      W.A[ii + k] = tt * inv;
+    }
+    __syncwarp();
+    if (lane == 0) W.A[kk + k] = lkk;
+    __syncwarp();
+  }
+  // L y = b, then L^T x = y (column by column; x overwrites y)
+  for (int i = 0; i < ncol; ++i) {
+    const double yi = W.y[i] / W.A[i * (i + 1) / 2 + i];
+    for (int j = i + 1 + lane; j < ncol; j += 32) W.y[j] -= W.A[j * (j + 1) / 2 + i] * yi;
+    __syncwarp();
+    if (lane == 0) W.y[i] = yi;
+    __syncwarp();
+  }
+  for (int i = ncol - 1; i >= 0; --i) {
+    const int ii = i * (i + 1) / 2;
+    const double xi = W.y[i] / W.A[ii + i];
+    for (int j = lane; j < i; j += 32) W.y[j] -= W.A[ii + j] * xi;
+    __syncwarp();
+    if (lane == 0) W.y[i] = xi;
+    __syncwarp();
+  }
+  if (lane < ncol) W.dcol[lane] = ok ? (float)W.y[lane] / W.cs[lane] : 0.f;
+  __syncwarp();
+  float dn2 = 0.f;
+  for (int c = 0; c < ncol; ++c) dn2 += W.dcol[c] * W.dcol[c];
+  float R;
+  if (max_p > 1e-2f || max_o > 0.6f) R = 0.38f;
+  else if (max_p > 1e-3f || max_o > 0.25f) R = 0.22f;
+  else if (max_p > 2e-4f || max_o > 0.08f) R = 0.12f;
+  else R = 0.05f;
+  const float dn = sqrtf(dn2);
+  const float sc = (dn > R) ? R / (dn + 1e-18f) : 1.f;
+  for (int a = lane; a < n_act; a += 32) W.dact[a] = 0.f;
+  __syncwarp();
+  if (lane < ncol) W.dact[sh.col_act[lane]] = (dn > R) ? W.dcol[lane] * sc : W.dcol[lane];
+  __syncwarp();
+  return fw2;
+}
+
+__device__ __forceinline__ float w_alpha(int i) {
+  return i == 0 ? 1.0f : i == 1 ? 0.5f : i == 2 ? 0.25f : i == 3 ? 0.1f : 0.025f;
+}
+
+// LM for flat seed index gs of class A (targets of its problem staged).
+__device__ void w_seed(const WideLaunch& P, const WideArgs& A, const WideShared& sh, const unsigned char* smem,
+                       const WideWarp& W, size_t gs, int lane) {
+  const int n_act = A.n_act, n_ee = A.n_ee;
+  const float Wt[6] = {P.pos_w, P.pos_w, P.pos_w, P.ori_w, P.ori_w, P.ori_w};
+  const bool use_coll = P.coll && sh.n_rs > 0;
+  for (int a = lane; a < n_act; a += 32) {
+    const float v = A.seeds[gs * n_act + a];
+    W.cfg[a] = v;
+    W.best[a] = v;
+    W.dact[a] = 0.f;
+  }
+  __syncwarp();
+  auto evaluate = [&](const float* q, float& pen) {
+    w_fk(sh, q, W, lane);
+    w_residual(sh, n_ee, W, lane);
+    pen = use_coll ? P.coll_w * w_penalty(P, sh, smem, W, lane) : 0.f;
+    return w_weighted_sq(W, n_ee, Wt) + pen;
+  };
+  float pen_cur;
+  float best_err = evaluate(W.cfg, pen_cur);
+  float lam = P.lam0;
+  for (int it = 0; it < P.max_iter; ++it) {
+    // current point: poses and residual (its penalty is carried), convergence, damped step
+    w_fk(sh, W.cfg, W, lane);
+    w_residual(sh, n_ee, W, lane);
+    bool all_conv = true;
+    float max_p = 0.f, max_o = 0.f;
+    for (int e = 0; e < n_ee; ++e) {
+      const float* r = W.r + 6 * e;
+      const float np = sqrtf(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+      const float no = sqrtf(r[3] * r[3] + r[4] * r[4] + r[5] * r[5]);
+      if (np >= P.eps_pos || no >= P.eps_ori) all_conv = false;
+      max_p = fmaxf(max_p, np);
+      max_o = fmaxf(max_o, no);
+    }
+    if (all_conv) break;
+    const float curr = w_direction(sh, n_act, n_ee, Wt, lam, max_p, max_o, W, lane) + pen_cur;
+    // line search: first minimum over the 5 step sizes
+    float best_a_err = 1e30f, best_a_pen = pen_cur;
+    int best_a = 0;
+    for (int t = 0; t < 5; ++t) {
+      const float al = w_alpha(t);
+      for (int a = lane; a < n_act; a += 32)
+        W.trial[a] = fmaxf(sh.lo[a], fminf(sh.hi[a], W.cfg[a] + al * W.dact[a]));
+      __syncwarp();
+      float pen;
+      const float err = evaluate(W.trial, pen);
+      if (err < best_a_err) { best_a_err = err; best_a = t; best_a_pen = pen; }
+    }
+    const float al = w_alpha(best_a);
+    const bool accept = best_a_err < curr * (1.0f - 1e-4f);
+    const bool improve = best_a_err < best_err;
+    for (int a = lane; a < n_act; a += 32) {
+      const float tv = fmaxf(sh.lo[a], fminf(sh.hi[a], W.cfg[a] + al * W.dact[a]));
+      if (improve) W.best[a] = tv;
+      if (accept) W.cfg[a] = tv;
+    }
+    __syncwarp();
+    if (accept) {
+      pen_cur = best_a_pen;
+      lam = fmaxf(lam * P.lam_down, 1e-10f);
+    } else {
+      lam = fminf(lam * P.lam_up, 1e6f);
+    }
+    if (improve) best_err = best_a_err;
+  }
+  for (int a = lane; a < n_act; a += 32) A.out_cfg[gs * n_act + a] = W.best[a];
+  if (lane == 0) A.out_err[gs] = best_err;
+  __syncwarp();
+}
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ WideWarp w_warp_area(const WideLayout& L, unsigned char* smem, int warp) {
+  unsigned char* b = smem + L.warps + L.warp_bytes * warp;
+  WideWarp W;
+  W.cfg = reinterpret_cast<float*>(b + L.w_cfg);
+  W.best = reinterpret_cast<float*>(b + L.w_best);
+  W.dact = reinterpret_cast<float*>(b + L.w_dact);
+  W.trial = reinterpret_cast<float*>(b + L.w_trial);
+  W.dcol = reinterpret_cast<float*>(b + L.w_dcol);
+  W.cs = reinterpret_cast<float*>(b + L.w_cs);
+  W.r = reinterpret_cast<float*>(b + L.w_r);
+  W.fw = reinterpret_cast<float*>(b + L.w_fw);
+  W.pee = reinterpret_cast<float*>(b + L.w_pee);
+  W.T = reinterpret_cast<float*>(b + L.w_T);
+  W.J = reinterpret_cast<float*>(b + L.w_J);
+  W.A = reinterpret_cast<double*>(b + L.w_A);
+  W.y = reinterpret_cast<double*>(b + L.w_y);
+  W.pos = reinterpret_cast<float4*>(b + L.w_pos);
+  return W;
+}
+
+// Grid launch (P.queue == null): block (x, y) runs seeds [x * chunk, ...) of
+// problem y of class 0.  Persistent launch: blocks take items from the list
+// through the counter P.queue[0] until it runs out, skipping items of
+// classes that use the other body.
+
+__global__ void __launch_bounds__(256, 2) lm_warp_kernel(const __grid_constant__ WideLaunch P) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_item;
+  __shared__ WideArgs s_args;
+  WideShared& sh = *reinterpret_cast<WideShared*>(smem);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  const WideWarp W = w_warp_area(P.L, smem, warp);
+  int staged_cls = -1, staged_pb = -1;
+  for (int round = 0;; ++round) {
+    int4 item;
+    if (P.queue) {
+      if (threadIdx.x == 0) s_item = atomicAdd(P.queue, 1);
+      __syncthreads();
+      const int it = s_item;
+      __syncthreads();
+      if (it >= P.n_items) break;
+      item = P.items[it];
+      if (item.x < 0 || item.x >= P.n_classes) continue;
+      int body;
+      pick_class(P.body, item.x, body);
+      if (body != kBodyWarp) continue;
+    } else {
+      if (round > 0) break;
+      const int first = blockIdx.x * P.grid_chunk;
+      item = make_int4(0, blockIdx.y, first, min(P.grid_chunk, P.cls[0].seed_stride - first));
+    }
+    if (item.x != staged_cls) {
+      if (threadIdx.x == 0) pick_class(P.cls, item.x, s_args);
+      __syncthreads();
+    }
+    const WideArgs& A = s_args;
+    if (item.y < 0 || item.y >= A.n_problems || item.z < 0 || item.w <= 0 || item.z + item.w > A.seed_stride) {
+      staged_cls = -1;  // malformed item: nothing is read or written for it
+      __syncthreads();
+      continue;
+    }
+    if (item.x != staged_cls) {
+      wide_stage_class(P, A, smem);
+      staged_cls = item.x;
+      staged_pb = -1;
+    }
+    if (item.y != staged_pb) {
+      wide_stage_targets(A, item.y, sh);
+      __syncthreads();
+      staged_pb = item.y;
+    }
+    for (int s = warp; s < item.w; s += nwarps)
+      w_seed(P, A, sh, smem, W, (size_t)item.y * A.seed_stride + item.z + s, lane);
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host launchers
+// ---------------------------------------------------------------------------
+
+static WideArgs wide_args(const pk_ik_class& c) {
+  WideArgs a{};
+  a.m = ModelArgs{c.twists, c.parent_tf, c.parent_idx, c.act_idx, c.mimic_mul, c.mimic_off, c.mimic_act_idx,
+                  c.topo_inv, c.n_joints, c.n_act};
+  a.seeds = c.seeds; a.target_jnts = c.target_jnts; a.ancestor_masks = c.ancestor_masks;
+  a.target_Ts = c.target_Ts; a.spheres_local = c.robot_spheres_local; a.sphere_joint = c.robot_sphere_joint_idx;
+  a.self_i = c.self_i; a.self_j = c.self_j; a.lower = c.lower; a.upper = c.upper; a.fixed_mask = c.fixed_mask;
+  a.out_cfg = c.out_cfg; a.out_err = c.out_err;
+  a.n_act = c.n_act; a.n_ee = c.n_ee; a.n_rs = c.n_robot_spheres; a.n_self = c.n_self;
+  a.seed_stride = c.seed_stride; a.n_problems = c.n_problems;
+  return a;
+}
+
+static void wide_options(WideLaunch& P, const pk_lm_options& o) {
+  P.max_iter = o.max_iter; P.pos_w = o.pos_weight; P.ori_w = o.ori_weight; P.lam0 = o.lambda_init;
+  P.lam_down = o.lambda_down; P.lam_up = o.lambda_up; P.eps_pos = o.eps_pos; P.eps_ori = o.eps_ori;
+  P.coll = o.enable_collision ? 1 : 0; P.coll_w = o.collision_weight; P.margin = o.collision_margin;
+}
+
+static constexpr int kWideThreads = 256;
+
+// Layout for the warp-body classes of P; PK_ERR_CAPACITY when it does not fit.
+static int wide_prepare(WideLaunch& P, int max_smem) {
+  int max_rs = 0, max_self = 0, max_joints = 1, max_act = 1, max_ee = 1;
+  for (int c = 0; c < P.n_classes; ++c) {
+    if (P.body[c] != kBodyWarp) continue;
+    const WideArgs& a = P.cls[c];
+    max_rs = std::max(max_rs, a.n_rs);
+    max_self = std::max(max_self, P.coll ? a.n_self : 0);
+    max_joints = std::max(max_joints, a.m.n_joints);
+    max_act = std::max(max_act, a.n_act);
+    max_ee = std::max(max_ee, a.n_ee);
+  }
+  P.L = wide_layout(max_rs, max_self, max_joints, max_act, max_ee, P.w, kWideThreads / 32);
+  PK_CHECK_CAP(P.L.total <= (size_t)max_smem,
+               "warp-body LM working set (%zu B of shared memory) exceeds %d B", P.L.total, max_smem);
+  return PK_OK;
+}
+
+static int validate_wide_class(const pk_ik_class& c, bool coll) {
+  PK_CHECK_ARG(c.n_problems >= 0 && c.seed_stride >= 0 && c.n_act >= 0 && c.n_joints >= 0 && c.n_ee >= 1 &&
+                   c.n_robot_spheres >= 0 && c.n_self >= 0,
+               "bad class extents");
+  PK_CHECK_CAP(c.n_joints <= PK_MAX_JOINTS, "n_joints=%d exceeds %d", c.n_joints, PK_MAX_JOINTS);
+  PK_CHECK_CAP(c.n_act <= PK_MAX_ACT, "n_act=%d exceeds %d", c.n_act, PK_MAX_ACT);
+  PK_CHECK_CAP(c.n_ee <= PK_MAX_EE, "n_ee=%d exceeds %d", c.n_ee, PK_MAX_EE);
+  PK_CHECK_ARG(c.twists && c.parent_tf && c.parent_idx && c.act_idx && c.mimic_mul && c.mimic_off &&
+                   c.mimic_act_idx && c.topo_inv && c.target_jnts && c.ancestor_masks && c.target_Ts &&
+                   c.lower && c.upper && c.fixed_mask && c.seeds && c.out_cfg && c.out_err,
+               "null buffer in class");
+  PK_CHECK_ARG(c.n_robot_spheres == 0 || (c.robot_spheres_local && c.robot_sphere_joint_idx),
+               "null robot spheres");
+  PK_CHECK_ARG(!coll || c.n_self == 0 || (c.self_i && c.self_j), "null self pairs");
+  return PK_OK;
+}
+
+static int device_smem_optin(int* out) {
+  int dev = 0;
+  if (int s = cuda_status(cudaGetDevice(&dev), "cudaGetDevice")) return s;
+  return cuda_status(cudaDeviceGetAttribute(out, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev),
+                     "cudaDeviceGetAttribute");
+}
+
+int launch_warp_grid(const pk_ik_class& c, const WorldArgs& w, const pk_lm_options& opt, cudaStream_t st) {
+  if (int s = validate_wide_class(c, opt.enable_collision != 0)) return s;
+  if (c.n_problems == 0 || c.seed_stride == 0) return PK_OK;
+  WideLaunch P{};
+  P.cls[0] = wide_args(c);
+  P.body[0] = kBodyWarp;
+  P.n_classes = 1;
+  P.w = w;
+  wide_options(P, opt);
+  P.queue = nullptr;
+  P.grid_chunk = 2 * (kWideThreads / 32);
+  int max_smem = 0;
+  if (int s = device_smem_optin(&max_smem)) return s;
+  if (int s = wide_prepare(P, max_smem)) return s;
+  if (int s = set_smem_limit((const void*)lm_warp_kernel, P.L.total)) return s;
+  dim3 grid((c.seed_stride + P.grid_chunk - 1) / P.grid_chunk, c.n_problems);
+  PK_CHECK_CAP(c.n_problems <= 65535, "n_problems=%d exceeds the grid limit 65535", c.n_problems);
+  lm_warp_kernel<<<grid, kWideThreads, P.L.total, st>>>(P);
+  return cuda_status(cudaGetLastError(), "lm_warp_kernel launch");
+}
+
+int launch_warp_batch(const BatchCall& b, cudaStream_t st, int* launched) {
+  WideLaunch P{};
+  bool any = false;
+  for (int c = 0; c < b.n_classes; ++c) {
+    P.cls[c] = wide_args(b.cls[c]);
+    P.body[c] = b.cls[c].body;
+    if (b.cls[c].body == kBodyWarp) {
+      if (int s = validate_wide_class(b.cls[c], b.opt.enable_collision != 0)) return s;
+      any = true;
+    }
+  }
+  if (!any || b.n_items == 0) return PK_OK;
+  P.n_classes = b.n_classes;
+  P.w = b.w;
+  wide_options(P, b.opt);
+  P.items = b.items;
+  P.n_items = b.n_items;
+  P.queue = b.queue + 1;
+  int max_smem = 0;
+  if (int s = device_smem_optin(&max_smem)) return s;
+  if (int s = wide_prepare(P, max_smem)) return s;
+  if (int s = set_smem_limit((const void*)lm_warp_kernel, P.L.total)) return s;
+  int blocks = b.blocks;
+  if (blocks <= 0) {
+    int dev = 0, sms = 0, per_sm = 0;
+    if (int s = cuda_status(cudaGetDevice(&dev), "cudaGetDevice")) return s;
+    if (int s = cuda_status(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attribute"))
+      return s;
+    if (int s = cuda_status(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lm_warp_kernel, kWideThreads,
+                                                                          P.L.total),
+                            "occupancy"))
+      return s;
+    blocks = std::max(1, sms * std::max(per_sm, 1));
+  }
+  lm_warp_kernel<<<blocks, kWideThreads, P.L.total, st>>>(P);
+  if (launched) ++*launched;
+  return cuda_status(cudaGetLastError(), "lm_warp_kernel launch");
+}
+
+}  // namespace pk

@@ -331,3 +331,85 @@ def mixed_classes(seed: int = 1004) -> list[MixedIkClass]:
         MixedIkClass(bi, random_spheres(bi, rng, per_link=8), (10, 16), 0.2),
         MixedIkClass(hu, random_spheres(hu, rng, per_link_range=(4, 12)), (10, 17), 0.1),
     ]
+
+
+@dataclass
+class MixedIkWorkload:
+    """Uneven IK batch: problems of several robot classes sharing one world."""
+    classes: list                 # [MixedIkClass]
+    world: World
+    problem_class: np.ndarray     # [P] class of each problem
+    n_seeds: np.ndarray           # [P] seeds of each problem
+    target_T: list                # per class [P_c, n_ee, 7] float32 (problems of that class, in order)
+    target_cfgs: list             # per class [P_c, n_act]
+    seeds: list                   # per class [P_c, max seeds of the class, n_act] (unused slots 0)
+    index_in_class: np.ndarray    # [P] position of problem p within its class
+    max_iter: int = 30
+    lambda_init: float = 1e-2
+    lambda_down: float = 0.1
+    lambda_up: float = 10.0
+    pos_weight: float = 50.0
+    ori_weight: float = 10.0
+    collision_weight: float = 1e4
+    collision_margin: float = 0.02
+    pos_tol: float = 1e-3
+    rot_tol: float = 1e-2
+
+
+def mixed_ik(n_problems: int = 4096, seed: int = 1004, n_obstacles: int = 500, seeds_range=(32, 256),
+             target_spread: float = 0.6, clearance: float = 0.03) -> MixedIkWorkload:
+    """Mixed persistent-batch IK: 40% 7-DOF chain, 30% 6-DOF chain, 20% 15-DOF
+    bimanual tree (two hand targets), 10% 29-DOF humanoid (two hand targets),
+    U{32..256} seeds per problem, 500 obstacle spheres.
+
+    As in ``ik``, each class's targets are FK of configurations within
+    +-target_spread rad of one nominal posture, and obstacle spheres (centres
+    U[-1.5,1.5]^3, radius U[0.05,0.2]) are kept only when every sphere of every
+    target configuration clears them by ``clearance``; seeds are uniform over
+    the joint limits.
+    """
+    from scipy.spatial import cKDTree
+
+    classes = mixed_classes(seed)
+    rng = np.random.default_rng(seed + 7)
+    fr = np.array([c.fraction for c in classes])
+    counts = np.floor(fr * n_problems).astype(int)
+    counts[0] += n_problems - counts.sum()
+    problem_class = np.repeat(np.arange(len(classes)), counts)
+    rng.shuffle(problem_class)
+    n_seeds = rng.integers(seeds_range[0], seeds_range[1] + 1, size=n_problems)
+    index_in_class = np.zeros(n_problems, np.int64)
+    for c in range(len(classes)):
+        idx = np.nonzero(problem_class == c)[0]
+        index_in_class[idx] = np.arange(len(idx))
+    target_T, target_cfgs, seeds, occupied, occ_r = [], [], [], [], []
+    for c, cl in enumerate(classes):
+        m = cl.model
+        Pc = int(counts[c])
+        nominal = m.random_cfgs(rng, 1)
+        cfgs = np.clip(nominal + rng.uniform(-target_spread, target_spread, size=(Pc, m.n_act)),
+                       m.lower, m.upper).astype(np.float32)
+        Tj = _scene_fk(m, cfgs)
+        tj = [m.link_joint(l) for l in cl.target_links]
+        target_T.append(Tj[:, tj].astype(np.float32))
+        target_cfgs.append(cfgs)
+        rs, jidx, _ = cl.spheres.flat_for_ik(m)
+        occupied.append(_sphere_world(m, rs, jidx, cfgs).reshape(-1, 3))
+        occ_r.append(np.tile(rs[:, 3], Pc))
+        sd = int(n_seeds[problem_class == c].max()) if Pc else 0
+        seeds.append(rng.uniform(m.lower, m.upper, size=(Pc, sd, m.n_act)).astype(np.float32))
+    occupied = np.concatenate(occupied)
+    occ_r = np.concatenate(occ_r)
+    tree = cKDTree(occupied)
+    r_max = float(occ_r.max())
+    obs = []
+    while len(obs) < n_obstacles:
+        o = np.concatenate([rng.uniform(-1.5, 1.5, 3), rng.uniform(0.05, 0.2, 1)])
+        near = tree.query_ball_point(o[:3], o[3] + r_max + clearance)
+        if not near or np.min(np.linalg.norm(occupied[near] - o[:3], axis=-1) - (occ_r[near] + o[3])) > clearance:
+            obs.append(o)
+    world = empty_world()
+    world.spheres = np.asarray(obs, np.float32).reshape(-1, 4)
+    return MixedIkWorkload(classes=classes, world=world, problem_class=problem_class, n_seeds=n_seeds,
+                           target_T=target_T, target_cfgs=target_cfgs, seeds=seeds,
+                           index_in_class=index_in_class)
