@@ -139,8 +139,10 @@ typedef struct pk_lm_options {
   int32_t enable_collision;
   float collision_weight;
   float collision_margin;
-  int32_t threads_per_seed; /* 0 = default (2); 1, 2, 4, 8 = lanes sharing one seed; 5 = one lane per line-search trial */
+  int32_t threads_per_seed; /* 0 = default (2); 1, 2, 4, 8 = lanes sharing one seed; 5 = one lane per line-search
+                              trial; 16, 32 = warp-per-seed body with that many lanes per seed */
   int32_t seeds_per_block;  /* 0 = choose automatically */
+  int32_t lanes_per_wide_seed; /* warp-per-seed body: lanes per seed, 16 (0 = default) or 32 */
 } pk_lm_options;
 
 /*

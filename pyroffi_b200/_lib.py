@@ -45,6 +45,7 @@ class LmOptions(C.Structure):
         ("collision_margin", _f32),
         ("threads_per_seed", _i32),
         ("seeds_per_block", _i32),
+        ("lanes_per_wide_seed", _i32),
     ]
 
 

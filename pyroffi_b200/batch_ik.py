@@ -12,7 +12,7 @@ a device counter until the list is empty.  The per-class FP64 verification
 and winner selection (``pk_ik_verify_select``) follow on the same stream.
 The whole solve can be captured once in a CUDA graph and replayed; an
 autotuner picks the seed-group kernel's lanes per seed and seeds per block
-by timing the actual batch.
+and the warp body's lanes per seed by timing the actual batch.
 
 It is the persistent form of calling ``ls_ik_solve_cuda_batch``
 (``src/pyroffi/optimization_engines/_ls_ik.py:1002-1172``) once per robot
@@ -55,7 +55,8 @@ class MixedIkBatch:
                  lambda_down: float = 0.1, lambda_up: float = 10.0, pos_weight: float = 50.0,
                  ori_weight: float = 10.0, collision_weight: float = 1e4, collision_margin: float = 0.02,
                  pos_tol: float = 1e-3, rot_tol: float = 1e-2, threads_per_seed: int = 0,
-                 seeds_per_block: int = 0, bodies=None, blocks: int = 0, device="cuda"):
+                 seeds_per_block: int = 0, lanes_per_wide_seed: int = 0, bodies=None, blocks: int = 0,
+                 device="cuda"):
         self.device = torch.device(device)
         self.classes = list(classes)
         if not 1 <= len(self.classes) <= 8:
@@ -69,7 +70,7 @@ class MixedIkBatch:
         coll = any(int(s.opt.enable_collision) for s in self.solvers)
         self.opt = _lib.LmOptions(max_iter, pos_weight, ori_weight, lambda_init, lambda_down, lambda_up,
                                   1e-8, 1e-8, int(coll), collision_weight, collision_margin,
-                                  threads_per_seed, seeds_per_block)
+                                  threads_per_seed, seeds_per_block, lanes_per_wide_seed)
         self.bodies = list(bodies) if bodies is not None else [
             default_body(c.model.n_act, s.n_ee) for c, s in zip(self.classes, self.solvers)]
         self.blocks = blocks
@@ -213,28 +214,34 @@ class MixedIkBatch:
         self._graph = g
 
     # -- autotuning ---------------------------------------------------------
-    def autotune(self, candidates=((2, 64), (4, 32), (1, 128), (8, 16)), reps: int = 2):
+    def autotune(self, candidates=((2, 64), (4, 32), (1, 128), (8, 16)), wide_lanes=(16, 32), reps: int = 2):
         """Time the prepared batch for each (threads_per_seed, seeds_per_block)
-        of the seed-group body (the item list is rebuilt for each, since the
-        item size is the block's seed count) and keep the fastest.  Returns
-        {(threads_per_seed, seeds_per_block): ms}."""
-        if not any(b == BODY_SEED_GROUP and self.counts[c] for c, b in enumerate(self.bodies)):
-            return {}
+        of the seed-group body and each lane count per seed of the warp body
+        (the item list is rebuilt for each, since a seed-group item holds one
+        block's seeds) and keep the fastest.  Returns
+        {(threads_per_seed, seeds_per_block, lanes_per_wide_seed): ms}."""
+        used = {b for c, b in enumerate(self.bodies) if self.counts[c]}
+        if BODY_SEED_GROUP not in used:
+            candidates = ((self.opt.threads_per_seed, self.opt.seeds_per_block),)
+        if BODY_WARP not in used:
+            wide_lanes = (self.opt.lanes_per_wide_seed,)
         results = {}
         for tps, spb in candidates:
-            self.opt.threads_per_seed, self.opt.seeds_per_block = tps, spb
-            self._build_items()
-            self.run_lm()
-            torch.cuda.synchronize(self.device)
-            ts = []
-            for _ in range(reps):
-                t0 = time.perf_counter()
+            for lanes in wide_lanes:
+                self.opt.threads_per_seed, self.opt.seeds_per_block = tps, spb
+                self.opt.lanes_per_wide_seed = lanes
+                self._build_items()
                 self.run_lm()
                 torch.cuda.synchronize(self.device)
-                ts.append(time.perf_counter() - t0)
-            results[(tps, spb)] = 1e3 * min(ts)
-        tps, spb = min(results, key=results.get)
-        self.opt.threads_per_seed, self.opt.seeds_per_block = tps, spb
+                ts = []
+                for _ in range(reps):
+                    t0 = time.perf_counter()
+                    self.run_lm()
+                    torch.cuda.synchronize(self.device)
+                    ts.append(time.perf_counter() - t0)
+                results[(tps, spb, lanes)] = 1e3 * min(ts)
+        tps, spb, lanes = min(results, key=results.get)
+        self.opt.threads_per_seed, self.opt.seeds_per_block, self.opt.lanes_per_wide_seed = tps, spb, lanes
         self._build_items()
         self._graph = None
         return results

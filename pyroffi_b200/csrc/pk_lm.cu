@@ -873,8 +873,13 @@ __device__ __forceinline__ void lm_seed_groups(const LmArgs& a, unsigned char* s
       continue;
     }
 
-    const float pen = penalty();
-    const float err = weighted_sq(r) + pen;
+    // The penalty is >= 0, so a trial whose pose error alone is not below
+    // the best trial so far cannot win (wsq + pen >= wsq in FP32 too): its
+    // penalty is skipped, which leaves every decision and output unchanged.
+    // (The test is uniform across the seed's lanes.)
+    const float wsq = weighted_sq(r);
+    const float pen = (ev < 0 || wsq < best_a_err) ? penalty() : 0.f;
+    const float err = wsq + pen;
     if (ev < 0) {
       pen_cur = pen;
       best_err = err;
@@ -1457,22 +1462,12 @@ static pk_ik_class class_of(const LmArgs& a) {
   return c;
 }
 
-static pk_lm_options options_of(const LmArgs& a) {
-  pk_lm_options o{};
-  o.max_iter = a.max_iter; o.pos_weight = a.pos_w; o.ori_weight = a.ori_w; o.lambda_init = a.lam0;
-  o.lambda_down = a.lam_down; o.lambda_up = a.lam_up; o.eps_pos = a.eps_pos; o.eps_ori = a.eps_ori;
-  o.enable_collision = a.coll; o.collision_weight = a.coll_w; o.collision_margin = a.margin;
-  return o;
-}
-
 static int launch_lm(LmArgs a, int tps, int spb, cudaStream_t st) {
   // threads_per_seed 5: the trial-lane kernel (5 lanes per seed, one
   // line-search trial each); 1, 2, 4, 8: the seed-group kernel with the
-  // collision penalty split across that many lanes; 32: one warp per seed
-  // (pk_lm_wide.cu), also taken for robots beyond the seed-group buckets
-  // (n_act > 16 or n_ee > 2); 0: the fastest measured default, 2 lanes x
-  // 64 seeds per block.
-  if (tps == 32 || a.n_act > 16 || a.n_ee > 2) return launch_warp_grid(class_of(a), a.w, options_of(a), st);
+  // collision penalty split across that many lanes; 0: the fastest measured
+  // default, 2 lanes x 64 seeds per block.  (16 and 32, the warp-per-seed
+  // body, are routed by lm_common.)
   if (tps <= 0) {
     tps = 2;
     if (spb <= 0) spb = 64;
@@ -1483,7 +1478,7 @@ static int launch_lm(LmArgs a, int tps, int spb, cudaStream_t st) {
     set_error("the LM kernel supports n_act <= 16 with n_ee <= 2 (got n_act=%d, n_ee=%d)", a.n_act, a.n_ee);
     return PK_ERR_CAPACITY;
   }
-  PK_CHECK_ARG(tps == 1 || tps == 2 || tps == 4 || tps == 8, "threads_per_seed must be 0, 1, 2, 4, 5, 8 or 32");
+  PK_CHECK_ARG(tps == 1 || tps == 2 || tps == 4 || tps == 8, "threads_per_seed must be 0, 1, 2, 4, 5, 8, 16 or 32");
   if (spb <= 0) spb = 128 / tps;
   PK_CHECK_ARG(spb * tps <= 128 && (spb * tps) % 32 == 0,
                "seeds_per_block * threads_per_seed must be a multiple of 32 and at most 128");
@@ -1547,6 +1542,14 @@ static int lm_common(void* stream, const pk_lm_options& o, const float* seeds, c
                "null world buffer");
   PK_CHECK_ARG(n_self == 0 || (self_i && self_j), "null self pairs");
   if (!a.coll) { a.n_self = 0; }
+  // threads_per_seed 16 or 32: the warp-per-seed body (pk_lm_wide.cu) with
+  // that many lanes per seed; robots beyond the seed-group kernel's buckets
+  // (n_act > 16 or n_ee > 2) take it too
+  if (o.threads_per_seed == 16 || o.threads_per_seed == 32 || a.n_act > 16 || a.n_ee > 2) {
+    pk_lm_options ow = o;
+    if (o.threads_per_seed == 16 || o.threads_per_seed == 32) ow.lanes_per_wide_seed = o.threads_per_seed;
+    return launch_warp_grid(class_of(a), a.w, ow, (cudaStream_t)stream);
+  }
   return launch_lm(a, o.threads_per_seed, o.seeds_per_block, (cudaStream_t)stream);
 }
 

@@ -375,12 +375,14 @@ __device__ inline void wide_stage_targets(const WideArgs& A, int pb, WideShared&
 }
 
 // ---------------------------------------------------------------------------
-// per-seed body (one warp)
+// per-seed body: a group of G lanes (G = 16: two seeds per warp; G = 32:
+// one) owns one seed; gl is the lane within the group, gm the group's mask.
 // ---------------------------------------------------------------------------
 
-__device__ __forceinline__ float w_warp_sum(float v) {
+template <int G>
+__device__ __forceinline__ float w_group_sum(float v, unsigned gm) {
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(gm, v, o);
   return v;
 }
 
@@ -407,10 +409,11 @@ __device__ __forceinline__ void w_store(float* T, int i, const Pose& P) {
 }
 
 // FK of configuration q (shared, n_act floats) into W.T, level by level.
-__device__ __forceinline__ void w_fk(const WideShared& sh, const float* q, const WideWarp& W, int lane) {
+template <int G>
+__device__ __forceinline__ void w_fk(const WideShared& sh, const float* q, const WideWarp& W, int gl, unsigned gm) {
   const JointTable& jt = sh.jt;
   for (int lv = 0; lv < sh.n_lvl; ++lv) {
-    for (int idx = sh.lvl_start[lv] + lane; idx < sh.lvl_start[lv + 1]; idx += 32) {
+    for (int idx = sh.lvl_start[lv] + gl; idx < sh.lvl_start[lv + 1]; idx += G) {
       const int i = sh.lvl_joint[idx];
       const int src = jt.src[i];
       const float qq = ((src < 0) ? 0.f : q[src]) * jt.mul[i] + jt.off[i];
@@ -418,14 +421,14 @@ __device__ __forceinline__ void w_fk(const WideShared& sh, const float* q, const
       const int p = jt.psorted[i];
       w_store(W.T, i, (p < 0) ? Tpc : pose_compose(w_load(W.T, p), Tpc));
     }
-    __syncwarp();
+    __syncwarp(gm);
   }
 }
 
 // Residual of every EE into W.r / W.pee (lane e), as the seed-group kernel's ee_residual.
-__device__ __forceinline__ void w_residual(const WideShared& sh, int n_ee, const WideWarp& W, int lane) {
-  if (lane < n_ee) {
-    const int e = lane;
+__device__ __forceinline__ void w_residual(const WideShared& sh, int n_ee, const WideWarp& W, int gl, unsigned gm) {
+  if (gl < n_ee) {
+    const int e = gl;
     const Pose T = w_load(W.T, sh.tsorted[e]);
     const float* g = sh.tgt[e];
     float* r = W.r + 6 * e;
@@ -445,12 +448,13 @@ __device__ __forceinline__ void w_residual(const WideShared& sh, int n_ee, const
     r[5] = qz * f;
     W.pee[3 * e] = T.tx; W.pee[3 * e + 1] = T.ty; W.pee[3 * e + 2] = T.tz;
   }
-  __syncwarp();
+  __syncwarp(gm);
 }
 
 // Collision penalty (before the weight) of the configuration whose poses are in W.T.
-__device__ float w_penalty(const WideLaunch& P, const WideShared& sh, const unsigned char* smem,
-                           const WideWarp& W, int lane) {
+template <int G>
+__device__ __noinline__ float w_penalty(const WideLaunch& P, const WideShared& sh, const unsigned char* smem,
+                                        const WideWarp& W, int gl, unsigned gm) {
   const WideLayout& L = P.L;
   const float4* rs4 = reinterpret_cast<const float4*>(smem + L.rs);
   const int* rsj = reinterpret_cast<const int*>(smem + L.rsj);
@@ -462,16 +466,16 @@ __device__ float w_penalty(const WideLaunch& P, const WideShared& sh, const unsi
   const int* cell_start = reinterpret_cast<const int*>(smem + L.cells);
   const unsigned short* cell_obs = reinterpret_cast<const unsigned short*>(smem + L.cell_obs);
   const int n_rs = sh.n_rs;
-  for (int k = lane; k < n_rs; k += 32) {
+  for (int k = gl; k < n_rs; k += G) {
     const float4 s = rs4[k];
     const float3 p = pose_apply(w_load(W.T, sh.js_joint[rsj[k]]), make_float3(s.x, s.y, s.z));
     W.pos[k] = make_float4(p.x, p.y, p.z, s.w);
   }
-  __syncwarp();
+  __syncwarp(gm);
   float pen = 0.f;
   const int Ms = P.w.Ms;
   if (Ms > 0) {
-    for (int j = lane; j < sh.n_js; j += 32) {
+    for (int j = gl; j < sh.n_js; j += G) {
       const float4 bl = sh.jb[j];
       const float3 B = pose_apply(w_load(W.T, sh.js_joint[j]), make_float3(bl.x, bl.y, bl.z));
       const int k0 = sh.jstart[j], k1 = sh.jstart[j + 1];
@@ -504,7 +508,7 @@ __device__ float w_penalty(const WideLaunch& P, const WideShared& sh, const unsi
   }
   const float margin = P.margin;
   if (P.w.Mc + P.w.Mb + P.w.Mh > 0) {
-    for (int k = lane; k < n_rs; k += 32) {
+    for (int k = gl; k < n_rs; k += G) {
       const float4 q = W.pos[k];
       const float3 p = make_float3(q.x, q.y, q.z);
       for (int m = 0; m < P.w.Mc; ++m) {
@@ -521,14 +525,14 @@ __device__ float w_penalty(const WideLaunch& P, const WideShared& sh, const unsi
       }
     }
   }
-  for (int q = lane; q < sh.n_pairs; q += 32) {
+  for (int q = gl; q < sh.n_pairs; q += G) {
     const int2 pr = pairs[q];
     const float4 a = W.pos[pr.x], b = W.pos[pr.y];
     const float ex = a.x - b.x, ey = a.y - b.y, ez = a.z - b.z;
     w_hinge(ex * ex + ey * ey + ez * ez, a.w + b.w + margin, pen);
   }
-  pen = w_warp_sum(pen);
-  __syncwarp();
+  pen = w_group_sum<G>(pen, gm);
+  __syncwarp(gm);
   return pen;
 }
 
@@ -544,16 +548,17 @@ __device__ __forceinline__ float w_weighted_sq(const WideWarp& W, int n_ee, cons
 
 // Damped step of the current point into W.dact (all actuated entries);
 // returns ||fw||^2.  Poses of the current point are in W.T, its residual in W.r.
-__device__ float w_direction(const WideShared& sh, int n_act, int n_ee, const float (&Wt)[6], float lam,
-                             float max_p, float max_o, const WideWarp& W, int lane) {
+template <int G, int MAXEE>
+__device__ __noinline__ float w_direction(const WideShared& sh, int n_act, int n_ee, const float (&Wt)[6], float lam,
+                                          float max_p, float max_o, const WideWarp& W, int gl, unsigned gm) {
   const JointTable& jt = sh.jt;
   const int ncol = sh.ncol, rows = 6 * n_ee;
-  // Jacobian column `lane`: weighted, Jacobi-scaled, stored column-major
-  if (lane < ncol) {
-    float Jc[W_MAXROWS];
+  // Jacobian columns c = gl, gl + G, ...: weighted, Jacobi-scaled, column-major
+  for (int c = gl; c < ncol; c += G) {
+    float Jc[6 * MAXEE];
 #pragma unroll
-    for (int k = 0; k < W_MAXROWS; ++k) Jc[k] = 0.f;
-    for (int t = sh.col_start[lane]; t < sh.col_start[lane + 1]; ++t) {
+    for (int k = 0; k < 6 * MAXEE; ++k) Jc[k] = 0.f;
+    for (int t = sh.col_start[c]; t < sh.col_start[c + 1]; ++t) {
       const int i = sh.col_joint[t];
       const float wt = sh.col_w[t];
       const Pose Tj = w_load(W.T, i);
@@ -561,7 +566,7 @@ __device__ float w_direction(const WideShared& sh, int n_act, int n_ee, const fl
       const int orig = jt.orig[i];
       const bool rev = jt.jkind[i] == 1;
 #pragma unroll
-      for (int e = 0; e < PK_MAX_EE; ++e) {
+      for (int e = 0; e < MAXEE; ++e) {
         if (e >= n_ee || !((sh.anc[e] >> orig) & 1ull)) continue;
         float col[6];
         if (rev) {
@@ -577,77 +582,76 @@ __device__ float w_direction(const WideShared& sh, int n_act, int n_ee, const fl
     }
     float sq = 0.f;
 #pragma unroll
-    for (int k = 0; k < W_MAXROWS; ++k) {
+    for (int k = 0; k < 6 * MAXEE; ++k) {
       if (k < rows) {
         Jc[k] *= Wt[k % 6];
         sq += Jc[k] * Jc[k];
       }
     }
     const float s = sqrtf(sq) + 1e-8f;
-    W.cs[lane] = s;
+    W.cs[c] = s;
 #pragma unroll
-    for (int k = 0; k < W_MAXROWS; ++k)
-      if (k < rows) W.J[lane * rows + k] = Jc[k] / s;
+    for (int k = 0; k < 6 * MAXEE; ++k)
+      if (k < rows) W.J[c * rows + k] = Jc[k] / s;
   }
-  if (lane < rows) W.fw[lane] = W.r[lane] * Wt[lane % 6];
-  __syncwarp();
+  for (int k = gl; k < rows; k += G) W.fw[k] = W.r[k] * Wt[k % 6];
+  __syncwarp(gm);
   float fw2 = 0.f;
   for (int k = 0; k < rows; ++k) fw2 += W.fw[k] * W.fw[k];
 
   // FP64 normal equations, packed lower triangle: lane j computes A[i][j]
   for (int i = 0; i < ncol; ++i) {
-    const int j = lane;
-    if (j <= i) {
+    for (int j = gl; j <= i; j += G) {
       double acc = 0.0;
       for (int k = 0; k < rows; ++k) acc += (double)W.J[i * rows + k] * (double)W.J[j * rows + k];
       if (i == j) acc += (double)lam;
       W.A[i * (i + 1) / 2 + j] = acc;
     }
   }
-  if (lane < ncol) {
+  for (int i = gl; i < ncol; i += G) {
     double rb = 0.0;
-    for (int k = 0; k < rows; ++k) rb += (double)W.J[lane * rows + k] * (double)W.fw[k];
-    W.y[lane] = -rb;
+    for (int k = 0; k < rows; ++k) rb += (double)W.J[i * rows + k] * (double)W.fw[k];
+    W.y[i] = -rb;
   }
-  __syncwarp();
+  __syncwarp(gm);
 
-  // Cholesky A = L L^T, left-looking; a non-positive pivot zeroes the step
+  // Cholesky A = L L^T, left-looking; a non-positive pivot zeroes the step.
+  // The diagonal keeps 1 / L[k][k] (every later use multiplies by it).
   bool ok = true;
   for (int k = 0; k < ncol; ++k) {
     const int kk = k * (k + 1) / 2;
     double s2 = W.A[kk + k];
     for (int q = 0; q < k; ++q) s2 -= W.A[kk + q] * W.A[kk + q];
     if (!(s2 > 0.0)) ok = false;
-    const double lkk = sqrt(ok ? s2 : 1.0);
-    const double inv = 1.0 / lkk;
-    for (int i = k + 1 + lane; i < ncol; i += 32) {
+    const double inv = 1.0 / sqrt(ok ? s2 : 1.0);
+    for (int i = k + 1 + gl; i < ncol; i += G) {
       const int ii = i * (i + 1) / 2;
       double tt = W.A[ii + k];
       for (int q = 0; q < k; ++q) tt -= W.A[ii + q] * W.A[kk + q];
       W.A[ii + k] = tt * inv;
     }
-    __syncwarp();
-    if (lane == 0) W.A[kk + k] = lkk;
-    __syncwarp();
+    __syncwarp(gm);
+    if (gl == 0) W.A[kk + k] = inv;
+    __syncwarp(gm);
   }
   // L y = b, then L^T x = y (column by column; x overwrites y)
   for (int i = 0; i < ncol; ++i) {
-    const double yi = W.y[i] / W.A[i * (i + 1) / 2 + i];
-    for (int j = i + 1 + lane; j < ncol; j += 32) W.y[j] -= W.A[j * (j + 1) / 2 + i] * yi;
-    __syncwarp();
-    if (lane == 0) W.y[i] = yi;
-    __syncwarp();
+    const double yi = W.y[i] * W.A[i * (i + 1) / 2 + i];
+    for (int j = i + 1 + gl; j < ncol; j += G) W.y[j] -= W.A[j * (j + 1) / 2 + i] * yi;
+    __syncwarp(gm);
+    if (gl == 0) W.y[i] = yi;
+    __syncwarp(gm);
   }
   for (int i = ncol - 1; i >= 0; --i) {
     const int ii = i * (i + 1) / 2;
-    const double xi = W.y[i] / W.A[ii + i];
-    for (int j = lane; j < i; j += 32) W.y[j] -= W.A[ii + j] * xi;
-    __syncwarp();
-    if (lane == 0) W.y[i] = xi;
-    __syncwarp();
+    const double xi = W.y[i] * W.A[ii + i];
+    for (int j = gl; j < i; j += G) W.y[j] -= W.A[ii + j] * xi;
+    __syncwarp(gm);
+    if (gl == 0) W.y[i] = xi;
+    __syncwarp(gm);
   }
-  if (lane < ncol) W.dcol[lane] = ok ? (float)W.y[lane] / W.cs[lane] : 0.f;
-  __syncwarp();
+  for (int c = gl; c < ncol; c += G) W.dcol[c] = ok ? (float)W.y[c] / W.cs[c] : 0.f;
+  __syncwarp(gm);
   float dn2 = 0.f;
   for (int c = 0; c < ncol; ++c) dn2 += W.dcol[c] * W.dcol[c];
   float R;
@@ -657,10 +661,10 @@ __device__ float w_direction(const WideShared& sh, int n_act, int n_ee, const fl
   else R = 0.05f;
   const float dn = sqrtf(dn2);
   const float sc = (dn > R) ? R / (dn + 1e-18f) : 1.f;
-  for (int a = lane; a < n_act; a += 32) W.dact[a] = 0.f;
-  __syncwarp();
-  if (lane < ncol) W.dact[sh.col_act[lane]] = (dn > R) ? W.dcol[lane] * sc : W.dcol[lane];
-  __syncwarp();
+  for (int a = gl; a < n_act; a += G) W.dact[a] = 0.f;
+  __syncwarp(gm);
+  for (int c = gl; c < ncol; c += G) W.dact[sh.col_act[c]] = (dn > R) ? W.dcol[c] * sc : W.dcol[c];
+  __syncwarp(gm);
   return fw2;
 }
 
@@ -669,22 +673,23 @@ __device__ __forceinline__ float w_alpha(int i) {
 }
 
 // LM for flat seed index gs of class A (targets of its problem staged).
+template <int G, int MAXEE>
 __device__ void w_seed(const WideLaunch& P, const WideArgs& A, const WideShared& sh, const unsigned char* smem,
-                       const WideWarp& W, size_t gs, int lane) {
+                       const WideWarp& W, size_t gs, int gl, unsigned gm) {
   const int n_act = A.n_act, n_ee = A.n_ee;
   const float Wt[6] = {P.pos_w, P.pos_w, P.pos_w, P.ori_w, P.ori_w, P.ori_w};
   const bool use_coll = P.coll && sh.n_rs > 0;
-  for (int a = lane; a < n_act; a += 32) {
+  for (int a = gl; a < n_act; a += G) {
     const float v = A.seeds[gs * n_act + a];
     W.cfg[a] = v;
     W.best[a] = v;
     W.dact[a] = 0.f;
   }
-  __syncwarp();
+  __syncwarp(gm);
   auto evaluate = [&](const float* q, float& pen) {
-    w_fk(sh, q, W, lane);
-    w_residual(sh, n_ee, W, lane);
-    pen = use_coll ? P.coll_w * w_penalty(P, sh, smem, W, lane) : 0.f;
+    w_fk<G>(sh, q, W, gl, gm);
+    w_residual(sh, n_ee, W, gl, gm);
+    pen = use_coll ? P.coll_w * w_penalty<G>(P, sh, smem, W, gl, gm) : 0.f;
     return w_weighted_sq(W, n_ee, Wt) + pen;
   };
   float pen_cur;
@@ -692,8 +697,8 @@ __device__ void w_seed(const WideLaunch& P, const WideArgs& A, const WideShared&
   float lam = P.lam0;
   for (int it = 0; it < P.max_iter; ++it) {
     // current point: poses and residual (its penalty is carried), convergence, damped step
-    w_fk(sh, W.cfg, W, lane);
-    w_residual(sh, n_ee, W, lane);
+    w_fk<G>(sh, W.cfg, W, gl, gm);
+    w_residual(sh, n_ee, W, gl, gm);
     bool all_conv = true;
     float max_p = 0.f, max_o = 0.f;
     for (int e = 0; e < n_ee; ++e) {
@@ -705,28 +710,34 @@ __device__ void w_seed(const WideLaunch& P, const WideArgs& A, const WideShared&
       max_o = fmaxf(max_o, no);
     }
     if (all_conv) break;
-    const float curr = w_direction(sh, n_act, n_ee, Wt, lam, max_p, max_o, W, lane) + pen_cur;
+    const float curr = w_direction<G, MAXEE>(sh, n_act, n_ee, Wt, lam, max_p, max_o, W, gl, gm) + pen_cur;
     // line search: first minimum over the 5 step sizes
     float best_a_err = 1e30f, best_a_pen = pen_cur;
     int best_a = 0;
     for (int t = 0; t < 5; ++t) {
       const float al = w_alpha(t);
-      for (int a = lane; a < n_act; a += 32)
+      for (int a = gl; a < n_act; a += G)
         W.trial[a] = fmaxf(sh.lo[a], fminf(sh.hi[a], W.cfg[a] + al * W.dact[a]));
-      __syncwarp();
-      float pen;
-      const float err = evaluate(W.trial, pen);
+      __syncwarp(gm);
+      // a trial whose pose error alone cannot beat the best trial skips its
+      // penalty (>= 0), which changes no decision or output
+      w_fk<G>(sh, W.trial, W, gl, gm);
+      w_residual(sh, n_ee, W, gl, gm);
+      const float wsq = w_weighted_sq(W, n_ee, Wt);
+      if (!(wsq < best_a_err)) continue;
+      const float pen = use_coll ? P.coll_w * w_penalty<G>(P, sh, smem, W, gl, gm) : 0.f;
+      const float err = wsq + pen;
       if (err < best_a_err) { best_a_err = err; best_a = t; best_a_pen = pen; }
     }
     const float al = w_alpha(best_a);
     const bool accept = best_a_err < curr * (1.0f - 1e-4f);
     const bool improve = best_a_err < best_err;
-    for (int a = lane; a < n_act; a += 32) {
+    for (int a = gl; a < n_act; a += G) {
       const float tv = fmaxf(sh.lo[a], fminf(sh.hi[a], W.cfg[a] + al * W.dact[a]));
       if (improve) W.best[a] = tv;
       if (accept) W.cfg[a] = tv;
     }
-    __syncwarp();
+    __syncwarp(gm);
     if (accept) {
       pen_cur = best_a_pen;
       lam = fmaxf(lam * P.lam_down, 1e-10f);
@@ -735,17 +746,17 @@ __device__ void w_seed(const WideLaunch& P, const WideArgs& A, const WideShared&
     }
     if (improve) best_err = best_a_err;
   }
-  for (int a = lane; a < n_act; a += 32) A.out_cfg[gs * n_act + a] = W.best[a];
-  if (lane == 0) A.out_err[gs] = best_err;
-  __syncwarp();
+  for (int a = gl; a < n_act; a += G) A.out_cfg[gs * n_act + a] = W.best[a];
+  if (gl == 0) A.out_err[gs] = best_err;
+  __syncwarp(gm);
 }
 
 // ---------------------------------------------------------------------------
 // kernels
 // ---------------------------------------------------------------------------
 
-__device__ __forceinline__ WideWarp w_warp_area(const WideLayout& L, unsigned char* smem, int warp) {
-  unsigned char* b = smem + L.warps + L.warp_bytes * warp;
+__device__ __forceinline__ WideWarp w_group_area(const WideLayout& L, unsigned char* smem, int group) {
+  unsigned char* b = smem + L.warps + L.warp_bytes * group;
   WideWarp W;
   W.cfg = reinterpret_cast<float*>(b + L.w_cfg);
   W.best = reinterpret_cast<float*>(b + L.w_best);
@@ -767,15 +778,17 @@ __device__ __forceinline__ WideWarp w_warp_area(const WideLayout& L, unsigned ch
 // Grid launch (P.queue == null): block (x, y) runs seeds [x * chunk, ...) of
 // problem y of class 0.  Persistent launch: blocks take items from the list
 // through the counter P.queue[0] until it runs out, skipping items of
-// classes that use the other body.
-
+// classes that use the other body.  Groups of G lanes take the item's seeds
+// in turn.
+template <int G, int MAXEE>
 __global__ void __launch_bounds__(256, 2) lm_warp_kernel(const __grid_constant__ WideLaunch P) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_item;
   __shared__ WideArgs s_args;
   WideShared& sh = *reinterpret_cast<WideShared*>(smem);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-  const WideWarp W = w_warp_area(P.L, smem, warp);
+  const int group = threadIdx.x / G, gl = threadIdx.x % G, ngroups = blockDim.x / G;
+  const unsigned gm = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));
+  const WideWarp W = w_group_area(P.L, smem, group);
   int staged_cls = -1, staged_pb = -1;
   for (int round = 0;; ++round) {
     int4 item;
@@ -815,8 +828,8 @@ __global__ void __launch_bounds__(256, 2) lm_warp_kernel(const __grid_constant__
       __syncthreads();
       staged_pb = item.y;
     }
-    for (int s = warp; s < item.w; s += nwarps)
-      w_seed(P, A, sh, smem, W, (size_t)item.y * A.seed_stride + item.z + s, lane);
+    for (int s = group; s < item.w; s += ngroups)
+      w_seed<G, MAXEE>(P, A, sh, smem, W, (size_t)item.y * A.seed_stride + item.z + s, gl, gm);
     __syncthreads();
   }
 }
@@ -846,8 +859,10 @@ static void wide_options(WideLaunch& P, const pk_lm_options& o) {
 
 static constexpr int kWideThreads = 256;
 
+static int wide_group(const pk_lm_options& o) { return o.lanes_per_wide_seed == 32 ? 32 : 16; }
+
 // Layout for the warp-body classes of P; PK_ERR_CAPACITY when it does not fit.
-static int wide_prepare(WideLaunch& P, int max_smem) {
+static int wide_prepare(WideLaunch& P, int max_smem, int G, int* max_ee_out) {
   int max_rs = 0, max_self = 0, max_joints = 1, max_act = 1, max_ee = 1;
   for (int c = 0; c < P.n_classes; ++c) {
     if (P.body[c] != kBodyWarp) continue;
@@ -858,10 +873,42 @@ static int wide_prepare(WideLaunch& P, int max_smem) {
     max_act = std::max(max_act, a.n_act);
     max_ee = std::max(max_ee, a.n_ee);
   }
-  P.L = wide_layout(max_rs, max_self, max_joints, max_act, max_ee, P.w, kWideThreads / 32);
+  P.L = wide_layout(max_rs, max_self, max_joints, max_act, max_ee, P.w, kWideThreads / G);
+  *max_ee_out = max_ee;
   PK_CHECK_CAP(P.L.total <= (size_t)max_smem,
                "warp-body LM working set (%zu B of shared memory) exceeds %d B", P.L.total, max_smem);
   return PK_OK;
+}
+
+template <int G, int MAXEE>
+static int run_warp_t(const WideLaunch& P, dim3 grid, bool persistent, int blocks, cudaStream_t st, int* launched) {
+  auto kern = lm_warp_kernel<G, MAXEE>;
+  if (int s = set_smem_limit((const void*)kern, P.L.total)) return s;
+  if (persistent) {
+    if (blocks <= 0) {
+      int dev = 0, sms = 0, per_sm = 0;
+      if (int s = cuda_status(cudaGetDevice(&dev), "cudaGetDevice")) return s;
+      if (int s = cuda_status(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attribute"))
+        return s;
+      if (int s = cuda_status(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kWideThreads, P.L.total),
+                              "occupancy"))
+        return s;
+      blocks = std::max(1, sms * std::max(per_sm, 1));
+    }
+    grid = dim3(blocks);
+  }
+  kern<<<grid, kWideThreads, P.L.total, st>>>(P);
+  if (launched) ++*launched;
+  return cuda_status(cudaGetLastError(), "lm_warp_kernel launch");
+}
+
+static int run_warp(const WideLaunch& P, int G, int max_ee, dim3 grid, bool persistent, int blocks, cudaStream_t st,
+                    int* launched) {
+  if (G == 32)
+    return max_ee <= 2 ? run_warp_t<32, 2>(P, grid, persistent, blocks, st, launched)
+                       : run_warp_t<32, 4>(P, grid, persistent, blocks, st, launched);
+  return max_ee <= 2 ? run_warp_t<16, 2>(P, grid, persistent, blocks, st, launched)
+                     : run_warp_t<16, 4>(P, grid, persistent, blocks, st, launched);
 }
 
 static int validate_wide_class(const pk_ik_class& c, bool coll) {
@@ -891,6 +938,7 @@ static int device_smem_optin(int* out) {
 int launch_warp_grid(const pk_ik_class& c, const WorldArgs& w, const pk_lm_options& opt, cudaStream_t st) {
   if (int s = validate_wide_class(c, opt.enable_collision != 0)) return s;
   if (c.n_problems == 0 || c.seed_stride == 0) return PK_OK;
+  PK_CHECK_CAP(c.n_problems <= 65535, "n_problems=%d exceeds the grid limit 65535", c.n_problems);
   WideLaunch P{};
   P.cls[0] = wide_args(c);
   P.body[0] = kBodyWarp;
@@ -898,15 +946,13 @@ int launch_warp_grid(const pk_ik_class& c, const WorldArgs& w, const pk_lm_optio
   P.w = w;
   wide_options(P, opt);
   P.queue = nullptr;
-  P.grid_chunk = 2 * (kWideThreads / 32);
-  int max_smem = 0;
+  const int G = wide_group(opt);
+  P.grid_chunk = 2 * (kWideThreads / G);
+  int max_smem = 0, max_ee = 1;
   if (int s = device_smem_optin(&max_smem)) return s;
-  if (int s = wide_prepare(P, max_smem)) return s;
-  if (int s = set_smem_limit((const void*)lm_warp_kernel, P.L.total)) return s;
-  dim3 grid((c.seed_stride + P.grid_chunk - 1) / P.grid_chunk, c.n_problems);
-  PK_CHECK_CAP(c.n_problems <= 65535, "n_problems=%d exceeds the grid limit 65535", c.n_problems);
-  lm_warp_kernel<<<grid, kWideThreads, P.L.total, st>>>(P);
-  return cuda_status(cudaGetLastError(), "lm_warp_kernel launch");
+  if (int s = wide_prepare(P, max_smem, G, &max_ee)) return s;
+  const dim3 grid((c.seed_stride + P.grid_chunk - 1) / P.grid_chunk, c.n_problems);
+  return run_warp(P, G, max_ee, grid, false, 0, st, nullptr);
 }
 
 int launch_warp_batch(const BatchCall& b, cudaStream_t st, int* launched) {
@@ -927,25 +973,11 @@ int launch_warp_batch(const BatchCall& b, cudaStream_t st, int* launched) {
   P.items = b.items;
   P.n_items = b.n_items;
   P.queue = b.queue + 1;
-  int max_smem = 0;
+  const int G = wide_group(b.opt);
+  int max_smem = 0, max_ee = 1;
   if (int s = device_smem_optin(&max_smem)) return s;
-  if (int s = wide_prepare(P, max_smem)) return s;
-  if (int s = set_smem_limit((const void*)lm_warp_kernel, P.L.total)) return s;
-  int blocks = b.blocks;
-  if (blocks <= 0) {
-    int dev = 0, sms = 0, per_sm = 0;
-    if (int s = cuda_status(cudaGetDevice(&dev), "cudaGetDevice")) return s;
-    if (int s = cuda_status(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attribute"))
-      return s;
-    if (int s = cuda_status(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lm_warp_kernel, kWideThreads,
-                                                                          P.L.total),
-                            "occupancy"))
-      return s;
-    blocks = std::max(1, sms * std::max(per_sm, 1));
-  }
-  lm_warp_kernel<<<blocks, kWideThreads, P.L.total, st>>>(P);
-  if (launched) ++*launched;
-  return cuda_status(cudaGetLastError(), "lm_warp_kernel launch");
+  if (int s = wide_prepare(P, max_smem, G, &max_ee)) return s;
+  return run_warp(P, G, max_ee, dim3(1), true, b.blocks, st, launched);
 }
 
 }  // namespace pk

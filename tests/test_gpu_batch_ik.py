@@ -52,7 +52,7 @@ def class_oracle(w, c, p, seeds, max_iter):
                      ws=w.world.spheres)
 
 
-@pytest.mark.parametrize("c,tps", [(3, 0), (2, 32), (0, 32)])
+@pytest.mark.parametrize("c,tps", [(3, 0), (3, 32), (2, 16), (2, 32), (0, 16)])
 @pytest.mark.parametrize("max_iter", [0, 1, 2])
 def test_warp_body_few_iterations_vs_oracle(mixed, c, tps, max_iter):
     w = mixed
@@ -91,7 +91,7 @@ def per_class_reference(w, b):
         if b.counts[c] == 0:
             out.append(None)
             continue
-        tps = 2 if b.bodies[c] == BODY_SEED_GROUP else 32
+        tps = 2 if b.bodies[c] == BODY_SEED_GROUP else 16
         s = BatchIkSolver(cl.model, cl.target_links, spheres=cl.spheres, world=w.world, device=DEV,
                           **opts(w, threads_per_seed=tps, seeds_per_block=64 if tps == 2 else 0))
         out.append(s.run_lm(b.targets[c], b.seeds[c]))
@@ -155,8 +155,8 @@ def test_batch_autotune_keeps_results(mixed):
     b = make_batch(w)
     b.run_lm()
     base = [e.clone() for e in b.out_err]
-    res = b.autotune(candidates=((2, 64), (4, 32)), reps=1)
-    assert set(res) == {(2, 64), (4, 32)}
+    res = b.autotune(candidates=((2, 64), (4, 32)), wide_lanes=(16, 32), reps=1)
+    assert set(res) == {(2, 64, 16), (2, 64, 32), (4, 32, 16), (4, 32, 32)}
     b.run_lm()
     # lanes per seed change the order of the penalty sum only; an accept test
     # on the edge may flip for a few seeds
