@@ -225,6 +225,26 @@ int pk_ik_batch(void* stream, const pk_lm_options* opt, const pk_ik_class* class
                 const int32_t* items, int32_t n_items, int32_t* queue, int32_t blocks);
 
 /*
+ * pk_ik_batch for callers that cannot allocate device memory when they
+ * solve (a handler inside a runtime that owns the device memory and gives
+ * this call no workspace, a real-time loop that must not allocate once it
+ * runs).  No counterpart in the reference.  Same arguments and results as
+ * pk_ik_batch without `queue`: the two work-queue counters live in a
+ * 256-byte array compiled into the library (it stays on every GPU that
+ * loaded the library until the process exits).  The first call on a device
+ * looks up that array's device address (cudaGetSymbolAddress), so make it
+ * before any stream capture.  Every call shares the array and clears the
+ * counters on `stream` before it starts: calls whose kernels overlap on the
+ * GPU (different streams, or different host threads) race on the counters
+ * and must be serialised by the caller.  A call that would need more
+ * counters than the array holds returns PK_ERR_CAPACITY.  Allocates nothing.
+ */
+int pk_ik_batch_static(void* stream, const pk_lm_options* opt, const pk_ik_class* classes, int32_t n_classes,
+                       const float* world_spheres, const float* world_capsules, const float* world_boxes,
+                       const float* world_halfspaces, int32_t Ms, int32_t Mc, int32_t Mb, int32_t Mh,
+                       const int32_t* items, int32_t n_items, int32_t blocks);
+
+/*
  * FP64 re-verification and winner selection (no reference counterpart; it
  * replaces the argmin of _ls_ik_solve_cuda_batch_jit,
  * src/pyroffi/optimization_engines/_ls_ik.py:974-999, and the FP64 check of

@@ -63,6 +63,7 @@ SIGNATURES: dict[str, list] = {
     "pk_ik_verify_select": [_p] * 4 + [_f32] + [_p] * 10 + [_f32, _f32] + [_p] * 4 + [_i32] * 5,
     "pk_fk_sphere_collision": [_p] * 20 + [_i64] + [_i32] * 8,
     "pk_ik_batch": [_p, C.POINTER(LmOptions), C.c_void_p, _i32] + [_p] * 4 + [_i32] * 4 + [_p, _i32, _p, _i32],
+    "pk_ik_batch_static": [_p, C.POINTER(LmOptions), C.c_void_p, _i32] + [_p] * 4 + [_i32] * 4 + [_p, _i32, _i32],
     "pk_fp32_fma_peak": [_p, _p, _i32, _i32],
     "pk_traj_cost_grad": [_p, C.c_void_p] + [_p] * 22 + [_i64] + [_i32] * 10,
 }

@@ -1744,3 +1744,59 @@ extern "C" int pk_ik_batch(void* stream, const pk_lm_options* opt, const pk_ik_c
   if (int s = launch_warp_batch(b, st, &launched)) return s;
   return launch_seed_group_batch(b, st, &launched);
 }
+
+// ---------------------------------------------------------------------------
+// pk_ik_batch_static: pk_ik_batch without caller-provided device memory.
+//
+// Some callers cannot allocate device memory at the time they solve: a
+// handler inside a runtime that owns all device memory and offers this call
+// no workspace, or a real-time control loop that must not allocate once it
+// runs.  This entry keeps the persistent kernels' only scratch -- the two
+// work-queue counters -- in a fixed array that is part of the library
+// image, so the call needs no allocation at all.
+// ---------------------------------------------------------------------------
+
+#include <mutex>
+
+#define PK_STATIC_QUEUE_INTS 64  // 256 bytes; one call needs 2
+
+namespace {
+
+// Loaded with the library on every GPU that runs it and kept until exit.
+static __device__ __align__(256) int32_t g_static_queue[PK_STATIC_QUEUE_INTS];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_static_mutex;
+int32_t* g_static_ptr[kMaxDevices] = {};
+
+// Device address of g_static_queue on the current device, looked up once per
+// device (host code only sees a stand-in for the symbol, never its address).
+int static_queue_address(int32_t** out) {
+  int dev = 0;
+  if (int s = cuda_status(cudaGetDevice(&dev), "cudaGetDevice")) return s;
+  PK_CHECK_CAP(dev >= 0 && dev < kMaxDevices, "device %d beyond the %d devices this entry supports", dev, kMaxDevices);
+  std::lock_guard<std::mutex> lock(g_static_mutex);
+  if (!g_static_ptr[dev]) {
+    void* p = nullptr;
+    if (int s = cuda_status(cudaGetSymbolAddress(&p, g_static_queue), "cudaGetSymbolAddress")) return s;
+    g_static_ptr[dev] = static_cast<int32_t*>(p);
+  }
+  *out = g_static_ptr[dev];
+  return PK_OK;
+}
+
+}  // namespace
+
+extern "C" int pk_ik_batch_static(void* stream, const pk_lm_options* opt, const pk_ik_class* classes,
+                                  int32_t n_classes, const float* world_spheres, const float* world_capsules,
+                                  const float* world_boxes, const float* world_halfspaces, int32_t Ms, int32_t Mc,
+                                  int32_t Mb, int32_t Mh, const int32_t* items, int32_t n_items, int32_t blocks) {
+  const int needed = 2;  // item counters of the two persistent kernels
+  PK_CHECK_CAP(needed <= PK_STATIC_QUEUE_INTS, "the call needs %d queue counters, the static area holds %d", needed,
+               PK_STATIC_QUEUE_INTS);
+  int32_t* queue = nullptr;
+  if (int s = static_queue_address(&queue)) return s;
+  // pk_ik_batch clears the counters with an async memset on `stream` before its launches
+  return pk_ik_batch(stream, opt, classes, n_classes, world_spheres, world_capsules, world_boxes, world_halfspaces,
+                     Ms, Mc, Mb, Mh, items, n_items, queue, blocks);
+}
