@@ -42,6 +42,8 @@ P_PER_GPU, SEEDS, ITERS = 256, 128, 30
 # + Jacobian 45*7 + normal equations and Cholesky ~800
 FLOP_PER_SEED_ITER = 6 * (130 * 7 + 60 + 33 * 56 + 12 * 56 * 100 + 12 * 200) + 45 * 7 + 800
 L2_FLUSH_BYTES = 256 << 20
+# DRAM bytes (read + write) of one launch of the LM kernel on this workload, from one ncu capture
+LM_DRAM_BYTES_PER_LAUNCH = 1080320 + 1336064
 
 
 def parse():
@@ -52,6 +54,7 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-sample", type=int, default=8, help="problems per CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true", help="skip the configs 1, 3, 4, 5 measurements")
     return ap.parse_args()
 
 
@@ -354,18 +357,172 @@ def run_ours(args):
             "gpu_launches": 2 * args.steps,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": None, "kernel": "lm_kernel<8,1,2>",
+                         "frac": achieved / peak, "traffic": LM_DRAM_BYTES_PER_LAUNCH,
+                         "traffic_unit": "bytes per launch (ncu dram__bytes_read+write, profiles/lm_kernel_ik_256x128.md)",
+                         "kernel": "lm_kernel<8,1,2>",
                          "peak_source": "measured FP32 FMA microbenchmark (pk_fp32_fma_peak), this run",
                          "flop_per_seed_iter": FLOP_PER_SEED_ITER},
             "kernel_ms": {"lm": statistics.mean(lm_ms), "verify_select": statistics.mean(step_ms) - statistics.mean(lm_ms)},
             "clocks": clock_summary,
             "cpu_baseline": cpu,
         }
+        if not args.no_secondary:
+            line["secondary"] = secondary_metrics(torch, dev, peak)
         print(json.dumps(line))
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+# ---------------------------------------------------------------------------
+# Secondary workloads (configs 1, 3, 4 and 5), one GPU, device-timed
+# ---------------------------------------------------------------------------
+
+def _timed_ms(torch, fn, flush, reps=5, warm=3):
+    """Median CUDA-event time of fn() on the current stream, L2 flushed before each rep."""
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+        flush.fill_(1.0)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        b.synchronize()
+        ts.append(a.elapsed_time(b))
+    return statistics.median(ts)
+
+
+def secondary_metrics(torch, dev, fp32_peak):
+    """Configs 1 (FK + sphere collision), 3 (trajectory cost + adjoint), 4
+    (mixed persistent batch IK) and 5 (FK + collision bandwidth sweep),
+    each against its roofline.  Seeded synthetic inputs, resident in HBM."""
+    from pyroffi_b200 import workloads as W
+    from pyroffi_b200.batch_ik import MixedIkBatch
+    from pyroffi_b200.collision import FkCollisionResult, fk_sphere_collision
+    from pyroffi_b200.device import DeviceRobot, DeviceSpheres, DeviceWorld
+    from pyroffi_b200.ik import BatchIkSolver
+    from pyroffi_b200.trajopt import TrajectoryCost
+
+    hbm = _measured_hbm()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    out = {}
+
+    # config 1: 7-DOF chain, 8 spheres per link, 64 obstacle spheres
+    w = W.fk_collision(B=65536)
+    R, S, Wd = DeviceRobot.upload(w.model, dev), DeviceSpheres.upload(w.spheres, dev), DeviceWorld.upload(w.world, dev)
+    N, Sp = w.spheres.n_links, w.spheres.S
+    K, M = N * Sp, sum(Wd.counts())
+    cfg = torch.as_tensor(w.cfg, device=dev)
+    c1 = cfg[:1024].contiguous()
+    r1 = fk_sphere_collision(R, S, Wd, c1)
+    ms_1024 = _timed_ms(torch, lambda: fk_sphere_collision(R, S, Wd, c1, out=r1), flush)
+    r2 = fk_sphere_collision(R, S, Wd, cfg, per_sphere=True)
+    ms_bkm = _timed_ms(torch, lambda: fk_sphere_collision(R, S, Wd, cfg, per_sphere=True, out=r2), flush)
+    n_valid = int((w.spheres.radii >= 0).sum())
+    bytes_cfg = 4 * w.model.n_act + 4 + 4 * 7 * N + 4 * K * M
+    flop_cfg = 130 * w.model.n_act + 33 * n_valid + 12 * n_valid * M
+    out["fk_collision_config1"] = {
+        "workload": "7-DOF chain, 8 spheres/link, 64 obstacle spheres; min distance + link poses",
+        "B1024_us_per_call": 1e3 * ms_1024, "B1024_configs_per_s": 1024 / (ms_1024 * 1e-3),
+        "B65536_bkm_ms": ms_bkm, "B65536_bkm_configs_per_s": 65536 / (ms_bkm * 1e-3),
+        "roofline": {"bound": "hbm", "achieved": 65536 * bytes_cfg / (ms_bkm * 1e-3) / 1e9, "peak": hbm,
+                     "unit": "GB/s", "frac": 65536 * bytes_cfg / (ms_bkm * 1e-3) / 1e9 / hbm,
+                     "bytes_per_config": bytes_cfg, "layout": f"[B, K={K}, M={M}] f32 + min + poses",
+                     "fp32_tflops": 65536 * flop_cfg / (ms_bkm * 1e-3) / 1e12, "kernel": "fk_sphere_collision_kernel"},
+    }
+    del r2
+
+    # config 3: 512 trajectories x 64 waypoints x 7 DOF, 256 spheres + 32 boxes
+    wt = W.trajectories()
+    tc = TrajectoryCost(wt.model, wt.spheres, wt.world, wt.link_pairs, margin=wt.margin, device=dev)
+    x = torch.as_tensor(wt.traj, device=dev)
+    ms_f = _timed_ms(torch, lambda: tc.cost(x), flush)
+    ms_b = _timed_ms(torch, lambda: tc.grad(x), flush)
+    ms_fb = _timed_ms(torch, lambda: tc.cost_and_grad(x), flush)
+    Bt, T = wt.traj.shape[:2]
+    f_fwd, f_bwd = 296646, 459326
+    out["traj_config3"] = {
+        "workload": "512 x 64 x 7 CHOMP cost + hand-written adjoint, 256 spheres + 32 boxes",
+        "forward_ms": ms_f, "backward_recompute_ms": ms_b, "fused_fwd_bwd_ms": ms_fb,
+        "fwd_bwd_traj_per_s": Bt / (ms_fb * 1e-3),
+        "roofline": {"bound": "fp32", "achieved": Bt * T * f_bwd / (ms_fb * 1e-3) / 1e12, "peak": fp32_peak,
+                     "unit": "TFLOP/s", "frac": Bt * T * f_bwd / (ms_fb * 1e-3) / 1e12 / fp32_peak,
+                     "flop_per_waypoint": f_bwd, "kernel": "traj_cost_kernel"},
+    }
+
+    # config 4: 4096 mixed IK problems in one persistent batch (CUDA graph)
+    wm = W.mixed_ik()
+    o = dict(max_iter=wm.max_iter, lambda_init=wm.lambda_init, lambda_down=wm.lambda_down, lambda_up=wm.lambda_up,
+             collision_weight=wm.collision_weight, collision_margin=wm.collision_margin, pos_tol=wm.pos_tol,
+             rot_tol=wm.rot_tol)
+    b = MixedIkBatch(wm.classes, wm.world, device=dev, **o)
+    b.prepare(wm.problem_class, wm.n_seeds)
+    b.load(wm.target_T, wm.seeds)
+    b.capture()
+    ms_batch = _timed_ms(torch, b.solve, flush, reps=3, warm=1)
+    res = b.solve()
+    torch.cuda.synchronize()
+    succ = sum(int(r.success.sum()) for r in res) / len(wm.problem_class)
+    plain = 0.0
+    for c, cl in enumerate(wm.classes):
+        s = BatchIkSolver(cl.model, cl.target_links, spheres=cl.spheres, world=wm.world, device=dev, **o)
+        tg, sd = torch.as_tensor(wm.target_T[c], device=dev), torch.as_tensor(wm.seeds[c], device=dev)
+        plain += _timed_ms(torch, lambda: s.solve(tg, sd), flush, reps=2, warm=1)
+    n_p = len(wm.problem_class)
+    out["batch_ik_config4"] = {
+        "workload": "4096 problems (40% 7-DOF, 30% 6-DOF, 20% 15-DOF bimanual, 10% 29-DOF humanoid), "
+                    "32-256 seeds, 500 obstacle spheres, 30 LM iterations",
+        "solves_per_s": n_p / (ms_batch * 1e-3), "ms_per_batch": ms_batch, "success_rate": succ,
+        "success_per_class": [float(r.success.float().mean()) for r in res],
+        "plain_per_class_padded_ms": plain, "speedup_vs_per_class_padded": plain / ms_batch,
+        "kernel_launches_per_batch": b.launches_per_solve(),
+    }
+    del b
+
+    # config 5: 16 spheres/link vs 4096 spheres + 256 oriented boxes, B = 1024 ... 262144
+    ws = W.sweep(B=262144)
+    R5, S5, W5 = DeviceRobot.upload(ws.model, dev), DeviceSpheres.upload(ws.spheres, dev), DeviceWorld.upload(ws.world, dev)
+    N5, M5 = ws.spheres.n_links, sum(W5.counts())
+    n_valid5 = int((ws.spheres.radii >= 0).sum())
+    Ms5, Mb5 = W5.counts()[0], W5.counts()[2]
+    flop5 = 130 * ws.model.n_act + 33 * n_valid5 + n_valid5 * (12 * Ms5 + 41 * Mb5)
+    bytes5 = 4 * ws.model.n_act + 4 + 4 * N5 * M5
+    cfg5 = torch.as_tensor(ws.cfg, device=dev)
+    bnm = torch.empty((262144, N5, M5), dtype=torch.float32, device=dev)
+    mind = torch.empty(262144, dtype=torch.float32, device=dev)
+    sweep = {}
+    for B in (1024, 16384, 65536, 262144):
+        cb = cfg5[:B]
+        rb = FkCollisionResult(mind[:B], None, None, bnm[:B])
+        ms = _timed_ms(torch, lambda: fk_sphere_collision(R5, S5, W5, cb, link_poses=False, per_link=True, out=rb),
+                       flush, reps=3)
+        sweep[str(B)] = {"ms": ms, "configs_per_s": B / (ms * 1e-3), "hbm_gbs": B * bytes5 / (ms * 1e-3) / 1e9,
+                         "fp32_tflops": B * flop5 / (ms * 1e-3) / 1e12,
+                         "fp32_frac": B * flop5 / (ms * 1e-3) / 1e12 / fp32_peak}
+    del bnm
+    pairs5 = W.active_link_pairs(ws.model, ws.spheres)
+    tc5 = TrajectoryCost(ws.model, ws.spheres, ws.world, pairs5, device=dev)
+    x5 = cfg5[:65536].reshape(1024, 64, -1).contiguous()
+    ms_fb5 = _timed_ms(torch, lambda: tc5.cost_and_grad(x5), flush, reps=3)
+    out["sweep_config5"] = {
+        "workload": "7-DOF chain, 16 spheres/link (112) vs 4096 spheres + 256 oriented boxes; [B, N, M] per-link rows",
+        "bytes_per_config": bytes5, "flop_per_config": flop5, "by_batch": sweep,
+        "roofline": {"bound": "fp32", "achieved": sweep["262144"]["fp32_tflops"], "peak": fp32_peak,
+                     "unit": "TFLOP/s", "frac": sweep["262144"]["fp32_frac"], "kernel": "fk_sphere_collision_kernel"},
+        "fwd_bwd_65536_configs_ms": ms_fb5,
+    }
+    return out
+
+
+def _measured_hbm():
+    try:
+        return float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"])
+    except Exception:
+        return 6650.0
 
 
 def main():
