@@ -61,7 +61,7 @@ struct WideArgs {
 // Byte offsets of the dynamic shared memory, sized for the largest class.
 struct WideLayout {
   size_t rs, rsj, rsk, pairs, ws, wc, wb, wh, cells, cell_obs, obox, warps, warp_bytes, total;
-  size_t w_cfg, w_best, w_dact, w_trial, w_dcol, w_cs, w_r, w_fw, w_pee, w_T, w_J, w_A, w_y, w_pos;
+  size_t w_cfg, w_best, w_dact, w_trial, w_dcol, w_cs, w_r, w_fw, w_pee, w_T, w_J, w_A, w_y, w_pos, w_slot;
   int max_rs, max_self, max_joints, max_act, max_rows, max_entries, nwarps;
 };
 
@@ -138,10 +138,16 @@ __host__ inline WideLayout wide_layout(int max_rs, int max_self, int max_joints,
   L.w_pee = q; q += 4 * 3 * PK_MAX_EE;
   q = w_align16(q);
   L.w_T = q; q = w_align16(q + 28 * (size_t)max_joints);
-  L.w_J = q; q = w_align16(q + 4 * (size_t)L.max_rows * max_act);
-  L.w_A = q; q = w_align16(q + 8 * (size_t)max_act * (max_act + 1) / 2);
-  L.w_y = q; q = w_align16(q + 8 * (size_t)PK_MAX_ACT);
-  L.w_pos = q; q = w_align16(q + 16 * (size_t)max_rs);
+  // The Jacobian (direction step) and the per-joint slot data (penalty) are
+  // never live together, nor are the normal equations and the sphere
+  // positions: each pair shares one region.
+  L.w_J = q;
+  L.w_slot = q;  // per sphere-carrying joint: B, R (float4); list range, offset (int4)
+  q = w_align16(q + std::max(4 * (size_t)L.max_rows * max_act, 32 * (size_t)max_joints));
+  L.w_A = q;
+  L.w_y = w_align16(q + 8 * (size_t)max_act * (max_act + 1) / 2);
+  L.w_pos = q;
+  q = w_align16(std::max(L.w_y + 8 * (size_t)PK_MAX_ACT, q + 16 * (size_t)max_rs));
   L.warp_bytes = q;
   L.warps = o;
   L.total = o + q * nwarps;
@@ -397,6 +403,8 @@ struct WideWarp {
   float *cfg, *best, *dact, *trial, *dcol, *cs, *r, *fw, *pee, *T, *J;
   double *A, *y;
   float4* pos;
+  float4* slotB;  // per slot: bounding centre (world) and radius
+  int4* slotL;    // per slot: first list entry, candidate count, offset in the flattened candidates, -
 };
 
 __device__ __forceinline__ Pose w_load(const float* T, int i) {
@@ -408,18 +416,22 @@ __device__ __forceinline__ void w_store(float* T, int i, const Pose& P) {
   p[0] = P.w; p[1] = P.x; p[2] = P.y; p[3] = P.z; p[4] = P.tx; p[5] = P.ty; p[6] = P.tz;
 }
 
-// FK of configuration q (shared, n_act floats) into W.T, level by level.
+// FK of configuration q (shared, n_act floats) into W.T: every joint's local
+// transform in parallel, then the compositions level by level in place
+// (a joint's parent is final before its level runs).
 template <int G>
 __device__ __forceinline__ void w_fk(const WideShared& sh, const float* q, const WideWarp& W, int gl, unsigned gm) {
   const JointTable& jt = sh.jt;
-  for (int lv = 0; lv < sh.n_lvl; ++lv) {
+  for (int i = gl; i < jt.n; i += G) {
+    const int src = jt.src[i];
+    w_store(W.T, i, joint_local(jt, i, ((src < 0) ? 0.f : q[src]) * jt.mul[i] + jt.off[i]));
+  }
+  __syncwarp(gm);
+  for (int lv = 1; lv < sh.n_lvl; ++lv) {
     for (int idx = sh.lvl_start[lv] + gl; idx < sh.lvl_start[lv + 1]; idx += G) {
       const int i = sh.lvl_joint[idx];
-      const int src = jt.src[i];
-      const float qq = ((src < 0) ? 0.f : q[src]) * jt.mul[i] + jt.off[i];
-      const Pose Tpc = joint_local(jt, i, qq);
       const int p = jt.psorted[i];
-      w_store(W.T, i, (p < 0) ? Tpc : pose_compose(w_load(W.T, p), Tpc));
+      if (p >= 0) w_store(W.T, i, pose_compose(w_load(W.T, p), w_load(W.T, i)));
     }
     __syncwarp(gm);
   }
@@ -475,33 +487,53 @@ __device__ __noinline__ float w_penalty(const WideLaunch& P, const WideShared& s
   float pen = 0.f;
   const int Ms = P.w.Ms;
   if (Ms > 0) {
+    // per sphere-carrying joint: bounding centre and its candidate obstacles
     for (int j = gl; j < sh.n_js; j += G) {
       const float4 bl = sh.jb[j];
       const float3 B = pose_apply(w_load(W.T, sh.js_joint[j]), make_float3(bl.x, bl.y, bl.z));
-      const int k0 = sh.jstart[j], k1 = sh.jstart[j + 1];
-      int e0 = 0, e1 = Ms;
-      const unsigned short* list = nullptr;
+      int e0 = 0, n = Ms;
       if (sh.grid_on) {
         const int ix = __float2int_rd((B.x - sh.glo.x) * sh.ginv.x);
         const int iy = __float2int_rd((B.y - sh.glo.y) * sh.ginv.y);
         const int iz = __float2int_rd((B.z - sh.glo.z) * sh.ginv.z);
         // outside the grid no obstacle is within reach of this joint
-        if ((unsigned)ix >= (unsigned)WG || (unsigned)iy >= (unsigned)WG || (unsigned)iz >= (unsigned)WG) continue;
-        const int cell = (ix * WG + iy) * WG + iz;
-        e0 = cell_start[cell];
-        e1 = cell_start[cell + 1];
-        list = cell_obs;
+        if ((unsigned)ix >= (unsigned)WG || (unsigned)iy >= (unsigned)WG || (unsigned)iz >= (unsigned)WG) {
+          n = 0;
+        } else {
+          const int cell = (ix * WG + iy) * WG + iz;
+          e0 = cell_start[cell];
+          n = cell_start[cell + 1] - e0;
+        }
       }
-      for (int e = e0; e < e1; ++e) {
-        const float4 O = ws4[list ? (int)list[e] : e];
-        const float rr = bl.w + O.w;
-        const float dx = B.x - O.x, dy = B.y - O.y, dz = B.z - O.z;
-        if (dx * dx + dy * dy + dz * dz < rr * fabsf(rr)) {
-          for (int k = k0; k < k1; ++k) {
-            const float4 p = W.pos[k];
-            const float ex = p.x - O.x, ey = p.y - O.y, ez = p.z - O.z;
-            w_hinge(ex * ex + ey * ey + ez * ez, p.w + O.w, pen);
-          }
+      W.slotB[j] = make_float4(B.x, B.y, B.z, bl.w);
+      W.slotL[j] = make_int4(e0, n, 0, 0);
+    }
+    __syncwarp(gm);
+    // offsets of each joint's candidates in the flattened list (serial: at most 64 joints)
+    int total = 0;
+    for (int j = 0; j < sh.n_js; ++j) total += W.slotL[j].y;
+    if (gl == 0) {
+      int run = 0;
+      for (int j = 0; j < sh.n_js; ++j) { W.slotL[j].z = run; run += W.slotL[j].y; }
+    }
+    __syncwarp(gm);
+    // lanes take (joint, candidate) pairs in turn: bounding-sphere test, then
+    // the joint's spheres against the candidate
+    int j = 0;
+    for (int it = gl; it < total; it += G) {
+      while (j + 1 < sh.n_js && W.slotL[j + 1].z <= it) ++j;
+      while (W.slotL[j].z > it) --j;
+      const int4 sl = W.slotL[j];
+      const int e = sl.x + (it - sl.z);
+      const float4 O = ws4[sh.grid_on ? (int)cell_obs[e] : e];
+      const float4 Bj = W.slotB[j];
+      const float rr = Bj.w + O.w;
+      const float dx = Bj.x - O.x, dy = Bj.y - O.y, dz = Bj.z - O.z;
+      if (dx * dx + dy * dy + dz * dz < rr * fabsf(rr)) {
+        for (int k = sh.jstart[j]; k < sh.jstart[j + 1]; ++k) {
+          const float4 p = W.pos[k];
+          const float ex = p.x - O.x, ey = p.y - O.y, ez = p.z - O.z;
+          w_hinge(ex * ex + ey * ey + ez * ez, p.w + O.w, pen);
         }
       }
     }
@@ -599,13 +631,19 @@ __device__ __noinline__ float w_direction(const WideShared& sh, int n_act, int n
   float fw2 = 0.f;
   for (int k = 0; k < rows; ++k) fw2 += W.fw[k] * W.fw[k];
 
-  // FP64 normal equations, packed lower triangle: lane j computes A[i][j]
-  for (int i = 0; i < ncol; ++i) {
-    for (int j = gl; j <= i; j += G) {
+  // FP64 normal equations, packed lower triangle: lanes take the entries
+  // e = i (i + 1) / 2 + j in turn
+  {
+    const int ne = ncol * (ncol + 1) / 2;
+    int i = 0, j = gl;
+    while (i < ncol && j > i) { j -= i + 1; ++i; }
+    for (int e = gl; e < ne; e += G) {
       double acc = 0.0;
       for (int k = 0; k < rows; ++k) acc += (double)W.J[i * rows + k] * (double)W.J[j * rows + k];
       if (i == j) acc += (double)lam;
-      W.A[i * (i + 1) / 2 + j] = acc;
+      W.A[e] = acc;
+      j += G;
+      while (i < ncol && j > i) { j -= i + 1; ++i; }
     }
   }
   for (int i = gl; i < ncol; i += G) {
@@ -772,6 +810,8 @@ __device__ __forceinline__ WideWarp w_group_area(const WideLayout& L, unsigned c
   W.A = reinterpret_cast<double*>(b + L.w_A);
   W.y = reinterpret_cast<double*>(b + L.w_y);
   W.pos = reinterpret_cast<float4*>(b + L.w_pos);
+  W.slotB = reinterpret_cast<float4*>(b + L.w_slot);
+  W.slotL = reinterpret_cast<int4*>(b + L.w_slot + 16 * (size_t)L.max_joints);
   return W;
 }
 
@@ -857,58 +897,76 @@ static void wide_options(WideLaunch& P, const pk_lm_options& o) {
   P.coll = o.enable_collision ? 1 : 0; P.coll_w = o.collision_weight; P.margin = o.collision_margin;
 }
 
-static constexpr int kWideThreads = 256;
-
 static int wide_group(const pk_lm_options& o) { return o.lanes_per_wide_seed == 32 ? 32 : 16; }
 
-// Layout for the warp-body classes of P; PK_ERR_CAPACITY when it does not fit.
-static int wide_prepare(WideLaunch& P, int max_smem, int G, int* max_ee_out) {
-  int max_rs = 0, max_self = 0, max_joints = 1, max_act = 1, max_ee = 1;
+struct WideMax {
+  int rs, self, joints, act, ee;
+};
+
+// Largest per-class extents over the warp-body classes of P.
+static WideMax wide_max(const WideLaunch& P) {
+  WideMax m{0, 0, 1, 1, 1};
   for (int c = 0; c < P.n_classes; ++c) {
     if (P.body[c] != kBodyWarp) continue;
     const WideArgs& a = P.cls[c];
-    max_rs = std::max(max_rs, a.n_rs);
-    max_self = std::max(max_self, P.coll ? a.n_self : 0);
-    max_joints = std::max(max_joints, a.m.n_joints);
-    max_act = std::max(max_act, a.n_act);
-    max_ee = std::max(max_ee, a.n_ee);
+    m.rs = std::max(m.rs, a.n_rs);
+    m.self = std::max(m.self, P.coll ? a.n_self : 0);
+    m.joints = std::max(m.joints, a.m.n_joints);
+    m.act = std::max(m.act, a.n_act);
+    m.ee = std::max(m.ee, a.n_ee);
   }
-  P.L = wide_layout(max_rs, max_self, max_joints, max_act, max_ee, P.w, kWideThreads / G);
-  *max_ee_out = max_ee;
-  PK_CHECK_CAP(P.L.total <= (size_t)max_smem,
-               "warp-body LM working set (%zu B of shared memory) exceeds %d B", P.L.total, max_smem);
-  return PK_OK;
+  return m;
 }
 
+// Chooses the block size (256, 128 or 64 threads) that keeps the most seeds
+// resident per SM within the shared-memory limit, sets P.L for it and
+// launches: a (problem, seed block) grid, or one persistent wave.
 template <int G, int MAXEE>
-static int run_warp_t(const WideLaunch& P, dim3 grid, bool persistent, int blocks, cudaStream_t st, int* launched) {
+static int run_warp_t(WideLaunch& P, const WideMax& mx, int grid_seeds, int grid_problems, bool persistent,
+                      int blocks, cudaStream_t st, int* launched) {
   auto kern = lm_warp_kernel<G, MAXEE>;
-  if (int s = set_smem_limit((const void*)kern, P.L.total)) return s;
-  if (persistent) {
-    if (blocks <= 0) {
-      int dev = 0, sms = 0, per_sm = 0;
-      if (int s = cuda_status(cudaGetDevice(&dev), "cudaGetDevice")) return s;
-      if (int s = cuda_status(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attribute"))
-        return s;
-      if (int s = cuda_status(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kWideThreads, P.L.total),
-                              "occupancy"))
-        return s;
-      blocks = std::max(1, sms * std::max(per_sm, 1));
-    }
-    grid = dim3(blocks);
+  int dev = 0, max_smem = 0, sms = 0;
+  if (int s = cuda_status(cudaGetDevice(&dev), "cudaGetDevice")) return s;
+  if (int s = cuda_status(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev), "attribute"))
+    return s;
+  if (int s = cuda_status(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attribute")) return s;
+  int best_threads = 0, best_per_sm = 0, best_groups = -1;
+  WideLayout best{};
+  for (int threads = 256; threads >= 64 && threads >= G; threads >>= 1) {
+    const WideLayout L = wide_layout(mx.rs, mx.self, mx.joints, mx.act, mx.ee, P.w, threads / G);
+    if (L.total > (size_t)max_smem) continue;
+    if (int s = set_smem_limit((const void*)kern, L.total)) return s;
+    int per_sm = 0;
+    if (int s = cuda_status(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, L.total), "occupancy"))
+      return s;
+    const int groups = per_sm * (threads / G);
+    if (groups > best_groups) { best_groups = groups; best_threads = threads; best_per_sm = per_sm; best = L; }
   }
-  kern<<<grid, kWideThreads, P.L.total, st>>>(P);
+  PK_CHECK_CAP(best_threads > 0 && best_per_sm > 0,
+               "warp-body LM working set does not fit in %d B of shared memory even for one seed group per block",
+               max_smem);
+  P.L = best;
+  if (int s = set_smem_limit((const void*)kern, best.total)) return s;
+  dim3 grid;
+  if (persistent) {
+    grid = dim3(blocks > 0 ? blocks : std::max(1, sms * best_per_sm));
+  } else {
+    P.grid_chunk = 2 * (best_threads / G);
+    grid = dim3((grid_seeds + P.grid_chunk - 1) / P.grid_chunk, grid_problems);
+  }
+  kern<<<grid, best_threads, best.total, st>>>(P);
   if (launched) ++*launched;
   return cuda_status(cudaGetLastError(), "lm_warp_kernel launch");
 }
 
-static int run_warp(const WideLaunch& P, int G, int max_ee, dim3 grid, bool persistent, int blocks, cudaStream_t st,
-                    int* launched) {
+static int run_warp(WideLaunch& P, int G, int grid_seeds, int grid_problems, bool persistent, int blocks,
+                    cudaStream_t st, int* launched) {
+  const WideMax mx = wide_max(P);
   if (G == 32)
-    return max_ee <= 2 ? run_warp_t<32, 2>(P, grid, persistent, blocks, st, launched)
-                       : run_warp_t<32, 4>(P, grid, persistent, blocks, st, launched);
-  return max_ee <= 2 ? run_warp_t<16, 2>(P, grid, persistent, blocks, st, launched)
-                     : run_warp_t<16, 4>(P, grid, persistent, blocks, st, launched);
+    return mx.ee <= 2 ? run_warp_t<32, 2>(P, mx, grid_seeds, grid_problems, persistent, blocks, st, launched)
+                      : run_warp_t<32, 4>(P, mx, grid_seeds, grid_problems, persistent, blocks, st, launched);
+  return mx.ee <= 2 ? run_warp_t<16, 2>(P, mx, grid_seeds, grid_problems, persistent, blocks, st, launched)
+                    : run_warp_t<16, 4>(P, mx, grid_seeds, grid_problems, persistent, blocks, st, launched);
 }
 
 static int validate_wide_class(const pk_ik_class& c, bool coll) {
@@ -928,12 +986,6 @@ static int validate_wide_class(const pk_ik_class& c, bool coll) {
   return PK_OK;
 }
 
-static int device_smem_optin(int* out) {
-  int dev = 0;
-  if (int s = cuda_status(cudaGetDevice(&dev), "cudaGetDevice")) return s;
-  return cuda_status(cudaDeviceGetAttribute(out, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev),
-                     "cudaDeviceGetAttribute");
-}
 
 int launch_warp_grid(const pk_ik_class& c, const WorldArgs& w, const pk_lm_options& opt, cudaStream_t st) {
   if (int s = validate_wide_class(c, opt.enable_collision != 0)) return s;
@@ -946,13 +998,7 @@ int launch_warp_grid(const pk_ik_class& c, const WorldArgs& w, const pk_lm_optio
   P.w = w;
   wide_options(P, opt);
   P.queue = nullptr;
-  const int G = wide_group(opt);
-  P.grid_chunk = 2 * (kWideThreads / G);
-  int max_smem = 0, max_ee = 1;
-  if (int s = device_smem_optin(&max_smem)) return s;
-  if (int s = wide_prepare(P, max_smem, G, &max_ee)) return s;
-  const dim3 grid((c.seed_stride + P.grid_chunk - 1) / P.grid_chunk, c.n_problems);
-  return run_warp(P, G, max_ee, grid, false, 0, st, nullptr);
+  return run_warp(P, wide_group(opt), c.seed_stride, c.n_problems, false, 0, st, nullptr);
 }
 
 int launch_warp_batch(const BatchCall& b, cudaStream_t st, int* launched) {
@@ -973,11 +1019,7 @@ int launch_warp_batch(const BatchCall& b, cudaStream_t st, int* launched) {
   P.items = b.items;
   P.n_items = b.n_items;
   P.queue = b.queue + 1;
-  const int G = wide_group(b.opt);
-  int max_smem = 0, max_ee = 1;
-  if (int s = device_smem_optin(&max_smem)) return s;
-  if (int s = wide_prepare(P, max_smem, G, &max_ee)) return s;
-  return run_warp(P, G, max_ee, dim3(1), true, b.blocks, st, launched);
+  return run_warp(P, wide_group(b.opt), 0, 0, true, b.blocks, st, launched);
 }
 
 }  // namespace pk
