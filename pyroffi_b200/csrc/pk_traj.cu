@@ -101,13 +101,18 @@ __device__ __forceinline__ float3 cross3(float3 a, float3 b) {
   return make_float3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
 }
 
-template <int MAXS>
-__global__ void __launch_bounds__(128) traj_cost_kernel(TrajArgs a) {
+// Lanes per waypoint: the world (link, obstacle) pairs and the self pairs of
+// one waypoint are split over a group of TG lanes (TG = 2 or 4); its FK,
+// force totals and joint gradient live once per waypoint in shared memory.
+template <int MAXS, int TG>
+__global__ void __launch_bounds__(64 * TG, 8 / TG) traj_cost_kernel(TrajArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   JointTable& jt = *reinterpret_cast<JointTable*>(smem_raw);
   unsigned char* p = smem_raw + sizeof(JointTable);
   const int N = a.N, S = a.S, T = a.T, n = a.m.n_act, nj = a.m.n_joints;
   const int nth = blockDim.x, tid = threadIdx.x;
+  const int ng = nth / TG, grp = tid / TG, gl = tid % TG;
+  const unsigned gm = ((1u << TG) - 1u) << ((tid & 31) & ~(TG - 1));
   float4* lsph = reinterpret_cast<float4*>(p); p += sizeof(float4) * N * S;       // link spheres
   float4* lbnd = reinterpret_cast<float4*>(p); p += sizeof(float4) * N;           // link bounding spheres
   int* lpj = reinterpret_cast<int*>(p); p += sizeof(int) * ((N + 3) & ~3);        // parent joint (sorted), -1 base
@@ -115,9 +120,9 @@ __global__ void __launch_bounds__(128) traj_cost_kernel(TrajArgs a) {
   float* acc = reinterpret_cast<float*>(p); p += sizeof(float) * ((T * n + 3) & ~3);  // acc, then its adjoint
   float* red = reinterpret_cast<float*>(p); p += sizeof(float) * ((nth + 3) & ~3);
   float* wpc = reinterpret_cast<float*>(p); p += sizeof(float) * ((T + 3) & ~3);
-  float* slots = reinterpret_cast<float*>(p); p += sizeof(float) * nj * 7 * nth;
-  float* lt = reinterpret_cast<float*>(p); p += sizeof(float) * N * 6 * nth;      // link force / moment totals
-  float* gq = reinterpret_cast<float*>(p); p += sizeof(float) * nj * nth;         // gradient per joint
+  float* slots = reinterpret_cast<float*>(p); p += sizeof(float) * nj * 7 * ng;   // per waypoint group
+  float* lt = reinterpret_cast<float*>(p); p += sizeof(float) * N * 6 * ng;       // link force / moment totals
+  float* gq = reinterpret_cast<float*>(p); p += sizeof(float) * nj * ng;          // gradient per joint
   p = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15));
 
   load_joint_table(jt, a.m);
@@ -158,14 +163,18 @@ __global__ void __launch_bounds__(128) traj_cost_kernel(TrajArgs a) {
 
   const bool want_grad = a.grad != nullptr;
   const float margin = a.margin;
-  for (int t = tid; t < T; t += nth) {
-    const PoseSlots ps{slots + tid, nth};
-    fk_thread(jt, [&](int i) { return xs[t * n + i]; }, ps);
-    float* L = lt + tid;
-    for (int i = 0; i < N * 6; ++i) L[i * nth] = 0.f;
+  const int M = a.w.total();
+  for (int t0 = 0; t0 < T; t0 += ng) {
+    const int t = t0 + grp;
+    if (t >= T) continue;  // the whole group skips
+    const PoseSlots ps{slots + grp, ng};
+    if (gl == 0) fk_thread(jt, [&](int i) { return xs[t * n + i]; }, ps);
+    float* L = lt + grp;
+    for (int i = gl; i < N * 6; i += TG) L[i * ng] = 0.f;
+    __syncwarp(gm);
     float cw = 0.f;
-    // world: (link, obstacle) hinge on the link's minimum sphere distance
-    const int M = a.w.total();
+    // world: (link, obstacle) hinge on the link's minimum sphere distance;
+    // lane gl takes obstacles gl, gl + TG, ...
     for (int l = 0; l < N; ++l) {
       const float4 bl = lbnd[l];
       if (bl.w < 0.f) continue;
@@ -174,7 +183,7 @@ __global__ void __launch_bounds__(128) traj_cost_kernel(TrajArgs a) {
       float cx[MAXS], cy[MAXS], cz[MAXS], cr[MAXS];
       bool have = false;
       float3 F = make_float3(0.f, 0.f, 0.f), Mo = make_float3(0.f, 0.f, 0.f);
-      for (int m = 0; m < M; ++m) {
+      for (int m = gl; m < M; m += TG) {
         if (obstacle_dist(ob, m, B, bl.w) >= margin) continue;  // exact lower bound of the link's distances
         if (!have) {
 #pragma unroll
@@ -211,80 +220,109 @@ __global__ void __launch_bounds__(128) traj_cost_kernel(TrajArgs a) {
         }
       }
       if (want_grad) {
-        L[(l * 6 + 0) * nth] += F.x; L[(l * 6 + 1) * nth] += F.y; L[(l * 6 + 2) * nth] += F.z;
-        L[(l * 6 + 3) * nth] += Mo.x; L[(l * 6 + 4) * nth] += Mo.y; L[(l * 6 + 5) * nth] += Mo.z;
-      }
-    }
-    // self: active link pairs, min over the same sphere index s
-    for (int pi = 0; pi < a.P; ++pi) {
-      const int li = a.pair_i[pi], lj = a.pair_j[pi];
-      if (li < 0 || lj < 0 || li >= N || lj >= N) continue;
-      const float4 bi = lbnd[li], bj = lbnd[lj];
-      if (bi.w < 0.f || bj.w < 0.f) continue;
-      const Pose Ti = lpj[li] < 0 ? pose_identity() : ps.load(lpj[li]);
-      const Pose Tj = lpj[lj] < 0 ? pose_identity() : ps.load(lpj[lj]);
-      const float3 Bi = pose_apply(Ti, make_float3(bi.x, bi.y, bi.z));
-      const float3 Bj = pose_apply(Tj, make_float3(bj.x, bj.y, bj.z));
-      {
-        const float dx = Bi.x - Bj.x, dy = Bi.y - Bj.y, dz = Bi.z - Bj.z;
-        if (sqrtf(dx * dx + dy * dy + dz * dz) - bi.w - bj.w >= margin) continue;
-      }
-      float dmin = FLT_MAX;
-      float3 ca = make_float3(0.f, 0.f, 0.f), cb = ca;
-      for (int s = 0; s < S; ++s) {
-        const float4 qa = lsph[li * S + s], qb = lsph[lj * S + s];
-        if (qa.w < 0.f || qb.w < 0.f) continue;
-        const float3 pa = pose_apply(Ti, make_float3(qa.x, qa.y, qa.z));
-        const float3 pb = pose_apply(Tj, make_float3(qb.x, qb.y, qb.z));
-        const float dx = pa.x - pb.x, dy = pa.y - pb.y, dz = pa.z - pb.z;
-        const float d = sqrtf(dx * dx + dy * dy + dz * dz) - (qa.w + qb.w);
-        if (d < dmin) { dmin = d; ca = pa; cb = pb; }
-      }
-      if (!(dmin < margin)) continue;
-      const float v = margin - dmin;
-      cw += v * v;
-      if (want_grad) {
-        const float dx = ca.x - cb.x, dy = ca.y - cb.y, dz = ca.z - cb.z;
-        const float nrm = sqrtf(dx * dx + dy * dy + dz * dz);
-        const float k = nrm > 0.f ? -2.f * v / nrm : 0.f;
-        const float3 f = make_float3(k * dx, k * dy, k * dz);  // force on sphere a; -f on sphere b
-        const float3 ma = cross3(ca, f), mb = cross3(cb, f);
-        L[(li * 6 + 0) * nth] += f.x; L[(li * 6 + 1) * nth] += f.y; L[(li * 6 + 2) * nth] += f.z;
-        L[(li * 6 + 3) * nth] += ma.x; L[(li * 6 + 4) * nth] += ma.y; L[(li * 6 + 5) * nth] += ma.z;
-        L[(lj * 6 + 0) * nth] -= f.x; L[(lj * 6 + 1) * nth] -= f.y; L[(lj * 6 + 2) * nth] -= f.z;
-        L[(lj * 6 + 3) * nth] -= mb.x; L[(lj * 6 + 4) * nth] -= mb.y; L[(lj * 6 + 5) * nth] -= mb.z;
-      }
-    }
-    wpc[t] = cw;
-    if (a.wp_coll) a.wp_coll[b * T + t] = cw;
-    if (want_grad) {
-      float* G = gq + tid;
-      for (int j = 0; j < nj; ++j) G[j * nth] = 0.f;
-      // every link's (F, M) acts on all joints from its parent joint to the root
-      for (int l = 0; l < N; ++l) {
-        const float3 F = make_float3(L[(l * 6 + 0) * nth], L[(l * 6 + 1) * nth], L[(l * 6 + 2) * nth]);
-        const float3 Mo = make_float3(L[(l * 6 + 3) * nth], L[(l * 6 + 4) * nth], L[(l * 6 + 5) * nth]);
-        if (F.x == 0.f && F.y == 0.f && F.z == 0.f && Mo.x == 0.f && Mo.y == 0.f && Mo.z == 0.f) continue;
-        for (int j = lpj[l]; j >= 0; j = jt.psorted[j]) {
-          const int kind = jt.kind[j];
-          if (kind == kFixed) continue;
-          const Pose Tj = ps.load(j);
-          const float* tw = jt.tw[j];
-          const float3 w = quat_rotate(Tj.w, Tj.x, Tj.y, Tj.z, make_float3(tw[3], tw[4], tw[5]));
-          const float3 vv = quat_rotate(Tj.w, Tj.x, Tj.y, Tj.z, make_float3(tw[0], tw[1], tw[2]));
-          // point velocity under dq_j: w x (c - p_j) + (R v); dJ/dq_j = sum F . that
-          const float3 pxF = cross3(make_float3(Tj.tx, Tj.ty, Tj.tz), F);
-          G[j * nth] += w.x * (Mo.x - pxF.x) + w.y * (Mo.y - pxF.y) + w.z * (Mo.z - pxF.z) +
-                        vv.x * F.x + vv.y * F.y + vv.z * F.z;
+#pragma unroll
+        for (int o = 1; o < TG; o <<= 1) {
+          F.x += __shfl_xor_sync(gm, F.x, o); F.y += __shfl_xor_sync(gm, F.y, o); F.z += __shfl_xor_sync(gm, F.z, o);
+          Mo.x += __shfl_xor_sync(gm, Mo.x, o); Mo.y += __shfl_xor_sync(gm, Mo.y, o); Mo.z += __shfl_xor_sync(gm, Mo.z, o);
+        }
+        if (gl == 0) {
+          L[(l * 6 + 0) * ng] += F.x; L[(l * 6 + 1) * ng] += F.y; L[(l * 6 + 2) * ng] += F.z;
+          L[(l * 6 + 3) * ng] += Mo.x; L[(l * 6 + 4) * ng] += Mo.y; L[(l * 6 + 5) * ng] += Mo.z;
         }
       }
-      float* grow = a.grad + (b * T + t) * n;
-      for (int c = 0; c < n; ++c) grow[c] = 0.f;
-      for (int j = 0; j < nj; ++j) {
-        const int src = jt.src[j];
-        if (src >= 0) grow[src] += a.w_coll * jt.mul[j] * G[j * nth];
+    }
+    __syncwarp(gm);
+    // self: active link pairs, min over the same sphere index s; lane gl takes
+    // pairs gl, gl + TG, ... and the lanes write their forces in turn
+    for (int p0 = 0; p0 < a.P; p0 += TG) {
+      const int pi = p0 + gl;
+      bool hit = false;
+      int li = 0, lj = 0;
+      float3 f = make_float3(0.f, 0.f, 0.f), ma = f, mb = f;
+      if (pi < a.P) {
+        li = a.pair_i[pi];
+        lj = a.pair_j[pi];
+        const bool ok = !(li < 0 || lj < 0 || li >= N || lj >= N) && lbnd[li].w >= 0.f && lbnd[lj].w >= 0.f;
+        if (ok) {
+          const float4 bi = lbnd[li], bj = lbnd[lj];
+          const Pose Ti = lpj[li] < 0 ? pose_identity() : ps.load(lpj[li]);
+          const Pose Tj = lpj[lj] < 0 ? pose_identity() : ps.load(lpj[lj]);
+          const float3 Bi = pose_apply(Ti, make_float3(bi.x, bi.y, bi.z));
+          const float3 Bj = pose_apply(Tj, make_float3(bj.x, bj.y, bj.z));
+          const float bx = Bi.x - Bj.x, by = Bi.y - Bj.y, bz = Bi.z - Bj.z;
+          if (sqrtf(bx * bx + by * by + bz * bz) - bi.w - bj.w < margin) {
+            float dmin = FLT_MAX;
+            float3 ca = make_float3(0.f, 0.f, 0.f), cb = ca;
+            for (int s = 0; s < S; ++s) {
+              const float4 qa = lsph[li * S + s], qb = lsph[lj * S + s];
+              if (qa.w < 0.f || qb.w < 0.f) continue;
+              const float3 pa = pose_apply(Ti, make_float3(qa.x, qa.y, qa.z));
+              const float3 pb = pose_apply(Tj, make_float3(qb.x, qb.y, qb.z));
+              const float dx = pa.x - pb.x, dy = pa.y - pb.y, dz = pa.z - pb.z;
+              const float d = sqrtf(dx * dx + dy * dy + dz * dz) - (qa.w + qb.w);
+              if (d < dmin) { dmin = d; ca = pa; cb = pb; }
+            }
+            if (dmin < margin) {
+              const float v = margin - dmin;
+              cw += v * v;
+              hit = true;
+              const float dx = ca.x - cb.x, dy = ca.y - cb.y, dz = ca.z - cb.z;
+              const float nrm = sqrtf(dx * dx + dy * dy + dz * dz);
+              const float k = nrm > 0.f ? -2.f * v / nrm : 0.f;
+              f = make_float3(k * dx, k * dy, k * dz);  // force on sphere a; -f on sphere b
+              ma = cross3(ca, f);
+              mb = cross3(cb, f);
+            }
+          }
+        }
+      }
+      if (want_grad) {
+        for (int r = 0; r < TG; ++r) {
+          if (gl == r && hit) {
+            L[(li * 6 + 0) * ng] += f.x; L[(li * 6 + 1) * ng] += f.y; L[(li * 6 + 2) * ng] += f.z;
+            L[(li * 6 + 3) * ng] += ma.x; L[(li * 6 + 4) * ng] += ma.y; L[(li * 6 + 5) * ng] += ma.z;
+            L[(lj * 6 + 0) * ng] -= f.x; L[(lj * 6 + 1) * ng] -= f.y; L[(lj * 6 + 2) * ng] -= f.z;
+            L[(lj * 6 + 3) * ng] -= mb.x; L[(lj * 6 + 4) * ng] -= mb.y; L[(lj * 6 + 5) * ng] -= mb.z;
+          }
+          __syncwarp(gm);
+        }
       }
     }
+#pragma unroll
+    for (int o = 1; o < TG; o <<= 1) cw += __shfl_xor_sync(gm, cw, o);
+    if (gl == 0) {
+      wpc[t] = cw;
+      if (a.wp_coll) a.wp_coll[b * T + t] = cw;
+      if (want_grad) {
+        float* G = gq + grp;
+        for (int j = 0; j < nj; ++j) G[j * ng] = 0.f;
+        // every link's (F, M) acts on all joints from its parent joint to the root
+        for (int l = 0; l < N; ++l) {
+          const float3 F = make_float3(L[(l * 6 + 0) * ng], L[(l * 6 + 1) * ng], L[(l * 6 + 2) * ng]);
+          const float3 Mo = make_float3(L[(l * 6 + 3) * ng], L[(l * 6 + 4) * ng], L[(l * 6 + 5) * ng]);
+          if (F.x == 0.f && F.y == 0.f && F.z == 0.f && Mo.x == 0.f && Mo.y == 0.f && Mo.z == 0.f) continue;
+          for (int j = lpj[l]; j >= 0; j = jt.psorted[j]) {
+            const int kind = jt.kind[j];
+            if (kind == kFixed) continue;
+            const Pose Tj = ps.load(j);
+            const float* tw = jt.tw[j];
+            const float3 w = quat_rotate(Tj.w, Tj.x, Tj.y, Tj.z, make_float3(tw[3], tw[4], tw[5]));
+            const float3 vv = quat_rotate(Tj.w, Tj.x, Tj.y, Tj.z, make_float3(tw[0], tw[1], tw[2]));
+            // point velocity under dq_j: w x (c - p_j) + (R v); dJ/dq_j = sum F . that
+            const float3 pxF = cross3(make_float3(Tj.tx, Tj.ty, Tj.tz), F);
+            G[j * ng] += w.x * (Mo.x - pxF.x) + w.y * (Mo.y - pxF.y) + w.z * (Mo.z - pxF.z) +
+                         vv.x * F.x + vv.y * F.y + vv.z * F.z;
+          }
+        }
+        float* grow = a.grad + (b * T + t) * n;
+        for (int c = 0; c < n; ++c) grow[c] = 0.f;
+        for (int j = 0; j < nj; ++j) {
+          const int src = jt.src[j];
+          if (src >= 0) grow[src] += a.w_coll * jt.mul[j] * G[j * ng];
+        }
+      }
+    }
+    __syncwarp(gm);
   }
   __syncthreads();
 
@@ -353,10 +391,11 @@ __global__ void __launch_bounds__(128) traj_cost_kernel(TrajArgs a) {
   }
 }
 
-static size_t traj_smem(const TrajArgs& a, int nth) {
+static size_t traj_smem(const TrajArgs& a, int nth, int TG) {
   size_t s = sizeof(JointTable) + sizeof(float4) * a.N * a.S + sizeof(float4) * a.N + sizeof(int) * ((a.N + 3) & ~3) +
              2 * sizeof(float) * ((a.T * a.m.n_act + 3) & ~3) + sizeof(float) * ((nth + 3) & ~3) +
-             sizeof(float) * ((a.T + 3) & ~3) + sizeof(float) * (size_t)nth * (a.m.n_joints * 7 + a.N * 6 + a.m.n_joints);
+             sizeof(float) * ((a.T + 3) & ~3) +
+             sizeof(float) * (size_t)(nth / TG) * (a.m.n_joints * 7 + a.N * 6 + a.m.n_joints);
   s = (s + 15) & ~size_t(15);
   return s + sizeof(float) * a.w.smem_floats();
 }
@@ -401,13 +440,20 @@ extern "C" int pk_traj_cost_grad(void* stream, const pk_traj_options* opt, const
   a.B = B; a.T = T; a.N = n_links; a.S = S; a.P = P;
   a.margin = opt->margin; a.w_smooth = opt->w_smooth; a.w_acc = opt->w_acc; a.w_jerk = opt->w_jerk;
   a.w_limits = opt->w_limits; a.w_coll = opt->w_coll;
-  int nth = 32;
-  while (nth < T && nth < 128) nth *= 2;
+  // lanes per waypoint: 4 when a waypoint has much world to test or the
+  // batch is too small to fill the GPU with 2-lane blocks, else 2
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int TG = (Ms + Mc + Mb + Mh >= 1024 || B <= 2LL * sms) ? 4 : 2;
+  int ng = 8;  // waypoint groups per block (TG lanes each)
+  while (ng < T && ng < 64) ng *= 2;
+  const int nth = ng * TG;
   PK_CHECK_CAP((size_t)(T - 4) * n_act <= (size_t)8 * nth, "trajectory too long for one block (T*n_act=%d)", T * n_act);
-  const size_t smem = traj_smem(a, nth);
+  const size_t smem = traj_smem(a, nth, TG);
   PK_CHECK_CAP(smem <= 200 * 1024, "trajectory working set (%zu B of shared memory) too large", smem);
   PK_CHECK_CAP(B < (1LL << 31), "batch too large");
-  auto kern = (S <= 8) ? traj_cost_kernel<8> : traj_cost_kernel<16>;
+  auto kern = (S <= 8) ? (TG == 4 ? traj_cost_kernel<8, 4> : traj_cost_kernel<8, 2>)
+                       : (TG == 4 ? traj_cost_kernel<16, 4> : traj_cost_kernel<16, 2>);
   if (int s = set_smem_limit((const void*)kern, smem)) return s;
   kern<<<(unsigned)B, nth, smem, (cudaStream_t)stream>>>(a);
   return cuda_status(cudaGetLastError(), "traj_cost_kernel launch");
