@@ -8,5 +8,6 @@ re-verification, all as hand-written CUDA kernels behind the C-ABI in
 """
 
 from . import robot, workloads  # noqa: F401
+from .urdf import load_urdf  # noqa: F401
 
 __version__ = "0.1.0"
