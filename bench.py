@@ -454,6 +454,23 @@ def secondary_metrics(torch, dev, fp32_peak):
                      "flop_per_waypoint": f_bwd, "kernel": "traj_cost_kernel"},
     }
 
+    # CHOMP optimiser on the adjoint: the config-3 trajectories, 100 iterations, one CUDA graph
+    from pyroffi_b200.chomp import ChompConfig, ChompOptimizer
+    ccfg = ChompConfig()
+    tcc = TrajectoryCost(wt.model, wt.spheres, wt.world, wt.link_pairs, margin=ccfg.collision_margin, device=dev)
+    opt = ChompOptimizer(tcc, ccfg)
+    s0, g0 = x[0, 0].clone(), x[0, -1].clone()
+    opt.run(x, s0, g0, graph=True)
+    ms_chomp = _timed_ms(torch, lambda: opt.run(x, s0, g0, graph=True), flush, reps=3, warm=1)
+    _, cc, _ = opt.run(x, s0, g0, graph=True)
+    out["chomp_config3"] = {
+        "workload": "CHOMP, 512 x 64 x 7 trajectories, 100 iterations (cost+gradient, truncated-CG covariant step, "
+                    "6-point line search per iteration), one CUDA graph",
+        "ms_per_run": ms_chomp, "iterations_per_s": ccfg.n_iters / (ms_chomp * 1e-3),
+        "trajectory_iterations_per_s": Bt * ccfg.n_iters / (ms_chomp * 1e-3),
+        "final_cost_mean": float(cc.mean()),
+    }
+
     # config 4: 4096 mixed IK problems in one persistent batch (CUDA graph)
     wm = W.mixed_ik()
     o = dict(max_iter=wm.max_iter, lambda_init=wm.lambda_init, lambda_down=wm.lambda_down, lambda_up=wm.lambda_up,
