@@ -471,6 +471,29 @@ def secondary_metrics(torch, dev, fp32_peak):
         "final_cost_mean": float(cc.mean()),
     }
 
+    # SCO optimiser: the config-3 trajectories, 10 outer x 30 inner L-BFGS iterations, one CUDA graph;
+    # its stages timed alone, and the reference's central-difference Jacobians for comparison
+    from pyroffi_b200.sco import ScoConfig, ScoOptimizer
+    scfg = ScoConfig()
+    sco = ScoOptimizer(wt.model, wt.spheres, wt.world, wt.link_pairs, scfg, device=dev)
+    sco.run(x, s0, g0, graph=True)
+    ms_sco = _timed_ms(torch, lambda: sco.run(x, s0, g0, graph=True), flush, reps=3, warm=1)
+    _, sc, _ = sco.run(x, s0, g0, graph=True)
+    ms_lin = _timed_ms(torch, lambda: sco.linearize(x), flush)
+    dl, Jl, _ = sco.linearize(x)
+    ms_inner = _timed_ms(torch, lambda: sco.inner(x, dl, Jl, scfg.w_collision, s0, g0), flush)
+    sco_fd = ScoOptimizer(wt.model, wt.spheres, wt.world, wt.link_pairs, scfg, fd_eps=1e-4, device=dev)
+    sco_fd.run(x, s0, g0, graph=True)
+    ms_sco_fd = _timed_ms(torch, lambda: sco_fd.run(x, s0, g0, graph=True), flush, reps=2, warm=1)
+    out["sco_config3"] = {
+        "workload": "SCO, 512 x 64 x 7 trajectories, 10 outer (analytic smooth-min linearisation) x 30 inner "
+                    "L-BFGS iterations, one CUDA graph",
+        "ms_per_run": ms_sco, "trajectories_per_s": Bt / (ms_sco * 1e-3),
+        "linearize_ms": ms_lin, "inner_solve_ms": ms_inner,
+        "ms_per_run_fd_jacobian": ms_sco_fd,
+        "final_cost_mean": float(sc.mean()),
+    }
+
     # config 4: 4096 mixed IK problems in one persistent batch (CUDA graph)
     wm = W.mixed_ik()
     o = dict(max_iter=wm.max_iter, lambda_init=wm.lambda_init, lambda_down=wm.lambda_down, lambda_up=wm.lambda_up,

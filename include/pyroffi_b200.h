@@ -16,6 +16,7 @@
 #ifndef PYROFFI_B200_H_
 #define PYROFFI_B200_H_
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -325,6 +326,96 @@ int pk_traj_cost_grad(void* stream, const pk_traj_options* opt, const float* tra
                       float* grad, float* wp_coll, int64_t B, int32_t T, int32_t n_act, int32_t n_joints,
                       int32_t n_links, int32_t S, int32_t P, int32_t Ms, int32_t Mc, int32_t Mb,
                       int32_t Mh);
+
+/* SCO trajectory optimisation settings: the fields of ScoTrajOptConfig
+ * (src/pyroffi/optimization_engines/_sco_optimization.py:52-104, defaults in
+ * brackets) and the reference kernel's fd_eps attribute
+ * (src/pyroffi/cuda_kernels/_sco_trajopt_cuda.py:152-163). */
+typedef struct pk_sco_options {
+  int32_t n_outer_iters;         /* [10] linearise-and-solve iterations */
+  int32_t n_inner_iters;         /* [30] L-BFGS steps per outer iteration */
+  int32_t m_lbfgs;               /* [6] L-BFGS history, 1..16 */
+  float w_smooth;                /* [1.0] */
+  float w_acc;                   /* [0.5] */
+  float w_jerk;                  /* [0.1] */
+  float w_limits;                /* [1.0] */
+  float w_trust;                 /* [0.5] */
+  float w_collision;             /* [1.0] first outer iteration's collision weight */
+  float w_collision_max;         /* [100.0] cap of the continuation and weight of the final ranking */
+  float penalty_scale;           /* [3.0] */
+  float collision_margin;        /* [0.01] */
+  float smooth_min_temperature;  /* [0.05] */
+  float fd_eps;                  /* 0: analytic Jacobians; > 0: central differences with this step
+                                    (the reference kernel uses 1e-4) */
+  int32_t self_all_pairs;        /* 1: a self pair's distance is the minimum over all sphere pairs
+                                    (the reference kernel); 0: over equal sphere indices (the JAX
+                                    compute_self_collision_distance) */
+  int32_t inner_threads;         /* threads per trajectory in the inner solve; 0 = automatic */
+} pk_sco_options;
+
+/*
+ * SCO linearisation (replaces _compute_coll_dists_and_jacs,
+ * _sco_optimization.py:258-289, and the finite differences of
+ * _sco_trajopt_cuda_kernel.cu:700-757).  For each of C configurations
+ * cfg[C, n_act]: dist[C, 5] the smooth-min distances of the groups (self,
+ * world spheres, capsules, boxes, halfspaces; 1e10 for a group without
+ * pairs), jac[C, 5, n_act] their analytic Jacobians, coll[C] the sum of
+ * -colldist_from_sdf(d, margin) over every self pair and (link, obstacle)
+ * pair distance.  Any output may be NULL (not all).  Link and world arrays as
+ * for pk_traj_cost_grad.
+ */
+int pk_sco_linearize(void* stream, const pk_sco_options* opt, const float* cfg, const float* twists,
+                     const float* parent_tf, const int32_t* parent_idx, const int32_t* act_idx,
+                     const float* mimic_mul, const float* mimic_off, const int32_t* mimic_act_idx,
+                     const int32_t* topo_inv, const int32_t* parent_joint_indices, const float* link_spheres,
+                     const int32_t* pair_i, const int32_t* pair_j, const float* world_spheres,
+                     const float* world_capsules, const float* world_boxes, const float* world_halfspaces,
+                     float* dist, float* jac, float* coll, int64_t C, int32_t n_act, int32_t n_joints,
+                     int32_t n_links, int32_t S, int32_t P, int32_t Ms, int32_t Mc, int32_t Mb, int32_t Mh);
+
+/*
+ * SCO inner solve (replaces _lbfgs_inner_solve, _sco_optimization.py:296-448,
+ * and _sco_trajopt_cuda_kernel.cu:759-888): for each trajectory traj[B, T,
+ * n_act] (the linearisation point), n_inner_iters L-BFGS steps on the convex
+ * model with dist[B, T, 5], jac[B, T, 5, n_act] and collision weight w_coll;
+ * traj is overwritten with the best iterate, endpoints set to start / goal.
+ * hist[B, 2, m_lbfgs, T, n_act] holds the L-BFGS history when it does not fit
+ * in shared memory (NULL otherwise; PK_ERR_INVALID when it is needed).
+ */
+int pk_sco_inner(void* stream, const pk_sco_options* opt, float* traj, const float* dist, const float* jac,
+                 const float* lower, const float* upper, const float* start, const float* goal, float* hist,
+                 float w_coll, int64_t B, int32_t T, int32_t n_act);
+
+/* Nonlinear ranking cost (replaces _eval_cost, _sco_optimization.py:455-474):
+ * cost[b] = w_smooth (w_acc acc^2 + w_jerk jerk^2) + w_limits limits +
+ * w_collision_max sum_t coll[b, t], with coll from pk_sco_linearize. */
+int pk_sco_final_cost(void* stream, const pk_sco_options* opt, const float* traj, const float* coll,
+                      const float* lower, const float* upper, float* cost, int64_t B, int32_t T, int32_t n_act);
+
+/* Bytes of device workspace pk_sco_trajopt needs for (B, T, n_act). */
+int pk_sco_workspace_bytes(const pk_sco_options* opt, int64_t B, int32_t T, int32_t n_act, size_t* bytes);
+
+/*
+ * Whole SCO optimisation (replaces the ScoTrajoptCudaFfi custom call,
+ * src/pyroffi/cuda_kernels/_sco_trajopt_cuda_kernel.cu:1094-1307, bound by
+ * _sco_trajopt_cuda.py:152-300): pins init_trajs[B, T, n_act] to start /
+ * goal, runs n_outer_iters x (linearise, inner solve, weight continuation)
+ * and writes out_trajs[B, T, n_act] and the ranking costs out_costs[B]; the
+ * caller takes argmin(out_costs) as the best trajectory, as the reference
+ * wrapper does.  workspace: pk_sco_workspace_bytes bytes, 256-byte aligned.
+ * All launches go to `stream` and nothing allocates, so the call can be
+ * captured in a CUDA graph.
+ */
+int pk_sco_trajopt(void* stream, const pk_sco_options* opt, const float* init_trajs, const float* start,
+                   const float* goal, const float* twists, const float* parent_tf, const int32_t* parent_idx,
+                   const int32_t* act_idx, const float* mimic_mul, const float* mimic_off,
+                   const int32_t* mimic_act_idx, const int32_t* topo_inv, const int32_t* parent_joint_indices,
+                   const float* link_spheres, const int32_t* pair_i, const int32_t* pair_j,
+                   const float* world_spheres, const float* world_capsules, const float* world_boxes,
+                   const float* world_halfspaces, const float* lower, const float* upper, float* out_trajs,
+                   float* out_costs, void* workspace, size_t workspace_bytes, int64_t B, int32_t T,
+                   int32_t n_act, int32_t n_joints, int32_t n_links, int32_t S, int32_t P, int32_t Ms,
+                   int32_t Mc, int32_t Mb, int32_t Mh);
 
 /*
  * FP32 FMA-pipe microbenchmark (no reference counterpart): `blocks` blocks of

@@ -66,6 +66,11 @@ SIGNATURES: dict[str, list] = {
     "pk_ik_batch_static": [_p, C.POINTER(LmOptions), C.c_void_p, _i32] + [_p] * 4 + [_i32] * 4 + [_p, _i32, _i32],
     "pk_fp32_fma_peak": [_p, _p, _i32, _i32],
     "pk_traj_cost_grad": [_p, C.c_void_p] + [_p] * 22 + [_i64] + [_i32] * 10,
+    "pk_sco_linearize": [_p, C.c_void_p] + [_p] * 20 + [_i64] + [_i32] * 9,
+    "pk_sco_inner": [_p, C.c_void_p] + [_p] * 8 + [_f32, _i64, _i32, _i32],
+    "pk_sco_final_cost": [_p, C.c_void_p] + [_p] * 5 + [_i64, _i32, _i32],
+    "pk_sco_workspace_bytes": [C.c_void_p, _i64, _i32, _i32, C.POINTER(C.c_size_t)],
+    "pk_sco_trajopt": [_p, C.c_void_p] + [_p] * 24 + [C.c_size_t, _i64] + [_i32] * 10,
 }
 
 
@@ -89,6 +94,17 @@ class TrajOptions(C.Structure):
 
     _fields_ = [("margin", _f32), ("w_smooth", _f32), ("w_acc", _f32), ("w_jerk", _f32),
                 ("w_limits", _f32), ("w_coll", _f32)]
+
+
+class ScoOptions(C.Structure):
+    """``pk_sco_options`` of the C-ABI."""
+
+    _fields_ = [("n_outer_iters", _i32), ("n_inner_iters", _i32), ("m_lbfgs", _i32), ("w_smooth", _f32),
+                ("w_acc", _f32), ("w_jerk", _f32), ("w_limits", _f32), ("w_trust", _f32), ("w_collision", _f32),
+                ("w_collision_max", _f32), ("penalty_scale", _f32), ("collision_margin", _f32),
+                ("smooth_min_temperature", _f32), ("fd_eps", _f32), ("self_all_pairs", _i32),
+                ("inner_threads", _i32)]
+
 
 _lock = threading.Lock()
 _lib: C.CDLL | None = None

@@ -66,6 +66,61 @@ __device__ __forceinline__ float obstacle_dist(const ObsView& o, int m, float3 c
   return d_sphere_halfspace(c, r, o.hs + 6 * m);
 }
 
+// Signed distance from sphere (c, r) to obstacle m and its gradient w.r.t. c.
+__device__ inline float obstacle_dist_grad(const ObsView& o, int m, float3 c, float r, float3& g) {
+  if (m < o.Ms) {
+    const float4 s = o.sph[m];
+    const float dx = c.x - s.x, dy = c.y - s.y, dz = c.z - s.z;
+    const float n = sqrtf(dx * dx + dy * dy + dz * dz);
+    const float inv = n > 0.f ? 1.f / n : 0.f;
+    g = make_float3(dx * inv, dy * inv, dz * inv);
+    return n - (r + s.w);
+  }
+  m -= o.Ms;
+  if (m < o.Mc) {
+    const float* cp = o.cap + 7 * m;
+    const float vx = cp[3] - cp[0], vy = cp[4] - cp[1], vz = cp[5] - cp[2];
+    const float len2 = vx * vx + vy * vy + vz * vz;
+    float t = 0.f;
+    if (len2 > 1e-12f) t = fmaxf(0.f, fminf(1.f, ((c.x - cp[0]) * vx + (c.y - cp[1]) * vy + (c.z - cp[2]) * vz) / len2));
+    const float dx = c.x - (cp[0] + t * vx), dy = c.y - (cp[1] + t * vy), dz = c.z - (cp[2] + t * vz);
+    const float n = sqrtf(dx * dx + dy * dy + dz * dz);
+    const float inv = n > 0.f ? 1.f / n : 0.f;
+    g = make_float3(dx * inv, dy * inv, dz * inv);
+    return n - (r + cp[6]);
+  }
+  m -= o.Mc;
+  if (m < o.Mb) {
+    const float* b = o.box + 15 * m;
+    const float dx = c.x - b[0], dy = c.y - b[1], dz = c.z - b[2];
+    const float l[3] = {dx * b[3] + dy * b[4] + dz * b[5], dx * b[6] + dy * b[7] + dz * b[8],
+                        dx * b[9] + dy * b[10] + dz * b[11]};
+    float q[3], gl[3];
+    for (int i = 0; i < 3; ++i) q[i] = fabsf(l[i]) - b[12 + i];
+    const float m0 = fmaxf(q[0], 0.f), m1 = fmaxf(q[1], 0.f), m2 = fmaxf(q[2], 0.f);
+    const float out = sqrtf(m0 * m0 + m1 * m1 + m2 * m2);
+    const float qmax = fmaxf(fmaxf(q[0], q[1]), q[2]);
+    if (out > 0.f) {
+      gl[0] = copysignf(m0 / out, l[0]); gl[1] = copysignf(m1 / out, l[1]); gl[2] = copysignf(m2 / out, l[2]);
+    } else {
+      const int im = (q[0] >= q[1] && q[0] >= q[2]) ? 0 : (q[1] >= q[2] ? 1 : 2);
+      gl[0] = gl[1] = gl[2] = 0.f;
+      gl[im] = copysignf(1.f, l[im]);
+    }
+    g = make_float3(gl[0] * b[3] + gl[1] * b[6] + gl[2] * b[9], gl[0] * b[4] + gl[1] * b[7] + gl[2] * b[10],
+                    gl[0] * b[5] + gl[1] * b[8] + gl[2] * b[11]);
+    return out + fminf(qmax, 0.f) - r;
+  }
+  m -= o.Mb;
+  const float* h = o.hs + 6 * m;
+  g = make_float3(h[0], h[1], h[2]);
+  return (c.x - h[3]) * h[0] + (c.y - h[4]) * h[1] + (c.z - h[5]) * h[2] - r;
+}
+
+__device__ __forceinline__ float3 cross3(float3 a, float3 b) {
+  return make_float3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+
 // Order-preserving float <-> int map for atomic min on signed floats.
 __device__ __forceinline__ int float_to_ordered(float f) {
   const int i = __float_as_int(f);

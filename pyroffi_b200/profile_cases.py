@@ -9,6 +9,8 @@ capture one warm launch.
     python -m pyroffi_b200.profile_cases wide        # warp-per-seed LM, 15-DOF bimanual, 64 problems x 64 seeds
     python -m pyroffi_b200.profile_cases traj        # trajectory cost + adjoint, 512 x 64 x 7
     python -m pyroffi_b200.profile_cases batch       # persistent mixed batch, 512 problems
+    python -m pyroffi_b200.profile_cases scolin      # SCO linearisation, 512 x 64 x 7 waypoints
+    python -m pyroffi_b200.profile_cases scoinner    # SCO inner L-BFGS solve, 512 trajectories
 """
 
 from __future__ import annotations
@@ -77,8 +79,20 @@ def _batch():
     return b.run_lm
 
 
+def _sco(stage):
+    from .sco import ScoConfig, ScoOptimizer
+    wt = W.trajectories()
+    dev = torch.device("cuda:0")
+    opt = ScoOptimizer(wt.model, wt.spheres, wt.world, wt.link_pairs, ScoConfig(), device=dev)
+    x = torch.as_tensor(wt.traj, device=dev)
+    if stage == "lin":
+        return lambda: opt.linearize(x)
+    d, J, _ = opt.linearize(x)
+    return lambda: opt.inner(x, d, J, 1.0, x[0, 0], x[0, -1])
+
+
 CASES = {"lm": _lm, "fkc1": lambda: _fkc(65536, False), "fkc5": lambda: _fkc(4096, True), "wide": _wide,
-         "traj": _traj, "batch": _batch}
+         "traj": _traj, "batch": _batch, "scolin": lambda: _sco("lin"), "scoinner": lambda: _sco("inner")}
 
 
 def main(argv=None) -> int:

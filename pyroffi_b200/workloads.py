@@ -292,6 +292,39 @@ def trajectories(Bt: int = 512, T: int = 64, seed: int = 1003) -> TrajWorkload:
     return TrajWorkload(model, spheres, world, traj, active_link_pairs(model, spheres))
 
 
+def random_capsules(rng, n, length=(0.1, 0.5), r_range=(0.03, 0.1)) -> np.ndarray:
+    """[n, 7]: (p1, p2, r) with p1 U[-1,1]^3 and p2 = p1 + a random direction times U[length]."""
+    p1 = rng.uniform(-1, 1, size=(n, 3))
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    p2 = p1 + d * rng.uniform(*length, size=(n, 1))
+    r = rng.uniform(*r_range, size=(n, 1))
+    return np.concatenate([p1, p2, r], axis=1).astype(np.float32)
+
+
+def mixed_trajectories(Bt: int = 4, T: int = 16, seed: int = 1006, n_spheres: int = 24, n_capsules: int = 6,
+                       n_boxes: int = 6, per_link: int = 4) -> TrajWorkload:
+    """Trajectories of the 7-DOF chain among all four obstacle kinds (spheres,
+    capsules, oriented boxes and a floor halfspace) -- the small SCO case."""
+    rng = np.random.default_rng(seed)
+    model = serial_chain(7, rng)
+    spheres = random_spheres(model, rng, per_link=per_link)
+    world = empty_world()
+    world.spheres = random_sphere_world(rng, n_spheres)
+    world.capsules = random_capsules(rng, n_capsules)
+    world.boxes = random_boxes(rng, n_boxes, oriented=True)
+    world.halfspaces = np.array([[0.0, 0.0, 1.0, 0.0, 0.0, -1.2]], np.float32)
+    start = model.random_cfgs(rng, 1)[0]
+    goal = model.random_cfgs(rng, 1)[0]
+    s = np.linspace(0.0, 1.0, T)[None, :, None]
+    traj = np.broadcast_to(start[None, None] * (1 - s) + goal[None, None] * s, (Bt, T, start.shape[0])).copy()
+    noise = rng.normal(0.0, 0.05, size=traj.shape)
+    noise[:, 0] = 0.0
+    noise[:, -1] = 0.0
+    traj = (traj + noise).astype(np.float32)
+    return TrajWorkload(model, spheres, world, traj, active_link_pairs(model, spheres))
+
+
 @dataclass
 class SweepWorkload:
     model: RobotModel
