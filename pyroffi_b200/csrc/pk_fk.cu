@@ -69,17 +69,6 @@ struct FusedArgs {
   int stage_world;          // obstacles in shared memory
 };
 
-// 1/sqrt(x) by the PTX approximate reciprocal square root (MUFU; a few ulp).
-__device__ __forceinline__ float rsqrt_approx(float x) {
-  float y;
-  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-  return y;
-}
-
-// sqrt(x) for x >= 0 as x * rsqrt(x + 1e-30): the 1e-30 keeps x = 0 finite
-// (giving 0) and is below FP32 resolution for any x above 1e-23.
-__device__ __forceinline__ float sqrt_fast(float x) { return x * rsqrt_approx(x + 1e-30f); }
-
 // |c - o| for a robot sphere centre c and obstacle sphere o.
 __device__ __forceinline__ float centre_dist(float4 c, float4 o) {
   const float dx = c.x - o.x, dy = c.y - o.y, dz = c.z - o.z;

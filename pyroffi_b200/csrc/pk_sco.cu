@@ -41,7 +41,6 @@
 namespace pk {
 
 constexpr int kScoG = 5;      // self, spheres, capsules, boxes, halfspaces
-constexpr int kScoAcc = 8;    // floats per (group, link) accumulator: max, sum, F, M
 constexpr int kScoMaxHist = 16;
 
 struct ScoLinArgs {
@@ -91,10 +90,10 @@ struct SoftAcc {
   // `count`: the term enters the sum (a self pair is counted by one of its links only)
   __device__ __forceinline__ void add(float e, bool count, bool want_force, float3 g, float3 c) {
     if (e > ref) {
-      scale(ref == -INFINITY ? 0.f : expf(ref - e));
+      scale(ref == -INFINITY ? 0.f : __expf(ref - e));
       ref = e;
     }
-    const float w = expf(e - ref);
+    const float w = __expf(e - ref);
     if (count) s += w;
     if (want_force) {
       F.x += w * g.x; F.y += w * g.y; F.z += w * g.z;
@@ -113,8 +112,8 @@ struct SoftAcc {
       const float mx = __shfl_xor_sync(gm, M.x, o), my = __shfl_xor_sync(gm, M.y, o),
                   mz = __shfl_xor_sync(gm, M.z, o);
       const float r = fmaxf(ref, r2);
-      const float k1 = (ref == -INFINITY) ? 0.f : expf(ref - r);
-      const float k2 = (r2 == -INFINITY) ? 0.f : expf(r2 - r);
+      const float k1 = (ref == -INFINITY) ? 0.f : __expf(ref - r);
+      const float k2 = (r2 == -INFINITY) ? 0.f : __expf(r2 - r);
       s = s * k1 + s2 * k2;
       F = make_float3(F.x * k1 + fx * k2, F.y * k1 + fy * k2, F.z * k1 + fz * k2);
       M = make_float3(M.x * k1 + mx * k2, M.y * k1 + my * k2, M.z * k1 + mz * k2);
@@ -133,10 +132,130 @@ __device__ __forceinline__ float group_sum(float v, unsigned gm) {
   return v;
 }
 
+// One world obstacle of a known kind in registers (1 sphere, 2 capsule, 3
+// box, 4 halfspace) and its signed distance to a sphere (c, r).
+template <int KIND>
+struct ScoObs;
+
+template <>
+struct ScoObs<1> {
+  float x, y, z, r;
+  __device__ __forceinline__ void load(const ObsView& ob, int k) {
+    const float4 s = ob.sph[k];
+    x = s.x; y = s.y; z = s.z; r = s.w;
+  }
+  __device__ __forceinline__ float dist(float cx, float cy, float cz, float cr) const {
+    const float dx = cx - x, dy = cy - y, dz = cz - z;
+    return sqrt_fast(dx * dx + dy * dy + dz * dz) - (cr + r);
+  }
+};
+
+template <>
+struct ScoObs<2> {
+  float ax, ay, az, vx, vy, vz, r, il2;  // p1, p2 - p1, radius, 1 / |p2 - p1|^2 (0 when degenerate)
+  __device__ __forceinline__ void load(const ObsView& ob, int k) {
+    const float* p = ob.cap + 7 * k;
+    ax = p[0]; ay = p[1]; az = p[2];
+    vx = p[3] - p[0]; vy = p[4] - p[1]; vz = p[5] - p[2];
+    r = p[6];
+    const float l2 = vx * vx + vy * vy + vz * vz;
+    il2 = l2 > 1e-12f ? 1.f / l2 : 0.f;
+  }
+  __device__ __forceinline__ float dist(float cx, float cy, float cz, float cr) const {
+    float t = ((cx - ax) * vx + (cy - ay) * vy + (cz - az) * vz) * il2;
+    t = fmaxf(0.f, fminf(1.f, t));
+    const float px = fmaf(t, vx, ax) - cx, py = fmaf(t, vy, ay) - cy, pz = fmaf(t, vz, az) - cz;
+    return sqrt_fast(px * px + py * py + pz * pz) - (cr + r);
+  }
+};
+
+template <>
+struct ScoObs<3> {
+  float p[15];  // centre, axis columns, half-lengths
+  __device__ __forceinline__ void load(const ObsView& ob, int k) {
+#pragma unroll
+    for (int i = 0; i < 15; ++i) p[i] = ob.box[15 * k + i];
+  }
+  __device__ __forceinline__ float dist(float cx, float cy, float cz, float cr) const {
+    const float dx = cx - p[0], dy = cy - p[1], dz = cz - p[2];
+    const float q1 = fabsf(dx * p[3] + dy * p[4] + dz * p[5]) - p[12];
+    const float q2 = fabsf(dx * p[6] + dy * p[7] + dz * p[8]) - p[13];
+    const float q3 = fabsf(dx * p[9] + dy * p[10] + dz * p[11]) - p[14];
+    const float m1 = fmaxf(q1, 0.f), m2 = fmaxf(q2, 0.f), m3 = fmaxf(q3, 0.f);
+    return sqrt_fast(m1 * m1 + m2 * m2 + m3 * m3) + fminf(fmaxf(fmaxf(q1, q2), q3), 0.f) - cr;
+  }
+};
+
+template <>
+struct ScoObs<4> {
+  float nx, ny, nz, off;  // normal, normal . point
+  __device__ __forceinline__ void load(const ObsView& ob, int k) {
+    const float* h = ob.hs + 6 * k;
+    nx = h[0]; ny = h[1]; nz = h[2];
+    off = h[3] * h[0] + h[4] * h[1] + h[5] * h[2];
+  }
+  __device__ __forceinline__ float dist(float cx, float cy, float cz, float cr) const {
+    return cx * nx + cy * ny + cz * nz - off - cr;
+  }
+};
+
+// Terms whose softmax weight is below exp(-kScoSkip) of the running maximum
+// (2e-9; an FP32 sum that already holds the maximum term, >= 1, absorbs
+// anything below 6e-8) are left out of the accumulators.
+constexpr float kScoSkip = 20.f;
+
+// One world group of one link: lane gl takes obstacles gl, gl + TG, ... of the
+// kind's `count` (global obstacle index base + k); returns the accumulator
+// merged over the group's lanes.  `gref`: the group's running maximum over
+// the links done so far.  An obstacle is skipped whole when the link's
+// bounding sphere (B, R) bounds its weight below the skip level (and, with
+// the collision sum wanted, its distance at or above the margin).
+template <int KIND, int MAXS, int TG>
+__device__ __forceinline__ SoftAcc world_group(const ScoLinArgs& a, const ObsView& ob, int base, int count, int gl,
+                                               unsigned gm, const float (&cx)[MAXS], const float (&cy)[MAXS],
+                                               const float (&cz)[MAXS], const float (&cr)[MAXS], float3 B, float R,
+                                               bool want_soft, bool want_j, float inv_tau, float gref,
+                                               float& csum) {
+  SoftAcc acc;
+  acc.init();
+  for (int k = gl; k < count; k += TG) {
+    ScoObs<KIND> o;
+    o.load(ob, k);
+    const float lb = o.dist(B.x, B.y, B.z, R);  // <= every sphere distance of the link
+    if (want_soft) {
+      if (-lb * inv_tau < fmaxf(acc.ref, gref) - kScoSkip && (!a.coll || lb >= a.margin)) continue;
+    } else if (lb >= a.margin) {
+      continue;  // adds exactly 0 to the collision sum
+    }
+    float dmin = FLT_MAX;
+    int arg = 0;
+#pragma unroll
+    for (int s = 0; s < MAXS; ++s) {  // padded spheres carry radius -1e30 and never win
+      const float d = o.dist(cx[s], cy[s], cz[s], cr[s]);
+      if (d < dmin) { dmin = d; arg = s; }
+    }
+    if (a.coll) csum -= colldist(dmin, a.margin);
+    if (!want_soft) continue;
+    const float e = -dmin * inv_tau;
+    if (e < fmaxf(acc.ref, gref) - kScoSkip) continue;
+    float3 cc = make_float3(0.f, 0.f, 0.f), gg = cc;
+    if (want_j) {
+      float rr = 0.f;
+#pragma unroll
+      for (int s = 0; s < MAXS; ++s)
+        if (s == arg) { cc = make_float3(cx[s], cy[s], cz[s]); rr = cr[s]; }
+      obstacle_dist_grad(ob, base + k, cc, rr, gg);
+    }
+    acc.add(e, true, want_j, gg, cc);
+  }
+  if (want_soft) acc.merge<TG>(gm);
+  return acc;
+}
+
 // Linearisation: group distances, their analytic Jacobians and/or the
 // nonlinear collision sum, TG lanes per configuration.
 template <int MAXS, int TG>
-__global__ void __launch_bounds__(128) sco_linearize_kernel(ScoLinArgs a) {
+__global__ void __launch_bounds__(128, MAXS <= 8 ? 4 : 3) sco_linearize_kernel(ScoLinArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   JointTable& jt = *reinterpret_cast<JointTable*>(smem_raw);
   unsigned char* p = smem_raw + sizeof(JointTable);
@@ -145,6 +264,7 @@ __global__ void __launch_bounds__(128) sco_linearize_kernel(ScoLinArgs a) {
   const int ng = nth / TG, grp = tid / TG, gl = tid % TG;
   const unsigned gm = ((1u << TG) - 1u) << ((tid & 31) & ~(TG - 1));
   float4* lsph = reinterpret_cast<float4*>(p); p += sizeof(float4) * N * S;
+  float4* lbnd = reinterpret_cast<float4*>(p); p += sizeof(float4) * N;  // link bounding spheres
   int* lpj = reinterpret_cast<int*>(p); p += sizeof(int) * N;    // parent joint (sorted), -1 base
   int* lcnt = reinterpret_cast<int*>(p); p += sizeof(int) * N;   // valid spheres of the link
   int* lcur = reinterpret_cast<int*>(p); p += sizeof(int) * N;   // CSR fill cursor
@@ -152,7 +272,6 @@ __global__ void __launch_bounds__(128) sco_linearize_kernel(ScoLinArgs a) {
   int* lpl = reinterpret_cast<int*>(p); p += sizeof(int) * 2 * P;    // entries 2 * pair + role
   p = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15));
   float* slots = reinterpret_cast<float*>(p); p += sizeof(float) * nj * 7 * ng;
-  float* accs = reinterpret_cast<float*>(p); p += sizeof(float) * kScoG * N * kScoAcc * ng;
   float* gjs = reinterpret_cast<float*>(p); p += sizeof(float) * nj * nth;
   p = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15));
 
@@ -168,6 +287,22 @@ __global__ void __launch_bounds__(128) sco_linearize_kernel(ScoLinArgs a) {
     int c = 0;
     for (int s = 0; s < S; ++s) c += a.link_spheres[4 * (l * S + s) + 3] >= 0.f;
     lcnt[l] = c;
+    // bounding sphere of the link's spheres (link frame); the slack keeps
+    // it conservative under rounding
+    float lo[3] = {3e38f, 3e38f, 3e38f}, hi[3] = {-3e38f, -3e38f, -3e38f};
+    for (int s = 0; s < S; ++s) {
+      const float* q = a.link_spheres + 4 * (l * S + s);
+      if (q[3] < 0.f) continue;
+      for (int k = 0; k < 3; ++k) { lo[k] = fminf(lo[k], q[k]); hi[k] = fmaxf(hi[k], q[k]); }
+    }
+    const float bx = 0.5f * (lo[0] + hi[0]), by = 0.5f * (lo[1] + hi[1]), bz = 0.5f * (lo[2] + hi[2]);
+    float R = 0.f;
+    for (int s = 0; s < S; ++s) {
+      const float* q = a.link_spheres + 4 * (l * S + s);
+      if (q[3] < 0.f) continue;
+      R = fmaxf(R, sqrtf((q[0] - bx) * (q[0] - bx) + (q[1] - by) * (q[1] - by) + (q[2] - bz) * (q[2] - bz)) + q[3]);
+    }
+    lbnd[l] = c ? make_float4(bx, by, bz, R + 1e-4f + 1e-5f * R) : make_float4(0.f, 0.f, 0.f, 0.f);
   }
   __syncthreads();
   if (tid == 0) {
@@ -193,73 +328,75 @@ __global__ void __launch_bounds__(128) sco_linearize_kernel(ScoLinArgs a) {
   const bool want_soft = a.dist != nullptr || a.jac != nullptr;
   const bool want_j = a.jac != nullptr;
   const float inv_tau = 1.f / a.tau;
-  const int Ms = a.w.Ms, Mc = a.w.Mc, Mb = a.w.Mb, M = a.w.total();
-  const int mlo[kScoG] = {0, 0, Ms, Ms + Mc, Ms + Mc + Mb};
-  const int mhi[kScoG] = {0, Ms, Ms + Mc, Ms + Mc + Mb, M};
-  float* A = accs + (size_t)grp * kScoG * N * kScoAcc;
+  const int Ms = a.w.Ms, Mc = a.w.Mc, Mb = a.w.Mb;
+  float* G = gjs + tid * nj;  // lane g < 5: group g's joint gradient, relative to its running maximum
   const PoseSlots ps{slots + grp, ng};
+  static_assert(TG >= kScoG, "one lane per group");
 
   for (long long c = (long long)blockIdx.x * ng + grp; c < a.C; c += (long long)gridDim.x * ng) {
     const float* q = a.cfg + c * n;
     if (gl == 0) fk_thread(jt, [&](int i) { return q[i]; }, ps);
+    // lane g < 5 owns group g: running maximum rg of -d/tau, sum sg of exp(-d/tau - rg), G
+    float rg = -INFINITY, sg = 0.f;
+    float gref[kScoG];  // every group's running maximum, known to all lanes
+#pragma unroll
+    for (int g = 0; g < kScoG; ++g) gref[g] = -INFINITY;
+    if (want_j && gl < kScoG)
+      for (int j = 0; j < nj; ++j) G[j] = 0.f;
     __syncwarp(gm);
     float csum = 0.f;
     for (int l = 0; l < N; ++l) {
-      if (lcnt[l] == 0) {
-        if (gl == 0 && want_soft) {
-          SoftAcc e;
-          e.init();
-          for (int g = 0; g < kScoG; ++g) e.store(A + (g * N + l) * kScoAcc);
-        }
-        continue;
-      }
+      if (lcnt[l] == 0) continue;
       const Pose Tl = lpj[l] < 0 ? pose_identity() : ps.load(lpj[l]);
       float cx[MAXS], cy[MAXS], cz[MAXS], cr[MAXS];
 #pragma unroll
       for (int s = 0; s < MAXS; ++s) {
         const float4 w = (s < S) ? lsph[l * S + s] : make_float4(0.f, 0.f, 0.f, -1.f);
         const float3 v = pose_apply(Tl, make_float3(w.x, w.y, w.z));
-        cx[s] = v.x; cy[s] = v.y; cz[s] = v.z; cr[s] = w.w;
+        cx[s] = v.x; cy[s] = v.y; cz[s] = v.z;
+        cr[s] = w.w < 0.f ? -1e30f : w.w;  // a padded sphere's distances read 1e30
       }
+      const float4 bl = lbnd[l];
+      const float3 Bw = pose_apply(Tl, make_float3(bl.x, bl.y, bl.z));
       // world groups: (link, obstacle) pairs, lane gl takes obstacles gl, gl + TG, ...
-      for (int g = 1; g < kScoG; ++g) {
-        SoftAcc acc;
-        acc.init();
-        for (int m = mlo[g] + gl; m < mhi[g]; m += TG) {
-          float dmin = FLT_MAX;
-          int arg = 0;
-#pragma unroll
-          for (int s = 0; s < MAXS; ++s) {
-            if (cr[s] < 0.f) continue;
-            const float d = obstacle_dist(ob, m, make_float3(cx[s], cy[s], cz[s]), cr[s]);
-            if (d < dmin) { dmin = d; arg = s; }
-          }
-          if (a.coll) csum -= colldist(dmin, a.margin);
-          if (!want_soft) continue;
-          float3 cc = make_float3(0.f, 0.f, 0.f), gg = cc;
-          if (want_j) {
-            float rr = 0.f;
-#pragma unroll
-            for (int s = 0; s < MAXS; ++s)
-              if (s == arg) { cc = make_float3(cx[s], cy[s], cz[s]); rr = cr[s]; }
-            obstacle_dist_grad(ob, m, cc, rr, gg);
-          }
-          acc.add(-dmin * inv_tau, true, want_j, gg, cc);
-        }
-        if (want_soft) {
-          acc.merge<TG>(gm);
-          if (gl == 0) acc.store(A + (g * N + l) * kScoAcc);
-        }
-      }
+      SoftAcc mine, t;
+      mine.init();
+      t = world_group<1, MAXS, TG>(a, ob, 0, Ms, gl, gm, cx, cy, cz, cr, Bw, bl.w, want_soft, want_j, inv_tau,
+                                   gref[1], csum);
+      if (gl == 1) mine = t;
+      t = world_group<2, MAXS, TG>(a, ob, Ms, Mc, gl, gm, cx, cy, cz, cr, Bw, bl.w, want_soft, want_j, inv_tau,
+                                   gref[2], csum);
+      if (gl == 2) mine = t;
+      t = world_group<3, MAXS, TG>(a, ob, Ms + Mc, Mb, gl, gm, cx, cy, cz, cr, Bw, bl.w, want_soft, want_j,
+                                   inv_tau, gref[3], csum);
+      if (gl == 3) mine = t;
+      t = world_group<4, MAXS, TG>(a, ob, Ms + Mc + Mb, a.w.Mh, gl, gm, cx, cy, cz, cr, Bw, bl.w, want_soft,
+                                   want_j, inv_tau, gref[4], csum);
+      if (gl == 4) mine = t;
       // self group: the pairs listing link l; lane gl takes entries gl, gl + TG, ...
       SoftAcc acc;
       acc.init();
       for (int k = lps[l] + gl; k < lps[l + 1]; k += TG) {
         const int e = lpl[k], pq = e >> 1, role = e & 1;
         const int o = role ? a.pair_i[pq] : a.pair_j[pq];
+        if (!want_soft && role) continue;  // the collision sum takes each pair once
         const Pose To = lpj[o] < 0 ? pose_identity() : ps.load(lpj[o]);
+        {
+          // bounding spheres: skip a pair whose weight is bounded below the skip
+          // level (or, for the collision sum alone, that is at least the margin apart)
+          const float4 bo = lbnd[o];
+          const float3 Bo = pose_apply(To, make_float3(bo.x, bo.y, bo.z));
+          const float dx = Bw.x - Bo.x, dy = Bw.y - Bo.y, dz = Bw.z - Bo.z;
+          const float lb = sqrt_fast(dx * dx + dy * dy + dz * dz) - (bl.w + bo.w);
+          if (want_soft) {
+            if (-lb * inv_tau < fmaxf(acc.ref, gref[0]) - kScoSkip && (!a.coll || lb >= a.margin)) continue;
+          } else if (lb >= a.margin) {
+            continue;
+          }
+        }
         float dmin = FLT_MAX;
-        float3 ca = make_float3(0.f, 0.f, 0.f), cb = ca;
+        int arga = 0;
+        float3 cb = make_float3(0.f, 0.f, 0.f);
         if (a.self_all) {
           // minimum over every (sphere of l, sphere of o)
           for (int sb = 0; sb < S; ++sb) {
@@ -268,10 +405,9 @@ __global__ void __launch_bounds__(128) sco_linearize_kernel(ScoLinArgs a) {
             const float3 pb = pose_apply(To, make_float3(qb.x, qb.y, qb.z));
 #pragma unroll
             for (int sa = 0; sa < MAXS; ++sa) {
-              if (cr[sa] < 0.f) continue;
               const float dx = cx[sa] - pb.x, dy = cy[sa] - pb.y, dz = cz[sa] - pb.z;
-              const float d = sqrtf(dx * dx + dy * dy + dz * dz) - (cr[sa] + qb.w);
-              if (d < dmin) { dmin = d; ca = make_float3(cx[sa], cy[sa], cz[sa]); cb = pb; }
+              const float d = sqrt_fast(dx * dx + dy * dy + dz * dz) - (cr[sa] + qb.w);
+              if (d < dmin) { dmin = d; arga = sa; cb = pb; }
             }
           }
         } else {
@@ -283,13 +419,19 @@ __global__ void __launch_bounds__(128) sco_linearize_kernel(ScoLinArgs a) {
             if (qb.w < 0.f) continue;
             const float3 pb = pose_apply(To, make_float3(qb.x, qb.y, qb.z));
             const float dx = cx[s] - pb.x, dy = cy[s] - pb.y, dz = cz[s] - pb.z;
-            const float d = sqrtf(dx * dx + dy * dy + dz * dz) - (cr[s] + qb.w);
-            if (d < dmin) { dmin = d; ca = make_float3(cx[s], cy[s], cz[s]); cb = pb; }
+            const float d = sqrt_fast(dx * dx + dy * dy + dz * dz) - (cr[s] + qb.w);
+            if (d < dmin) { dmin = d; arga = s; cb = pb; }
           }
         }
-        if (dmin == FLT_MAX) continue;  // no common sphere index
+        if (!(dmin < 1e29f)) continue;  // no valid sphere pair (no common sphere index)
         if (a.coll && role == 0) csum -= colldist(dmin, a.margin);
         if (!want_soft) continue;
+        const float ev = -dmin * inv_tau;
+        if (ev < fmaxf(acc.ref, gref[0]) - kScoSkip) continue;
+        float3 ca = make_float3(0.f, 0.f, 0.f);
+#pragma unroll
+        for (int s = 0; s < MAXS; ++s)
+          if (s == arga) ca = make_float3(cx[s], cy[s], cz[s]);
         float3 nrm = make_float3(0.f, 0.f, 0.f);
         if (want_j) {
           const float dx = ca.x - cb.x, dy = ca.y - cb.y, dz = ca.z - cb.z;
@@ -297,62 +439,62 @@ __global__ void __launch_bounds__(128) sco_linearize_kernel(ScoLinArgs a) {
           const float inv = len > 0.f ? 1.f / len : 0.f;
           nrm = make_float3(dx * inv, dy * inv, dz * inv);
         }
-        acc.add(-dmin * inv_tau, role == 0, want_j, nrm, ca);
+        acc.add(ev, role == 0, want_j, nrm, ca);
       }
       if (want_soft) {
         acc.merge<TG>(gm);
-        if (gl == 0) acc.store(A + l * kScoAcc);
+        if (gl == 0) mine = acc;
+        // lane g folds link l into group g
+        if (gl < kScoG && mine.ref != -INFINITY) {
+          if (mine.ref > rg) {
+            const float k = (rg == -INFINITY) ? 0.f : __expf(rg - mine.ref);
+            sg *= k;
+            if (want_j)
+              for (int j = 0; j < nj; ++j) G[j] *= k;
+            rg = mine.ref;
+          }
+          const float k = __expf(mine.ref - rg);
+          sg += k * mine.s;
+          if (want_j) {
+            const float3 F = make_float3(k * mine.F.x, k * mine.F.y, k * mine.F.z);
+            const float3 Mo = make_float3(k * mine.M.x, k * mine.M.y, k * mine.M.z);
+            if (F.x != 0.f || F.y != 0.f || F.z != 0.f || Mo.x != 0.f || Mo.y != 0.f || Mo.z != 0.f) {
+              // every joint from the link's parent joint to the root moves the link
+              for (int j = lpj[l]; j >= 0; j = jt.psorted[j]) {
+                if (jt.kind[j] == kFixed) continue;
+                const Pose Tj = ps.load(j);
+                const float* tw = jt.tw[j];
+                const float3 w = quat_rotate(Tj.w, Tj.x, Tj.y, Tj.z, make_float3(tw[3], tw[4], tw[5]));
+                const float3 vv = quat_rotate(Tj.w, Tj.x, Tj.y, Tj.z, make_float3(tw[0], tw[1], tw[2]));
+                const float3 pxF = cross3(make_float3(Tj.tx, Tj.ty, Tj.tz), F);
+                G[j] += w.x * (Mo.x - pxF.x) + w.y * (Mo.y - pxF.y) + w.z * (Mo.z - pxF.z) + vv.x * F.x +
+                        vv.y * F.y + vv.z * F.z;
+              }
+            }
+          }
+        }
+        const int lane0 = (tid & 31) & ~(TG - 1);
+#pragma unroll
+        for (int g = 0; g < kScoG; ++g) gref[g] = __shfl_sync(gm, rg, lane0 + g);
       }
     }
     if (a.coll) {
       csum = group_sum<TG>(csum, gm);
       if (gl == 0) a.coll[c] = csum;
     }
-    __syncwarp(gm);
-    if (want_soft) {
-      // lane gl finishes groups gl, gl + TG, ...
-      for (int g = gl; g < kScoG; g += TG) {
-        const float* Ag = A + g * N * kScoAcc;
-        float rg = -INFINITY;
-        for (int l = 0; l < N; ++l) rg = fmaxf(rg, Ag[l * kScoAcc]);
-        float sum = 0.f;
-        if (rg != -INFINITY)
-          for (int l = 0; l < N; ++l) {
-            const float r = Ag[l * kScoAcc];
-            if (r != -INFINITY) sum += Ag[l * kScoAcc + 1] * expf(r - rg);
-          }
-        const bool has = sum > 0.f;
-        const float lse = has ? logf(sum) + rg : 0.f;
-        if (a.dist) a.dist[c * kScoG + g] = has ? -a.tau * lse : 1e10f;
-        if (!want_j) continue;
-        float* G = gjs + tid * nj;
-        for (int j = 0; j < nj; ++j) G[j] = 0.f;
-        if (has) {
-          for (int l = 0; l < N; ++l) {
-            const float* q8 = Ag + l * kScoAcc;
-            if (q8[0] == -INFINITY) continue;
-            const float k = expf(q8[0] - lse);
-            const float3 F = make_float3(k * q8[2], k * q8[3], k * q8[4]);
-            const float3 Mo = make_float3(k * q8[5], k * q8[6], k * q8[7]);
-            if (F.x == 0.f && F.y == 0.f && F.z == 0.f && Mo.x == 0.f && Mo.y == 0.f && Mo.z == 0.f) continue;
-            for (int j = lpj[l]; j >= 0; j = jt.psorted[j]) {
-              if (jt.kind[j] == kFixed) continue;
-              const Pose Tj = ps.load(j);
-              const float* tw = jt.tw[j];
-              const float3 w = quat_rotate(Tj.w, Tj.x, Tj.y, Tj.z, make_float3(tw[3], tw[4], tw[5]));
-              const float3 vv = quat_rotate(Tj.w, Tj.x, Tj.y, Tj.z, make_float3(tw[0], tw[1], tw[2]));
-              const float3 pxF = cross3(make_float3(Tj.tx, Tj.ty, Tj.tz), F);
-              G[j] += w.x * (Mo.x - pxF.x) + w.y * (Mo.y - pxF.y) + w.z * (Mo.z - pxF.z) + vv.x * F.x +
-                      vv.y * F.y + vv.z * F.z;
-            }
-          }
-        }
-        float* out = a.jac + (c * kScoG + g) * n;
+    if (want_soft && gl < kScoG) {
+      const bool has = sg > 0.f;
+      const float lse = has ? logf(sg) + rg : 0.f;
+      if (a.dist) a.dist[c * kScoG + gl] = has ? -a.tau * lse : 1e10f;
+      if (want_j) {
+        // softmax weights exp(-d/tau - lse) = exp(-d/tau - rg) / sg
+        const float inv = has ? 1.f / sg : 0.f;
+        float* out = a.jac + (c * kScoG + gl) * n;
         for (int col = 0; col < n; ++col) {
           float v = 0.f;
           for (int j = 0; j < nj; ++j)
             if (jt.src[j] == col) v += jt.mul[j] * G[j];
-          out[col] = v;
+          out[col] = v * inv;
         }
       }
     }
@@ -405,61 +547,75 @@ struct InnerView {
   float *x, *qk, *g, *gp, *dir, *bx, *acc, *gacc, *J, *dk, *dl, *gc, *lo, *hi, *rho, *syv, *yyv, *alph, *red, *Sb, *Yb;
 };
 
+// A thread's walk over a row-major [rows, n] element space, i = tid, tid +
+// nth, ...: its (row, column) advance without a division per step.
+struct Walk {
+  int t0, d0, dt, dd, n;
+  __device__ __forceinline__ void step(int& t, int& d) const {
+    t += dt;
+    d += dd;
+    if (d >= n) { d -= n; ++t; }
+  }
+};
+
 // Cost and gradient of the convex model at v.x; leaves acc(x) in v.acc and
-// d_lin in v.dl.
-__device__ float inner_cost_grad(const ScoInnerArgs& a, const InnerView& v) {
-  const int T = a.T, n = a.n, Tn = T * n, K = T > 4 ? T - 4 : 0, tid = threadIdx.x, nth = blockDim.x;
+// d_lin in v.dl.  Row k of acc is the stencil over rows k..k+4 of x, so the
+// element loops index acc and x by i +- q n.
+__device__ float inner_cost_grad(const ScoInnerArgs& a, const InnerView& v, const Walk& W) {
+  const int T = a.T, n = a.n, Tn = T * n, K = T > 4 ? T - 4 : 0, Kn = K * n, tid = threadIdx.x,
+            nth = blockDim.x;
   float part = 0.f;
   __syncthreads();  // x is complete
-  for (int i = tid; i < K * n; i += nth) {
-    const int k = i / n, d = i - k * n;
+  for (int i = tid; i < Kn; i += nth) {
     float s = 0.f;
 #pragma unroll
-    for (int q = 0; q < 5; ++q) s += kSt[q] * v.x[(k + q) * n + d];
+    for (int q = 0; q < 5; ++q) s += kSt[q] * v.x[i + q * n];
     v.acc[i] = s;
   }
   for (int i = tid; i < T * kScoG; i += nth) {
     const int t = i / kScoG;
     float dl = v.dk[i];
     const float* Jr = v.J + i * n;
-    for (int d = 0; d < n; ++d) dl += Jr[d] * (v.x[t * n + d] - v.qk[t * n + d]);
+    const float* xr = v.x + t * n;
+    const float* qr = v.qk + t * n;
+    for (int d = 0; d < n; ++d) dl += Jr[d] * (xr[d] - qr[d]);
     v.dl[i] = dl;
     const float viol = fmaxf(0.f, a.margin - dl);
     part += a.w_coll * viol * viol;
     v.gc[i] = -2.f * a.w_coll * viol;
   }
   __syncthreads();
-  for (int i = tid; i < K * n; i += nth) {
-    const int k = i / n;
+  for (int i = tid; i < Kn; i += nth) {
     const float c = v.acc[i];
     part += a.w_smooth * a.w_acc * c * c;
     float ga = 2.f * a.w_acc * c;
-    if (k + 1 < K) {
+    if (i + n < Kn) {
       const float j = v.acc[i + n] - c;
       part += a.w_smooth * a.w_jerk * j * j;
       ga -= 2.f * a.w_jerk * j;
     }
-    if (k >= 1) ga += 2.f * a.w_jerk * (c - v.acc[i - n]);
+    if (i >= n) ga += 2.f * a.w_jerk * (c - v.acc[i - n]);
     v.gacc[i] = ga;
   }
   __syncthreads();
-  for (int i = tid; i < Tn; i += nth) {
-    const int t = i / n, d = i - t * n;
+  for (int i = tid, t = W.t0, d = W.d0; i < Tn; i += nth, W.step(t, d)) {
     float gs = 0.f;
 #pragma unroll
     for (int q = 0; q < 5; ++q) {
-      const int k = t - q;
-      if (k >= 0 && k < K) gs += kSt[q] * v.gacc[k * n + d];
+      const int k = i - q * n;
+      if (k >= 0 && k < Kn) gs += kSt[q] * v.gacc[k];
     }
-    const float xv = v.x[i];
-    const float viol = fmaxf(0.f, xv - v.hi[d]) + fmaxf(0.f, v.lo[d] - xv);
+    const float xv = v.x[i], lo = v.lo[d], hi = v.hi[d];
+    const float viol = fmaxf(0.f, xv - hi) + fmaxf(0.f, lo - xv);
     part += a.w_limits * viol * viol;
-    const float sgn = xv > v.hi[d] ? 1.f : (xv < v.lo[d] ? -1.f : 0.f);
+    const float sgn = xv > hi ? 1.f : (xv < lo ? -1.f : 0.f);
     const float delta = xv - v.qk[i];
     part += a.w_trust * delta * delta;
     float gcol = 0.f;
+    const float* gct = v.gc + t * kScoG;
+    const float* Jt = v.J + t * kScoG * n + d;
 #pragma unroll
-    for (int g = 0; g < kScoG; ++g) gcol += v.gc[t * kScoG + g] * v.J[(t * kScoG + g) * n + d];
+    for (int g = 0; g < kScoG; ++g) gcol += gct[g] * Jt[g * n];
     float gi = a.w_smooth * gs + 2.f * a.w_limits * viol * sgn + gcol + 2.f * a.w_trust * delta;
     if (t == 0 || t == T - 1) gi = 0.f;
     v.g[i] = gi;
@@ -470,7 +626,7 @@ __device__ float inner_cost_grad(const ScoInnerArgs& a, const InnerView& v) {
 }
 
 template <bool SMEM_HIST>
-__global__ void __launch_bounds__(256) sco_inner_kernel(ScoInnerArgs a) {
+__global__ void __launch_bounds__(256, 2) sco_inner_kernel(ScoInnerArgs a) {
   extern __shared__ __align__(16) float sm[];
   const int T = a.T, n = a.n, Tn = T * n, K = T > 4 ? T - 4 : 0, m = a.m;
   const int tid = threadIdx.x, nth = blockDim.x;
@@ -509,12 +665,13 @@ __global__ void __launch_bounds__(256) sco_inner_kernel(ScoInnerArgs a) {
   for (int i = tid; i < kScoG * T; i += nth) v.dk[i] = a.dist[b * kScoG * T + i];
   for (int i = tid; i < n; i += nth) { v.lo[i] = a.lower[i]; v.hi[i] = a.upper[i]; }
 
-  float cost = inner_cost_grad(a, v);
+  const Walk W{tid / n, tid % n, nth / n, nth % n, n};
+  float cost = inner_cost_grad(a, v, W);
   float best_cost = cost;
   int m_used = 0, newest = 0;
   for (int it = 0; it < a.iters; ++it) {
     if (it > 0) {
-      cost = inner_cost_grad(a, v);
+      cost = inner_cost_grad(a, v, W);
       // curvature pair (s, y) = (last step, gradient change)
       float r[2] = {0.f, 0.f};
       for (int i = tid; i < Tn; i += nth) {
@@ -570,56 +727,58 @@ __global__ void __launch_bounds__(256) sco_inner_kernel(ScoInnerArgs a) {
       }
       for (int i = tid; i < Tn; i += nth) v.dir[i] = -v.dir[i];
     }
-    for (int i = tid; i < Tn; i += nth) {
-      const int t = i / n;
-      if (t == 0 || t == T - 1) v.dir[i] = 0.f;  // pinned endpoints
-    }
+    for (int i = tid; i < Tn; i += nth)
+      if (i < n || i >= Tn - n) v.dir[i] = 0.f;  // pinned endpoints
     __syncthreads();
     // 5-point line search: acc and d_lin are linear in the step, so the trial
     // costs take acc(x) + a acc(dir) and d_lin(x) + a J dir
-    for (int i = tid; i < K * n; i += nth) {
-      const int k = i / n, d = i - k * n;
+    const int Kn = K * n;
+    for (int i = tid; i < Kn; i += nth) {
       float s = 0.f;
 #pragma unroll
-      for (int q = 0; q < 5; ++q) s += kSt[q] * v.dir[(k + q) * n + d];
+      for (int q = 0; q < 5; ++q) s += kSt[q] * v.dir[i + q * n];
       v.gacc[i] = s;
     }
     for (int i = tid; i < T * kScoG; i += nth) {
       const int t = i / kScoG;
       float s = 0.f;
       const float* Jr = v.J + i * n;
-      for (int d = 0; d < n; ++d) s += Jr[d] * v.dir[t * n + d];
+      const float* dr = v.dir + t * n;
+      for (int d = 0; d < n; ++d) s += Jr[d] * dr[d];
       v.gc[i] = s;
     }
     __syncthreads();
     float tc[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
-    for (int i = tid; i < K * n; i += nth) {
-      const int k = i / n;
+    for (int i = tid; i < Kn; i += nth) {
+      const float c = v.acc[i], cd = v.gacc[i];
+      const bool jerk = i + n < Kn;
+      const float c1 = jerk ? v.acc[i + n] : 0.f, cd1 = jerk ? v.gacc[i + n] : 0.f;
 #pragma unroll
       for (int ai = 0; ai < 5; ++ai) {
         const float al = kLsAlpha[ai];
-        const float c0 = v.acc[i] + al * v.gacc[i];
+        const float c0 = c + al * cd;
         tc[ai] += a.w_smooth * a.w_acc * c0 * c0;
-        if (k + 1 < K) {
-          const float j = (v.acc[i + n] + al * v.gacc[i + n]) - c0;
+        if (jerk) {
+          const float j = (c1 + al * cd1) - c0;
           tc[ai] += a.w_smooth * a.w_jerk * j * j;
         }
       }
     }
-    for (int i = tid; i < Tn; i += nth) {
-      const int d = i % n;
+    for (int i = tid, t = W.t0, d = W.d0; i < Tn; i += nth, W.step(t, d)) {
+      const float x0 = v.x[i], p0 = v.dir[i], q0 = v.qk[i], lo = v.lo[d], hi = v.hi[d];
 #pragma unroll
       for (int ai = 0; ai < 5; ++ai) {
-        const float xv = v.x[i] + kLsAlpha[ai] * v.dir[i];
-        const float viol = fmaxf(0.f, xv - v.hi[d]) + fmaxf(0.f, v.lo[d] - xv);
-        const float delta = xv - v.qk[i];
+        const float xv = x0 + kLsAlpha[ai] * p0;
+        const float viol = fmaxf(0.f, xv - hi) + fmaxf(0.f, lo - xv);
+        const float delta = xv - q0;
         tc[ai] += a.w_limits * viol * viol + a.w_trust * delta * delta;
       }
     }
     for (int i = tid; i < T * kScoG; i += nth) {
+      const float dl = v.dl[i], gd = v.gc[i];
 #pragma unroll
       for (int ai = 0; ai < 5; ++ai) {
-        const float viol = fmaxf(0.f, a.margin - (v.dl[i] + kLsAlpha[ai] * v.gc[i]));
+        const float viol = fmaxf(0.f, a.margin - (dl + kLsAlpha[ai] * gd));
         tc[ai] += a.w_coll * viol * viol;
       }
     }
@@ -642,10 +801,8 @@ __global__ void __launch_bounds__(256) sco_inner_kernel(ScoInnerArgs a) {
   }
   __syncthreads();
   float* out = a.traj + b * Tn;
-  for (int i = tid; i < Tn; i += nth) {
-    const int t = i / n, d = i - t * n;
+  for (int i = tid, t = W.t0, d = W.d0; i < Tn; i += nth, W.step(t, d))
     out[i] = t == 0 ? a.start[d] : (t == T - 1 ? a.goal[d] : v.bx[i]);
-  }
 }
 
 // Nonlinear ranking cost per trajectory: smoothness + limits + w * sum_t coll[t].
@@ -727,9 +884,9 @@ __global__ void sco_fd_jac_kernel(const float* dfd, float* dist, float* jac, lon
 
 static size_t lin_smem(const ScoLinArgs& a, int nth, int TG) {
   const int ng = nth / TG, nj = a.m.n_joints;
-  size_t s = sizeof(JointTable) + sizeof(float4) * a.N * a.S + sizeof(int) * (3 * a.N + a.N + 1 + 2 * a.P);
+  size_t s = sizeof(JointTable) + sizeof(float4) * a.N * (a.S + 1) + sizeof(int) * (3 * a.N + a.N + 1 + 2 * a.P);
   s = (s + 15) & ~size_t(15);
-  s += sizeof(float) * ((size_t)nj * 7 * ng + (size_t)kScoG * a.N * kScoAcc * ng + (size_t)nj * nth);
+  s += sizeof(float) * ((size_t)nj * 7 * ng + (size_t)nj * nth);
   s = (s + 15) & ~size_t(15);
   return s + sizeof(float) * a.w.smem_floats();
 }
@@ -753,7 +910,7 @@ static int launch_linearize(const ScoLinArgs& a, cudaStream_t st) {
 
 static int inner_threads(const pk_sco_options* o, int Tn) {
   if (o->inner_threads > 0) return o->inner_threads;
-  return Tn <= 512 ? 64 : (Tn <= 1536 ? 128 : 256);
+  return Tn <= 1536 ? 128 : 256;
 }
 
 static size_t inner_smem_bytes(int T, int n, int m, bool hist) {

@@ -11,6 +11,7 @@ capture one warm launch.
     python -m pyroffi_b200.profile_cases batch       # persistent mixed batch, 512 problems
     python -m pyroffi_b200.profile_cases scolin      # SCO linearisation, 512 x 64 x 7 waypoints
     python -m pyroffi_b200.profile_cases scoinner    # SCO inner L-BFGS solve, 512 trajectories
+    python -m pyroffi_b200.profile_cases sco         # whole SCO run (10 x 30 iterations), 512 x 64 x 7
 """
 
 from __future__ import annotations
@@ -87,12 +88,15 @@ def _sco(stage):
     x = torch.as_tensor(wt.traj, device=dev)
     if stage == "lin":
         return lambda: opt.linearize(x)
+    if stage == "run":
+        return lambda: opt.run(x, x[0, 0], x[0, -1])
     d, J, _ = opt.linearize(x)
     return lambda: opt.inner(x, d, J, 1.0, x[0, 0], x[0, -1])
 
 
 CASES = {"lm": _lm, "fkc1": lambda: _fkc(65536, False), "fkc5": lambda: _fkc(4096, True), "wide": _wide,
-         "traj": _traj, "batch": _batch, "scolin": lambda: _sco("lin"), "scoinner": lambda: _sco("inner")}
+         "traj": _traj, "batch": _batch, "scolin": lambda: _sco("lin"), "scoinner": lambda: _sco("inner"),
+         "sco": lambda: _sco("run")}
 
 
 def main(argv=None) -> int:
