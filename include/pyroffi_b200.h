@@ -418,6 +418,54 @@ int pk_sco_trajopt(void* stream, const pk_sco_options* opt, const float* init_tr
                    int32_t Mc, int32_t Mb, int32_t Mh);
 
 /*
+ * HJCD-IK coarse phase: greedy coordinate descent on every seed.  Replaces
+ * "hjcd_ik_coarse_cuda" (HjcdIkCoarseCudaFfi,
+ * src/pyroffi/cuda_kernels/_hjcd_ik_cuda_kernel.cu:91-321, handler :697-764):
+ * buffers and attributes in the order of its Bind(), then the extents.
+ * seeds[P, S, n_act], target_jnts[n_ee], ancestor_masks[n_ee, n_joints],
+ * target_Ts[P, n_ee, 7], robot_spheres_local[n_rs, 4] with
+ * robot_sphere_joint_idx[n_rs], fixed_mask[n_act] (int32, may be NULL).
+ * Outputs out[P, S, n_act] and out_err[P, S] (unweighted squared error plus
+ * collision_weight * sum (d - margin)^2 over sphere/obstacle pairs closer
+ * than the margin).  At most 16 actuated joints and 4 EEs.
+ */
+int pk_hjcd_ik_coarse_cuda(void* stream, const float* seeds, const float* twists, const float* parent_tf,
+                           const int32_t* parent_idx, const int32_t* act_idx, const float* mimic_mul,
+                           const float* mimic_off, const int32_t* mimic_act_idx, const int32_t* topo_inv,
+                           const int32_t* target_jnts, const int32_t* ancestor_masks, const float* target_Ts,
+                           const float* robot_spheres_local, const int32_t* robot_sphere_joint_idx,
+                           const float* world_spheres, const float* world_capsules, const float* world_boxes,
+                           const float* world_halfspaces, const float* lower, const float* upper,
+                           const int32_t* fixed_mask, int64_t k_max, int64_t enable_collision,
+                           float collision_weight, float collision_margin, float* out, float* out_err,
+                           int32_t n_problems, int32_t n_seeds, int32_t n_act, int32_t n_joints, int32_t n_ee,
+                           int32_t n_robot_spheres, int32_t Ms, int32_t Mc, int32_t Mb, int32_t Mh);
+
+/*
+ * HJCD-IK refinement: Levenberg-Marquardt with adaptive row weights, a soft
+ * joint-limit prior, stall kicks from noise[P, S, max_iter, n_act] and
+ * best-iterate tracking.  Replaces "hjcd_ik_lm_cuda" (HjcdIkLmCudaFfi,
+ * _hjcd_ik_cuda_kernel.cu:324-695, handler :766-850): buffers and attributes
+ * in the order of its Bind().  Outputs out[P, S, n_act] (best configuration
+ * per seed), out_err[P, S] and stop_flag[P] (1 when a seed of the problem met
+ * eps_pos / eps_ori; every seed of that problem then stops at the next
+ * iteration).  At most 16 actuated joints and 4 EEs.
+ */
+int pk_hjcd_ik_lm_cuda(void* stream, const float* seeds, const float* noise, const float* twists,
+                       const float* parent_tf, const int32_t* parent_idx, const int32_t* act_idx,
+                       const float* mimic_mul, const float* mimic_off, const int32_t* mimic_act_idx,
+                       const int32_t* topo_inv, const int32_t* target_jnts, const int32_t* ancestor_masks,
+                       const float* target_Ts, const float* robot_spheres_local,
+                       const int32_t* robot_sphere_joint_idx, const float* world_spheres,
+                       const float* world_capsules, const float* world_boxes, const float* world_halfspaces,
+                       const float* lower, const float* upper, const int32_t* fixed_mask, int64_t max_iter,
+                       int64_t stall_patience, float lambda_init, float limit_prior_weight, float kick_scale,
+                       float eps_pos, float eps_ori, int64_t enable_collision, float collision_weight,
+                       float collision_margin, float* out, float* out_err, int32_t* stop_flag,
+                       int32_t n_problems, int32_t n_seeds, int32_t n_act, int32_t n_joints, int32_t n_ee,
+                       int32_t n_robot_spheres, int32_t Ms, int32_t Mc, int32_t Mb, int32_t Mh);
+
+/*
  * FP32 FMA-pipe microbenchmark (no reference counterpart): `blocks` blocks of
  * 256 threads, each thread 8 independent FMA chains of `iters` steps, i.e.
  * 4096 * iters * blocks FLOPs.  Time it with events on `stream`; it gives

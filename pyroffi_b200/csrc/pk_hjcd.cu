@@ -1,0 +1,699 @@
+// HJCD-IK on the GPU: greedy coordinate-descent coarse search followed by
+// Levenberg-Marquardt refinement with a joint-limit prior and stall kicks --
+// the drop-in for the hjcd_ik_coarse_cuda / hjcd_ik_lm_cuda custom calls
+// (src/pyroffi/cuda_kernels/_hjcd_ik_cuda_kernel.cu:91-695, bound by
+// src/pyroffi/cuda_kernels/_hjcd_ik_cuda.py).
+//
+// Coarse phase (:91-321), per seed, k_max steps: stacked residual and
+// Jacobian of every EE; row weights 1 (position) and
+// clamp(|r_pos| / |r_ori|, 0.05, 1) (orientation, set to 0 while the EE is
+// 1 mm or more away); of the free joints, the one with the largest predicted
+// decrease (J_a^T f)^2 / |J_a|^2 takes the step -J_a^T f / |J_a|^2, clamped to
+// the limits.  The score is the unweighted squared error plus the collision
+// penalty.
+//
+// Refinement (:324-695), per seed, max_iter iterations: the same adaptive row
+// weights (without gating), Jacobi column scaling, FP64 normal equations with
+// LM damping and the soft joint-limit prior lpw / h^2 (q - mid), fixed joints
+// masked, Cholesky (a non-positive pivot gives a zero step), the trust-region
+// clip, a 5-point line search on the unweighted error (the first trial that
+// is a new minimum and a sufficient decrease ends it), accept with lambda
+// x0.5 / reject x3, all-time best tracking, and a Gaussian kick from the
+// caller's noise after stall_patience rejections.  A seed whose EEs are all
+// within (eps_pos, eps_ori) stops, and so do the other seeds of its problem
+// from the next iteration on.
+//
+// B200 mapping.  Coarse: one thread per seed, grid (seed blocks, problems),
+// robot, limits, world and robot spheres in shared memory, joint poses in
+// per-thread shared slots.  Refinement: one warp per problem, one lane per
+// refinement seed (32 at a time); the problem's stop flag is a warp vote, so
+// every seed of a problem stops at the same iteration and results do not
+// depend on scheduling (the reference polls a global flag across blocks).
+#include <float.h>
+
+#include "pk_obstacles.cuh"
+
+namespace pk {
+
+struct HjcdArgs {
+  ModelArgs m;
+  WorldArgs w;
+  const float* seeds;          // [P, S, n]
+  const float* noise;          // [P, S, iters, n] (refinement kicks)
+  const int* target_jnts;      // [n_ee]
+  const int* ancestor_masks;   // [n_ee, n_joints]
+  const float* target_Ts;      // [P, n_ee, 7]
+  const float* rs_local;       // [n_rs, 4] robot spheres in their joint frames
+  const int* rs_joint;         // [n_rs]
+  const float* lower;
+  const float* upper;
+  const int* fixed_mask;       // [n]
+  float* out;                  // [P, S, n]
+  float* out_err;              // [P, S]
+  int* stop_flag;              // [P] or null
+  int P, S, n_ee, n_rs, iters, stall_patience, enable_collision, stage_world;
+  float collision_weight, collision_margin, lambda_init, limit_prior_weight, kick_scale, eps_pos, eps_ori;
+};
+
+constexpr int kHjcdWarps = 4;  // refinement: problems per block
+
+struct HjcdShared {
+  JointTable jt;
+  float tgt[kHjcdWarps][PK_MAX_EE][7];
+  unsigned long long anc[PK_MAX_EE];  // ancestor joints of each EE (original indices)
+  int tsorted[PK_MAX_EE];             // sorted position of each EE's joint
+  float lo[PK_MAX_ACT], hi[PK_MAX_ACT];
+  int fixed[PK_MAX_ACT];              // fixed or padding
+};
+
+__device__ __forceinline__ float clampf(float x, float lo, float hi) { return fmaxf(lo, fminf(hi, x)); }
+
+// Robot description, EE targets of `p0 + i` for i < n_tgt in slot i, limits,
+// robot spheres (joint-frame centre and radius, sorted joint position) and
+// optionally the world.  Ends with __syncthreads().
+__device__ void hjcd_stage(const HjcdArgs& a, HjcdShared& sh, float4* rs, int* rsj, float* world_dst, ObsView& ob,
+                           int p0, int n_tgt) {
+  load_joint_table(sh.jt, a.m);
+  const int n = a.m.n_act, nj = a.m.n_joints, tid = threadIdx.x, nth = blockDim.x;
+  for (int e = tid; e < a.n_ee; e += nth) {
+    unsigned long long m = 0ull;
+    for (int j = 0; j < nj && j < 64; ++j)
+      if (a.ancestor_masks[e * nj + j]) m |= 1ull << j;
+    sh.anc[e] = m;
+    const int tj = a.target_jnts[e];
+    sh.tsorted[e] = (tj >= 0 && tj < nj) ? sh.jt.sorted_of[tj] : 0;
+  }
+  for (int i = tid; i < n_tgt * a.n_ee * 7; i += nth) {
+    const int w = i / (a.n_ee * 7), r = i - w * a.n_ee * 7;
+    const int p = p0 + w;
+    sh.tgt[w][r / 7][r % 7] = p < a.P ? a.target_Ts[(size_t)p * a.n_ee * 7 + r] : 0.f;
+  }
+  for (int c = tid; c < PK_MAX_ACT; c += nth) {
+    const bool live = c < n;
+    sh.lo[c] = live ? a.lower[c] : 0.f;
+    sh.hi[c] = live ? a.upper[c] : 0.f;
+    sh.fixed[c] = live ? (a.fixed_mask ? a.fixed_mask[c] != 0 : 0) : 1;
+  }
+  for (int i = tid; i < a.n_rs; i += nth) {
+    const float* q = a.rs_local + 4 * i;
+    rs[i] = make_float4(q[0], q[1], q[2], q[3]);
+    const int j = a.rs_joint[i];
+    rsj[i] = (j >= 0 && j < nj) ? sh.jt.sorted_of[j] : -1;
+  }
+  if (a.stage_world) {
+    ob = stage_world(a.w, world_dst);
+  } else {
+    ob.sph = reinterpret_cast<const float4*>(a.w.spheres);
+    ob.cap = a.w.capsules;
+    ob.box = a.w.boxes;
+    ob.hs = a.w.halfspaces;
+    ob.Ms = a.w.Ms; ob.Mc = a.w.Mc; ob.Mb = a.w.Mb; ob.Mh = a.w.Mh;
+  }
+  __syncthreads();
+}
+
+// Residual of every EE against target slot `w`: world position difference and
+// the rotation vector of q_ee conj(q_tgt) (w >= 0; 2 v below |v| = 1e-6).
+template <int MAXEE>
+__device__ __forceinline__ void hjcd_residual(const HjcdShared& sh, const PoseSlots& ps, int n_ee, int w,
+                                              float (&r)[6 * MAXEE], float (&pee)[3 * MAXEE]) {
+#pragma unroll
+  for (int e = 0; e < MAXEE; ++e) {
+    if (e >= n_ee) {
+#pragma unroll
+      for (int c = 0; c < 6; ++c) r[6 * e + c] = 0.f;
+      pee[3 * e] = pee[3 * e + 1] = pee[3 * e + 2] = 0.f;
+      continue;
+    }
+    const Pose T = ps.load(sh.tsorted[e]);
+    const float* g = sh.tgt[w][e];
+    r[6 * e + 0] = T.tx - g[4];
+    r[6 * e + 1] = T.ty - g[5];
+    r[6 * e + 2] = T.tz - g[6];
+    const float bw = g[0], bx = -g[1], by = -g[2], bz = -g[3];
+    float qw = T.w * bw - T.x * bx - T.y * by - T.z * bz;
+    float qx = T.w * bx + T.x * bw + T.y * bz - T.z * by;
+    float qy = T.w * by - T.x * bz + T.y * bw + T.z * bx;
+    float qz = T.w * bz + T.x * by - T.y * bx + T.z * bw;
+    if (qw < 0.f) { qw = -qw; qx = -qx; qy = -qy; qz = -qz; }
+    const float s = sqrtf(qx * qx + qy * qy + qz * qz);
+    const float f = s > 1e-6f ? 2.f * atan2f(s, qw) / s : 2.f;
+    r[6 * e + 3] = qx * f;
+    r[6 * e + 4] = qy * f;
+    r[6 * e + 5] = qz * f;
+    pee[3 * e] = T.tx; pee[3 * e + 1] = T.ty; pee[3 * e + 2] = T.tz;
+  }
+}
+
+// Stacked geometric Jacobian J[k][c] (revolute z x (p_ee - p_j) / z,
+// prismatic z / 0, times the mimic multiplier, restricted to each EE's
+// ancestors).
+template <int MAXA, int MAXEE>
+__device__ __forceinline__ void hjcd_jacobian(const HjcdShared& sh, const PoseSlots& ps, int n_ee,
+                                              const float (&pee)[3 * MAXEE], float (&J)[6 * MAXEE][MAXA]) {
+  const JointTable& jt = sh.jt;
+#pragma unroll
+  for (int k = 0; k < 6 * MAXEE; ++k)
+#pragma unroll
+    for (int c = 0; c < MAXA; ++c) J[k][c] = 0.f;
+  for (int i = 0; i < jt.n; ++i) {
+    const int jk = jt.jkind[i];
+    const int a1 = jt.a1[i], a2 = jt.a2[i];
+    if (jk == 0 || (a1 < 0 && a2 < 0)) continue;
+    const Pose Tj = ps.load(i);
+    const float3 z = quat_rotate(Tj.w, Tj.x, Tj.y, Tj.z, make_float3(jt.axis[i][0], jt.axis[i][1], jt.axis[i][2]));
+    const float sm = jt.mul[i];
+    const int orig = jt.orig[i];
+#pragma unroll
+    for (int e = 0; e < MAXEE; ++e) {
+      if (e >= n_ee || orig >= 64 || !((sh.anc[e] >> orig) & 1ull)) continue;
+      float col[6];
+      if (jk == 1) {
+        const float ax = pee[3 * e] - Tj.tx, ay = pee[3 * e + 1] - Tj.ty, az = pee[3 * e + 2] - Tj.tz;
+        col[0] = z.y * az - z.z * ay; col[1] = z.z * ax - z.x * az; col[2] = z.x * ay - z.y * ax;
+        col[3] = z.x; col[4] = z.y; col[5] = z.z;
+      } else {
+        col[0] = z.x; col[1] = z.y; col[2] = z.z; col[3] = col[4] = col[5] = 0.f;
+      }
+#pragma unroll
+      for (int c = 0; c < MAXA; ++c) {
+        const float wsel = ((c == a1) ? sm : 0.f) + ((c == a2) ? sm : 0.f);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) J[6 * e + k][c] += wsel * col[k];
+      }
+    }
+  }
+}
+
+// Collision penalty weight * sum over (robot sphere, obstacle) with d < margin
+// of (d - margin)^2, from the joint poses in `ps`.
+__device__ __forceinline__ float hjcd_penalty(const HjcdArgs& a, const PoseSlots& ps, const float4* rs,
+                                              const int* rsj, const ObsView& ob) {
+  if (!a.enable_collision || a.n_rs <= 0) return 0.f;
+  const int M = ob.Ms + ob.Mc + ob.Mb + ob.Mh;
+  const float margin = a.collision_margin;
+  float pen = 0.f;
+  for (int i = 0; i < a.n_rs; ++i) {
+    const int j = rsj[i];
+    if (j < 0) continue;
+    const float4 q = rs[i];
+    const float3 c = pose_apply(ps.load(j), make_float3(q.x, q.y, q.z));
+    for (int m = 0; m < M; ++m) {
+      const float d = obstacle_dist(ob, m, c, q.w);
+      if (d < margin) {
+        const float e = d - margin;
+        pen += e * e;
+      }
+    }
+  }
+  return a.collision_weight * pen;
+}
+
+template <int MAXA>
+__device__ __forceinline__ float reg_at(const float (&v)[MAXA], int i) {
+  float r = 0.f;
+#pragma unroll
+  for (int c = 0; c < MAXA; ++c)
+    if (c == i) r = v[c];
+  return r;
+}
+
+__device__ __forceinline__ size_t hjcd_world_offset(const HjcdArgs& a) {
+  size_t s = sizeof(HjcdShared) + sizeof(float4) * a.n_rs + sizeof(int) * a.n_rs;
+  return (s + 15) & ~size_t(15);
+}
+
+// ---------------------------------------------------------------------------
+// coarse phase: one thread per seed
+// ---------------------------------------------------------------------------
+
+template <int MAXA, int MAXEE>
+__global__ void __launch_bounds__(128) hjcd_coarse_kernel(HjcdArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  HjcdShared& sh = *reinterpret_cast<HjcdShared*>(smem_raw);
+  float4* rs = reinterpret_cast<float4*>(smem_raw + sizeof(HjcdShared));
+  int* rsj = reinterpret_cast<int*>(rs + a.n_rs);
+  float* world = reinterpret_cast<float*>(smem_raw + hjcd_world_offset(a));
+  float* slots = world + (a.stage_world ? a.w.smem_floats() : 0);
+  const int p = blockIdx.y, tid = threadIdx.x, n = a.m.n_act;
+  ObsView ob;
+  hjcd_stage(a, sh, rs, rsj, world, ob, p, 1);
+  const int s = blockIdx.x * blockDim.x + tid;
+  if (s >= a.S) return;
+  const size_t gs = (size_t)p * a.S + s;
+  const PoseSlots ps{slots + tid, (int)blockDim.x};
+  float cfg[MAXA];
+#pragma unroll
+  for (int c = 0; c < MAXA; ++c) cfg[c] = c < n ? a.seeds[gs * n + c] : 0.f;
+  auto cfg_at = [&](int i) { return reg_at(cfg, i); };
+  float r[6 * MAXEE], pee[3 * MAXEE];
+  float J[6 * MAXEE][MAXA];
+  for (int it = 0; it < a.iters; ++it) {
+    fk_thread(sh.jt, cfg_at, ps);
+    hjcd_residual<MAXEE>(sh, ps, a.n_ee, 0, r, pee);
+    hjcd_jacobian<MAXA, MAXEE>(sh, ps, a.n_ee, pee, J);
+    // adaptive row weights, orientation gated off 1 mm or more from the target
+    float fw[6 * MAXEE];
+#pragma unroll
+    for (int e = 0; e < MAXEE; ++e) {
+      const float pn = sqrtf(r[6 * e] * r[6 * e] + r[6 * e + 1] * r[6 * e + 1] + r[6 * e + 2] * r[6 * e + 2]);
+      const float on = sqrtf(r[6 * e + 3] * r[6 * e + 3] + r[6 * e + 4] * r[6 * e + 4] + r[6 * e + 5] * r[6 * e + 5]);
+      float wo = clampf((pn + 1e-8f) / (on + 1e-8f), 0.05f, 1.f);
+      if (pn >= 1e-3f) wo = 0.f;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        const float wk = k < 3 ? 1.f : wo;
+        fw[6 * e + k] = r[6 * e + k] * wk;
+#pragma unroll
+        for (int c = 0; c < MAXA; ++c) J[6 * e + k][c] *= wk;
+      }
+    }
+    int best = -1;
+    float best_impr = -1.f, best_step = 0.f;
+#pragma unroll
+    for (int c = 0; c < MAXA; ++c) {
+      float dot = 0.f, sq = 0.f;
+#pragma unroll
+      for (int k = 0; k < 6 * MAXEE; ++k) {
+        dot += J[k][c] * fw[k];
+        sq += J[k][c] * J[k][c];
+      }
+      sq += 1e-8f;
+      const float impr = dot * dot / sq;
+      if (!sh.fixed[c] && impr > best_impr) { best_impr = impr; best = c; best_step = -dot / sq; }
+    }
+    if (best < 0) break;
+#pragma unroll
+    for (int c = 0; c < MAXA; ++c)
+      if (c == best) cfg[c] = clampf(cfg[c] + best_step, sh.lo[c], sh.hi[c]);
+  }
+  fk_thread(sh.jt, cfg_at, ps);
+  hjcd_residual<MAXEE>(sh, ps, a.n_ee, 0, r, pee);
+  float err = 0.f;
+#pragma unroll
+  for (int k = 0; k < 6 * MAXEE; ++k) err += r[k] * r[k];
+  err += hjcd_penalty(a, ps, rs, rsj, ob);
+  a.out_err[gs] = err;
+  for (int c = 0; c < n; ++c) a.out[gs * n + c] = reg_at(cfg, c);
+}
+
+// ---------------------------------------------------------------------------
+// refinement: one warp per problem, one lane per seed
+// ---------------------------------------------------------------------------
+
+// Unweighted squared error plus penalty at the joint poses in `ps`.
+template <int MAXEE>
+__device__ __forceinline__ float hjcd_error(const HjcdArgs& a, const HjcdShared& sh, const PoseSlots& ps, int w,
+                                            const float4* rs, const int* rsj, const ObsView& ob,
+                                            float (&r)[6 * MAXEE], float (&pee)[3 * MAXEE]) {
+  hjcd_residual<MAXEE>(sh, ps, a.n_ee, w, r, pee);
+  float err = 0.f;
+#pragma unroll
+  for (int k = 0; k < 6 * MAXEE; ++k) err += r[k] * r[k];
+  return err + hjcd_penalty(a, ps, rs, rsj, ob);
+}
+
+// LM step of the current point: adaptive row weights, Jacobi column scaling,
+// FP64 normal equations with damping and the joint-limit prior, fixed and
+// padding columns masked, Cholesky (zero step on a non-positive pivot),
+// unscaling and the trust-region clip.
+template <int MAXA, int MAXEE>
+__device__ __forceinline__ void hjcd_direction(const HjcdArgs& a, const HjcdShared& sh, const PoseSlots& ps,
+                                               const float (&r)[6 * MAXEE], const float (&pee)[3 * MAXEE],
+                                               const float (&cfg)[MAXA], float lam, float (&delta)[MAXA]) {
+  const int n_ee = a.n_ee;
+  float J[6 * MAXEE][MAXA];
+  hjcd_jacobian<MAXA, MAXEE>(sh, ps, n_ee, pee, J);
+  float fw[6 * MAXEE];
+  float max_p = 0.f, max_o = 0.f;
+#pragma unroll
+  for (int e = 0; e < MAXEE; ++e) {
+    const float pn = sqrtf(r[6 * e] * r[6 * e] + r[6 * e + 1] * r[6 * e + 1] + r[6 * e + 2] * r[6 * e + 2]);
+    const float on = sqrtf(r[6 * e + 3] * r[6 * e + 3] + r[6 * e + 4] * r[6 * e + 4] + r[6 * e + 5] * r[6 * e + 5]);
+    if (e < n_ee) { max_p = fmaxf(max_p, pn); max_o = fmaxf(max_o, on); }
+    const float wo = clampf((pn + 1e-8f) / (on + 1e-8f), 0.05f, 1.f);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      const float wk = k < 3 ? 1.f : wo;
+      fw[6 * e + k] = r[6 * e + k] * wk;
+#pragma unroll
+      for (int c = 0; c < MAXA; ++c) J[6 * e + k][c] *= wk;
+    }
+  }
+  float cs[MAXA];
+#pragma unroll
+  for (int c = 0; c < MAXA; ++c) {
+    float sq = 0.f;
+#pragma unroll
+    for (int k = 0; k < 6 * MAXEE; ++k) sq += J[k][c] * J[k][c];
+    cs[c] = sqrtf(sq) + 1e-8f;
+  }
+#pragma unroll
+  for (int k = 0; k < 6 * MAXEE; ++k)
+#pragma unroll
+    for (int c = 0; c < MAXA; ++c) J[k][c] = J[k][c] / cs[c];
+  double A[MAXA * (MAXA + 1) / 2];
+  double rhs[MAXA];
+#pragma unroll
+  for (int i = 0; i < MAXA; ++i) {
+    const bool fi = sh.fixed[i];
+#pragma unroll
+    for (int j = 0; j <= i; ++j) {
+      double acc = 0.0;
+#pragma unroll
+      for (int k = 0; k < 6 * MAXEE; ++k) acc += (double)J[k][i] * (double)J[k][j];
+      const bool fj = sh.fixed[j];
+      A[i * (i + 1) / 2 + j] = (fi || fj) ? ((i == j) ? 1.0 : 0.0) : acc;
+    }
+    double rb = 0.0;
+#pragma unroll
+    for (int k = 0; k < 6 * MAXEE; ++k) rb += (double)J[k][i] * (double)fw[k];
+    if (fi) {
+      rhs[i] = 0.0;
+    } else {
+      const double hr = (double)((sh.hi[i] - sh.lo[i]) * 0.5f + 1e-8f);
+      const double mid = (double)((sh.lo[i] + sh.hi[i]) * 0.5f);
+      const double dpr = (double)a.limit_prior_weight / (hr * hr);
+      A[i * (i + 1) / 2 + i] += (double)lam + dpr / ((double)cs[i] * (double)cs[i]);
+      rhs[i] = -(rb + dpr * (double)(cfg[i] - (float)mid) / (double)cs[i]);
+    }
+  }
+  bool ok = true;
+#pragma unroll
+  for (int k = 0; k < MAXA; ++k) {
+    double s2 = A[k * (k + 1) / 2 + k];
+#pragma unroll
+    for (int q = 0; q < k; ++q) s2 -= A[k * (k + 1) / 2 + q] * A[k * (k + 1) / 2 + q];
+    if (!(s2 > 0.0)) ok = false;
+    const double lkk = sqrt(ok ? s2 : 1.0);
+    const double inv = 1.0 / lkk;
+    A[k * (k + 1) / 2 + k] = lkk;
+#pragma unroll
+    for (int i = k + 1; i < MAXA; ++i) {
+      double tt = A[i * (i + 1) / 2 + k];
+#pragma unroll
+      for (int q = 0; q < k; ++q) tt -= A[i * (i + 1) / 2 + q] * A[k * (k + 1) / 2 + q];
+      A[i * (i + 1) / 2 + k] = tt * inv;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < MAXA; ++i) {
+    double s2 = rhs[i];
+#pragma unroll
+    for (int q = 0; q < i; ++q) s2 -= A[i * (i + 1) / 2 + q] * rhs[q];
+    rhs[i] = s2 / A[i * (i + 1) / 2 + i];
+  }
+#pragma unroll
+  for (int i = MAXA - 1; i >= 0; --i) {
+    double s2 = rhs[i];
+#pragma unroll
+    for (int q = i + 1; q < MAXA; ++q) s2 -= A[q * (q + 1) / 2 + i] * rhs[q];
+    rhs[i] = s2 / A[i * (i + 1) / 2 + i];
+  }
+  float dn2 = 0.f;
+#pragma unroll
+  for (int c = 0; c < MAXA; ++c) {
+    delta[c] = ok ? (float)rhs[c] / cs[c] : 0.f;
+    dn2 += delta[c] * delta[c];
+  }
+  float R;
+  if (max_p > 1e-2f || max_o > 0.6f) R = 0.38f;
+  else if (max_p > 1e-3f || max_o > 0.25f) R = 0.22f;
+  else if (max_p > 2e-4f || max_o > 0.08f) R = 0.12f;
+  else R = 0.05f;
+  const float dn = sqrtf(dn2);
+  if (dn > R) {
+    const float sc = R / (dn + 1e-18f);
+#pragma unroll
+    for (int c = 0; c < MAXA; ++c) delta[c] *= sc;
+  }
+}
+
+template <int MAXA, int MAXEE>
+__global__ void __launch_bounds__(32 * kHjcdWarps) hjcd_lm_kernel(HjcdArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  HjcdShared& sh = *reinterpret_cast<HjcdShared*>(smem_raw);
+  float4* rs = reinterpret_cast<float4*>(smem_raw + sizeof(HjcdShared));
+  int* rsj = reinterpret_cast<int*>(rs + a.n_rs);
+  float* world = reinterpret_cast<float*>(smem_raw + hjcd_world_offset(a));
+  float* slots = world + (a.stage_world ? a.w.smem_floats() : 0);
+  const int tid = threadIdx.x, wid = tid >> 5, lane = tid & 31, n = a.m.n_act;
+  const int p0 = blockIdx.x * kHjcdWarps;
+  ObsView ob;
+  hjcd_stage(a, sh, rs, rsj, world, ob, p0, kHjcdWarps);
+  const int p = p0 + wid;
+  if (p >= a.P) return;  // whole warp
+  const PoseSlots ps{slots + tid, (int)blockDim.x};
+  const float alphas[5] = {1.f, 0.5f, 0.25f, 0.1f, 0.025f};
+  bool stop = false;  // warp-uniform: a seed of this problem has converged
+  for (int s0 = 0; s0 < a.S; s0 += 32) {
+    const int s = s0 + lane;
+    const bool live = s < a.S;
+    const size_t gs = (size_t)p * a.S + (live ? s : 0);
+    float cfg[MAXA], best_cfg[MAXA];
+#pragma unroll
+    for (int c = 0; c < MAXA; ++c) cfg[c] = best_cfg[c] = (live && c < n) ? a.seeds[gs * n + c] : 0.f;
+    auto cur_at = [&](int i) { return reg_at(cfg, i); };
+    float r[6 * MAXEE], pee[3 * MAXEE];
+    fk_thread(sh.jt, cur_at, ps);
+    float best_err = hjcd_error<MAXEE>(a, sh, ps, wid, rs, rsj, ob, r, pee);
+    float lam = a.lambda_init;
+    int stall = 0;
+    bool done = !live || stop;
+    for (int it = 0; it < a.iters; ++it) {
+      if (stop) done = true;
+      if (__all_sync(0xffffffffu, done)) break;
+      bool conv = false;
+      float curr = 0.f;
+      if (!done) {
+        fk_thread(sh.jt, cur_at, ps);
+        curr = hjcd_error<MAXEE>(a, sh, ps, wid, rs, rsj, ob, r, pee);
+        conv = true;
+#pragma unroll
+        for (int e = 0; e < MAXEE; ++e) {
+          if (e >= a.n_ee) continue;
+          const float pn = sqrtf(r[6 * e] * r[6 * e] + r[6 * e + 1] * r[6 * e + 1] + r[6 * e + 2] * r[6 * e + 2]);
+          const float on =
+              sqrtf(r[6 * e + 3] * r[6 * e + 3] + r[6 * e + 4] * r[6 * e + 4] + r[6 * e + 5] * r[6 * e + 5]);
+          if (pn >= a.eps_pos || on >= a.eps_ori) conv = false;
+        }
+      }
+      if (__any_sync(0xffffffffu, !done && conv)) stop = true;
+      if (conv) done = true;
+      if (done) continue;
+      float delta[MAXA];
+      hjcd_direction<MAXA, MAXEE>(a, sh, ps, r, pee, cfg, lam, delta);
+      // line search on the unweighted error
+      float best_a_err = 1e30f;
+      int best_ai = 0;
+      for (int ai = 0; ai < 5; ++ai) {
+        float trial[MAXA];
+#pragma unroll
+        for (int c = 0; c < MAXA; ++c) trial[c] = clampf(cfg[c] + alphas[ai] * delta[c], sh.lo[c], sh.hi[c]);
+        fk_thread(sh.jt, [&](int i) { return reg_at(trial, i); }, ps);
+        float rt[6 * MAXEE], pt[3 * MAXEE];
+        const float et = hjcd_error<MAXEE>(a, sh, ps, wid, rs, rsj, ob, rt, pt);
+        if (et < best_a_err) {
+          best_a_err = et;
+          best_ai = ai;
+          if (et < curr * (1.f - 1e-4f)) break;
+        }
+      }
+      float trial[MAXA];
+#pragma unroll
+      for (int c = 0; c < MAXA; ++c) trial[c] = clampf(cfg[c] + alphas[best_ai] * delta[c], sh.lo[c], sh.hi[c]);
+      if (best_a_err < curr * (1.f - 1e-4f)) {
+#pragma unroll
+        for (int c = 0; c < MAXA; ++c) cfg[c] = trial[c];
+        lam = fmaxf(lam * 0.5f, 1e-10f);
+        stall = 0;
+      } else {
+        lam = fminf(lam * 3.f, 1e6f);
+        ++stall;
+      }
+      if (best_a_err < best_err) {
+        best_err = best_a_err;
+#pragma unroll
+        for (int c = 0; c < MAXA; ++c) best_cfg[c] = trial[c];
+      }
+      if (stall >= a.stall_patience) {
+        const float* kn = a.noise + (gs * a.iters + it) * n;
+#pragma unroll
+        for (int c = 0; c < MAXA; ++c)
+          if (c < n && !sh.fixed[c]) cfg[c] = clampf(cfg[c] + kn[c] * a.kick_scale, sh.lo[c], sh.hi[c]);
+        lam = a.lambda_init;
+        stall = 0;
+      }
+    }
+    if (live) {
+      for (int c = 0; c < n; ++c) a.out[gs * n + c] = reg_at(best_cfg, c);
+      a.out_err[gs] = best_err;
+    }
+  }
+  if (lane == 0 && a.stop_flag) a.stop_flag[p] = stop ? 1 : 0;
+}
+
+static size_t hjcd_smem(const HjcdArgs& a, int nth) {
+  size_t s = sizeof(HjcdShared) + sizeof(float4) * a.n_rs + sizeof(int) * a.n_rs;
+  s = (s + 15) & ~size_t(15);
+  if (a.stage_world) s += sizeof(float) * a.w.smem_floats();
+  return s + sizeof(float) * (size_t)a.m.n_joints * 7 * nth;
+}
+
+}  // namespace pk
+
+using namespace pk;
+
+namespace {
+
+int hjcd_common(HjcdArgs& a, int n_act, int n_joints, int n_ee, int nth, size_t* smem_out) {
+  PK_CHECK_ARG(a.P >= 0 && a.S >= 0 && n_act >= 0 && n_joints >= 0 && n_ee >= 0 && a.n_rs >= 0, "negative extent");
+  PK_CHECK_CAP(n_joints <= PK_MAX_JOINTS, "n_joints=%d exceeds %d", n_joints, PK_MAX_JOINTS);
+  PK_CHECK_CAP(n_act <= 16, "HJCD takes at most 16 actuated joints (got %d)", n_act);
+  PK_CHECK_CAP(n_ee >= 1 && n_ee <= PK_MAX_EE, "n_ee=%d must be in [1, %d]", n_ee, PK_MAX_EE);
+  PK_CHECK_ARG(a.iters >= 0, "negative iteration count");
+  a.stage_world = a.w.smem_floats() * sizeof(float) <= 48 * 1024;
+  size_t smem = hjcd_smem(a, nth);
+  if (smem > 200 * 1024 && a.stage_world) {
+    a.stage_world = 0;
+    smem = hjcd_smem(a, nth);
+  }
+  PK_CHECK_CAP(smem <= 200 * 1024, "HJCD working set (%zu B of shared memory) too large", smem);
+  *smem_out = smem;
+  return PK_OK;
+}
+
+template <int MAXA, int MAXEE>
+int launch_coarse(const HjcdArgs& a, int nth, size_t smem, cudaStream_t st) {
+  auto k = hjcd_coarse_kernel<MAXA, MAXEE>;
+  if (int s = set_smem_limit((const void*)k, smem)) return s;
+  const dim3 grid((unsigned)((a.S + nth - 1) / nth), (unsigned)a.P);
+  k<<<grid, nth, smem, st>>>(a);
+  return cuda_status(cudaGetLastError(), "hjcd_coarse_kernel launch");
+}
+
+template <int MAXA, int MAXEE>
+int launch_lm(const HjcdArgs& a, size_t smem, cudaStream_t st) {
+  auto k = hjcd_lm_kernel<MAXA, MAXEE>;
+  if (int s = set_smem_limit((const void*)k, smem)) return s;
+  const unsigned blocks = (unsigned)((a.P + kHjcdWarps - 1) / kHjcdWarps);
+  k<<<blocks, 32 * kHjcdWarps, smem, st>>>(a);
+  return cuda_status(cudaGetLastError(), "hjcd_lm_kernel launch");
+}
+
+HjcdArgs hjcd_args(const float* seeds, const float* twists, const float* parent_tf, const int32_t* parent_idx,
+                   const int32_t* act_idx, const float* mimic_mul, const float* mimic_off,
+                   const int32_t* mimic_act_idx, const int32_t* topo_inv, const int32_t* target_jnts,
+                   const int32_t* ancestor_masks, const float* target_Ts, const float* rs_local,
+                   const int32_t* rs_joint, const float* ws, const float* wc, const float* wb, const float* wh,
+                   const float* lower, const float* upper, const int32_t* fixed_mask, float* out, float* out_err,
+                   int32_t P, int32_t S, int32_t n_act, int32_t n_joints, int32_t n_ee, int32_t n_rs, int32_t Ms,
+                   int32_t Mc, int32_t Mb, int32_t Mh) {
+  HjcdArgs a{};
+  a.m = ModelArgs{twists, parent_tf, parent_idx, act_idx, mimic_mul, mimic_off, mimic_act_idx, topo_inv, n_joints,
+                  n_act};
+  a.w = WorldArgs{ws, wc, wb, wh, Ms, Mc, Mb, Mh};
+  a.seeds = seeds; a.target_jnts = target_jnts; a.ancestor_masks = ancestor_masks; a.target_Ts = target_Ts;
+  a.rs_local = rs_local; a.rs_joint = rs_joint; a.lower = lower; a.upper = upper; a.fixed_mask = fixed_mask;
+  a.out = out; a.out_err = out_err;
+  a.P = P; a.S = S; a.n_ee = n_ee; a.n_rs = n_rs;
+  return a;
+}
+
+int check_buffers(const HjcdArgs& a) {
+  PK_CHECK_ARG(a.seeds && a.m.twists && a.m.parent_tf && a.m.parent_idx && a.m.act_idx && a.m.mimic_mul &&
+                   a.m.mimic_off && a.m.mimic_act_idx && a.m.topo_inv && a.target_jnts && a.ancestor_masks &&
+                   a.target_Ts && a.lower && a.upper && a.out && a.out_err,
+               "null buffer");
+  PK_CHECK_ARG(a.n_rs == 0 || (a.rs_local && a.rs_joint), "null robot spheres");
+  PK_CHECK_ARG((a.w.Ms == 0 || a.w.spheres) && (a.w.Mc == 0 || a.w.capsules) && (a.w.Mb == 0 || a.w.boxes) &&
+                   (a.w.Mh == 0 || a.w.halfspaces),
+               "null world buffer");
+  return PK_OK;
+}
+
+}  // namespace
+
+extern "C" int pk_hjcd_ik_coarse_cuda(void* stream, const float* seeds, const float* twists, const float* parent_tf,
+                                      const int32_t* parent_idx, const int32_t* act_idx, const float* mimic_mul,
+                                      const float* mimic_off, const int32_t* mimic_act_idx, const int32_t* topo_inv,
+                                      const int32_t* target_jnts, const int32_t* ancestor_masks,
+                                      const float* target_Ts, const float* robot_spheres_local,
+                                      const int32_t* robot_sphere_joint_idx, const float* world_spheres,
+                                      const float* world_capsules, const float* world_boxes,
+                                      const float* world_halfspaces, const float* lower, const float* upper,
+                                      const int32_t* fixed_mask, int64_t k_max, int64_t enable_collision,
+                                      float collision_weight, float collision_margin, float* out, float* out_err,
+                                      int32_t n_problems, int32_t n_seeds, int32_t n_act, int32_t n_joints,
+                                      int32_t n_ee, int32_t n_robot_spheres, int32_t Ms, int32_t Mc, int32_t Mb,
+                                      int32_t Mh) {
+  HjcdArgs a = hjcd_args(seeds, twists, parent_tf, parent_idx, act_idx, mimic_mul, mimic_off, mimic_act_idx,
+                         topo_inv, target_jnts, ancestor_masks, target_Ts, robot_spheres_local,
+                         robot_sphere_joint_idx, world_spheres, world_capsules, world_boxes, world_halfspaces, lower,
+                         upper, fixed_mask, out, out_err, n_problems, n_seeds, n_act, n_joints, n_ee,
+                         n_robot_spheres, Ms, Mc, Mb, Mh);
+  PK_CHECK_ARG(k_max >= 0 && k_max < (1LL << 31), "bad k_max");
+  a.iters = (int)k_max;
+  a.enable_collision = enable_collision ? 1 : 0;
+  a.collision_weight = collision_weight;
+  a.collision_margin = collision_margin;
+  const int nth = n_seeds < 128 ? ((n_seeds + 31) / 32) * 32 : 128;
+  size_t smem = 0;
+  if (int s = hjcd_common(a, n_act, n_joints, n_ee, nth < 32 ? 32 : nth, &smem)) return s;
+  if (n_problems == 0 || n_seeds == 0) return PK_OK;
+  if (int s = check_buffers(a)) return s;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int t = nth < 32 ? 32 : nth;
+  if (n_act <= 8 && n_ee == 1) return launch_coarse<8, 1>(a, t, smem, st);
+  if (n_ee <= 2) return launch_coarse<16, 2>(a, t, smem, st);
+  return launch_coarse<16, 4>(a, t, smem, st);
+}
+
+extern "C" int pk_hjcd_ik_lm_cuda(void* stream, const float* seeds, const float* noise, const float* twists,
+                                  const float* parent_tf, const int32_t* parent_idx, const int32_t* act_idx,
+                                  const float* mimic_mul, const float* mimic_off, const int32_t* mimic_act_idx,
+                                  const int32_t* topo_inv, const int32_t* target_jnts, const int32_t* ancestor_masks,
+                                  const float* target_Ts, const float* robot_spheres_local,
+                                  const int32_t* robot_sphere_joint_idx, const float* world_spheres,
+                                  const float* world_capsules, const float* world_boxes,
+                                  const float* world_halfspaces, const float* lower, const float* upper,
+                                  const int32_t* fixed_mask, int64_t max_iter, int64_t stall_patience,
+                                  float lambda_init, float limit_prior_weight, float kick_scale, float eps_pos,
+                                  float eps_ori, int64_t enable_collision, float collision_weight,
+                                  float collision_margin, float* out, float* out_err, int32_t* stop_flag,
+                                  int32_t n_problems, int32_t n_seeds, int32_t n_act, int32_t n_joints,
+                                  int32_t n_ee, int32_t n_robot_spheres, int32_t Ms, int32_t Mc, int32_t Mb,
+                                  int32_t Mh) {
+  HjcdArgs a = hjcd_args(seeds, twists, parent_tf, parent_idx, act_idx, mimic_mul, mimic_off, mimic_act_idx,
+                         topo_inv, target_jnts, ancestor_masks, target_Ts, robot_spheres_local,
+                         robot_sphere_joint_idx, world_spheres, world_capsules, world_boxes, world_halfspaces, lower,
+                         upper, fixed_mask, out, out_err, n_problems, n_seeds, n_act, n_joints, n_ee,
+                         n_robot_spheres, Ms, Mc, Mb, Mh);
+  PK_CHECK_ARG(max_iter >= 0 && max_iter < (1LL << 31), "bad max_iter");
+  PK_CHECK_ARG(stall_patience >= 1 && stall_patience < (1LL << 31), "stall_patience must be >= 1");
+  a.noise = noise;
+  a.stop_flag = stop_flag;
+  a.iters = (int)max_iter;
+  a.stall_patience = (int)stall_patience;
+  a.lambda_init = lambda_init;
+  a.limit_prior_weight = limit_prior_weight;
+  a.kick_scale = kick_scale;
+  a.eps_pos = eps_pos;
+  a.eps_ori = eps_ori;
+  a.enable_collision = enable_collision ? 1 : 0;
+  a.collision_weight = collision_weight;
+  a.collision_margin = collision_margin;
+  size_t smem = 0;
+  if (int s = hjcd_common(a, n_act, n_joints, n_ee, 32 * kHjcdWarps, &smem)) return s;
+  if (n_problems == 0) return PK_OK;
+  PK_CHECK_ARG(n_seeds == 0 || max_iter == 0 || noise, "null noise");
+  if (int s = check_buffers(a)) return s;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (n_seeds == 0) {
+    if (stop_flag) return cuda_status(cudaMemsetAsync(stop_flag, 0, sizeof(int32_t) * n_problems, st), "memset");
+    return PK_OK;
+  }
+  if (n_act <= 8 && n_ee == 1) return launch_lm<8, 1>(a, smem, st);
+  if (n_ee <= 2) return launch_lm<16, 2>(a, smem, st);
+  return launch_lm<16, 4>(a, smem, st);
+}
