@@ -494,6 +494,32 @@ def secondary_metrics(torch, dev, fp32_peak):
         "final_cost_mean": float(sc.mean()),
     }
 
+    # HJCD-IK on config 2's problems (collision-aware, 100 obstacle spheres): 32 coarse seeds x 20
+    # coordinate-descent steps, 30 refinement seeds x 40 LM iterations (the reference benchmark's
+    # HJCD settings), FP64 verification of the winners
+    from pyroffi_b200.hjcd import HjcdSolver
+    wi = W.ik()
+    hj = HjcdSolver(wi.model, wi.target_link, spheres=wi.spheres, world=wi.world, enable_collision=True, device=dev)
+    vs = BatchIkSolver(wi.model, wi.target_link, device=dev)
+    tgt_h = torch.as_tensor(wi.target_T, device=dev)
+    prev_h = torch.as_tensor(wi.seeds[:, 0], device=dev)
+    gen_h = torch.Generator(device=dev)
+    hkw = dict(num_seeds=32, coarse_max_iter=20, lm_max_iter=40, lambda_init=1e-3, limit_prior_weight=1e-4,
+               kick_scale=0.02, generator=gen_h)
+    gen_h.manual_seed(0)
+    hj.solve(tgt_h, prev_h, **hkw)
+    ms_hj = _timed_ms(torch, lambda: hj.solve(tgt_h, prev_h, **hkw), flush, reps=5, warm=1)
+    gen_h.manual_seed(0)
+    _, _, parts_h = hj.solve(tgt_h, prev_h, return_all=True, **hkw)
+    _, _, _, ok_h = vs.verify_select(parts_h[5], parts_h[6], tgt_h)
+    P_h = wi.target_T.shape[0]
+    out["hjcd_config2"] = {
+        "workload": f"HJCD-IK, {P_h} problems of config 2 (7-DOF chain, 100 obstacle spheres, collision on), "
+                    "32 coarse seeds x 20 steps, 30 refinement seeds x 40 LM iterations",
+        "ms_per_solve_batch": ms_hj, "solves_per_s": P_h / (ms_hj * 1e-3),
+        "success_rate": float(ok_h.float().mean()),
+    }
+
     # config 4: 4096 mixed IK problems in one persistent batch (CUDA graph)
     wm = W.mixed_ik()
     o = dict(max_iter=wm.max_iter, lambda_init=wm.lambda_init, lambda_down=wm.lambda_down, lambda_up=wm.lambda_up,

@@ -55,23 +55,50 @@ struct HjcdArgs {
   float collision_weight, collision_margin, lambda_init, limit_prior_weight, kick_scale, eps_pos, eps_ori;
 };
 
-constexpr int kHjcdWarps = 4;  // refinement: problems per block
+constexpr int kHjcdThreads = 128;  // refinement: one block per problem
+constexpr int kHjcdTps = 4;        // refinement: lanes per seed (they split the collision penalty)
 
 struct HjcdShared {
   JointTable jt;
-  float tgt[kHjcdWarps][PK_MAX_EE][7];
+  float tgt[1][PK_MAX_EE][7];
   unsigned long long anc[PK_MAX_EE];  // ancestor joints of each EE (original indices)
   int tsorted[PK_MAX_EE];             // sorted position of each EE's joint
   float lo[PK_MAX_ACT], hi[PK_MAX_ACT];
   int fixed[PK_MAX_ACT];              // fixed or padding
+  int n_groups;                       // joint groups of the robot spheres
 };
 
 __device__ __forceinline__ float clampf(float x, float lo, float hi) { return fmaxf(lo, fminf(hi, x)); }
 
+// Robot spheres in shared memory, grouped by the joint that carries them.
+struct RobotSpheresS {
+  float4* sph;     // [n_rs] joint-frame centre, radius; group k is gstart[k] .. gstart[k + 1]
+  float4* bound;   // [nj] bounding sphere of each group (joint frame)
+  int* start;      // [nj + 1] staging scratch
+  int* gstart;     // [nj + 1]
+  int* joint;      // [nj] sorted joint of each group
+  int ng;
+};
+
+__device__ __forceinline__ size_t hjcd_spheres_bytes(int n_rs, int nj) {
+  return sizeof(float4) * ((size_t)n_rs + nj) + sizeof(int) * (3 * (size_t)nj + 2);
+}
+
+__device__ __forceinline__ RobotSpheresS hjcd_spheres_at(unsigned char* p, int n_rs, int nj) {
+  RobotSpheresS R;
+  R.sph = reinterpret_cast<float4*>(p);
+  R.bound = R.sph + n_rs;
+  R.start = reinterpret_cast<int*>(R.bound + nj);
+  R.gstart = R.start + nj + 1;
+  R.joint = R.gstart + nj + 1;
+  R.ng = 0;
+  return R;
+}
+
 // Robot description, EE targets of `p0 + i` for i < n_tgt in slot i, limits,
 // robot spheres (joint-frame centre and radius, sorted joint position) and
 // optionally the world.  Ends with __syncthreads().
-__device__ void hjcd_stage(const HjcdArgs& a, HjcdShared& sh, float4* rs, int* rsj, float* world_dst, ObsView& ob,
+__device__ void hjcd_stage(const HjcdArgs& a, HjcdShared& sh, RobotSpheresS& R, float* world_dst, ObsView& ob,
                            int p0, int n_tgt) {
   load_joint_table(sh.jt, a.m);
   const int n = a.m.n_act, nj = a.m.n_joints, tid = threadIdx.x, nth = blockDim.x;
@@ -94,11 +121,50 @@ __device__ void hjcd_stage(const HjcdArgs& a, HjcdShared& sh, float4* rs, int* r
     sh.hi[c] = live ? a.upper[c] : 0.f;
     sh.fixed[c] = live ? (a.fixed_mask ? a.fixed_mask[c] != 0 : 0) : 1;
   }
-  for (int i = tid; i < a.n_rs; i += nth) {
-    const float* q = a.rs_local + 4 * i;
-    rs[i] = make_float4(q[0], q[1], q[2], q[3]);
-    const int j = a.rs_joint[i];
-    rsj[i] = (j >= 0 && j < nj) ? sh.jt.sorted_of[j] : -1;
+  __syncthreads();  // sorted_of is complete
+  if (tid == 0) {
+    // robot spheres grouped by (sorted) joint, in sphere order within a group;
+    // spheres on an out-of-range joint are dropped
+    for (int j = 0; j <= nj; ++j) R.start[j] = 0;
+    for (int i = 0; i < a.n_rs; ++i) {
+      const int j = a.rs_joint[i];
+      if (j >= 0 && j < nj) ++R.start[sh.jt.sorted_of[j] + 1];
+    }
+    int ng = 0, off = 0;
+    for (int j = 0; j < nj; ++j) {
+      const int c = R.start[j + 1];
+      if (c) { R.joint[ng] = j; R.gstart[ng] = off; ++ng; off += c; }
+      R.start[j + 1] = off;  // fill cursor base: start[j] .. start[j + 1]
+    }
+    R.gstart[ng] = off;
+    sh.n_groups = ng;
+    // start[j] now holds where joint j's spheres begin: the fill cursor
+    for (int i = 0; i < a.n_rs; ++i) {
+      const int j = a.rs_joint[i];
+      if (j < 0 || j >= nj) continue;
+      const float* q = a.rs_local + 4 * i;
+      R.sph[R.start[sh.jt.sorted_of[j]]++] = make_float4(q[0], q[1], q[2], q[3]);
+    }
+  }
+  __syncthreads();
+  R.ng = sh.n_groups;
+  for (int k = tid; k < R.ng; k += nth) {
+    // bounding sphere of group k in its joint frame; the slack keeps it
+    // conservative under rounding
+    float lo[3] = {3e38f, 3e38f, 3e38f}, hi[3] = {-3e38f, -3e38f, -3e38f};
+    for (int i = R.gstart[k]; i < R.gstart[k + 1]; ++i) {
+      const float4 q = R.sph[i];
+      lo[0] = fminf(lo[0], q.x); hi[0] = fmaxf(hi[0], q.x);
+      lo[1] = fminf(lo[1], q.y); hi[1] = fmaxf(hi[1], q.y);
+      lo[2] = fminf(lo[2], q.z); hi[2] = fmaxf(hi[2], q.z);
+    }
+    const float bx = 0.5f * (lo[0] + hi[0]), by = 0.5f * (lo[1] + hi[1]), bz = 0.5f * (lo[2] + hi[2]);
+    float rad = 0.f;
+    for (int i = R.gstart[k]; i < R.gstart[k + 1]; ++i) {
+      const float4 q = R.sph[i];
+      rad = fmaxf(rad, sqrtf((q.x - bx) * (q.x - bx) + (q.y - by) * (q.y - by) + (q.z - bz) * (q.z - bz)) + q.w);
+    }
+    R.bound[k] = make_float4(bx, by, bz, rad + 1e-4f + 1e-5f * fabsf(rad));
   }
   if (a.stage_world) {
     ob = stage_world(a.w, world_dst);
@@ -186,26 +252,35 @@ __device__ __forceinline__ void hjcd_jacobian(const HjcdShared& sh, const PoseSl
 }
 
 // Collision penalty weight * sum over (robot sphere, obstacle) with d < margin
-// of (d - margin)^2, from the joint poses in `ps`.
-__device__ __forceinline__ float hjcd_penalty(const HjcdArgs& a, const PoseSlots& ps, const float4* rs,
-                                              const int* rsj, const ObsView& ob) {
-  if (!a.enable_collision || a.n_rs <= 0) return 0.f;
+// of (d - margin)^2, from the joint poses in `ps`.  The TPS lanes of a seed
+// group split the obstacles and every lane returns the group's total.  An
+// obstacle at least the margin from a joint group's bounding sphere adds
+// exactly 0 for every sphere of the group and is skipped.
+template <int TPS>
+__device__ __forceinline__ float hjcd_penalty(const HjcdArgs& a, const PoseSlots& ps, const RobotSpheresS& R,
+                                              const ObsView& ob, int gl, unsigned gmask) {
+  if (!a.enable_collision || R.ng == 0) return 0.f;
   const int M = ob.Ms + ob.Mc + ob.Mb + ob.Mh;
   const float margin = a.collision_margin;
   float pen = 0.f;
-  for (int i = 0; i < a.n_rs; ++i) {
-    const int j = rsj[i];
-    if (j < 0) continue;
-    const float4 q = rs[i];
-    const float3 c = pose_apply(ps.load(j), make_float3(q.x, q.y, q.z));
-    for (int m = 0; m < M; ++m) {
-      const float d = obstacle_dist(ob, m, c, q.w);
-      if (d < margin) {
-        const float e = d - margin;
-        pen += e * e;
+  for (int k = 0; k < R.ng; ++k) {
+    const Pose Tj = ps.load(R.joint[k]);
+    const float4 jb = R.bound[k];
+    const float3 B = pose_apply(Tj, make_float3(jb.x, jb.y, jb.z));
+    for (int m = gl; m < M; m += TPS) {
+      if (obstacle_dist(ob, m, B, jb.w) >= margin) continue;
+      for (int i = R.gstart[k]; i < R.gstart[k + 1]; ++i) {
+        const float4 q = R.sph[i];
+        const float d = obstacle_dist(ob, m, pose_apply(Tj, make_float3(q.x, q.y, q.z)), q.w);
+        if (d < margin) {
+          const float e = d - margin;
+          pen += e * e;
+        }
       }
     }
   }
+#pragma unroll
+  for (int o = 1; o < TPS; o <<= 1) pen += __shfl_xor_sync(gmask, pen, o);
   return a.collision_weight * pen;
 }
 
@@ -219,7 +294,7 @@ __device__ __forceinline__ float reg_at(const float (&v)[MAXA], int i) {
 }
 
 __device__ __forceinline__ size_t hjcd_world_offset(const HjcdArgs& a) {
-  size_t s = sizeof(HjcdShared) + sizeof(float4) * a.n_rs + sizeof(int) * a.n_rs;
+  size_t s = sizeof(HjcdShared) + hjcd_spheres_bytes(a.n_rs, a.m.n_joints);
   return (s + 15) & ~size_t(15);
 }
 
@@ -231,13 +306,12 @@ template <int MAXA, int MAXEE>
 __global__ void __launch_bounds__(128) hjcd_coarse_kernel(HjcdArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   HjcdShared& sh = *reinterpret_cast<HjcdShared*>(smem_raw);
-  float4* rs = reinterpret_cast<float4*>(smem_raw + sizeof(HjcdShared));
-  int* rsj = reinterpret_cast<int*>(rs + a.n_rs);
+  RobotSpheresS R = hjcd_spheres_at(smem_raw + sizeof(HjcdShared), a.n_rs, a.m.n_joints);
   float* world = reinterpret_cast<float*>(smem_raw + hjcd_world_offset(a));
   float* slots = world + (a.stage_world ? a.w.smem_floats() : 0);
   const int p = blockIdx.y, tid = threadIdx.x, n = a.m.n_act;
   ObsView ob;
-  hjcd_stage(a, sh, rs, rsj, world, ob, p, 1);
+  hjcd_stage(a, sh, R, world, ob, p, 1);
   const int s = blockIdx.x * blockDim.x + tid;
   if (s >= a.S) return;
   const size_t gs = (size_t)p * a.S + s;
@@ -292,7 +366,7 @@ __global__ void __launch_bounds__(128) hjcd_coarse_kernel(HjcdArgs a) {
   float err = 0.f;
 #pragma unroll
   for (int k = 0; k < 6 * MAXEE; ++k) err += r[k] * r[k];
-  err += hjcd_penalty(a, ps, rs, rsj, ob);
+  err += hjcd_penalty<1>(a, ps, R, ob, 0, 0u);
   a.out_err[gs] = err;
   for (int c = 0; c < n; ++c) a.out[gs * n + c] = reg_at(cfg, c);
 }
@@ -302,15 +376,15 @@ __global__ void __launch_bounds__(128) hjcd_coarse_kernel(HjcdArgs a) {
 // ---------------------------------------------------------------------------
 
 // Unweighted squared error plus penalty at the joint poses in `ps`.
-template <int MAXEE>
-__device__ __forceinline__ float hjcd_error(const HjcdArgs& a, const HjcdShared& sh, const PoseSlots& ps, int w,
-                                            const float4* rs, const int* rsj, const ObsView& ob,
+template <int MAXEE, int TPS>
+__device__ __forceinline__ float hjcd_error(const HjcdArgs& a, const HjcdShared& sh, const PoseSlots& ps,
+                                            const RobotSpheresS& R, const ObsView& ob, int gl, unsigned gmask,
                                             float (&r)[6 * MAXEE], float (&pee)[3 * MAXEE]) {
-  hjcd_residual<MAXEE>(sh, ps, a.n_ee, w, r, pee);
+  hjcd_residual<MAXEE>(sh, ps, a.n_ee, 0, r, pee);
   float err = 0.f;
 #pragma unroll
   for (int k = 0; k < 6 * MAXEE; ++k) err += r[k] * r[k];
-  return err + hjcd_penalty(a, ps, rs, rsj, ob);
+  return err + hjcd_penalty<TPS>(a, ps, R, ob, gl, gmask);
 }
 
 // LM step of the current point: adaptive row weights, Jacobi column scaling,
@@ -429,25 +503,23 @@ __device__ __forceinline__ void hjcd_direction(const HjcdArgs& a, const HjcdShar
   }
 }
 
-template <int MAXA, int MAXEE>
-__global__ void __launch_bounds__(32 * kHjcdWarps) hjcd_lm_kernel(HjcdArgs a) {
+template <int MAXA, int MAXEE, int TPS>
+__global__ void __launch_bounds__(kHjcdThreads) hjcd_lm_kernel(HjcdArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   HjcdShared& sh = *reinterpret_cast<HjcdShared*>(smem_raw);
-  float4* rs = reinterpret_cast<float4*>(smem_raw + sizeof(HjcdShared));
-  int* rsj = reinterpret_cast<int*>(rs + a.n_rs);
+  RobotSpheresS R = hjcd_spheres_at(smem_raw + sizeof(HjcdShared), a.n_rs, a.m.n_joints);
   float* world = reinterpret_cast<float*>(smem_raw + hjcd_world_offset(a));
   float* slots = world + (a.stage_world ? a.w.smem_floats() : 0);
-  const int tid = threadIdx.x, wid = tid >> 5, lane = tid & 31, n = a.m.n_act;
-  const int p0 = blockIdx.x * kHjcdWarps;
+  const int tid = threadIdx.x, n = a.m.n_act, p = blockIdx.x;
+  const int G = blockDim.x / TPS, grp = tid / TPS, gl = tid % TPS;
+  const unsigned gmask = (TPS == 32 ? 0xffffffffu : ((1u << TPS) - 1u)) << ((tid & 31) & ~(TPS - 1));
   ObsView ob;
-  hjcd_stage(a, sh, rs, rsj, world, ob, p0, kHjcdWarps);
-  const int p = p0 + wid;
-  if (p >= a.P) return;  // whole warp
+  hjcd_stage(a, sh, R, world, ob, p, 1);
   const PoseSlots ps{slots + tid, (int)blockDim.x};
   const float alphas[5] = {1.f, 0.5f, 0.25f, 0.1f, 0.025f};
-  bool stop = false;  // warp-uniform: a seed of this problem has converged
-  for (int s0 = 0; s0 < a.S; s0 += 32) {
-    const int s = s0 + lane;
+  bool stop = false;  // block-uniform: a seed of this problem has converged
+  for (int s0 = 0; s0 < a.S; s0 += G) {
+    const int s = s0 + grp;
     const bool live = s < a.S;
     const size_t gs = (size_t)p * a.S + (live ? s : 0);
     float cfg[MAXA], best_cfg[MAXA];
@@ -455,19 +527,22 @@ __global__ void __launch_bounds__(32 * kHjcdWarps) hjcd_lm_kernel(HjcdArgs a) {
     for (int c = 0; c < MAXA; ++c) cfg[c] = best_cfg[c] = (live && c < n) ? a.seeds[gs * n + c] : 0.f;
     auto cur_at = [&](int i) { return reg_at(cfg, i); };
     float r[6 * MAXEE], pee[3 * MAXEE];
-    fk_thread(sh.jt, cur_at, ps);
-    float best_err = hjcd_error<MAXEE>(a, sh, ps, wid, rs, rsj, ob, r, pee);
+    float best_err = 0.f;
+    if (live) {
+      fk_thread(sh.jt, cur_at, ps);
+      best_err = hjcd_error<MAXEE, TPS>(a, sh, ps, R, ob, gl, gmask, r, pee);
+    }
     float lam = a.lambda_init;
     int stall = 0;
     bool done = !live || stop;
     for (int it = 0; it < a.iters; ++it) {
       if (stop) done = true;
-      if (__all_sync(0xffffffffu, done)) break;
+      if (__syncthreads_and(done)) break;
       bool conv = false;
       float curr = 0.f;
       if (!done) {
         fk_thread(sh.jt, cur_at, ps);
-        curr = hjcd_error<MAXEE>(a, sh, ps, wid, rs, rsj, ob, r, pee);
+        curr = hjcd_error<MAXEE, TPS>(a, sh, ps, R, ob, gl, gmask, r, pee);
         conv = true;
 #pragma unroll
         for (int e = 0; e < MAXEE; ++e) {
@@ -478,12 +553,12 @@ __global__ void __launch_bounds__(32 * kHjcdWarps) hjcd_lm_kernel(HjcdArgs a) {
           if (pn >= a.eps_pos || on >= a.eps_ori) conv = false;
         }
       }
-      if (__any_sync(0xffffffffu, !done && conv)) stop = true;
+      if (__syncthreads_or(!done && conv)) stop = true;
       if (conv) done = true;
       if (done) continue;
+      // the TPS lanes of a group hold the same state and compute the same step
       float delta[MAXA];
       hjcd_direction<MAXA, MAXEE>(a, sh, ps, r, pee, cfg, lam, delta);
-      // line search on the unweighted error
       float best_a_err = 1e30f;
       int best_ai = 0;
       for (int ai = 0; ai < 5; ++ai) {
@@ -492,7 +567,7 @@ __global__ void __launch_bounds__(32 * kHjcdWarps) hjcd_lm_kernel(HjcdArgs a) {
         for (int c = 0; c < MAXA; ++c) trial[c] = clampf(cfg[c] + alphas[ai] * delta[c], sh.lo[c], sh.hi[c]);
         fk_thread(sh.jt, [&](int i) { return reg_at(trial, i); }, ps);
         float rt[6 * MAXEE], pt[3 * MAXEE];
-        const float et = hjcd_error<MAXEE>(a, sh, ps, wid, rs, rsj, ob, rt, pt);
+        const float et = hjcd_error<MAXEE, TPS>(a, sh, ps, R, ob, gl, gmask, rt, pt);
         if (et < best_a_err) {
           best_a_err = et;
           best_ai = ai;
@@ -525,16 +600,17 @@ __global__ void __launch_bounds__(32 * kHjcdWarps) hjcd_lm_kernel(HjcdArgs a) {
         stall = 0;
       }
     }
-    if (live) {
+    if (live && gl == 0) {
       for (int c = 0; c < n; ++c) a.out[gs * n + c] = reg_at(best_cfg, c);
       a.out_err[gs] = best_err;
     }
   }
-  if (lane == 0 && a.stop_flag) a.stop_flag[p] = stop ? 1 : 0;
+  if (tid == 0 && a.stop_flag) a.stop_flag[p] = stop ? 1 : 0;
 }
 
 static size_t hjcd_smem(const HjcdArgs& a, int nth) {
-  size_t s = sizeof(HjcdShared) + sizeof(float4) * a.n_rs + sizeof(int) * a.n_rs;
+  size_t s = sizeof(HjcdShared) + sizeof(float4) * ((size_t)a.n_rs + a.m.n_joints) +
+             sizeof(int) * (3 * (size_t)a.m.n_joints + 2);
   s = (s + 15) & ~size_t(15);
   if (a.stage_world) s += sizeof(float) * a.w.smem_floats();
   return s + sizeof(float) * (size_t)a.m.n_joints * 7 * nth;
@@ -574,10 +650,9 @@ int launch_coarse(const HjcdArgs& a, int nth, size_t smem, cudaStream_t st) {
 
 template <int MAXA, int MAXEE>
 int launch_lm(const HjcdArgs& a, size_t smem, cudaStream_t st) {
-  auto k = hjcd_lm_kernel<MAXA, MAXEE>;
+  auto k = hjcd_lm_kernel<MAXA, MAXEE, kHjcdTps>;
   if (int s = set_smem_limit((const void*)k, smem)) return s;
-  const unsigned blocks = (unsigned)((a.P + kHjcdWarps - 1) / kHjcdWarps);
-  k<<<blocks, 32 * kHjcdWarps, smem, st>>>(a);
+  k<<<(unsigned)a.P, kHjcdThreads, smem, st>>>(a);
   return cuda_status(cudaGetLastError(), "hjcd_lm_kernel launch");
 }
 
@@ -684,7 +759,7 @@ extern "C" int pk_hjcd_ik_lm_cuda(void* stream, const float* seeds, const float*
   a.collision_weight = collision_weight;
   a.collision_margin = collision_margin;
   size_t smem = 0;
-  if (int s = hjcd_common(a, n_act, n_joints, n_ee, 32 * kHjcdWarps, &smem)) return s;
+  if (int s = hjcd_common(a, n_act, n_joints, n_ee, kHjcdThreads, &smem)) return s;
   if (n_problems == 0) return PK_OK;
   PK_CHECK_ARG(n_seeds == 0 || max_iter == 0 || noise, "null noise");
   if (int s = check_buffers(a)) return s;

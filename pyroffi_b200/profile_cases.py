@@ -12,6 +12,7 @@ capture one warm launch.
     python -m pyroffi_b200.profile_cases scolin      # SCO linearisation, 512 x 64 x 7 waypoints
     python -m pyroffi_b200.profile_cases scoinner    # SCO inner L-BFGS solve, 512 trajectories
     python -m pyroffi_b200.profile_cases sco         # whole SCO run (10 x 30 iterations), 512 x 64 x 7
+    python -m pyroffi_b200.profile_cases hjcd        # HJCD-IK solve, 256 problems, collision on
 """
 
 from __future__ import annotations
@@ -94,9 +95,20 @@ def _sco(stage):
     return lambda: opt.inner(x, d, J, 1.0, x[0, 0], x[0, -1])
 
 
+def _hjcd():
+    from .hjcd import HjcdSolver
+    w = W.ik()
+    dev = torch.device("cuda:0")
+    s = HjcdSolver(w.model, w.target_link, spheres=w.spheres, world=w.world, enable_collision=True, device=dev)
+    tg, prev = torch.as_tensor(w.target_T, device=dev), torch.as_tensor(w.seeds[:, 0], device=dev)
+    g = torch.Generator(device=dev).manual_seed(0)
+    return lambda: s.solve(tg, prev, num_seeds=32, lambda_init=1e-3, limit_prior_weight=1e-4, kick_scale=0.02,
+                           generator=g)
+
+
 CASES = {"lm": _lm, "fkc1": lambda: _fkc(65536, False), "fkc5": lambda: _fkc(4096, True), "wide": _wide,
          "traj": _traj, "batch": _batch, "scolin": lambda: _sco("lin"), "scoinner": lambda: _sco("inner"),
-         "sco": lambda: _sco("run")}
+         "sco": lambda: _sco("run"), "hjcd": _hjcd}
 
 
 def main(argv=None) -> int:
