@@ -466,6 +466,28 @@ int pk_hjcd_ik_lm_cuda(void* stream, const float* seeds, const float* noise, con
                        int32_t n_robot_spheres, int32_t Ms, int32_t Mc, int32_t Mb, int32_t Mh);
 
 /*
+ * SQP-IK: multi-seed sequential quadratic programming IK with the joint
+ * limits as hard bounds on each step (box QP: Newton step, clamp,
+ * n_inner_iters active-set re-solves), fixed row weights, 5-point line search,
+ * best-iterate tracking.  Replaces "sqp_ik_cuda" (SqpIkCudaFfi,
+ * src/pyroffi/cuda_kernels/_sqp_ik_cuda_kernel.cu:70-591): buffers and
+ * attributes in the order of its Bind(), then the extents.  Outputs
+ * out[P, S, n_act] and out_err[P, S] (weighted squared error plus the
+ * collision penalty).  At most 16 actuated joints and 4 EEs.
+ */
+int pk_sqp_ik_cuda(void* stream, const float* seeds, const float* twists, const float* parent_tf,
+                   const int32_t* parent_idx, const int32_t* act_idx, const float* mimic_mul, const float* mimic_off,
+                   const int32_t* mimic_act_idx, const int32_t* topo_inv, const int32_t* target_jnts,
+                   const int32_t* ancestor_masks, const float* target_Ts, const float* robot_spheres_local,
+                   const int32_t* robot_sphere_joint_idx, const float* world_spheres, const float* world_capsules,
+                   const float* world_boxes, const float* world_halfspaces, const float* lower, const float* upper,
+                   const int32_t* fixed_mask, int64_t max_iter, int64_t n_inner_iters, float pos_weight,
+                   float ori_weight, float lambda_init, float eps_pos, float eps_ori, int64_t enable_collision,
+                   float collision_weight, float collision_margin, float* out, float* out_err, int32_t n_problems,
+                   int32_t n_seeds, int32_t n_act, int32_t n_joints, int32_t n_ee, int32_t n_robot_spheres,
+                   int32_t Ms, int32_t Mc, int32_t Mb, int32_t Mh);
+
+/*
  * FP32 FMA-pipe microbenchmark (no reference counterpart): `blocks` blocks of
  * 256 threads, each thread 8 independent FMA chains of `iters` steps, i.e.
  * 4096 * iters * blocks FLOPs.  Time it with events on `stream`; it gives

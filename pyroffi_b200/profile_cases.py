@@ -13,6 +13,7 @@ capture one warm launch.
     python -m pyroffi_b200.profile_cases scoinner    # SCO inner L-BFGS solve, 512 trajectories
     python -m pyroffi_b200.profile_cases sco         # whole SCO run (10 x 30 iterations), 512 x 64 x 7
     python -m pyroffi_b200.profile_cases hjcd        # HJCD-IK solve, 256 problems, collision on
+    python -m pyroffi_b200.profile_cases sqp         # SQP-IK solve, 256 problems, collision on
 """
 
 from __future__ import annotations
@@ -106,9 +107,19 @@ def _hjcd():
                            generator=g)
 
 
+def _sqp():
+    from .sqp import SqpSolver
+    w = W.ik()
+    dev = torch.device("cuda:0")
+    s = SqpSolver(w.model, w.target_link, spheres=w.spheres, world=w.world, enable_collision=True, device=dev)
+    tg, prev = torch.as_tensor(w.target_T, device=dev), torch.as_tensor(w.seeds[:, 0], device=dev)
+    g = torch.Generator(device=dev).manual_seed(0)
+    return lambda: s.solve(tg, prev, num_seeds=32, generator=g)
+
+
 CASES = {"lm": _lm, "fkc1": lambda: _fkc(65536, False), "fkc5": lambda: _fkc(4096, True), "wide": _wide,
          "traj": _traj, "batch": _batch, "scolin": lambda: _sco("lin"), "scoinner": lambda: _sco("inner"),
-         "sco": lambda: _sco("run"), "hjcd": _hjcd}
+         "sco": lambda: _sco("run"), "hjcd": _hjcd, "sqp": _sqp}
 
 
 def main(argv=None) -> int:

@@ -10,18 +10,15 @@ import pytest
 import torch
 
 from oracle import hjcd as ohjcd
-from oracle import kinematics as okin
 from oracle import lm as olm
 from pyroffi_b200 import workloads as W
 from pyroffi_b200.hjcd import HjcdSolver
 
+from ik_cases import agree, bimanual, t
+
 pytestmark = pytest.mark.gpu
 DEV = "cuda:0"
 REF_KW = dict(lambda_init=1e-3, limit_prior_weight=1e-4, kick_scale=0.02)   # tests/bench_ik.py:193-201
-
-
-def t(a, dt=torch.float32):
-    return torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device=DEV)
 
 
 def chain(P=3, S=32, seed=1002, coll=False):
@@ -35,24 +32,6 @@ def chain(P=3, S=32, seed=1002, coll=False):
         oc = dict(world=w.world.arrays(), spheres_local=w.spheres_local, sphere_joint=w.sphere_joint, margin=0.02,
                   weight=1e4)
     return w, sol, tj, anc, tgt, oc
-
-
-def bimanual(P=3, S=32, seed=7):
-    cl = W.mixed_classes()[2]
-    m = cl.model
-    rng = np.random.default_rng(seed)
-    cfg = m.random_cfgs(rng, P)
-    links = okin.forward_kinematics(cfg.astype(np.float64), m.as_dict())
-    tgt = np.stack([links[:, l] for l in cl.target_links], axis=1).astype(np.float32)    # [P, 2, 7]
-    seeds = rng.uniform(m.lower, m.upper, size=(P, S, m.n_act)).astype(np.float32)
-    sol = HjcdSolver(m, cl.target_links, device=DEV)
-    tj = [m.link_joint(l) for l in cl.target_links]
-    anc = [m.ancestor_mask(l) for l in cl.target_links]
-    return m, sol, tj, anc, tgt, seeds
-
-
-def agree(a, b, rtol=1e-3, atol=1e-7):
-    return float(np.mean(np.abs(a - b) <= rtol * np.abs(b) + atol))
 
 
 @pytest.mark.parametrize("coll", [False, True])
