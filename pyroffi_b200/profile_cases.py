@@ -14,6 +14,7 @@ capture one warm launch.
     python -m pyroffi_b200.profile_cases sco         # whole SCO run (10 x 30 iterations), 512 x 64 x 7
     python -m pyroffi_b200.profile_cases hjcd        # HJCD-IK solve, 256 problems, collision on
     python -m pyroffi_b200.profile_cases sqp         # SQP-IK solve, 256 problems, collision on
+    python -m pyroffi_b200.profile_cases chomp       # CHOMP, 512 x 64 x 7 trajectories, 5 iterations (eager)
 """
 
 from __future__ import annotations
@@ -117,9 +118,21 @@ def _sqp():
     return lambda: s.solve(tg, prev, num_seeds=32, generator=g)
 
 
+def _chomp():
+    from .chomp import ChompConfig, ChompOptimizer
+    from .trajopt import TrajectoryCost
+    wt = W.trajectories()
+    dev = torch.device("cuda:0")
+    cfg = ChompConfig(n_iters=5)
+    tc = TrajectoryCost(wt.model, wt.spheres, wt.world, wt.link_pairs, margin=cfg.collision_margin, device=dev)
+    opt = ChompOptimizer(tc, cfg)
+    x = torch.as_tensor(wt.traj, device=dev)
+    return lambda: opt.run(x, x[0, 0], x[0, -1])
+
+
 CASES = {"lm": _lm, "fkc1": lambda: _fkc(65536, False), "fkc5": lambda: _fkc(4096, True), "wide": _wide,
          "traj": _traj, "batch": _batch, "scolin": lambda: _sco("lin"), "scoinner": lambda: _sco("inner"),
-         "sco": lambda: _sco("run"), "hjcd": _hjcd, "sqp": _sqp}
+         "sco": lambda: _sco("run"), "hjcd": _hjcd, "sqp": _sqp, "chomp": _chomp}
 
 
 def main(argv=None) -> int:
