@@ -327,6 +327,20 @@ int pk_traj_cost_grad(void* stream, const pk_traj_options* opt, const float* tra
                       int32_t n_links, int32_t S, int32_t P, int32_t Ms, int32_t Mc, int32_t Mb,
                       int32_t Mh);
 
+/*
+ * CHOMP descent direction (no reference counterpart; it replaces the
+ * clipping and covariant-update steps of chomp_trajopt,
+ * src/pyroffi/optimization_engines/_chomp_optimization.py:155-241, 297-318):
+ * per trajectory of grad[B, T, n_act], g * min(1, clip / |g|) (no clip when
+ * grad_clip_norm <= 0), ends set to 0, then dir = -M^-1 g on every joint's
+ * interior timeline by n_cg_iters truncated FP64 CG steps (relative
+ * tolerance cg_tol) on M x = 6x + reg x - 4(x[t-1] + x[t+1]) + x[t-2] + x[t+2];
+ * covariant = 0 gives dir = -g.  At most 128 interior waypoints.
+ */
+int pk_chomp_direction(void* stream, const float* grad, float* dir, int64_t B, int32_t T, int32_t n_act,
+                       int32_t n_cg_iters, float grad_clip_norm, float smoothness_reg, float cg_tol,
+                       int32_t covariant);
+
 /* SCO trajectory optimisation settings: the fields of ScoTrajOptConfig
  * (src/pyroffi/optimization_engines/_sco_optimization.py:52-104, defaults in
  * brackets) and the reference kernel's fd_eps attribute

@@ -8,12 +8,13 @@ the device:
 
 * cost and gradient of all B trajectories from one ``pk_traj_cost_grad``
   launch (``TrajectoryCost.cost_and_grad``);
-* global-norm gradient clipping per trajectory, pinned endpoints;
-* covariant direction: the interior of each joint's timeline is solved
+* global-norm gradient clipping per trajectory, pinned endpoints, and the
+  covariant direction -- the interior of each joint's timeline solved
   against the pentadiagonal smoothness metric ``6x - 4(x[t-1] + x[t+1]) +
   (x[t-2] + x[t+2]) + reg x`` by the same truncated conjugate gradient as the
-  reference (``n_cg_iters`` steps, relative tolerance ``cg_tol``), batched
-  over all (trajectory, joint) timelines, in FP64;
+  reference (``n_cg_iters`` steps, relative tolerance ``cg_tol``) in FP64 --
+  in one ``pk_chomp_direction`` launch (a warp per (trajectory, joint)
+  timeline);
 * line search over ``step_size * (1, .5, .25, .1, .05, 0)``: the 6B trial
   trajectories are costed in one more launch, the first minimum wins and is
   taken when it improves the cost by ``min_cost_improve``;
@@ -31,6 +32,8 @@ from dataclasses import dataclass
 
 import torch
 
+from . import _lib
+from ._tensors import f32, ptr, stream_ptr
 from .trajopt import TrajectoryCost
 
 
@@ -60,53 +63,16 @@ class ChompConfig:
 LINE_SEARCH = (1.0, 0.5, 0.25, 0.1, 0.05, 0.0)
 
 
-def metric_apply(x: torch.Tensor, reg: float) -> torch.Tensor:
-    """The interior smoothness metric along dim 1 of x [V, Tin] (zero outside)."""
-    y = 6.0 * x + reg * x
-    y[:, 1:] -= 4.0 * x[:, :-1]
-    y[:, :-1] -= 4.0 * x[:, 1:]
-    y[:, 2:] += x[:, :-2]
-    y[:, :-2] += x[:, 2:]
-    return y
-
-
-def cg_solve(b: torch.Tensor, reg: float, n_iters: int, tol: float) -> torch.Tensor:
-    """Truncated CG for M x = b, one system per row of b [V, Tin]; a row
-    stops updating once its squared residual falls below (tol |b| + 1e-12)^2."""
-    x = torch.zeros_like(b)
-    r = b.clone()
-    p = r.clone()
-    rr = (r * r).sum(dim=1)
-    bnorm = torch.sqrt((b * b).sum(dim=1) + 1e-18)
-    tol2 = (tol * bnorm + 1e-12) ** 2
-    active = torch.ones_like(rr, dtype=torch.bool)
-    for _ in range(n_iters):
-        Ap = metric_apply(p, reg)
-        alpha = rr / ((p * Ap).sum(dim=1) + 1e-9)
-        x_new = x + alpha[:, None] * p
-        r_new = r - alpha[:, None] * Ap
-        rr_new = (r_new * r_new).sum(dim=1)
-        beta = rr_new / (rr + 1e-9)
-        p_new = r_new + beta[:, None] * p
-        a = active[:, None]
-        x = torch.where(a, x_new, x)
-        r = torch.where(a, r_new, r)
-        p = torch.where(a, p_new, p)
-        rr = torch.where(active, rr_new, rr)
-        active = active & (rr_new > tol2)
-    return x
-
-
-def _direction(grad: torch.Tensor, cfg: ChompConfig) -> torch.Tensor:
-    B, T, n = grad.shape
-    if not cfg.use_covariant_update or T <= 2:
-        return -grad
-    # FP64: truncated CG on this ill-conditioned metric is rounding-sensitive
-    # (FP32 runs drift by tens of percent from the FP64 iterates)
-    g = grad[:, 1:-1, :].permute(0, 2, 1).reshape(B * n, T - 2).to(torch.float64)
-    x = cg_solve(g, cfg.smoothness_reg, cfg.n_cg_iters, cfg.cg_tol)
-    d = torch.zeros_like(grad)
-    d[:, 1:-1, :] = -x.to(grad.dtype).reshape(B, n, T - 2).permute(0, 2, 1)
+def covariant_direction(grad: torch.Tensor, cfg: ChompConfig) -> torch.Tensor:
+    """Clipped, endpoint-pinned descent direction [B, T, n]: -M^-1 g on each
+    joint's interior timeline by the truncated FP64 CG, or -g without the
+    covariant update (one ``pk_chomp_direction`` launch)."""
+    g = f32(grad)
+    B, T, n = (int(v) for v in g.shape)
+    d = torch.empty_like(g)
+    _lib.call("pk_chomp_direction", stream_ptr(g.device), ptr(g), ptr(d), B, T, n, int(cfg.n_cg_iters),
+              float(cfg.grad_clip_norm), float(cfg.smoothness_reg), float(cfg.cg_tol),
+              int(bool(cfg.use_covariant_update)))
     return d
 
 
@@ -140,13 +106,7 @@ class ChompOptimizer:
         w = cfg.w_collision
         for _ in range(cfg.n_iters):
             c, g = self._costs(traj, w, grad=True)
-            if cfg.grad_clip_norm > 0:
-                gn = torch.sqrt((g * g).sum(dim=(1, 2)))
-                scale = torch.where(gn > cfg.grad_clip_norm, cfg.grad_clip_norm / (gn + 1e-12), torch.ones_like(gn))
-                g = g * scale[:, None, None]
-            g[:, 0] = 0.0
-            g[:, -1] = 0.0
-            d = _direction(g, cfg)
+            d = covariant_direction(g, cfg)
             trials = traj[None] + torch.clamp(alphas[:, None, None, None] * d[None], -cfg.max_delta_per_step,
                                               cfg.max_delta_per_step)
             trials[:, :, 0] = start

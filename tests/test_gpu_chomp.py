@@ -7,7 +7,7 @@ import torch
 
 from oracle import chomp as ochomp
 from pyroffi_b200 import workloads as W
-from pyroffi_b200.chomp import ChompConfig, ChompOptimizer, cg_solve
+from pyroffi_b200.chomp import ChompConfig, ChompOptimizer, covariant_direction
 from pyroffi_b200.trajopt import TrajectoryCost
 
 pytestmark = pytest.mark.gpu
@@ -19,12 +19,28 @@ def small():
     return w
 
 
-def test_cg_matches_oracle():
-    rng = np.random.default_rng(0)
-    b = rng.normal(size=(5, 20))
-    got = cg_solve(torch.as_tensor(b, dtype=torch.float64, device=DEV), 1e-3, 24, 1e-4).cpu().numpy()
-    for i in range(5):
-        np.testing.assert_allclose(got[i], ochomp.cg_solve(b[i].copy(), 1e-3, 24, 1e-4), rtol=1e-8, atol=1e-10)
+@pytest.mark.parametrize("T,n,clip,covariant", [(64, 7, 10.0, True), (12, 3, 0.0, True), (130, 9, 0.5, True),
+                                                (20, 4, 10.0, False)])
+def test_direction_kernel_matches_oracle(T, n, clip, covariant):
+    # clipping, pinned ends and the FP64 truncated CG of every joint timeline
+    rng = np.random.default_rng(T + n)
+    g = (rng.normal(size=(5, T, n)) * rng.uniform(0.1, 10.0, size=(5, 1, 1))).astype(np.float32)
+    g[1, :, 0] *= 1e-9                                            # a timeline that stops after one step
+    cfg = ChompConfig(grad_clip_norm=clip, use_covariant_update=covariant)
+    got = covariant_direction(torch.as_tensor(g, device=DEV), cfg).cpu().numpy()
+    for b in range(5):
+        gb = g[b].astype(np.float64)
+        gn = np.sqrt(np.sum(g[b].astype(np.float64) ** 2))
+        if clip > 0 and gn > clip:
+            gb = gb * (clip / (gn + 1e-12))
+        want = np.zeros_like(gb)
+        for j in range(n):
+            if covariant:
+                want[1:-1, j] = -ochomp.cg_solve(gb[1:-1, j].copy(), cfg.smoothness_reg, cfg.n_cg_iters, cfg.cg_tol)
+            else:
+                want[1:-1, j] = -gb[1:-1, j]
+        np.testing.assert_allclose(got[b], want, rtol=1e-5, atol=1e-6 * (np.abs(want).max() + 1e-30))
+        assert np.all(got[b, 0] == 0) and np.all(got[b, -1] == 0)
 
 
 @pytest.mark.parametrize("n_iters", [1, 3])
