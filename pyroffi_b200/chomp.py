@@ -15,9 +15,11 @@ the device:
   reference (``n_cg_iters`` steps, relative tolerance ``cg_tol``) in FP64 --
   in one ``pk_chomp_direction`` launch (a warp per (trajectory, joint)
   timeline);
-* line search over ``step_size * (1, .5, .25, .1, .05, 0)``: the 6B trial
-  trajectories are costed in one more launch, the first minimum wins and is
-  taken when it improves the cost by ``min_cost_improve``;
+* line search over ``step_size * (1, .5, .25, .1, .05, 0)``: the 5B trial
+  trajectories of the non-zero steps are costed in one more launch (the zero
+  step's trial is the current trajectory, costed by the gradient launch), the
+  first minimum wins and is taken when it improves the cost by
+  ``min_cost_improve``;
 * per-trajectory early stop after ``early_stop_patience`` stalled steps; the
   collision weight grows by ``collision_penalty_scale`` per step up to
   ``w_collision_max``; the final ranking uses ``w_collision_max``.
@@ -107,11 +109,16 @@ class ChompOptimizer:
         for _ in range(cfg.n_iters):
             c, g = self._costs(traj, w, grad=True)
             d = covariant_direction(g, cfg)
-            trials = traj[None] + torch.clamp(alphas[:, None, None, None] * d[None], -cfg.max_delta_per_step,
+            # the last trial step is 0: that trial is the current trajectory, whose cost
+            # the gradient launch has just produced, so only the others are costed
+            a_nz = alphas[:-1]
+            trials = traj[None] + torch.clamp(a_nz[:, None, None, None] * d[None], -cfg.max_delta_per_step,
                                               cfg.max_delta_per_step)
             trials[:, :, 0] = start
             trials[:, :, -1] = goal
-            tc = self._costs(trials.reshape(-1, *traj.shape[1:]).contiguous(), w).reshape(len(LINE_SEARCH), B)
+            tc = self._costs(trials.reshape(-1, *traj.shape[1:]).contiguous(), w).reshape(len(LINE_SEARCH) - 1, B)
+            tc = torch.cat([tc, c[None]], dim=0)
+            trials = torch.cat([trials, traj[None]], dim=0)
             best_cost, best_idx = torch.min(tc, dim=0)          # first minimum
             best = trials[best_idx, torch.arange(B, device=dev)]
             improved = best_cost < (c - cfg.min_cost_improve)
