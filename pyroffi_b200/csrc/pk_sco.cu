@@ -255,7 +255,7 @@ __device__ __forceinline__ SoftAcc world_group(const ScoLinArgs& a, const ObsVie
 // Linearisation: group distances, their analytic Jacobians and/or the
 // nonlinear collision sum, TG lanes per configuration.
 template <int MAXS, int TG>
-__global__ void __launch_bounds__(128, MAXS <= 8 ? 4 : 3) sco_linearize_kernel(ScoLinArgs a) {
+__global__ void __launch_bounds__(128, MAXS <= 8 ? 4 : (MAXS <= 16 ? 3 : 2)) sco_linearize_kernel(ScoLinArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   JointTable& jt = *reinterpret_cast<JointTable*>(smem_raw);
   unsigned char* p = smem_raw + sizeof(JointTable);
@@ -901,8 +901,10 @@ static int launch_linearize(const ScoLinArgs& a, cudaStream_t st) {
   const long long ng = nth / TG;
   long long blocks = (a.C + ng - 1) / ng;
   if (blocks > 64LL * sms) blocks = 64LL * sms;  // grid-stride beyond that
-  auto kern = a.S <= 4 ? sco_linearize_kernel<4, TG> : (a.S <= 8 ? sco_linearize_kernel<8, TG>
-                                                                  : sco_linearize_kernel<16, TG>);
+  auto kern = a.S <= 4    ? sco_linearize_kernel<4, TG>
+              : a.S <= 8  ? sco_linearize_kernel<8, TG>
+              : a.S <= 16 ? sco_linearize_kernel<16, TG>
+                          : sco_linearize_kernel<32, TG>;
   if (int s = set_smem_limit((const void*)kern, smem)) return s;
   kern<<<(unsigned)blocks, nth, smem, st>>>(a);
   return cuda_status(cudaGetLastError(), "sco_linearize_kernel launch");
@@ -983,7 +985,7 @@ WsLayout ws_layout(const pk_sco_options* o, long long B, int T, int n) {
 int check_robot(int64_t n_act, int32_t n_joints, int32_t n_links, int32_t S, int32_t P) {
   PK_CHECK_ARG(n_act >= 0 && n_links >= 0 && S >= 0 && P >= 0 && n_joints >= 0, "negative extent");
   PK_CHECK_CAP(n_joints <= PK_MAX_JOINTS, "n_joints=%d exceeds %d", n_joints, PK_MAX_JOINTS);
-  PK_CHECK_CAP(S <= 16, "at most 16 spheres per link (got %d)", S);
+  PK_CHECK_CAP(S <= 32, "at most 32 spheres per link (got %d)", S);
   return PK_OK;
 }
 

@@ -363,7 +363,7 @@ extern "C" int pk_traj_cost_grad(void* stream, const pk_traj_options* opt, const
   PK_CHECK_ARG(opt != nullptr, "null options");
   PK_CHECK_ARG(B >= 0 && T >= 0 && n_act >= 0 && n_links >= 0 && S >= 0 && P >= 0, "negative extent");
   PK_CHECK_CAP(n_joints <= PK_MAX_JOINTS, "n_joints=%d exceeds %d", n_joints, PK_MAX_JOINTS);
-  PK_CHECK_CAP(S <= 16, "at most 16 spheres per link (got %d)", S);
+  PK_CHECK_CAP(S <= 32, "at most 32 spheres per link (got %d)", S);
   PK_CHECK_ARG(T >= 5, "the 4th-order smoothness stencil needs T >= 5 waypoints (got %d)", T);
   if (B == 0) return PK_OK;
   PK_CHECK_ARG(traj && twists && parent_tf && parent_idx && act_idx && mimic_mul && mimic_off && mimic_act_idx &&
@@ -397,8 +397,9 @@ extern "C" int pk_traj_cost_grad(void* stream, const pk_traj_options* opt, const
   const size_t smem = traj_smem(a, nth, TG);
   PK_CHECK_CAP(smem <= 200 * 1024, "trajectory working set (%zu B of shared memory) too large", smem);
   PK_CHECK_CAP(B < (1LL << 31), "batch too large");
-  auto kern = (S <= 8) ? (TG == 4 ? traj_cost_kernel<8, 4> : traj_cost_kernel<8, 2>)
-                       : (TG == 4 ? traj_cost_kernel<16, 4> : traj_cost_kernel<16, 2>);
+  auto kern = (S <= 8)    ? (TG == 4 ? traj_cost_kernel<8, 4> : traj_cost_kernel<8, 2>)
+              : (S <= 16) ? (TG == 4 ? traj_cost_kernel<16, 4> : traj_cost_kernel<16, 2>)
+                          : (TG == 4 ? traj_cost_kernel<32, 4> : traj_cost_kernel<32, 2>);
   if (int s = set_smem_limit((const void*)kern, smem)) return s;
   kern<<<(unsigned)B, nth, smem, (cudaStream_t)stream>>>(a);
   return cuda_status(cudaGetLastError(), "traj_cost_kernel launch");
