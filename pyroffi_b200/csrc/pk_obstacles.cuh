@@ -29,10 +29,12 @@ struct WorldArgs {
   const float* halfspaces;
   int Ms, Mc, Mb, Mh;
   __host__ __device__ int total() const { return Ms + Mc + Mb + Mh; }
-  // floats needed to stage everything in shared memory (spheres first, 16-byte aligned)
+  // floats needed to stage everything in shared memory: spheres, capsules,
+  // boxes, halfspaces, each array starting on a 16-byte boundary
   __host__ __device__ size_t smem_floats() const {
-    return (size_t)Ms * 4 + (size_t)Mc * 7 + (size_t)Mb * 15 + (size_t)Mh * 6;
+    return (size_t)Ms * 4 + round4((size_t)Mc * 7) + round4((size_t)Mb * 15) + round4((size_t)Mh * 6);
   }
+  __host__ __device__ static size_t round4(size_t v) { return (v + 3) & ~size_t(3); }
 };
 
 struct ObsView {
@@ -43,22 +45,65 @@ struct ObsView {
   int Ms, Mc, Mb, Mh;
 };
 
-// Copies the obstacle arrays into shared memory at `dst` (16-byte aligned)
-// with all threads of the block; the caller synchronises afterwards.
+// Copies the obstacle arrays into shared memory at `dst` (16-byte aligned),
+// each array starting on a 16-byte boundary; called by every thread of the
+// block, and the caller synchronises afterwards.  The 16-byte-aligned bulk of
+// each array goes through the TMA bulk-copy engine: one thread issues
+// cp.async.bulk global -> shared with the completion counted in bytes on an
+// mbarrier, and every thread waits on that barrier (the wait is bounded).  An
+// array whose source is not 16-byte aligned, and the bytes past the last
+// 16-byte multiple, are copied with plain loads.
 __device__ inline ObsView stage_world(const WorldArgs& w, float* dst) {
+  __shared__ __align__(8) unsigned long long s_bar;
+  const float* src[4] = {w.spheres, w.capsules, w.boxes, w.halfspaces};
+  const int nf[4] = {w.Ms * 4, w.Mc * 7, w.Mb * 15, w.Mh * 6};
+  float* d[4];
+  unsigned bulk[4];
+  unsigned total = 0;
+  float* q = dst;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    d[k] = q;
+    q += WorldArgs::round4((size_t)nf[k]);
+    const bool aligned = nf[k] > 0 && (reinterpret_cast<uintptr_t>(src[k]) & 15) == 0;
+    bulk[k] = aligned ? ((unsigned)nf[k] * 4u) & ~15u : 0u;
+    total += bulk[k];
+  }
+  const int tid = threadIdx.x, nth = blockDim.x;
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    for (int i = (int)(bulk[k] / 4) + tid; i < nf[k]; i += nth) d[k][i] = src[k][i];
+  if (total > 0) {
+    const unsigned bar = (unsigned)__cvta_generic_to_shared(&s_bar);
+    if (tid == 0) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(total) : "memory");
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if (bulk[k])
+          asm volatile(
+              "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                  (unsigned)__cvta_generic_to_shared(d[k])),
+              "l"(src[k]), "r"(bulk[k]), "r"(bar)
+              : "memory");
+    }
+    unsigned done = 0;
+    for (int it = 0; it < (1 << 22) && !done; ++it)
+      asm volatile(
+          "{\n .reg .pred P;\n mbarrier.try_wait.parity.shared::cta.b64 P, [%1], 0;\n selp.u32 %0, 1, 0, P;\n}"
+          : "=r"(done)
+          : "r"(bar)
+          : "memory");
+  }
   ObsView v;
-  float* p = dst;
-  for (int i = threadIdx.x; i < w.Ms * 4; i += blockDim.x) p[i] = w.spheres[i];
-  v.sph = reinterpret_cast<const float4*>(p);
-  p += w.Ms * 4;
-  for (int i = threadIdx.x; i < w.Mc * 7; i += blockDim.x) p[i] = w.capsules[i];
-  v.cap = p;
-  p += w.Mc * 7;
-  for (int i = threadIdx.x; i < w.Mb * 15; i += blockDim.x) p[i] = w.boxes[i];
-  v.box = p;
-  p += w.Mb * 15;
-  for (int i = threadIdx.x; i < w.Mh * 6; i += blockDim.x) p[i] = w.halfspaces[i];
-  v.hs = p;
+  v.sph = reinterpret_cast<const float4*>(d[0]);
+  v.cap = d[1];
+  v.box = d[2];
+  v.hs = d[3];
   v.Ms = w.Ms; v.Mc = w.Mc; v.Mb = w.Mb; v.Mh = w.Mh;
   return v;
 }
