@@ -367,7 +367,7 @@ def run_ours(args):
             "cpu_baseline": cpu,
         }
         if not args.no_secondary:
-            line["secondary"] = secondary_metrics(torch, dev, peak)
+            line["secondary"] = secondary_metrics(torch, dev, peak, cpu=not args.no_cpu_baseline)
         print(json.dumps(line))
     if world > 1:
         dist.barrier()
@@ -396,7 +396,15 @@ def _timed_ms(torch, fn, flush, reps=5, warm=3):
     return statistics.median(ts)
 
 
-def secondary_metrics(torch, dev, fp32_peak):
+def _cpu_rate(fn, units):
+    """Units per second of the oracle call fn() on the host (one run after a warm-up)."""
+    fn()
+    t0 = time.perf_counter()
+    fn()
+    return units / (time.perf_counter() - t0)
+
+
+def secondary_metrics(torch, dev, fp32_peak, cpu=True):
     """Configs 1 (FK + sphere collision), 3 (trajectory cost + adjoint), 4
     (mixed persistent batch IK) and 5 (FK + collision bandwidth sweep),
     each against its roofline.  Seeded synthetic inputs, resident in HBM."""
@@ -435,6 +443,19 @@ def secondary_metrics(torch, dev, fp32_peak):
                      "fp32_tflops": 65536 * flop_cfg / (ms_bkm * 1e-3) / 1e12, "kernel": "fk_sphere_collision_kernel"},
     }
     del r2
+    if cpu:
+        from oracle import collision as ocoll
+        from oracle import kinematics as okin
+        cs = w.cfg[:256].astype(np.float64)
+
+        def fkc_oracle():
+            links = okin.forward_kinematics(cs, w.model.as_dict())
+            cen = ocoll.transform_points(links[:, :, None, :], w.spheres.centers.astype(np.float64)[None])
+            d = ocoll.point_vs_world(cen, np.broadcast_to(w.spheres.radii, cen.shape[:-1]), *w.world.arrays())
+            return np.where(w.spheres.radii[None, :, :, None] < 0, np.inf, d).reshape(len(cs), -1).min(axis=1)
+        out["fk_collision_config1"]["cpu_baseline"] = {
+            "value": _cpu_rate(fkc_oracle, len(cs)), "unit": "configs/s", "cores": 1, "kind": "port",
+            "sample": "256 configurations, FP64 numpy oracle (FK, sphere centres, all sphere-obstacle distances, min)"}
 
     # config 3: 512 trajectories x 64 waypoints x 7 DOF, 256 spheres + 32 boxes
     wt = W.trajectories()
@@ -453,6 +474,19 @@ def secondary_metrics(torch, dev, fp32_peak):
                      "unit": "TFLOP/s", "frac": Bt * T * f_bwd / (ms_fb * 1e-3) / 1e12 / fp32_peak,
                      "flop_per_waypoint": f_bwd, "kernel": "traj_cost_kernel"},
     }
+
+    if cpu:
+        from oracle import traj as otraj
+        md = wt.model.as_dict()
+
+        def traj_oracle():
+            for b in range(2):
+                otraj.total_cost(wt.traj[b], md, wt.spheres.centers, wt.spheres.radii, wt.link_pairs,
+                                 wt.world.arrays(), margin=wt.margin, w_smooth=1.0, w_acc=0.5, w_jerk=0.1,
+                                 w_limits=1.0, w_coll=3.0, lower=wt.model.lower, upper=wt.model.upper)
+        out["traj_config3"]["cpu_baseline"] = {
+            "value": _cpu_rate(traj_oracle, 2), "unit": "trajectory costs/s (forward only)", "cores": 1,
+            "kind": "port", "sample": "2 trajectories x 64 waypoints, FP64 numpy oracle cost (no gradient)"}
 
     # CHOMP optimiser on the adjoint: the config-3 trajectories, 100 iterations, one CUDA graph
     from pyroffi_b200.chomp import ChompConfig, ChompOptimizer
