@@ -128,8 +128,9 @@ __global__ void __launch_bounds__(64 * TG, 8 / TG) traj_cost_kernel(TrajArgs a) 
       float cx[MAXS], cy[MAXS], cz[MAXS], cr[MAXS];
       bool have = false;
       float3 F = make_float3(0.f, 0.f, 0.f), Mo = make_float3(0.f, 0.f, 0.f);
-      for (int m = gl; m < M; m += TG) {
-        if (obstacle_dist(ob, m, B, bl.w) >= margin) continue;  // exact lower bound of the link's distances
+      // narrow phase of obstacle m: the link's minimum sphere distance, its
+      // hinge and the force at the sphere that attains it
+      auto narrow = [&](int m) {
         if (!have) {
 #pragma unroll
           for (int s = 0; s < MAXS; ++s) {
@@ -147,7 +148,7 @@ __global__ void __launch_bounds__(64 * TG, 8 / TG) traj_cost_kernel(TrajArgs a) 
           const float d = obstacle_dist(ob, m, make_float3(cx[s], cy[s], cz[s]), cr[s]);
           if (d < dmin) { dmin = d; arg = s; }
         }
-        if (arg < 0 || !(dmin < margin)) continue;
+        if (arg < 0 || !(dmin < margin)) return;
         const float v = margin - dmin;
         cw += v * v;
         if (want_grad) {
@@ -163,6 +164,41 @@ __global__ void __launch_bounds__(64 * TG, 8 / TG) traj_cost_kernel(TrajArgs a) 
           const float3 cm = cross3(c, f);
           Mo.x += cm.x; Mo.y += cm.y; Mo.z += cm.z;
         }
+      };
+      // broad phase, one loop per obstacle kind: the link's bounding sphere
+      // (B, R) is a lower bound of all its sphere distances, so an obstacle
+      // it does not bring within the margin adds nothing.  The tests compare
+      // squared lengths (no square root); the bound's slack covers rounding.
+      const float Rm = bl.w + margin;
+      for (int k = gl; k < ob.Ms; k += TG) {
+        const float4 o = ob.sph[k];
+        const float dx = B.x - o.x, dy = B.y - o.y, dz = B.z - o.z;
+        const float rr = Rm + o.w;
+        if (dx * dx + dy * dy + dz * dz < rr * fabsf(rr)) narrow(k);
+      }
+      for (int k = gl; k < ob.Mc; k += TG) {
+        const float* cp = ob.cap + 7 * k;
+        const float vx = cp[3] - cp[0], vy = cp[4] - cp[1], vz = cp[5] - cp[2];
+        const float len2 = vx * vx + vy * vy + vz * vz;
+        float t = 0.f;
+        if (len2 > 1e-12f) t = fmaxf(0.f, fminf(1.f, ((B.x - cp[0]) * vx + (B.y - cp[1]) * vy + (B.z - cp[2]) * vz) / len2));
+        const float dx = B.x - (cp[0] + t * vx), dy = B.y - (cp[1] + t * vy), dz = B.z - (cp[2] + t * vz);
+        const float rr = Rm + cp[6];
+        if (dx * dx + dy * dy + dz * dz < rr * fabsf(rr)) narrow(ob.Ms + k);
+      }
+      for (int k = gl; k < ob.Mb; k += TG) {
+        const float* b = ob.box + 15 * k;
+        const float dx = B.x - b[0], dy = B.y - b[1], dz = B.z - b[2];
+        const float q1 = fmaxf(fabsf(dx * b[3] + dy * b[4] + dz * b[5]) - b[12], 0.f);
+        const float q2 = fmaxf(fabsf(dx * b[6] + dy * b[7] + dz * b[8]) - b[13], 0.f);
+        const float q3 = fmaxf(fabsf(dx * b[9] + dy * b[10] + dz * b[11]) - b[14], 0.f);
+        // inside the box the outside part is 0 and the bound is <= 0 < margin
+        if (q1 * q1 + q2 * q2 + q3 * q3 < Rm * fabsf(Rm)) narrow(ob.Ms + ob.Mc + k);
+      }
+      for (int k = gl; k < ob.Mh; k += TG) {
+        const float* h = ob.hs + 6 * k;
+        if ((B.x - h[3]) * h[0] + (B.y - h[4]) * h[1] + (B.z - h[5]) * h[2] - bl.w < margin)
+          narrow(ob.Ms + ob.Mc + ob.Mb + k);
       }
       if (want_grad) {
 #pragma unroll
@@ -195,7 +231,8 @@ __global__ void __launch_bounds__(64 * TG, 8 / TG) traj_cost_kernel(TrajArgs a) 
           const float3 Bi = pose_apply(Ti, make_float3(bi.x, bi.y, bi.z));
           const float3 Bj = pose_apply(Tj, make_float3(bj.x, bj.y, bj.z));
           const float bx = Bi.x - Bj.x, by = Bi.y - Bj.y, bz = Bi.z - Bj.z;
-          if (sqrtf(bx * bx + by * by + bz * bz) - bi.w - bj.w < margin) {
+          const float rb = bi.w + bj.w + margin;
+          if (bx * bx + by * by + bz * bz < rb * fabsf(rb)) {
             float dmin = FLT_MAX;
             float3 ca = make_float3(0.f, 0.f, 0.f), cb = ca;
             for (int s = 0; s < S; ++s) {
