@@ -173,6 +173,69 @@ __device__ inline float obstacle_dist_grad(const ObsView& o, int m, float3 c, fl
   return (c.x - h[3]) * h[0] + (c.y - h[4]) * h[1] + (c.z - h[5]) * h[2] - r;
 }
 
+// Broad phase: may the ball (B, R) come within `margin` of obstacle m (index
+// over spheres, capsules, boxes, halfspaces in that order)?  The ball bounds a
+// group of spheres, so its distance bounds theirs from below and a `false`
+// means every one of them is at least `margin` from the obstacle.  Squared
+// lengths instead of square roots; the caller's ball carries the slack that
+// covers the rounding.  KIND is the obstacle's kind (0-3) when the caller
+// knows it, -1 to dispatch on m.
+template <int KIND = -1>
+__device__ __forceinline__ bool obstacle_near(const ObsView& ob, int m, float3 B, float R, float margin) {
+  const float Rm = R + margin;
+  if (KIND == 0 || (KIND < 0 && m < ob.Ms)) {
+    const float4 o = ob.sph[m];
+    const float dx = B.x - o.x, dy = B.y - o.y, dz = B.z - o.z;
+    const float rr = Rm + o.w;
+    return dx * dx + dy * dy + dz * dz < rr * fabsf(rr);
+  }
+  m -= ob.Ms;
+  if (KIND == 1 || (KIND < 0 && m < ob.Mc)) {
+    const float* cp = ob.cap + 7 * m;
+    const float vx = cp[3] - cp[0], vy = cp[4] - cp[1], vz = cp[5] - cp[2];
+    const float len2 = vx * vx + vy * vy + vz * vz;
+    float t = 0.f;
+    if (len2 > 1e-12f)
+      t = fmaxf(0.f, fminf(1.f, ((B.x - cp[0]) * vx + (B.y - cp[1]) * vy + (B.z - cp[2]) * vz) / len2));
+    const float dx = B.x - (cp[0] + t * vx), dy = B.y - (cp[1] + t * vy), dz = B.z - (cp[2] + t * vz);
+    const float rr = Rm + cp[6];
+    return dx * dx + dy * dy + dz * dz < rr * fabsf(rr);
+  }
+  m -= ob.Mc;
+  if (KIND == 2 || (KIND < 0 && m < ob.Mb)) {
+    const float* b = ob.box + 15 * m;
+    const float dx = B.x - b[0], dy = B.y - b[1], dz = B.z - b[2];
+    const float q1 = fmaxf(fabsf(dx * b[3] + dy * b[4] + dz * b[5]) - b[12], 0.f);
+    const float q2 = fmaxf(fabsf(dx * b[6] + dy * b[7] + dz * b[8]) - b[13], 0.f);
+    const float q3 = fmaxf(fabsf(dx * b[9] + dy * b[10] + dz * b[11]) - b[14], 0.f);
+    // a centre inside the box has a bound <= -R, below any margin > -R
+    return q1 * q1 + q2 * q2 + q3 * q3 < Rm * fabsf(Rm) || Rm <= 0.f;
+  }
+  m -= ob.Mb;
+  const float* h = ob.hs + 6 * m;
+  return (B.x - h[3]) * h[0] + (B.y - h[4]) * h[1] + (B.z - h[5]) * h[2] - R < margin;
+}
+
+// Calls f(m) for each obstacle m of this lane's share -- every stride-th
+// obstacle of each kind from `lane` -- that obstacle_near keeps: one loop per
+// kind, so the test does not dispatch.
+template <class F>
+__device__ __forceinline__ void for_each_near_obstacle(const ObsView& ob, float3 B, float R, float margin, int lane,
+                                                       int stride, F&& f) {
+  int base = 0;
+  for (int k = lane; k < ob.Ms; k += stride)
+    if (obstacle_near<0>(ob, base + k, B, R, margin)) f(base + k);
+  base += ob.Ms;
+  for (int k = lane; k < ob.Mc; k += stride)
+    if (obstacle_near<1>(ob, base + k, B, R, margin)) f(base + k);
+  base += ob.Mc;
+  for (int k = lane; k < ob.Mb; k += stride)
+    if (obstacle_near<2>(ob, base + k, B, R, margin)) f(base + k);
+  base += ob.Mb;
+  for (int k = lane; k < ob.Mh; k += stride)
+    if (obstacle_near<3>(ob, base + k, B, R, margin)) f(base + k);
+}
+
 __device__ __forceinline__ float3 cross3(float3 a, float3 b) {
   return make_float3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
 }

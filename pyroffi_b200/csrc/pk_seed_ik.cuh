@@ -242,7 +242,7 @@ __device__ __forceinline__ float seed_ik_penalty(const SeedIkArgs& a, const Pose
     const float4 jb = R.bound[k];
     const float3 B = pose_apply(Tj, make_float3(jb.x, jb.y, jb.z));
     for (int m = gl; m < M; m += TPS) {
-      if (obstacle_dist(ob, m, B, jb.w) >= margin) continue;
+      if (!obstacle_near(ob, m, B, jb.w, margin)) continue;
       for (int i = R.gstart[k]; i < R.gstart[k + 1]; ++i) {
         const float4 q = R.sph[i];
         const float d = obstacle_dist(ob, m, pose_apply(Tj, make_float3(q.x, q.y, q.z)), q.w);

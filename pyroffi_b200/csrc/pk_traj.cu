@@ -108,7 +108,6 @@ __global__ void __launch_bounds__(64 * TG, 8 / TG) traj_cost_kernel(TrajArgs a) 
 
   const bool want_grad = a.grad != nullptr;
   const float margin = a.margin;
-  const int M = a.w.total();
   for (int t0 = 0; t0 < T; t0 += ng) {
     const int t = t0 + grp;
     if (t >= T) continue;  // the whole group skips
@@ -119,7 +118,7 @@ __global__ void __launch_bounds__(64 * TG, 8 / TG) traj_cost_kernel(TrajArgs a) 
     __syncwarp(gm);
     float cw = 0.f;
     // world: (link, obstacle) hinge on the link's minimum sphere distance;
-    // lane gl takes obstacles gl, gl + TG, ...
+    // lane gl takes obstacles gl, gl + TG, ... of each kind
     for (int l = 0; l < N; ++l) {
       const float4 bl = lbnd[l];
       if (bl.w < 0.f) continue;
@@ -165,41 +164,7 @@ __global__ void __launch_bounds__(64 * TG, 8 / TG) traj_cost_kernel(TrajArgs a) 
           Mo.x += cm.x; Mo.y += cm.y; Mo.z += cm.z;
         }
       };
-      // broad phase, one loop per obstacle kind: the link's bounding sphere
-      // (B, R) is a lower bound of all its sphere distances, so an obstacle
-      // it does not bring within the margin adds nothing.  The tests compare
-      // squared lengths (no square root); the bound's slack covers rounding.
-      const float Rm = bl.w + margin;
-      for (int k = gl; k < ob.Ms; k += TG) {
-        const float4 o = ob.sph[k];
-        const float dx = B.x - o.x, dy = B.y - o.y, dz = B.z - o.z;
-        const float rr = Rm + o.w;
-        if (dx * dx + dy * dy + dz * dz < rr * fabsf(rr)) narrow(k);
-      }
-      for (int k = gl; k < ob.Mc; k += TG) {
-        const float* cp = ob.cap + 7 * k;
-        const float vx = cp[3] - cp[0], vy = cp[4] - cp[1], vz = cp[5] - cp[2];
-        const float len2 = vx * vx + vy * vy + vz * vz;
-        float t = 0.f;
-        if (len2 > 1e-12f) t = fmaxf(0.f, fminf(1.f, ((B.x - cp[0]) * vx + (B.y - cp[1]) * vy + (B.z - cp[2]) * vz) / len2));
-        const float dx = B.x - (cp[0] + t * vx), dy = B.y - (cp[1] + t * vy), dz = B.z - (cp[2] + t * vz);
-        const float rr = Rm + cp[6];
-        if (dx * dx + dy * dy + dz * dz < rr * fabsf(rr)) narrow(ob.Ms + k);
-      }
-      for (int k = gl; k < ob.Mb; k += TG) {
-        const float* b = ob.box + 15 * k;
-        const float dx = B.x - b[0], dy = B.y - b[1], dz = B.z - b[2];
-        const float q1 = fmaxf(fabsf(dx * b[3] + dy * b[4] + dz * b[5]) - b[12], 0.f);
-        const float q2 = fmaxf(fabsf(dx * b[6] + dy * b[7] + dz * b[8]) - b[13], 0.f);
-        const float q3 = fmaxf(fabsf(dx * b[9] + dy * b[10] + dz * b[11]) - b[14], 0.f);
-        // inside the box the outside part is 0 and the bound is <= 0 < margin
-        if (q1 * q1 + q2 * q2 + q3 * q3 < Rm * fabsf(Rm)) narrow(ob.Ms + ob.Mc + k);
-      }
-      for (int k = gl; k < ob.Mh; k += TG) {
-        const float* h = ob.hs + 6 * k;
-        if ((B.x - h[3]) * h[0] + (B.y - h[4]) * h[1] + (B.z - h[5]) * h[2] - bl.w < margin)
-          narrow(ob.Ms + ob.Mc + ob.Mb + k);
-      }
+      for_each_near_obstacle(ob, B, bl.w, margin, gl, TG, narrow);
       if (want_grad) {
 #pragma unroll
         for (int o = 1; o < TG; o <<= 1) {
