@@ -472,7 +472,9 @@ def secondary_metrics(torch, dev, fp32_peak, cpu=True):
         "fwd_bwd_traj_per_s": Bt / (ms_fb * 1e-3),
         "roofline": {"bound": "fp32", "achieved": Bt * T * f_bwd / (ms_fb * 1e-3) / 1e12, "peak": fp32_peak,
                      "unit": "TFLOP/s", "frac": Bt * T * f_bwd / (ms_fb * 1e-3) / 1e12 / fp32_peak,
-                     "flop_per_waypoint": f_bwd, "kernel": "traj_cost_kernel"},
+                     "flop_per_waypoint": f_bwd, "kernel": "traj_cost_kernel",
+                     "flop_basis": "dense evaluation (every link sphere against every obstacle); the kernel skips "
+                                   "(link, obstacle) pairs beyond the margin, so this is dense-equivalent throughput"},
     }
 
     if cpu:

@@ -46,7 +46,7 @@ __global__ void __launch_bounds__(128) hjcd_coarse_kernel(SeedIkArgs a) {
   SeedIkShared& sh = *reinterpret_cast<SeedIkShared*>(smem_raw);
   RobotSpheresS R = seed_ik_spheres_at(smem_raw + sizeof(SeedIkShared), a.n_rs, a.m.n_joints);
   float* world = reinterpret_cast<float*>(smem_raw + seed_ik_world_offset(a));
-  float* slots = world + (a.stage_world ? a.w.smem_floats() : 0);
+  float* slots = reinterpret_cast<float*>(smem_raw + seed_ik_slots_offset(a));
   const int p = blockIdx.y, tid = threadIdx.x, n = a.m.n_act;
   ObsView ob;
   seed_ik_stage(a, sh, R, world, ob, p, 1);
@@ -247,7 +247,7 @@ __global__ void __launch_bounds__(kHjcdThreads) hjcd_lm_kernel(SeedIkArgs a) {
   SeedIkShared& sh = *reinterpret_cast<SeedIkShared*>(smem_raw);
   RobotSpheresS R = seed_ik_spheres_at(smem_raw + sizeof(SeedIkShared), a.n_rs, a.m.n_joints);
   float* world = reinterpret_cast<float*>(smem_raw + seed_ik_world_offset(a));
-  float* slots = world + (a.stage_world ? a.w.smem_floats() : 0);
+  float* slots = reinterpret_cast<float*>(smem_raw + seed_ik_slots_offset(a));
   const int tid = threadIdx.x, n = a.m.n_act, p = blockIdx.x;
   const int G = blockDim.x / TPS, grp = tid / TPS, gl = tid % TPS;
   const unsigned gmask = (TPS == 32 ? 0xffffffffu : ((1u << TPS) - 1u)) << ((tid & 31) & ~(TPS - 1));
@@ -441,7 +441,7 @@ extern "C" int pk_hjcd_ik_lm_cuda(void* stream, const float* seeds, const float*
   a.collision_weight = collision_weight;
   a.collision_margin = collision_margin;
   size_t smem = 0;
-  if (int s = seed_ik_common(a, n_act, n_joints, n_ee, kHjcdThreads, &smem)) return s;
+  if (int s = seed_ik_common(a, n_act, n_joints, n_ee, kHjcdThreads, &smem, true)) return s;
   if (n_problems == 0) return PK_OK;
   PK_CHECK_ARG(n_seeds == 0 || max_iter == 0 || noise, "null noise");
   if (int s = seed_ik_check_buffers(a)) return s;

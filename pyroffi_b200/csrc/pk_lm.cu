@@ -39,6 +39,7 @@
 #include <algorithm>
 
 #include "pk_batch.cuh"
+#include "pk_obstacle_grid.cuh"
 
 namespace pk {
 
@@ -114,9 +115,6 @@ __host__ __device__ __forceinline__ int lm_pos_stride(int n_rs, int n_joints) {
   return (3 * n_rs + 3 * n_joints) | 1;  // sphere positions, then joint bounding centres
 }
 
-// Obstacle grid resolution per axis (cells = PK_LM_GRID^3, indices packed in 4 bits).
-#define PK_LM_GRID 8
-
 // Byte offsets of the LM block's dynamic shared memory.
 struct LmLayout {
   size_t rs, ws, pairs, pair4, gjoint, gstart, rsj, rsk, cells, cell_obs, wc, wb, wh, slots, pos, scratch, total;
@@ -149,7 +147,7 @@ __host__ __device__ inline LmLayout lm_layout(const LmArgs& a, int tps, int thre
   L.gstart = o; o = lm_align16(o + 4 * (size_t)(n_self + 2));
   L.rsj = o; o = lm_align16(o + 4 * (size_t)n_rs);
   L.rsk = o; o = lm_align16(o + 4 * (size_t)n_rs);
-  L.cells = o; o = lm_align16(o + (L.grid ? 4 * (size_t)(PK_LM_GRID * PK_LM_GRID * PK_LM_GRID + 1) : 0));
+  L.cells = o; o = lm_align16(o + (L.grid ? 4 * (size_t)(kObsGridCells + 1) : 0));
   L.cell_obs = o; o = lm_align16(o + 2 * (size_t)L.max_entries);
   L.wc = o; o = lm_align16(o + 28 * (size_t)a.w.Mc);
   L.wb = o; o = lm_align16(o + 60 * (size_t)a.w.Mb);
@@ -215,7 +213,6 @@ struct PenaltyCtx {
   const unsigned short* cell_obs;
   float* pos;            // this seed: sphere world positions [n_rs][3], then bounding centres [n_js][3]
   float3 glo, ginv;      // grid origin and inverse cell size
-  int G;
   int n_rs, n_js, n_groups, Ms_pad, Mc, Mb, Mh;
   float margin;
 };
@@ -278,12 +275,8 @@ __device__ float penalty_share(const PenaltyCtx& c, const PoseSlots& ps, int t, 
     const float Bx = pb[3 * j], By = pb[3 * j + 1], Bz = pb[3 * j + 2];
     const int k0 = c.jstart[j], k1 = c.jstart[j + 1];
     if (c.cell_start) {
-      const int ix = __float2int_rd((Bx - c.glo.x) * c.ginv.x);
-      const int iy = __float2int_rd((By - c.glo.y) * c.ginv.y);
-      const int iz = __float2int_rd((Bz - c.glo.z) * c.ginv.z);
-      // outside the grid no obstacle is within reach of this joint
-      if ((unsigned)ix >= (unsigned)c.G || (unsigned)iy >= (unsigned)c.G || (unsigned)iz >= (unsigned)c.G) continue;
-      const int cell = (ix * c.G + iy) * c.G + iz;
+      const int cell = obstacle_grid_cell(c.glo, c.ginv, make_float3(Bx, By, Bz));
+      if (cell < 0) continue;  // outside the grid no obstacle is within reach of this joint
       const int e1 = c.cell_start[cell + 1];
       for (int e = c.cell_start[cell] + t; e < e1; e += TPS) {
         const float4 O = c.ws[c.cell_obs[e]];
@@ -678,83 +671,19 @@ __device__ void lm_stage(const LmArgs& a, unsigned char* smem_raw, const LmLayou
       }
     }
     sh.n_groups = n_groups;
-    // obstacle-grid bounds: the union of every world sphere's ball of radius
-    // r + margin + (largest joint bounding radius), slightly inflated
+    // obstacle-grid bounds (world radii already carry the margin)
     sh.grid_on = 0;
     if (L.grid && n_js > 0) {
-      float lo[3] = {3e38f, 3e38f, 3e38f}, hi[3] = {-3e38f, -3e38f, -3e38f};
-      for (int o = 0; o < a.w.Ms; ++o) {
-        const float4 O = ws4[o];
-        const float rho = O.w + rmax + 1e-3f;
-        lo[0] = fminf(lo[0], O.x - rho); hi[0] = fmaxf(hi[0], O.x + rho);
-        lo[1] = fminf(lo[1], O.y - rho); hi[1] = fmaxf(hi[1], O.y + rho);
-        lo[2] = fminf(lo[2], O.z - rho); hi[2] = fmaxf(hi[2], O.z + rho);
-      }
-      sh.glo = make_float3(lo[0], lo[1], lo[2]);
-      sh.ginv = make_float3(PK_LM_GRID / fmaxf(hi[0] - lo[0], 1e-6f), PK_LM_GRID / fmaxf(hi[1] - lo[1], 1e-6f),
-                            PK_LM_GRID / fmaxf(hi[2] - lo[2], 1e-6f));
+      obstacle_grid_bounds(ws4, a.w.Ms, rmax, sh.glo, sh.ginv);
       sh.rmax = rmax;
       sh.grid_on = 1;
     }
   }
   __syncthreads();
 
-  // Obstacle grid: PK_LM_GRID^3 cells over those bounds; obstacle o is listed
-  // in every cell its inflated ball's bounding box touches, in increasing o
-  // (each cell's list is built by one thread, so the order is deterministic).
-  if (sh.grid_on) {
-    constexpr int G = PK_LM_GRID, NC = G * G * G;
-    int* obox = scratch;
-    for (int o = tid; o < a.w.Ms; o += blockDim.x) {
-      const float4 O = ws4[o];
-      const float rho = O.w + sh.rmax + 1e-3f;
-      const float c3[3] = {O.x, O.y, O.z}, l3[3] = {sh.glo.x, sh.glo.y, sh.glo.z}, i3[3] = {sh.ginv.x, sh.ginv.y, sh.ginv.z};
-      int packed = 0;
-      for (int d = 0; d < 3; ++d) {
-        const int i0 = min(max(__float2int_rd((c3[d] - rho - l3[d]) * i3[d]), 0), G - 1);
-        const int i1 = min(max(__float2int_rd((c3[d] + rho - l3[d]) * i3[d]), 0), G - 1);
-        packed |= (i0 | (i1 << 4)) << (8 * d);
-      }
-      obox[o] = packed;
-    }
-    __syncthreads();
-    for (int cell = tid; cell < NC; cell += blockDim.x) {
-      const int ix = cell / (G * G), iy = (cell / G) % G, iz = cell % G;
-      int n = 0;
-      for (int o = 0; o < a.w.Ms; ++o) {
-        const int b = obox[o];
-        n += (ix >= (b & 15)) & (ix <= ((b >> 4) & 15)) & (iy >= ((b >> 8) & 15)) & (iy <= ((b >> 12) & 15)) &
-             (iz >= ((b >> 16) & 15)) & (iz <= ((b >> 20) & 15));
-      }
-      cell_start[cell] = n;
-    }
-    __syncthreads();
-    if (tid == 0) {
-      int run = 0;
-      for (int cell = 0; cell < NC; ++cell) {
-        const int n = cell_start[cell];
-        cell_start[cell] = run;
-        run += n;
-      }
-      cell_start[NC] = run;
-      if (run > L.max_entries) sh.grid_on = 0;  // does not fit: scan all obstacles instead
-    }
-    __syncthreads();
-    if (sh.grid_on) {
-      for (int cell = tid; cell < NC; cell += blockDim.x) {
-        const int ix = cell / (G * G), iy = (cell / G) % G, iz = cell % G;
-        int at = cell_start[cell];
-        for (int o = 0; o < a.w.Ms; ++o) {
-          const int b = obox[o];
-          if ((ix >= (b & 15)) & (ix <= ((b >> 4) & 15)) & (iy >= ((b >> 8) & 15)) & (iy <= ((b >> 12) & 15)) &
-              (iz >= ((b >> 16) & 15)) & (iz <= ((b >> 20) & 15)))
-            cell_obs[at++] = (unsigned short)o;
-        }
-      }
-    }
-    __syncthreads();
-  }
-
+  if (sh.grid_on)
+    obstacle_grid_build(ws4, a.w.Ms, sh.rmax, sh.glo, sh.ginv, scratch, cell_start, cell_obs, L.max_entries,
+                        sh.grid_on);
 }
 
 // `count` seeds of problem pb, with the block's shared memory already
@@ -795,7 +724,7 @@ __device__ __forceinline__ void lm_seed_groups(const LmArgs& a, unsigned char* s
   pc.rs = rs4; pc.jb = sh.jb; pc.jstart = sh.jstart; pc.jlist = sh.jlist;
   pc.ws = ws4; pc.wc = wc; pc.wb = wb; pc.wh = wh; pc.pairs = pairs; pc.gjoint = gjoint; pc.gstart = gstart;
   pc.cell_start = sh.grid_on ? cell_start : nullptr; pc.cell_obs = cell_obs;
-  pc.pos = pos + (size_t)g * PS; pc.glo = sh.glo; pc.ginv = sh.ginv; pc.G = PK_LM_GRID;
+  pc.pos = pos + (size_t)g * PS; pc.glo = sh.glo; pc.ginv = sh.ginv;
   pc.n_rs = sh.n_rs; pc.n_js = sh.n_js; pc.n_groups = sh.n_groups; pc.Ms_pad = L.ms_pad;
   pc.Mc = a.w.Mc; pc.Mb = a.w.Mb; pc.Mh = a.w.Mh; pc.margin = a.margin;
 
@@ -1032,11 +961,8 @@ __device__ float coop_penalty(const CoopCtx& c, const PoseSlots& psk, int t, uns
     int e0 = 0, e1 = c.Ms;
     const unsigned short* list = nullptr;
     if (c.cell_start) {
-      const int ix = __float2int_rd((B.x - c.glo.x) * c.ginv.x);
-      const int iy = __float2int_rd((B.y - c.glo.y) * c.ginv.y);
-      const int iz = __float2int_rd((B.z - c.glo.z) * c.ginv.z);
-      if ((unsigned)ix >= PK_LM_GRID || (unsigned)iy >= PK_LM_GRID || (unsigned)iz >= PK_LM_GRID) continue;
-      const int cell = (ix * PK_LM_GRID + iy) * PK_LM_GRID + iz;
+      const int cell = obstacle_grid_cell(c.glo, c.ginv, B);
+      if (cell < 0) continue;
       e0 = c.cell_start[cell];
       e1 = c.cell_start[cell + 1];
       list = c.cell_obs;

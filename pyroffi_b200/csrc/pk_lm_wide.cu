@@ -34,10 +34,10 @@
 #include <algorithm>
 
 #include "pk_batch.cuh"
+#include "pk_obstacle_grid.cuh"
 
 namespace pk {
 
-constexpr int WG = 8;                  // obstacle grid cells per axis (coordinates packed in 4 bits)
 constexpr int W_MAXROWS = 6 * PK_MAX_EE;
 
 struct WideArgs {
@@ -122,7 +122,7 @@ __host__ inline WideLayout wide_layout(int max_rs, int max_self, int max_joints,
   L.wc = o; o = w_align16(o + 28 * (size_t)w.Mc);
   L.wb = o; o = w_align16(o + 60 * (size_t)w.Mb);
   L.wh = o; o = w_align16(o + 24 * (size_t)w.Mh);
-  L.cells = o; o = w_align16(o + (L.max_entries ? 4 * (size_t)(WG * WG * WG + 1) : 0));
+  L.cells = o; o = w_align16(o + (L.max_entries ? 4 * (size_t)(kObsGridCells + 1) : 0));
   L.cell_obs = o; o = w_align16(o + 2 * (size_t)L.max_entries);
   L.obox = o; o = w_align16(o + (L.max_entries ? 4 * (size_t)w.Ms : 0));
   // one warp's area
@@ -302,75 +302,17 @@ __device__ void wide_stage_class(const WideLaunch& P, const WideArgs& A, unsigne
       }
     }
     sh.n_pairs = n_pairs;
-    // grid bounds: union of every world sphere's ball of radius r + margin + rmax
+    // obstacle-grid bounds (world radii already carry the margin)
     sh.grid_on = 0;
     if (L.max_entries > 0 && n_js > 0 && P.coll) {
-      float lo3[3] = {3e38f, 3e38f, 3e38f}, hi3[3] = {-3e38f, -3e38f, -3e38f};
-      for (int o = 0; o < w.Ms; ++o) {
-        const float4 O = ws4[o];
-        const float rho = O.w + rmax + 1e-3f;
-        lo3[0] = fminf(lo3[0], O.x - rho); hi3[0] = fmaxf(hi3[0], O.x + rho);
-        lo3[1] = fminf(lo3[1], O.y - rho); hi3[1] = fmaxf(hi3[1], O.y + rho);
-        lo3[2] = fminf(lo3[2], O.z - rho); hi3[2] = fmaxf(hi3[2], O.z + rho);
-      }
-      sh.glo = make_float3(lo3[0], lo3[1], lo3[2]);
-      sh.ginv = make_float3(WG / fmaxf(hi3[0] - lo3[0], 1e-6f), WG / fmaxf(hi3[1] - lo3[1], 1e-6f),
-                            WG / fmaxf(hi3[2] - lo3[2], 1e-6f));
+      obstacle_grid_bounds(ws4, w.Ms, rmax, sh.glo, sh.ginv);
       sh.grid_on = 1;
     }
   }
   __syncthreads();
 
-  // obstacle grid: obstacle o is listed in every cell its inflated ball's
-  // bounding box touches, in increasing o (one thread per cell)
-  if (sh.grid_on) {
-    constexpr int NC = WG * WG * WG;
-    for (int o = tid; o < w.Ms; o += blockDim.x) {
-      const float4 O = ws4[o];
-      const float rho = O.w + sh.rmax + 1e-3f;
-      const float c3[3] = {O.x, O.y, O.z}, l3[3] = {sh.glo.x, sh.glo.y, sh.glo.z},
-                  i3[3] = {sh.ginv.x, sh.ginv.y, sh.ginv.z};
-      int packed = 0;
-      for (int d = 0; d < 3; ++d) {
-        const int i0 = min(max(__float2int_rd((c3[d] - rho - l3[d]) * i3[d]), 0), WG - 1);
-        const int i1 = min(max(__float2int_rd((c3[d] + rho - l3[d]) * i3[d]), 0), WG - 1);
-        packed |= (i0 | (i1 << 4)) << (8 * d);
-      }
-      obox[o] = packed;
-    }
-    __syncthreads();
-    auto inside = [&](int b, int ix, int iy, int iz) {
-      return (ix >= (b & 15)) & (ix <= ((b >> 4) & 15)) & (iy >= ((b >> 8) & 15)) & (iy <= ((b >> 12) & 15)) &
-             (iz >= ((b >> 16) & 15)) & (iz <= ((b >> 20) & 15));
-    };
-    for (int cell = tid; cell < NC; cell += blockDim.x) {
-      const int ix = cell / (WG * WG), iy = (cell / WG) % WG, iz = cell % WG;
-      int cnt = 0;
-      for (int o = 0; o < w.Ms; ++o) cnt += inside(obox[o], ix, iy, iz);
-      cell_start[cell] = cnt;
-    }
-    __syncthreads();
-    if (tid == 0) {
-      int run = 0;
-      for (int cell = 0; cell < NC; ++cell) {
-        const int c = cell_start[cell];
-        cell_start[cell] = run;
-        run += c;
-      }
-      cell_start[NC] = run;
-      if (run > L.max_entries) sh.grid_on = 0;  // does not fit: scan every obstacle instead
-    }
-    __syncthreads();
-    if (sh.grid_on) {
-      for (int cell = tid; cell < NC; cell += blockDim.x) {
-        const int ix = cell / (WG * WG), iy = (cell / WG) % WG, iz = cell % WG;
-        int at = cell_start[cell];
-        for (int o = 0; o < w.Ms; ++o)
-          if (inside(obox[o], ix, iy, iz)) cell_obs[at++] = (unsigned short)o;
-      }
-    }
-    __syncthreads();
-  }
+  if (sh.grid_on)
+    obstacle_grid_build(ws4, w.Ms, sh.rmax, sh.glo, sh.ginv, obox, cell_start, cell_obs, L.max_entries, sh.grid_on);
 }
 
 // Targets of problem pb (threads < n_ee); the caller synchronises.
@@ -493,14 +435,11 @@ __device__ __noinline__ float w_penalty(const WideLaunch& P, const WideShared& s
       const float3 B = pose_apply(w_load(W.T, sh.js_joint[j]), make_float3(bl.x, bl.y, bl.z));
       int e0 = 0, n = Ms;
       if (sh.grid_on) {
-        const int ix = __float2int_rd((B.x - sh.glo.x) * sh.ginv.x);
-        const int iy = __float2int_rd((B.y - sh.glo.y) * sh.ginv.y);
-        const int iz = __float2int_rd((B.z - sh.glo.z) * sh.ginv.z);
+        const int cell = obstacle_grid_cell(sh.glo, sh.ginv, B);
         // outside the grid no obstacle is within reach of this joint
-        if ((unsigned)ix >= (unsigned)WG || (unsigned)iy >= (unsigned)WG || (unsigned)iz >= (unsigned)WG) {
+        if (cell < 0) {
           n = 0;
         } else {
-          const int cell = (ix * WG + iy) * WG + iz;
           e0 = cell_start[cell];
           n = cell_start[cell + 1] - e0;
         }

@@ -1,0 +1,100 @@
+// Uniform grid over the sphere obstacles, built per block in shared memory:
+// a query ball of radius at most `reach` whose centre lies in cell c can only
+// reach obstacles listed in c.  Shared by the LM kernels and the per-seed IK
+// (HJCD, SQP) kernels.
+//
+// Obstacle o (centre x_o, radius r_o) is listed in every cell that the
+// bounding box of the ball of radius r_o + reach + 1e-3 around x_o touches,
+// in increasing o; the grid spans the union of those boxes, so a centre
+// outside it is out of reach of every obstacle.  If |B - x_o| < R + r_o with
+// R <= reach then B lies in that box and the cell of B lists o: cell indices
+// are monotone in the coordinate, and the 1e-3 covers the rounding of the
+// caller's test.
+#pragma once
+
+namespace pk {
+
+constexpr int kObsGrid = 8;                                      // cells per axis (indices packed in 4 bits)
+constexpr int kObsGridCells = kObsGrid * kObsGrid * kObsGrid;
+
+// Origin and inverse cell size of the grid (one thread).
+__device__ inline void obstacle_grid_bounds(const float4* ws, int Ms, float reach, float3& lo, float3& inv) {
+  float l[3] = {3e38f, 3e38f, 3e38f}, h[3] = {-3e38f, -3e38f, -3e38f};
+  for (int o = 0; o < Ms; ++o) {
+    const float4 O = ws[o];
+    const float rho = O.w + reach + 1e-3f;
+    l[0] = fminf(l[0], O.x - rho); h[0] = fmaxf(h[0], O.x + rho);
+    l[1] = fminf(l[1], O.y - rho); h[1] = fmaxf(h[1], O.y + rho);
+    l[2] = fminf(l[2], O.z - rho); h[2] = fmaxf(h[2], O.z + rho);
+  }
+  lo = make_float3(l[0], l[1], l[2]);
+  inv = make_float3(kObsGrid / fmaxf(h[0] - l[0], 1e-6f), kObsGrid / fmaxf(h[1] - l[1], 1e-6f),
+                    kObsGrid / fmaxf(h[2] - l[2], 1e-6f));
+}
+
+// Cell lists: cell_start[kObsGridCells + 1] offsets into cell_obs; obox[Ms]
+// is scratch.  Called by every thread of the block with block-uniform
+// arguments; `on` (shared) is cleared when the lists would exceed
+// max_entries, and the caller then scans every obstacle instead.  Each
+// cell's list is written by one thread, so the order is deterministic.
+__device__ inline void obstacle_grid_build(const float4* ws, int Ms, float reach, float3 lo, float3 inv, int* obox,
+                                           int* cell_start, unsigned short* cell_obs, int max_entries, int& on) {
+  constexpr int G = kObsGrid;
+  const int tid = threadIdx.x, nth = blockDim.x;
+  for (int o = tid; o < Ms; o += nth) {
+    const float4 O = ws[o];
+    const float rho = O.w + reach + 1e-3f;
+    const float c3[3] = {O.x, O.y, O.z}, l3[3] = {lo.x, lo.y, lo.z}, i3[3] = {inv.x, inv.y, inv.z};
+    int packed = 0;
+    for (int d = 0; d < 3; ++d) {
+      const int i0 = min(max(__float2int_rd((c3[d] - rho - l3[d]) * i3[d]), 0), G - 1);
+      const int i1 = min(max(__float2int_rd((c3[d] + rho - l3[d]) * i3[d]), 0), G - 1);
+      packed |= (i0 | (i1 << 4)) << (8 * d);
+    }
+    obox[o] = packed;
+  }
+  __syncthreads();
+  auto inside = [](int b, int ix, int iy, int iz) {
+    return (ix >= (b & 15)) & (ix <= ((b >> 4) & 15)) & (iy >= ((b >> 8) & 15)) & (iy <= ((b >> 12) & 15)) &
+           (iz >= ((b >> 16) & 15)) & (iz <= ((b >> 20) & 15));
+  };
+  for (int cell = tid; cell < kObsGridCells; cell += nth) {
+    const int ix = cell / (G * G), iy = (cell / G) % G, iz = cell % G;
+    int cnt = 0;
+    for (int o = 0; o < Ms; ++o) cnt += inside(obox[o], ix, iy, iz);
+    cell_start[cell] = cnt;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    int run = 0;
+    for (int cell = 0; cell < kObsGridCells; ++cell) {
+      const int c = cell_start[cell];
+      cell_start[cell] = run;
+      run += c;
+    }
+    cell_start[kObsGridCells] = run;
+    if (run > max_entries) on = 0;
+  }
+  __syncthreads();
+  if (on) {
+    for (int cell = tid; cell < kObsGridCells; cell += nth) {
+      const int ix = cell / (G * G), iy = (cell / G) % G, iz = cell % G;
+      int at = cell_start[cell];
+      for (int o = 0; o < Ms; ++o)
+        if (inside(obox[o], ix, iy, iz)) cell_obs[at++] = (unsigned short)o;
+    }
+  }
+  __syncthreads();
+}
+
+// Cell of point B, or -1 outside the grid (no obstacle within reach).
+__device__ __forceinline__ int obstacle_grid_cell(float3 lo, float3 inv, float3 B) {
+  const int ix = __float2int_rd((B.x - lo.x) * inv.x);
+  const int iy = __float2int_rd((B.y - lo.y) * inv.y);
+  const int iz = __float2int_rd((B.z - lo.z) * inv.z);
+  if ((unsigned)ix >= (unsigned)kObsGrid || (unsigned)iy >= (unsigned)kObsGrid || (unsigned)iz >= (unsigned)kObsGrid)
+    return -1;
+  return (ix * kObsGrid + iy) * kObsGrid + iz;
+}
+
+}  // namespace pk

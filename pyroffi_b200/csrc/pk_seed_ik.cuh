@@ -6,6 +6,9 @@
 
 #include <float.h>
 
+#include <algorithm>
+
+#include "pk_obstacle_grid.cuh"
 #include "pk_obstacles.cuh"
 
 namespace pk {
@@ -30,6 +33,7 @@ struct SeedIkArgs {
   float collision_weight, collision_margin, lambda_init, limit_prior_weight, kick_scale, eps_pos, eps_ori;
   int n_inner;                 // SQP: active-set re-solves per step
   float pos_weight, ori_weight;  // SQP: fixed row weights
+  int grid_entries;            // capacity of the sphere-obstacle grid's lists (0: no grid)
 };
 
 struct SeedIkShared {
@@ -40,11 +44,14 @@ struct SeedIkShared {
   float lo[PK_MAX_ACT], hi[PK_MAX_ACT];
   int fixed[PK_MAX_ACT];              // fixed or padding
   int n_groups;                       // joint groups of the robot spheres
+  int grid_on;                        // the sphere-obstacle grid is built
+  float3 glo, ginv;                   // its origin and inverse cell size
 };
 
 __device__ __forceinline__ float clampf(float x, float lo, float hi) { return fmaxf(lo, fminf(hi, x)); }
 
-// Robot spheres in shared memory, grouped by the joint that carries them.
+// Robot spheres in shared memory, grouped by the joint that carries them,
+// and the grid of world spheres within reach of a group's bounding sphere.
 struct RobotSpheresS {
   float4* sph;     // [n_rs] joint-frame centre, radius; group k is gstart[k] .. gstart[k + 1]
   float4* bound;   // [nj] bounding sphere of each group (joint frame)
@@ -52,10 +59,31 @@ struct RobotSpheresS {
   int* gstart;     // [nj + 1]
   int* joint;      // [nj] sorted joint of each group
   int ng;
+  const int* cell_start;            // obstacle grid (null: scan every world sphere)
+  const unsigned short* cell_obs;
+  float3 glo, ginv;
 };
 
-__device__ __forceinline__ size_t seed_ik_spheres_bytes(int n_rs, int nj) {
+__host__ __device__ __forceinline__ size_t seed_ik_spheres_bytes(int n_rs, int nj) {
   return sizeof(float4) * ((size_t)n_rs + nj) + sizeof(int) * (3 * (size_t)nj + 2);
+}
+
+// Dynamic shared memory: SeedIkShared, robot spheres, the world (when staged),
+// the obstacle grid (cell offsets, lists, scratch), then the pose slots.
+__host__ __device__ inline size_t seed_ik_align16(size_t x) { return (x + 15) & ~size_t(15); }
+__host__ __device__ inline size_t seed_ik_world_offset(const SeedIkArgs& a) {
+  return seed_ik_align16(sizeof(SeedIkShared) + seed_ik_spheres_bytes(a.n_rs, a.m.n_joints));
+}
+__host__ __device__ inline size_t seed_ik_grid_offset(const SeedIkArgs& a) {
+  return seed_ik_world_offset(a) + (a.stage_world ? sizeof(float) * a.w.smem_floats() : 0);
+}
+__host__ __device__ inline size_t seed_ik_grid_bytes(const SeedIkArgs& a) {
+  if (!a.grid_entries) return 0;
+  return seed_ik_align16(sizeof(int) * (kObsGridCells + 1)) + seed_ik_align16(2 * (size_t)a.grid_entries) +
+         seed_ik_align16(sizeof(int) * (size_t)a.w.Ms);
+}
+__host__ __device__ inline size_t seed_ik_slots_offset(const SeedIkArgs& a) {
+  return seed_ik_grid_offset(a) + seed_ik_grid_bytes(a);
 }
 
 __device__ __forceinline__ RobotSpheresS seed_ik_spheres_at(unsigned char* p, int n_rs, int nj) {
@@ -150,6 +178,34 @@ __device__ inline void seed_ik_stage(const SeedIkArgs& a, SeedIkShared& sh, Robo
     ob.Ms = a.w.Ms; ob.Mc = a.w.Mc; ob.Mb = a.w.Mb; ob.Mh = a.w.Mh;
   }
   __syncthreads();
+  // world-sphere grid for queries by group bounding spheres: reach = the
+  // largest bounding radius + the margin
+  R.cell_start = nullptr;
+  R.cell_obs = nullptr;
+  if (a.grid_entries && R.ng > 0) {
+    unsigned char* g = reinterpret_cast<unsigned char*>(world_dst) + (seed_ik_grid_offset(a) - seed_ik_world_offset(a));
+    int* cell_start = reinterpret_cast<int*>(g);
+    unsigned short* cell_obs =
+        reinterpret_cast<unsigned short*>(g + seed_ik_align16(sizeof(int) * (kObsGridCells + 1)));
+    int* obox = reinterpret_cast<int*>(reinterpret_cast<unsigned char*>(cell_obs) +
+                                       seed_ik_align16(2 * (size_t)a.grid_entries));
+    float reach = 0.f;
+    for (int k = 0; k < R.ng; ++k) reach = fmaxf(reach, R.bound[k].w);
+    reach += a.collision_margin;
+    if (tid == 0) {
+      obstacle_grid_bounds(ob.sph, ob.Ms, reach, sh.glo, sh.ginv);
+      sh.grid_on = 1;
+    }
+    __syncthreads();
+    obstacle_grid_build(ob.sph, ob.Ms, reach, sh.glo, sh.ginv, obox, cell_start, cell_obs, a.grid_entries,
+                        sh.grid_on);
+    if (sh.grid_on) {
+      R.cell_start = cell_start;
+      R.cell_obs = cell_obs;
+      R.glo = sh.glo;
+      R.ginv = sh.ginv;
+    }
+  }
 }
 
 // Residual of every EE against target slot `w`: world position difference and
@@ -229,7 +285,9 @@ __device__ __forceinline__ void seed_ik_jacobian(const SeedIkShared& sh, const P
 // of (d - margin)^2, from the joint poses in `ps`.  The TPS lanes of a seed
 // group split the obstacles and every lane returns the group's total.  An
 // obstacle at least the margin from a joint group's bounding sphere adds
-// exactly 0 for every sphere of the group and is skipped.
+// exactly 0 for every sphere of the group and is skipped; with the grid, the
+// world spheres tested are those listed in the cell of the group's bounding
+// centre.
 template <int TPS>
 __device__ __forceinline__ float seed_ik_penalty(const SeedIkArgs& a, const PoseSlots& ps, const RobotSpheresS& R,
                                               const ObsView& ob, int gl, unsigned gmask) {
@@ -241,8 +299,7 @@ __device__ __forceinline__ float seed_ik_penalty(const SeedIkArgs& a, const Pose
     const Pose Tj = ps.load(R.joint[k]);
     const float4 jb = R.bound[k];
     const float3 B = pose_apply(Tj, make_float3(jb.x, jb.y, jb.z));
-    for (int m = gl; m < M; m += TPS) {
-      if (!obstacle_near(ob, m, B, jb.w, margin)) continue;
+    auto narrow = [&](int m) {
       for (int i = R.gstart[k]; i < R.gstart[k + 1]; ++i) {
         const float4 q = R.sph[i];
         const float d = obstacle_dist(ob, m, pose_apply(Tj, make_float3(q.x, q.y, q.z)), q.w);
@@ -251,7 +308,21 @@ __device__ __forceinline__ float seed_ik_penalty(const SeedIkArgs& a, const Pose
           pen += e * e;
         }
       }
+    };
+    int m0 = 0;
+    if (R.cell_start) {
+      const int cell = obstacle_grid_cell(R.glo, R.ginv, B);
+      if (cell >= 0) {
+        const int e1 = R.cell_start[cell + 1];
+        for (int e = R.cell_start[cell] + gl; e < e1; e += TPS) {
+          const int m = R.cell_obs[e];
+          if (obstacle_near<0>(ob, m, B, jb.w, margin)) narrow(m);
+        }
+      }
+      m0 = ob.Ms;  // the other kinds are scanned
     }
+    for (int m = m0 + gl; m < M; m += TPS)
+      if (obstacle_near(ob, m, B, jb.w, margin)) narrow(m);
   }
 #pragma unroll
   for (int o = 1; o < TPS; o <<= 1) pen += __shfl_xor_sync(gmask, pen, o);
@@ -267,29 +338,28 @@ __device__ __forceinline__ float reg_at(const float (&v)[MAXA], int i) {
   return r;
 }
 
-__device__ __forceinline__ size_t seed_ik_world_offset(const SeedIkArgs& a) {
-  size_t s = sizeof(SeedIkShared) + seed_ik_spheres_bytes(a.n_rs, a.m.n_joints);
-  return (s + 15) & ~size_t(15);
-}
-
 static inline size_t seed_ik_smem(const SeedIkArgs& a, int nth) {
-  size_t s = sizeof(SeedIkShared) + sizeof(float4) * ((size_t)a.n_rs + a.m.n_joints) +
-             sizeof(int) * (3 * (size_t)a.m.n_joints + 2);
-  s = (s + 15) & ~size_t(15);
-  if (a.stage_world) s += sizeof(float) * a.w.smem_floats();
-  return s + sizeof(float) * (size_t)a.m.n_joints * 7 * nth;
+  return seed_ik_slots_offset(a) + sizeof(float) * (size_t)a.m.n_joints * 7 * nth;
 }
 
 // Host side: extents and capacity checks and the shared-memory size (the
-// world is staged when it fits), argument packing, null-buffer checks.
-static inline int seed_ik_common(SeedIkArgs& a, int n_act, int n_joints, int n_ee, int nth, size_t* smem_out) {
+// world is staged when it fits; with `grid`, a staged world of 32 or more
+// spheres gets the obstacle grid), argument packing, null-buffer checks.
+static inline int seed_ik_common(SeedIkArgs& a, int n_act, int n_joints, int n_ee, int nth, size_t* smem_out,
+                                 bool grid = false) {
   PK_CHECK_ARG(a.P >= 0 && a.S >= 0 && n_act >= 0 && n_joints >= 0 && n_ee >= 0 && a.n_rs >= 0, "negative extent");
   PK_CHECK_CAP(n_joints <= PK_MAX_JOINTS, "n_joints=%d exceeds %d", n_joints, PK_MAX_JOINTS);
   PK_CHECK_CAP(n_act <= 16, "at most 16 actuated joints (got %d)", n_act);
   PK_CHECK_CAP(n_ee >= 1 && n_ee <= PK_MAX_EE, "n_ee=%d must be in [1, %d]", n_ee, PK_MAX_EE);
   PK_CHECK_ARG(a.iters >= 0, "negative iteration count");
   a.stage_world = a.w.smem_floats() * sizeof(float) <= 48 * 1024;
+  const bool want_grid = grid && a.enable_collision && a.stage_world && a.w.Ms >= 32 && a.w.Ms <= 65535;
+  a.grid_entries = want_grid ? std::min(std::max(16 * a.w.Ms, 1024), 8192) : 0;
   size_t smem = seed_ik_smem(a, nth);
+  if (smem > 200 * 1024 && a.grid_entries) {
+    a.grid_entries = 0;
+    smem = seed_ik_smem(a, nth);
+  }
   if (smem > 200 * 1024 && a.stage_world) {
     a.stage_world = 0;
     smem = seed_ik_smem(a, nth);

@@ -208,7 +208,7 @@ __global__ void __launch_bounds__(kSqpThreads) sqp_kernel(SeedIkArgs a) {
   SeedIkShared& sh = *reinterpret_cast<SeedIkShared*>(smem_raw);
   RobotSpheresS R = seed_ik_spheres_at(smem_raw + sizeof(SeedIkShared), a.n_rs, a.m.n_joints);
   float* world = reinterpret_cast<float*>(smem_raw + seed_ik_world_offset(a));
-  float* slots = world + (a.stage_world ? a.w.smem_floats() : 0);
+  float* slots = reinterpret_cast<float*>(smem_raw + seed_ik_slots_offset(a));
   const int tid = threadIdx.x, n = a.m.n_act, p = blockIdx.y;
   const int G = blockDim.x / TPS, grp = tid / TPS, gl = tid % TPS;
   const unsigned gmask = ((1u << TPS) - 1u) << ((tid & 31) & ~(TPS - 1));
@@ -324,7 +324,7 @@ extern "C" int pk_sqp_ik_cuda(void* stream, const float* seeds, const float* twi
   a.collision_weight = collision_weight;
   a.collision_margin = collision_margin;
   size_t smem = 0;
-  if (int s = seed_ik_common(a, n_act, n_joints, n_ee, kSqpThreads, &smem)) return s;
+  if (int s = seed_ik_common(a, n_act, n_joints, n_ee, kSqpThreads, &smem, true)) return s;
   if (n_problems == 0 || n_seeds == 0) return PK_OK;
   if (int s = seed_ik_check_buffers(a)) return s;
   cudaStream_t st = (cudaStream_t)stream;
