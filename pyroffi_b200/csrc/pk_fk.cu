@@ -142,6 +142,15 @@ __device__ __forceinline__ float reg_dist(const ObsReg& o, float4 c) {
   }
 }
 
+// Per-link rows read each link's spheres in pairs, so that the sphere-quad
+// loop runs on packed FP32x2 arithmetic: for spheres 2q and 2q + 1 of link k
+// of configuration c, float4 A = (x0, x1, y0, y1) and B = (z0, z1, -r0, -r1)
+// at cc[((c * N + k) * SP + q) * 2 + {0, 1}], SP = ceil(S / 2).  A padding
+// sphere (radius < 0, or the odd slot) is stored at 1e18 with -r = 1: its
+// packed distances (~1.7e18) never win the minimum, and the scalar rows skip
+// it by its radius.
+__device__ __forceinline__ int link_pair_count(int S) { return (S + 1) >> 1; }
+
 // Rows of one configuration against one register obstacle (a single column
 // m per lane): per-sphere rows (R = K) or per-link minima (R = N).  Returns
 // the lane's minimum; stores go to o, o + M, ... when `store`.
@@ -152,9 +161,12 @@ __device__ __forceinline__ float single_rows(const ObsReg& ob, const float4* cc,
   for (int k = 0; k < R; ++k) {
     float d = 1e9f;
     if (PER_LINK) {
-      for (int s = 0; s < S; ++s) {
-        const float4 ce = cc[s * N + k];
-        if (ce.w >= 0.f) d = fminf(d, reg_dist<KIND>(ob, ce));
+      const int SP = (S + 1) >> 1;
+      for (int q = 0; q < SP; ++q) {
+        const float4 A = cc[(k * SP + q) * 2], B = cc[(k * SP + q) * 2 + 1];
+        const float4 c0 = make_float4(A.x, A.z, B.x, -B.z), c1 = make_float4(A.y, A.w, B.y, -B.w);
+        if (c0.w >= 0.f) d = fminf(d, reg_dist<KIND>(ob, c0));
+        if (c1.w >= 0.f) d = fminf(d, reg_dist<KIND>(ob, c1));
       }
     } else {
       const float4 ce = cc[k];
@@ -185,9 +197,11 @@ __device__ __forceinline__ float single_rows(const ObsReg& ob, const float4* cc,
 // spheres gives 1e9).
 template <bool PER_LINK>
 __device__ __forceinline__ void distance_rows(const FusedArgs& a, const ObsView& ob,
-                                              const float4* centres, int* cmin, long long b0,
+                                              const float4* centres, const int* lany, int* cmin, long long b0,
                                               int nc, float* out, bool do_min) {
   const int N = a.N, S = a.S, K = N * S;
+  const int SP = link_pair_count(S);
+  const int CK = PER_LINK ? 2 * N * SP : K;  // float4 per configuration
   const int M = ob.Ms + ob.Mc + ob.Mb + ob.Mh;
   const int R = PER_LINK ? N : K;
   if (M == 0 || R == 0 || nc == 0) return;
@@ -220,10 +234,15 @@ __device__ __forceinline__ void distance_rows(const FusedArgs& a, const ObsView&
     } else if (!is_quad && active) {
       single = load_obstacle(ob, m0);
     }
+    // negated obstacle centres, duplicated for the packed per-link loop
+    const float2 nx0 = make_float2(-o0.x, -o0.x), ny0 = make_float2(-o0.y, -o0.y), nz0 = make_float2(-o0.z, -o0.z);
+    const float2 nx1 = make_float2(-o1.x, -o1.x), ny1 = make_float2(-o1.y, -o1.y), nz1 = make_float2(-o1.z, -o1.z);
+    const float2 nx2 = make_float2(-o2.x, -o2.x), ny2 = make_float2(-o2.y, -o2.y), nz2 = make_float2(-o2.z, -o2.z);
+    const float2 nx3 = make_float2(-o3.x, -o3.x), ny3 = make_float2(-o3.y, -o3.y), nz3 = make_float2(-o3.z, -o3.z);
     const int c1 = min(nc, (chunk + 1) * cchunk);
     for (int c = chunk * cchunk; c < c1; ++c) {
       float vmin = 1e9f;
-      const float4* cc = centres + c * K;
+      const float4* cc = centres + c * CK;
       if (is_quad && active) {
         // quad rows k = sub, sub + rpw, ...; output pointer advanced only when storing
         float* o = store ? out + ((b0 + c) * R + sub) * (long long)M + m0 : nullptr;
@@ -231,19 +250,33 @@ __device__ __forceinline__ void distance_rows(const FusedArgs& a, const ObsView&
         for (int k = sub; k < R; k += rpw, o += ostep) {
           float4 d;
           if (PER_LINK) {
+            // two spheres per packed op: |c - o| = d2 * rsqrt(d2), d2 = dx^2 + dy^2 + dz^2 + 1e-30
+            // (the scalar centre_dist, operation for operation), minus r
             d = make_float4(1e9f, 1e9f, 1e9f, 1e9f);
-            bool any = false;
+            const float4* pr = cc + k * SP * 2;
 #pragma unroll 2
-            for (int s = 0; s < S; ++s) {
-              const float4 ce = cc[s * N + k];
-              if (ce.w < 0.f) continue;
-              any = true;
-              d.x = fminf(d.x, centre_dist(ce, o0) - ce.w);
-              d.y = fminf(d.y, centre_dist(ce, o1) - ce.w);
-              d.z = fminf(d.z, centre_dist(ce, o2) - ce.w);
-              d.w = fminf(d.w, centre_dist(ce, o3) - ce.w);
+            for (int q = 0; q < SP; ++q) {
+              const float4 A = pr[2 * q], B = pr[2 * q + 1];
+              const float2 cx = make_float2(A.x, A.y), cy = make_float2(A.z, A.w), cz = make_float2(B.x, B.y);
+              const float2 nr = make_float2(B.z, B.w);
+              auto one = [&](const float2& nx, const float2& ny, const float2& nz, float& acc) {
+                const float2 dx = __fadd2_rn(cx, nx), dy = __fadd2_rn(cy, ny), dz = __fadd2_rn(cz, nz);
+                float2 d2 = __ffma2_rn(dz, dz, make_float2(1e-30f, 1e-30f));
+                d2 = __ffma2_rn(dy, dy, d2);
+                d2 = __ffma2_rn(dx, dx, d2);
+                const float2 t = __fadd2_rn(__fmul2_rn(d2, make_float2(rsqrt_approx(d2.x), rsqrt_approx(d2.y))), nr);
+                acc = fminf(acc, fminf(t.x, t.y));
+              };
+              one(nx0, ny0, nz0, d.x);
+              one(nx1, ny1, nz1, d.y);
+              one(nx2, ny2, nz2, d.z);
+              one(nx3, ny3, nz3, d.w);
             }
-            if (any) { d.x -= o0.w; d.y -= o1.w; d.z -= o2.w; d.w -= o3.w; }
+            if (lany[k]) {
+              d.x -= o0.w; d.y -= o1.w; d.z -= o2.w; d.w -= o3.w;
+            } else {
+              d = make_float4(1e9f, 1e9f, 1e9f, 1e9f);
+            }
           } else {
             const float4 ce = cc[k];
             if (ce.w >= 0.f) {
@@ -287,8 +320,11 @@ __global__ void __launch_bounds__(256, 3) fk_sphere_collision_kernel(FusedArgs a
   unsigned char* p = smem_raw + sizeof(JointTable);
   const int cpb = a.cpb, N = a.N, S = a.S, K = N * S;
   const int M = a.w.total();
-  float4* centres = reinterpret_cast<float4*>(p);          // [cpb][K]
-  p += sizeof(float4) * (size_t)cpb * K;
+  const int SP = link_pair_count(S);
+  float4* centres = reinterpret_cast<float4*>(p);          // [cpb][K], or [cpb][N][SP][2] in link pairs
+  p += sizeof(float4) * (size_t)cpb * max(K, 2 * N * SP);
+  int* lany = reinterpret_cast<int*>(p);                    // [N] link has a sphere
+  p += sizeof(int) * (size_t)((N + 3) & ~3);
   float* lp = reinterpret_cast<float*>(p);                  // [cpb][N][7]
   p += sizeof(float) * (size_t)cpb * N * 7;
   int* cmin = reinterpret_cast<int*>(p);                    // [cpb]
@@ -334,22 +370,55 @@ __global__ void __launch_bounds__(256, 3) fk_sphere_collision_kernel(FusedArgs a
     for (int g = tid; g < tot; g += T) dst[g] = lp[g];
   }
 
-  // phase 2: sphere centres, k = s*N + n
-  for (int g = tid; g < nc * K; g += T) {
-    const int c = g / K, k = g - c * K;
-    const int s = k / N, n = k - s * N;
+  // phase 2: sphere centres, per sphere (k = s*N + n) or in link pairs
+  auto world_centre = [&](int c, int n, int s) {
     const float4 ls = *reinterpret_cast<const float4*>(a.link_spheres + ((size_t)n * S + s) * 4);
     const float* q = lp + ((size_t)c * N + n) * 7;
     const Pose Tl{q[0], q[1], q[2], q[3], q[4], q[5], q[6]};
     const float3 w = pose_apply(Tl, make_float3(ls.x, ls.y, ls.z));
-    centres[g] = make_float4(w.x, w.y, w.z, ls.w);
+    return make_float4(w.x, w.y, w.z, ls.w);
+  };
+  auto write_pairs = [&]() {
+    const int K2 = 2 * N * SP;
+    for (int g = tid; g < nc * K2; g += T) {
+      const int c = g / K2, r = g - c * K2;
+      const int n = r / (2 * SP), s = r - n * 2 * SP;
+      float4 w = s < S ? world_centre(c, n, s) : make_float4(0.f, 0.f, 0.f, -1.f);
+      if (!(w.w >= 0.f)) w = make_float4(1e18f, 1e18f, 1e18f, -1.f);
+      float* d = reinterpret_cast<float*>(centres + (size_t)c * K2 + ((size_t)n * SP + (s >> 1)) * 2);
+      const int h = s & 1;
+      d[h] = w.x; d[2 + h] = w.y; d[4 + h] = w.z; d[6 + h] = -w.w;
+    }
+  };
+  const bool per_link = a.dist_bnm || !a.dist_bkm;
+  if (per_link)
+    for (int n = tid; n < N; n += T) {
+      int any = 0;
+      for (int s = 0; s < S; ++s) any |= a.link_spheres[((size_t)n * S + s) * 4 + 3] >= 0.f;
+      lany[n] = any;
+    }
+  if (a.dist_bkm) {
+    for (int g = tid; g < nc * K; g += T) {
+      const int c = g / K, k = g - c * K;
+      const int s = k / N, n = k - s * N;
+      centres[g] = world_centre(c, n, s);
+    }
+  } else {
+    write_pairs();
   }
   __syncthreads();
 
   // phase 3: distances (per-sphere rows, per-link rows, or the minimum only)
   // (the per-link pass gives the minimum when only that, or nothing, is requested)
-  if (a.dist_bkm) distance_rows<false>(a, ob, centres, cmin, b0, nc, a.dist_bkm, true);
-  if (a.dist_bnm || !a.dist_bkm) distance_rows<true>(a, ob, centres, cmin, b0, nc, a.dist_bnm, !a.dist_bkm);
+  if (a.dist_bkm) {
+    distance_rows<false>(a, ob, centres, lany, cmin, b0, nc, a.dist_bkm, true);
+    if (per_link) {
+      __syncthreads();
+      write_pairs();
+      __syncthreads();
+    }
+  }
+  if (per_link) distance_rows<true>(a, ob, centres, lany, cmin, b0, nc, a.dist_bnm, !a.dist_bkm);
   __syncthreads();
   if (a.min_dist)
     for (int c = tid; c < nc; c += T) a.min_dist[b0 + c] = ordered_to_float(cmin[c]);
@@ -425,8 +494,10 @@ extern "C" int pk_fk_sphere_collision(
   const int threads = 256;
   int cpb = 32;
   auto smem_for = [&](int c, bool stage) {
-    size_t b = sizeof(JointTable) + sizeof(float4) * (size_t)c * K + sizeof(float) * (size_t)c * n_links * 7 +
-               sizeof(int) * (size_t)((c + 3) & ~3) + sizeof(float) * (size_t)n_joints * 7 * (c + 1) + 16;
+    const size_t per_cfg = std::max((size_t)K, 2 * (size_t)n_links * (size_t)((S + 1) / 2));
+    size_t b = sizeof(JointTable) + sizeof(float4) * (size_t)c * per_cfg + sizeof(int) * (size_t)((n_links + 3) & ~3) +
+               sizeof(float) * (size_t)c * n_links * 7 + sizeof(int) * (size_t)((c + 3) & ~3) +
+               sizeof(float) * (size_t)n_joints * 7 * (c + 1) + 16;
     if (stage) b += sizeof(float) * w.smem_floats();
     return b;
   };
