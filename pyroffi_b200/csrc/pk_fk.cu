@@ -151,6 +151,33 @@ __device__ __forceinline__ float reg_dist(const ObsReg& o, float4 c) {
 // it by its radius.
 __device__ __forceinline__ int link_pair_count(int S) { return (S + 1) >> 1; }
 
+// Signed distances of the sphere pair (A, B) in the link-pair layout to a
+// register box: reg_dist<2> on packed FP32x2, the projections written as
+// fma(dz, a_z, fma(dy, a_y, dx * a_x)).
+__device__ __forceinline__ float2 box_dist2(const ObsReg& o, float4 A, float4 B) {
+  const float2 dx = __fadd2_rn(make_float2(A.x, A.y), make_float2(-o.p[0], -o.p[0]));
+  const float2 dy = __fadd2_rn(make_float2(A.z, A.w), make_float2(-o.p[1], -o.p[1]));
+  const float2 dz = __fadd2_rn(make_float2(B.x, B.y), make_float2(-o.p[2], -o.p[2]));
+  float2 q[3], m[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const float ax = o.p[3 + 3 * i], ay = o.p[4 + 3 * i], az = o.p[5 + 3 * i], h = o.p[12 + i];
+    float2 l = __fmul2_rn(dx, make_float2(ax, ax));
+    l = __ffma2_rn(dy, make_float2(ay, ay), l);
+    l = __ffma2_rn(dz, make_float2(az, az), l);
+    q[i] = make_float2(fabsf(l.x) - h, fabsf(l.y) - h);
+    m[i] = make_float2(fmaxf(q[i].x, 0.f), fmaxf(q[i].y, 0.f));
+  }
+  float2 x = __fmul2_rn(m[0], m[0]);
+  x = __ffma2_rn(m[1], m[1], x);
+  x = __ffma2_rn(m[2], m[2], x);
+  const float2 xe = __fadd2_rn(x, make_float2(1e-30f, 1e-30f));
+  const float2 out = __fmul2_rn(x, make_float2(rsqrt_approx(xe.x), rsqrt_approx(xe.y)));
+  const float2 in = make_float2(fminf(fmaxf(fmaxf(q[0].x, q[1].x), q[2].x), 0.f),
+                                fminf(fmaxf(fmaxf(q[0].y, q[1].y), q[2].y), 0.f));
+  return __fadd2_rn(__fadd2_rn(out, in), make_float2(B.z, B.w));
+}
+
 // Rows of one configuration against one register obstacle (a single column
 // m per lane): per-sphere rows (R = K) or per-link minima (R = N).  Returns
 // the lane's minimum; stores go to o, o + M, ... when `store`.
@@ -164,9 +191,17 @@ __device__ __forceinline__ float single_rows(const ObsReg& ob, const float4* cc,
       const int SP = (S + 1) >> 1;
       for (int q = 0; q < SP; ++q) {
         const float4 A = cc[(k * SP + q) * 2], B = cc[(k * SP + q) * 2 + 1];
-        const float4 c0 = make_float4(A.x, A.z, B.x, -B.z), c1 = make_float4(A.y, A.w, B.y, -B.w);
-        if (c0.w >= 0.f) d = fminf(d, reg_dist<KIND>(ob, c0));
-        if (c1.w >= 0.f) d = fminf(d, reg_dist<KIND>(ob, c1));
+        if (KIND == 2) {
+          // boxes on packed FP32x2 over the sphere pair; padding spheres are
+          // far away and masked by their radius
+          const float2 t = box_dist2(ob, A, B);
+          if (B.z <= 0.f) d = fminf(d, t.x);
+          if (B.w <= 0.f) d = fminf(d, t.y);
+        } else {
+          const float4 c0 = make_float4(A.x, A.z, B.x, -B.z), c1 = make_float4(A.y, A.w, B.y, -B.w);
+          if (c0.w >= 0.f) d = fminf(d, reg_dist<KIND>(ob, c0));
+          if (c1.w >= 0.f) d = fminf(d, reg_dist<KIND>(ob, c1));
+        }
       }
     } else {
       const float4 ce = cc[k];
