@@ -199,6 +199,29 @@ struct ScoObs<4> {
   }
 };
 
+// A link's spheres in the world frame, held in register pairs (spheres 2p,
+// 2p + 1) so the sphere-obstacle loops run on packed FP32x2 arithmetic.
+// Padded spheres carry radius -1e30: their distances read about 1e30.
+template <int MAXS>
+struct LinkSpheres {
+  static_assert(MAXS % 2 == 0, "spheres come in pairs");
+  float2 x[MAXS / 2], y[MAXS / 2], z[MAXS / 2], r[MAXS / 2];
+  __device__ __forceinline__ float X(int s) const { return (s & 1) ? x[s >> 1].y : x[s >> 1].x; }
+  __device__ __forceinline__ float Y(int s) const { return (s & 1) ? y[s >> 1].y : y[s >> 1].x; }
+  __device__ __forceinline__ float Z(int s) const { return (s & 1) ? z[s >> 1].y : z[s >> 1].x; }
+  __device__ __forceinline__ float R(int s) const { return (s & 1) ? r[s >> 1].y : r[s >> 1].x; }
+  // |c_s - p| - (r_s + rp) for spheres 2q, 2q + 1 (sqrt_fast, operation for operation)
+  __device__ __forceinline__ float2 dist2(int q, float2 npx, float2 npy, float2 npz, float2 rp) const {
+    const float2 dx = __fadd2_rn(x[q], npx), dy = __fadd2_rn(y[q], npy), dz = __fadd2_rn(z[q], npz);
+    float2 d2 = __fmul2_rn(dx, dx);
+    d2 = __ffma2_rn(dy, dy, d2);
+    d2 = __ffma2_rn(dz, dz, d2);
+    const float2 e = __fadd2_rn(d2, make_float2(1e-30f, 1e-30f));
+    const float2 len = __fmul2_rn(d2, make_float2(rsqrt_approx(e.x), rsqrt_approx(e.y)));
+    return __ffma2_rn(__fadd2_rn(r[q], rp), make_float2(-1.f, -1.f), len);
+  }
+};
+
 // Terms whose softmax weight is below exp(-kScoSkip) of the running maximum
 // (2e-9; an FP32 sum that already holds the maximum term, >= 1, absorbs
 // anything below 6e-8) are left out of the accumulators.
@@ -212,8 +235,7 @@ constexpr float kScoSkip = 20.f;
 // the collision sum wanted, its distance at or above the margin).
 template <int KIND, int MAXS, int TG>
 __device__ __forceinline__ SoftAcc world_group(const ScoLinArgs& a, const ObsView& ob, int base, int count, int gl,
-                                               unsigned gm, const float (&cx)[MAXS], const float (&cy)[MAXS],
-                                               const float (&cz)[MAXS], const float (&cr)[MAXS], float3 B, float R,
+                                               unsigned gm, const LinkSpheres<MAXS>& L, float3 B, float R,
                                                bool want_soft, bool want_j, float inv_tau, float gref,
                                                float& csum) {
   SoftAcc acc;
@@ -229,10 +251,21 @@ __device__ __forceinline__ SoftAcc world_group(const ScoLinArgs& a, const ObsVie
     }
     float dmin = FLT_MAX;
     int arg = 0;
+    if constexpr (KIND == 1) {
+      const float2 nx = make_float2(-o.x, -o.x), ny = make_float2(-o.y, -o.y), nz = make_float2(-o.z, -o.z);
+      const float2 ro = make_float2(o.r, o.r);
 #pragma unroll
-    for (int s = 0; s < MAXS; ++s) {  // padded spheres carry radius -1e30 and never win
-      const float d = o.dist(cx[s], cy[s], cz[s], cr[s]);
-      if (d < dmin) { dmin = d; arg = s; }
+      for (int q = 0; q < MAXS / 2; ++q) {  // padded spheres carry radius -1e30 and never win
+        const float2 d = L.dist2(q, nx, ny, nz, ro);
+        if (d.x < dmin) { dmin = d.x; arg = 2 * q; }
+        if (d.y < dmin) { dmin = d.y; arg = 2 * q + 1; }
+      }
+    } else {
+#pragma unroll
+      for (int s = 0; s < MAXS; ++s) {
+        const float d = o.dist(L.X(s), L.Y(s), L.Z(s), L.R(s));
+        if (d < dmin) { dmin = d; arg = s; }
+      }
     }
     if (a.coll) csum -= colldist(dmin, a.margin);
     if (!want_soft) continue;
@@ -243,7 +276,7 @@ __device__ __forceinline__ SoftAcc world_group(const ScoLinArgs& a, const ObsVie
       float rr = 0.f;
 #pragma unroll
       for (int s = 0; s < MAXS; ++s)
-        if (s == arg) { cc = make_float3(cx[s], cy[s], cz[s]); rr = cr[s]; }
+        if (s == arg) { cc = make_float3(L.X(s), L.Y(s), L.Z(s)); rr = L.R(s); }
       obstacle_dist_grad(ob, base + k, cc, rr, gg);
     }
     acc.add(e, true, want_j, gg, cc);
@@ -348,29 +381,32 @@ __global__ void __launch_bounds__(128, MAXS <= 8 ? 4 : (MAXS <= 16 ? 3 : 2)) sco
     for (int l = 0; l < N; ++l) {
       if (lcnt[l] == 0) continue;
       const Pose Tl = lpj[l] < 0 ? pose_identity() : ps.load(lpj[l]);
-      float cx[MAXS], cy[MAXS], cz[MAXS], cr[MAXS];
+      LinkSpheres<MAXS> ls;
 #pragma unroll
-      for (int s = 0; s < MAXS; ++s) {
-        const float4 w = (s < S) ? lsph[l * S + s] : make_float4(0.f, 0.f, 0.f, -1.f);
-        const float3 v = pose_apply(Tl, make_float3(w.x, w.y, w.z));
-        cx[s] = v.x; cy[s] = v.y; cz[s] = v.z;
-        cr[s] = w.w < 0.f ? -1e30f : w.w;  // a padded sphere's distances read 1e30
+      for (int q = 0; q < MAXS / 2; ++q) {
+        const float4 w0 = (2 * q < S) ? lsph[l * S + 2 * q] : make_float4(0.f, 0.f, 0.f, -1.f);
+        const float4 w1 = (2 * q + 1 < S) ? lsph[l * S + 2 * q + 1] : make_float4(0.f, 0.f, 0.f, -1.f);
+        const float3 v0 = pose_apply(Tl, make_float3(w0.x, w0.y, w0.z));
+        const float3 v1 = pose_apply(Tl, make_float3(w1.x, w1.y, w1.z));
+        ls.x[q] = make_float2(v0.x, v1.x); ls.y[q] = make_float2(v0.y, v1.y); ls.z[q] = make_float2(v0.z, v1.z);
+        // a padded sphere's distances read 1e30
+        ls.r[q] = make_float2(w0.w < 0.f ? -1e30f : w0.w, w1.w < 0.f ? -1e30f : w1.w);
       }
       const float4 bl = lbnd[l];
       const float3 Bw = pose_apply(Tl, make_float3(bl.x, bl.y, bl.z));
       // world groups: (link, obstacle) pairs, lane gl takes obstacles gl, gl + TG, ...
       SoftAcc mine, t;
       mine.init();
-      t = world_group<1, MAXS, TG>(a, ob, 0, Ms, gl, gm, cx, cy, cz, cr, Bw, bl.w, want_soft, want_j, inv_tau,
+      t = world_group<1, MAXS, TG>(a, ob, 0, Ms, gl, gm, ls, Bw, bl.w, want_soft, want_j, inv_tau,
                                    gref[1], csum);
       if (gl == 1) mine = t;
-      t = world_group<2, MAXS, TG>(a, ob, Ms, Mc, gl, gm, cx, cy, cz, cr, Bw, bl.w, want_soft, want_j, inv_tau,
+      t = world_group<2, MAXS, TG>(a, ob, Ms, Mc, gl, gm, ls, Bw, bl.w, want_soft, want_j, inv_tau,
                                    gref[2], csum);
       if (gl == 2) mine = t;
-      t = world_group<3, MAXS, TG>(a, ob, Ms + Mc, Mb, gl, gm, cx, cy, cz, cr, Bw, bl.w, want_soft, want_j,
+      t = world_group<3, MAXS, TG>(a, ob, Ms + Mc, Mb, gl, gm, ls, Bw, bl.w, want_soft, want_j,
                                    inv_tau, gref[3], csum);
       if (gl == 3) mine = t;
-      t = world_group<4, MAXS, TG>(a, ob, Ms + Mc + Mb, a.w.Mh, gl, gm, cx, cy, cz, cr, Bw, bl.w, want_soft,
+      t = world_group<4, MAXS, TG>(a, ob, Ms + Mc + Mb, a.w.Mh, gl, gm, ls, Bw, bl.w, want_soft,
                                    want_j, inv_tau, gref[4], csum);
       if (gl == 4) mine = t;
       // self group: the pairs listing link l; lane gl takes entries gl, gl + TG, ...
@@ -403,23 +439,24 @@ __global__ void __launch_bounds__(128, MAXS <= 8 ? 4 : (MAXS <= 16 ? 3 : 2)) sco
             const float4 qb = lsph[o * S + sb];
             if (qb.w < 0.f) continue;
             const float3 pb = pose_apply(To, make_float3(qb.x, qb.y, qb.z));
+            const float2 nx = make_float2(-pb.x, -pb.x), ny = make_float2(-pb.y, -pb.y), nz = make_float2(-pb.z, -pb.z);
 #pragma unroll
-            for (int sa = 0; sa < MAXS; ++sa) {
-              const float dx = cx[sa] - pb.x, dy = cy[sa] - pb.y, dz = cz[sa] - pb.z;
-              const float d = sqrt_fast(dx * dx + dy * dy + dz * dz) - (cr[sa] + qb.w);
-              if (d < dmin) { dmin = d; arga = sa; cb = pb; }
+            for (int q = 0; q < MAXS / 2; ++q) {
+              const float2 d = ls.dist2(q, nx, ny, nz, make_float2(qb.w, qb.w));
+              if (d.x < dmin) { dmin = d.x; arga = 2 * q; cb = pb; }
+              if (d.y < dmin) { dmin = d.y; arga = 2 * q + 1; cb = pb; }
             }
           }
         } else {
           // minimum over equal sphere indices
 #pragma unroll
           for (int s = 0; s < MAXS; ++s) {
-            if (s >= S || cr[s] < 0.f) continue;
+            if (s >= S || ls.R(s) < 0.f) continue;
             const float4 qb = lsph[o * S + s];
             if (qb.w < 0.f) continue;
             const float3 pb = pose_apply(To, make_float3(qb.x, qb.y, qb.z));
-            const float dx = cx[s] - pb.x, dy = cy[s] - pb.y, dz = cz[s] - pb.z;
-            const float d = sqrt_fast(dx * dx + dy * dy + dz * dz) - (cr[s] + qb.w);
+            const float dx = ls.X(s) - pb.x, dy = ls.Y(s) - pb.y, dz = ls.Z(s) - pb.z;
+            const float d = sqrt_fast(dx * dx + dy * dy + dz * dz) - (ls.R(s) + qb.w);
             if (d < dmin) { dmin = d; arga = s; cb = pb; }
           }
         }
@@ -431,7 +468,7 @@ __global__ void __launch_bounds__(128, MAXS <= 8 ? 4 : (MAXS <= 16 ? 3 : 2)) sco
         float3 ca = make_float3(0.f, 0.f, 0.f);
 #pragma unroll
         for (int s = 0; s < MAXS; ++s)
-          if (s == arga) ca = make_float3(cx[s], cy[s], cz[s]);
+          if (s == arga) ca = make_float3(ls.X(s), ls.Y(s), ls.Z(s));
         float3 nrm = make_float3(0.f, 0.f, 0.f);
         if (want_j) {
           const float dx = ca.x - cb.x, dy = ca.y - cb.y, dz = ca.z - cb.z;

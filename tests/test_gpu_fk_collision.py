@@ -246,3 +246,25 @@ def test_fused_per_link_rows(case, both):
     np.testing.assert_allclose(res.min_dist.cpu().numpy(), dmin, atol=2e-5)
     if both:
         np.testing.assert_allclose(res.dist_bkm.cpu().numpy(), bkm, atol=2e-5, rtol=1e-6)
+
+
+@pytest.mark.parametrize("case", ["sweep", "padded"])
+def test_per_link_rows_identical_with_and_without_per_sphere_rows(case):
+    """The per-link pass reads the link-pair centre layout; with per-sphere rows
+    requested too, the centres are rewritten in pairs after that pass.  Both
+    routes must give the same bits."""
+    if case == "sweep":
+        w = W.sweep(B=40)
+        model, spheres, world, cfg = w.model, w.spheres, w.world, w.cfg
+    else:
+        rng = np.random.default_rng(8)
+        model = R.bimanual_tree(rng)
+        spheres = R.random_spheres(model, rng, per_link_range=(0, 5))
+        world = W.empty_world()
+        world.spheres, world.capsules, world.boxes, world.halfspaces = mixed_world(rng, Ms=13, Mc=2, Mb=5, Mh=1)
+        cfg = model.random_cfgs(rng, 33)
+    args = (DeviceRobot.upload(model, DEV), DeviceSpheres.upload(spheres, DEV), DeviceWorld.upload(world, DEV),
+            tt(cfg))
+    a = fk_sphere_collision(*args, per_sphere=False, per_link=True)
+    b = fk_sphere_collision(*args, per_sphere=True, per_link=True)
+    assert torch.equal(a.dist_bnm, b.dist_bnm)

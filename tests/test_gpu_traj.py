@@ -80,3 +80,30 @@ def test_autograd_adapter():
     _, g = tc.cost_and_grad(x.detach())
     np.testing.assert_allclose(x.grad.cpu().numpy(), (g * torch.arange(1, 5, device=DEV)[:, None, None]).cpu().numpy(),
                                rtol=1e-6, atol=1e-6)
+
+
+@pytest.mark.parametrize("margin", [0.01, 0.3])
+def test_all_obstacle_kinds_match_oracle(margin):
+    """Spheres, capsules, oriented boxes and a halfspace (each kind has its own
+    broad-phase loop); the large margin keeps most (link, obstacle) pairs and
+    puts link bounding centres inside boxes."""
+    w = W.mixed_trajectories(Bt=6, T=12)
+    tc = TrajectoryCost(w.model, w.spheres, w.world, w.link_pairs, margin=margin, w_smooth=1.0, w_acc=0.5,
+                        w_jerk=0.1, w_limits=1.0, w_coll=3.0, device=DEV)
+    x = torch.as_tensor(w.traj, device=DEV)
+    c, g = tc.cost_and_grad(x)
+    md = w.model.as_dict()
+    for b in range(6):
+        xb = w.traj[b].astype(np.float64)
+        ref = otr.total_cost(xb, md, w.spheres.centers, w.spheres.radii, w.link_pairs, w.world.arrays(),
+                             margin=margin, w_smooth=1.0, w_acc=0.5, w_jerk=0.1, w_limits=1.0, w_coll=3.0,
+                             lower=w.model.lower, upper=w.model.upper)
+        assert abs(float(c[b]) - ref) <= 1e-4 * abs(ref) + 1e-5, (b, float(c[b]), ref)
+    b = int(np.argmax(tc.waypoint_collision(x).cpu().numpy().sum(1)))
+    tcc = TrajectoryCost(w.model, w.spheres, w.world, w.link_pairs, margin=margin, w_smooth=0.0, w_acc=0.0,
+                         w_jerk=0.0, w_limits=0.0, w_coll=1.0, device=DEV)
+    gc = tcc.grad(x).cpu().numpy()[b].astype(np.float64)
+    ref = otr.collision_grad_fd(w.traj[b].astype(np.float64), md, w.spheres.centers, w.spheres.radii, w.link_pairs,
+                                w.world.arrays(), margin)
+    assert np.linalg.norm(ref) > 0
+    assert np.linalg.norm(gc - ref) / np.linalg.norm(ref) < 1e-4
