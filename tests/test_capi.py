@@ -79,3 +79,62 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setattr(_lib, "_lib", None)
     with pytest.raises(RuntimeError, match="no CPU fallback"):
         _lib.load()
+
+
+def _seed_ik_call(name, P=4, S=8, n_act=7, n_joints=7, n_ee=1, extra=()):
+    """HJCD coarse / SQP entry with dummy pointers: 21 buffers, the scalar
+    attributes `extra`, two outputs, then the extents."""
+    lib = _lib.load()
+    d = C.c_void_p(16)
+    return getattr(lib, name)(None, *([d] * 21), *extra, d, d, P, S, n_act, n_joints, n_ee, 0, 0, 0, 0, 0)
+
+
+_HJCD_COARSE = (20, 0, 1e4, 0.02)
+_SQP = (60, 2, 50.0, 10.0, 5e-3, 1e-8, 1e-8, 0, 1e4, 0.02)
+
+
+@pytest.mark.parametrize("name,extra", [("pk_hjcd_ik_coarse_cuda", _HJCD_COARSE), ("pk_sqp_ik_cuda", _SQP)])
+def test_seed_ik_entries_validate_on_the_host(lib, name, extra):
+    assert _seed_ik_call(name, P=-1, extra=extra) == _lib.PK_ERR_INVALID
+    assert b"negative" in lib.pk_last_error()
+    assert _seed_ik_call(name, n_act=17, n_joints=17, extra=extra) == _lib.PK_ERR_CAPACITY
+    assert b"16 actuated" in lib.pk_last_error()
+    assert _seed_ik_call(name, n_ee=0, extra=extra) == _lib.PK_ERR_CAPACITY
+    assert _seed_ik_call(name, n_ee=5, extra=extra) == _lib.PK_ERR_CAPACITY
+    assert _seed_ik_call(name, n_joints=65, extra=extra) == _lib.PK_ERR_CAPACITY
+    assert _seed_ik_call(name, P=0, extra=extra) == _lib.PK_OK          # no problems: nothing to do
+
+
+def test_hjcd_refinement_validates_on_the_host(lib):
+    d = C.c_void_p(16)
+    args = (20, 6, 1e-3, 1e-4, 0.02, 1e-8, 1e-8, 0, 1e4, 0.02)
+
+    def call(P, S, n_act, n_ee=1, noise=d):
+        return lib.pk_hjcd_ik_lm_cuda(None, d, noise, *([d] * 20), *args, d, d, d, P, S, n_act, n_act, n_ee,
+                                      0, 0, 0, 0, 0)
+    assert call(-2, 8, 7) == _lib.PK_ERR_INVALID
+    assert call(4, 8, 20) == _lib.PK_ERR_CAPACITY
+    assert call(4, 8, 7, noise=None) == _lib.PK_ERR_INVALID               # kicks need the noise buffer
+    assert b"noise" in lib.pk_last_error()
+    assert call(0, 8, 7) == _lib.PK_OK
+
+
+def test_chomp_direction_validates_on_the_host(lib):
+    d = C.c_void_p(16)
+    assert lib.pk_chomp_direction(None, d, d, -1, 64, 7, 24, 10.0, 1.0, 1e-6, 1) == _lib.PK_ERR_INVALID
+    assert lib.pk_chomp_direction(None, d, d, 4, 131, 7, 24, 10.0, 1.0, 1e-6, 1) == _lib.PK_ERR_CAPACITY
+    assert lib.pk_chomp_direction(None, d, d, 0, 64, 7, 24, 10.0, 1.0, 1e-6, 1) == _lib.PK_OK
+    assert lib.pk_chomp_direction(None, None, None, 4, 64, 7, 24, 10.0, 1.0, 1e-6, 1) == _lib.PK_ERR_INVALID
+
+
+def test_trajectory_cost_validates_on_the_host(lib):
+    d = C.c_void_p(16)
+    opt = _lib.TrajOptions(0.01, 1.0, 0.5, 0.1, 1.0, 3.0)
+
+    def call(B, T, S, o=C.byref(opt)):
+        return lib.pk_traj_cost_grad(None, o, *([d] * 22), B, T, 7, 7, 8, S, 0, 4, 0, 0, 0)
+    assert call(4, 64, 33) == _lib.PK_ERR_CAPACITY                      # 32 spheres per link at most
+    assert call(4, 4, 8) == _lib.PK_ERR_INVALID                         # the jerk stencil needs 5 waypoints
+    assert call(-1, 64, 8) == _lib.PK_ERR_INVALID
+    assert call(4, 64, 8, o=None) == _lib.PK_ERR_INVALID
+    assert call(0, 64, 8) == _lib.PK_OK
