@@ -108,23 +108,34 @@ __device__ inline ObsView stage_world(const WorldArgs& w, float* dst) {
   return v;
 }
 
-// Signed distance from sphere (c, r) to obstacle m (exact IEEE sqrt).
+// Obstacle kind as a type (0 sphere, 1 capsule, 2 box, 3 halfspace), for
+// callers that know it at compile time.
+template <int K>
+struct ObsKind {
+  static constexpr int value = K;
+};
+
+// Signed distance from sphere (c, r) to obstacle m (exact IEEE sqrt).  KIND
+// is m's kind when the caller knows it, -1 to dispatch on m.
+template <int KIND = -1>
 __device__ __forceinline__ float obstacle_dist(const ObsView& o, int m, float3 c, float r) {
-  if (m < o.Ms) {
+  if (KIND == 0 || (KIND < 0 && m < o.Ms)) {
     const float4 s = o.sph[m];
     return d_sphere_sphere(c, r, s.x, s.y, s.z, s.w);
   }
   m -= o.Ms;
-  if (m < o.Mc) return d_sphere_capsule(c, r, o.cap + 7 * m);
+  if (KIND == 1 || (KIND < 0 && m < o.Mc)) return d_sphere_capsule(c, r, o.cap + 7 * m);
   m -= o.Mc;
-  if (m < o.Mb) return d_sphere_box(c, r, o.box + 15 * m);
+  if (KIND == 2 || (KIND < 0 && m < o.Mb)) return d_sphere_box(c, r, o.box + 15 * m);
   m -= o.Mb;
   return d_sphere_halfspace(c, r, o.hs + 6 * m);
 }
 
-// Signed distance from sphere (c, r) to obstacle m and its gradient w.r.t. c.
+// Signed distance from sphere (c, r) to obstacle m and its gradient w.r.t. c
+// (KIND as for obstacle_dist).
+template <int KIND = -1>
 __device__ inline float obstacle_dist_grad(const ObsView& o, int m, float3 c, float r, float3& g) {
-  if (m < o.Ms) {
+  if (KIND == 0 || (KIND < 0 && m < o.Ms)) {
     const float4 s = o.sph[m];
     const float dx = c.x - s.x, dy = c.y - s.y, dz = c.z - s.z;
     const float n = sqrtf(dx * dx + dy * dy + dz * dz);
@@ -133,7 +144,7 @@ __device__ inline float obstacle_dist_grad(const ObsView& o, int m, float3 c, fl
     return n - (r + s.w);
   }
   m -= o.Ms;
-  if (m < o.Mc) {
+  if (KIND == 1 || (KIND < 0 && m < o.Mc)) {
     const float* cp = o.cap + 7 * m;
     const float vx = cp[3] - cp[0], vy = cp[4] - cp[1], vz = cp[5] - cp[2];
     const float len2 = vx * vx + vy * vy + vz * vz;
@@ -146,7 +157,7 @@ __device__ inline float obstacle_dist_grad(const ObsView& o, int m, float3 c, fl
     return n - (r + cp[6]);
   }
   m -= o.Mc;
-  if (m < o.Mb) {
+  if (KIND == 2 || (KIND < 0 && m < o.Mb)) {
     const float* b = o.box + 15 * m;
     const float dx = c.x - b[0], dy = c.y - b[1], dz = c.z - b[2];
     const float l[3] = {dx * b[3] + dy * b[4] + dz * b[5], dx * b[6] + dy * b[7] + dz * b[8],
@@ -216,24 +227,24 @@ __device__ __forceinline__ bool obstacle_near(const ObsView& ob, int m, float3 B
   return (B.x - h[3]) * h[0] + (B.y - h[4]) * h[1] + (B.z - h[5]) * h[2] - R < margin;
 }
 
-// Calls f(m) for each obstacle m of this lane's share -- every stride-th
-// obstacle of each kind from `lane` -- that obstacle_near keeps: one loop per
-// kind, so the test does not dispatch.
+// Calls f(m, ObsKind<kind>()) for each obstacle m of this lane's share --
+// every stride-th obstacle of each kind from `lane` -- that obstacle_near
+// keeps: one loop per kind, so neither the test nor f needs to dispatch.
 template <class F>
 __device__ __forceinline__ void for_each_near_obstacle(const ObsView& ob, float3 B, float R, float margin, int lane,
                                                        int stride, F&& f) {
   int base = 0;
   for (int k = lane; k < ob.Ms; k += stride)
-    if (obstacle_near<0>(ob, base + k, B, R, margin)) f(base + k);
+    if (obstacle_near<0>(ob, base + k, B, R, margin)) f(base + k, ObsKind<0>());
   base += ob.Ms;
   for (int k = lane; k < ob.Mc; k += stride)
-    if (obstacle_near<1>(ob, base + k, B, R, margin)) f(base + k);
+    if (obstacle_near<1>(ob, base + k, B, R, margin)) f(base + k, ObsKind<1>());
   base += ob.Mc;
   for (int k = lane; k < ob.Mb; k += stride)
-    if (obstacle_near<2>(ob, base + k, B, R, margin)) f(base + k);
+    if (obstacle_near<2>(ob, base + k, B, R, margin)) f(base + k, ObsKind<2>());
   base += ob.Mb;
   for (int k = lane; k < ob.Mh; k += stride)
-    if (obstacle_near<3>(ob, base + k, B, R, margin)) f(base + k);
+    if (obstacle_near<3>(ob, base + k, B, R, margin)) f(base + k, ObsKind<3>());
 }
 
 __device__ __forceinline__ float3 cross3(float3 a, float3 b) {

@@ -277,7 +277,7 @@ __device__ __forceinline__ SoftAcc world_group(const ScoLinArgs& a, const ObsVie
 #pragma unroll
       for (int s = 0; s < MAXS; ++s)
         if (s == arg) { cc = make_float3(L.X(s), L.Y(s), L.Z(s)); rr = L.R(s); }
-      obstacle_dist_grad(ob, base + k, cc, rr, gg);
+      obstacle_dist_grad<KIND - 1>(ob, base + k, cc, rr, gg);
     }
     acc.add(e, true, want_j, gg, cc);
   }

@@ -129,7 +129,8 @@ __global__ void __launch_bounds__(64 * TG, 8 / TG) traj_cost_kernel(TrajArgs a) 
       float3 F = make_float3(0.f, 0.f, 0.f), Mo = make_float3(0.f, 0.f, 0.f);
       // narrow phase of obstacle m: the link's minimum sphere distance, its
       // hinge and the force at the sphere that attains it
-      auto narrow = [&](int m) {
+      auto narrow = [&](int m, auto kind) {
+        constexpr int K = decltype(kind)::value;
         if (!have) {
 #pragma unroll
           for (int s = 0; s < MAXS; ++s) {
@@ -144,7 +145,7 @@ __global__ void __launch_bounds__(64 * TG, 8 / TG) traj_cost_kernel(TrajArgs a) 
 #pragma unroll
         for (int s = 0; s < MAXS; ++s) {
           if (cr[s] < 0.f) continue;
-          const float d = obstacle_dist(ob, m, make_float3(cx[s], cy[s], cz[s]), cr[s]);
+          const float d = obstacle_dist<K>(ob, m, make_float3(cx[s], cy[s], cz[s]), cr[s]);
           if (d < dmin) { dmin = d; arg = s; }
         }
         if (arg < 0 || !(dmin < margin)) return;
@@ -156,7 +157,7 @@ __global__ void __launch_bounds__(64 * TG, 8 / TG) traj_cost_kernel(TrajArgs a) 
 #pragma unroll
           for (int s = 0; s < MAXS; ++s)
             if (s == arg) { c = make_float3(cx[s], cy[s], cz[s]); rr = cr[s]; }
-          obstacle_dist_grad(ob, m, c, rr, g);
+          obstacle_dist_grad<K>(ob, m, c, rr, g);
           const float k = -2.f * v;  // d(v^2)/dd
           const float3 f = make_float3(k * g.x, k * g.y, k * g.z);
           F.x += f.x; F.y += f.y; F.z += f.z;
