@@ -299,10 +299,12 @@ __device__ __forceinline__ float seed_ik_penalty(const SeedIkArgs& a, const Pose
     const Pose Tj = ps.load(R.joint[k]);
     const float4 jb = R.bound[k];
     const float3 B = pose_apply(Tj, make_float3(jb.x, jb.y, jb.z));
-    auto narrow = [&](int m) {
+    // KIND: the obstacle's kind, or -1 to dispatch on m
+    auto narrow = [&](int m, auto kind) {
+      constexpr int KIND = decltype(kind)::value;
       for (int i = R.gstart[k]; i < R.gstart[k + 1]; ++i) {
         const float4 q = R.sph[i];
-        const float d = obstacle_dist(ob, m, pose_apply(Tj, make_float3(q.x, q.y, q.z)), q.w);
+        const float d = obstacle_dist<KIND>(ob, m, pose_apply(Tj, make_float3(q.x, q.y, q.z)), q.w);
         if (d < margin) {
           const float e = d - margin;
           pen += e * e;
@@ -316,13 +318,13 @@ __device__ __forceinline__ float seed_ik_penalty(const SeedIkArgs& a, const Pose
         const int e1 = R.cell_start[cell + 1];
         for (int e = R.cell_start[cell] + gl; e < e1; e += TPS) {
           const int m = R.cell_obs[e];
-          if (obstacle_near<0>(ob, m, B, jb.w, margin)) narrow(m);
+          if (obstacle_near<0>(ob, m, B, jb.w, margin)) narrow(m, ObsKind<0>());
         }
       }
       m0 = ob.Ms;  // the other kinds are scanned
     }
     for (int m = m0 + gl; m < M; m += TPS)
-      if (obstacle_near(ob, m, B, jb.w, margin)) narrow(m);
+      if (obstacle_near(ob, m, B, jb.w, margin)) narrow(m, ObsKind<-1>());
   }
 #pragma unroll
   for (int o = 1; o < TPS; o <<= 1) pen += __shfl_xor_sync(gmask, pen, o);
