@@ -108,6 +108,65 @@ __device__ inline ObsView stage_world(const WorldArgs& w, float* dst) {
   return v;
 }
 
+// A link's spheres in the world frame, held in register pairs (spheres 2q,
+// 2q + 1) so the sphere-obstacle loops run on packed FP32x2 arithmetic.
+// Padded spheres carry radius -1e30: their distances read about 1e30 and
+// never win a minimum.  Each pair method computes, element by element, the
+// same operations as its scalar counterpart.
+template <int MAXS>
+struct LinkSpheres {
+  static_assert(MAXS % 2 == 0, "spheres come in pairs");
+  float2 x[MAXS / 2], y[MAXS / 2], z[MAXS / 2], r[MAXS / 2];
+  __device__ __forceinline__ float X(int s) const { return (s & 1) ? x[s >> 1].y : x[s >> 1].x; }
+  __device__ __forceinline__ float Y(int s) const { return (s & 1) ? y[s >> 1].y : y[s >> 1].x; }
+  __device__ __forceinline__ float Z(int s) const { return (s & 1) ? z[s >> 1].y : z[s >> 1].x; }
+  __device__ __forceinline__ float R(int s) const { return (s & 1) ? r[s >> 1].y : r[s >> 1].x; }
+  // squared distance of spheres 2q, 2q + 1 to the point -(npx, npy, npz)
+  __device__ __forceinline__ float2 sq_dist2(int q, float2 npx, float2 npy, float2 npz) const {
+    const float2 dx = __fadd2_rn(x[q], npx), dy = __fadd2_rn(y[q], npy), dz = __fadd2_rn(z[q], npz);
+    float2 d2 = __fmul2_rn(dx, dx);
+    d2 = __ffma2_rn(dy, dy, d2);
+    return __ffma2_rn(dz, dz, d2);
+  }
+  // |c_s - p| - (r_s + rp) with sqrt_fast
+  __device__ __forceinline__ float2 sphere_dist2_fast(int q, float2 npx, float2 npy, float2 npz, float2 rp) const {
+    const float2 d2 = sq_dist2(q, npx, npy, npz);
+    const float2 e = __fadd2_rn(d2, make_float2(1e-30f, 1e-30f));
+    const float2 len = __fmul2_rn(d2, make_float2(rsqrt_approx(e.x), rsqrt_approx(e.y)));
+    return __ffma2_rn(__fadd2_rn(r[q], rp), make_float2(-1.f, -1.f), len);
+  }
+  // d_sphere_sphere against world sphere o (IEEE sqrt)
+  __device__ __forceinline__ float2 sphere_dist2(int q, float4 o) const {
+    const float2 d2 = sq_dist2(q, make_float2(-o.x, -o.x), make_float2(-o.y, -o.y), make_float2(-o.z, -o.z));
+    const float2 len = make_float2(sqrtf(d2.x), sqrtf(d2.y));
+    return __ffma2_rn(__fadd2_rn(r[q], make_float2(o.w, o.w)), make_float2(-1.f, -1.f), len);
+  }
+  // d_sphere_box against box b (centre, axis columns, half-lengths; IEEE sqrt)
+  __device__ __forceinline__ float2 box_dist2(int q, const float* b) const {
+    const float2 dx = __fadd2_rn(x[q], make_float2(-b[0], -b[0]));
+    const float2 dy = __fadd2_rn(y[q], make_float2(-b[1], -b[1]));
+    const float2 dz = __fadd2_rn(z[q], make_float2(-b[2], -b[2]));
+    float2 qv[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      float2 p = __fmul2_rn(dx, make_float2(b[3 + 3 * i], b[3 + 3 * i]));
+      p = __ffma2_rn(dy, make_float2(b[4 + 3 * i], b[4 + 3 * i]), p);
+      p = __ffma2_rn(dz, make_float2(b[5 + 3 * i], b[5 + 3 * i]), p);
+      qv[i] = make_float2(fabsf(p.x) - b[12 + i], fabsf(p.y) - b[12 + i]);
+    }
+    const float2 m1 = make_float2(fmaxf(qv[0].x, 0.f), fmaxf(qv[0].y, 0.f));
+    const float2 m2 = make_float2(fmaxf(qv[1].x, 0.f), fmaxf(qv[1].y, 0.f));
+    const float2 m3 = make_float2(fmaxf(qv[2].x, 0.f), fmaxf(qv[2].y, 0.f));
+    float2 s2 = __fmul2_rn(m1, m1);
+    s2 = __ffma2_rn(m2, m2, s2);
+    s2 = __ffma2_rn(m3, m3, s2);
+    const float2 out = make_float2(sqrtf(s2.x), sqrtf(s2.y));
+    const float2 in = make_float2(fminf(fmaxf(fmaxf(qv[0].x, qv[1].x), qv[2].x), 0.f),
+                                  fminf(fmaxf(fmaxf(qv[0].y, qv[1].y), qv[2].y), 0.f));
+    return __ffma2_rn(r[q], make_float2(-1.f, -1.f), __fadd2_rn(out, in));
+  }
+};
+
 // Obstacle kind as a type (0 sphere, 1 capsule, 2 box, 3 halfspace), for
 // callers that know it at compile time.
 template <int K>

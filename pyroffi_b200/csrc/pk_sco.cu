@@ -199,29 +199,6 @@ struct ScoObs<4> {
   }
 };
 
-// A link's spheres in the world frame, held in register pairs (spheres 2p,
-// 2p + 1) so the sphere-obstacle loops run on packed FP32x2 arithmetic.
-// Padded spheres carry radius -1e30: their distances read about 1e30.
-template <int MAXS>
-struct LinkSpheres {
-  static_assert(MAXS % 2 == 0, "spheres come in pairs");
-  float2 x[MAXS / 2], y[MAXS / 2], z[MAXS / 2], r[MAXS / 2];
-  __device__ __forceinline__ float X(int s) const { return (s & 1) ? x[s >> 1].y : x[s >> 1].x; }
-  __device__ __forceinline__ float Y(int s) const { return (s & 1) ? y[s >> 1].y : y[s >> 1].x; }
-  __device__ __forceinline__ float Z(int s) const { return (s & 1) ? z[s >> 1].y : z[s >> 1].x; }
-  __device__ __forceinline__ float R(int s) const { return (s & 1) ? r[s >> 1].y : r[s >> 1].x; }
-  // |c_s - p| - (r_s + rp) for spheres 2q, 2q + 1 (sqrt_fast, operation for operation)
-  __device__ __forceinline__ float2 dist2(int q, float2 npx, float2 npy, float2 npz, float2 rp) const {
-    const float2 dx = __fadd2_rn(x[q], npx), dy = __fadd2_rn(y[q], npy), dz = __fadd2_rn(z[q], npz);
-    float2 d2 = __fmul2_rn(dx, dx);
-    d2 = __ffma2_rn(dy, dy, d2);
-    d2 = __ffma2_rn(dz, dz, d2);
-    const float2 e = __fadd2_rn(d2, make_float2(1e-30f, 1e-30f));
-    const float2 len = __fmul2_rn(d2, make_float2(rsqrt_approx(e.x), rsqrt_approx(e.y)));
-    return __ffma2_rn(__fadd2_rn(r[q], rp), make_float2(-1.f, -1.f), len);
-  }
-};
-
 // Terms whose softmax weight is below exp(-kScoSkip) of the running maximum
 // (2e-9; an FP32 sum that already holds the maximum term, >= 1, absorbs
 // anything below 6e-8) are left out of the accumulators.
@@ -256,7 +233,7 @@ __device__ __forceinline__ SoftAcc world_group(const ScoLinArgs& a, const ObsVie
       const float2 ro = make_float2(o.r, o.r);
 #pragma unroll
       for (int q = 0; q < MAXS / 2; ++q) {  // padded spheres carry radius -1e30 and never win
-        const float2 d = L.dist2(q, nx, ny, nz, ro);
+        const float2 d = L.sphere_dist2_fast(q, nx, ny, nz, ro);
         if (d.x < dmin) { dmin = d.x; arg = 2 * q; }
         if (d.y < dmin) { dmin = d.y; arg = 2 * q + 1; }
       }
@@ -442,7 +419,7 @@ __global__ void __launch_bounds__(128, MAXS <= 8 ? 4 : (MAXS <= 16 ? 3 : 2)) sco
             const float2 nx = make_float2(-pb.x, -pb.x), ny = make_float2(-pb.y, -pb.y), nz = make_float2(-pb.z, -pb.z);
 #pragma unroll
             for (int q = 0; q < MAXS / 2; ++q) {
-              const float2 d = ls.dist2(q, nx, ny, nz, make_float2(qb.w, qb.w));
+              const float2 d = ls.sphere_dist2_fast(q, nx, ny, nz, make_float2(qb.w, qb.w));
               if (d.x < dmin) { dmin = d.x; arga = 2 * q; cb = pb; }
               if (d.y < dmin) { dmin = d.y; arga = 2 * q + 1; cb = pb; }
             }

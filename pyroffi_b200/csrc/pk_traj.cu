@@ -124,7 +124,7 @@ __global__ void __launch_bounds__(64 * TG, 8 / TG) traj_cost_kernel(TrajArgs a) 
       if (bl.w < 0.f) continue;
       const Pose Tl = lpj[l] < 0 ? pose_identity() : ps.load(lpj[l]);
       const float3 B = pose_apply(Tl, make_float3(bl.x, bl.y, bl.z));
-      float cx[MAXS], cy[MAXS], cz[MAXS], cr[MAXS];
+      LinkSpheres<MAXS> ls;
       bool have = false;
       float3 F = make_float3(0.f, 0.f, 0.f), Mo = make_float3(0.f, 0.f, 0.f);
       // narrow phase of obstacle m: the link's minimum sphere distance, its
@@ -133,22 +133,34 @@ __global__ void __launch_bounds__(64 * TG, 8 / TG) traj_cost_kernel(TrajArgs a) 
         constexpr int K = decltype(kind)::value;
         if (!have) {
 #pragma unroll
-          for (int s = 0; s < MAXS; ++s) {
-            const float4 q = (s < S) ? lsph[l * S + s] : make_float4(0.f, 0.f, 0.f, -1.f);
-            const float3 w = pose_apply(Tl, make_float3(q.x, q.y, q.z));
-            cx[s] = w.x; cy[s] = w.y; cz[s] = w.z; cr[s] = q.w;
+          for (int q = 0; q < MAXS / 2; ++q) {
+            const float4 a0 = (2 * q < S) ? lsph[l * S + 2 * q] : make_float4(0.f, 0.f, 0.f, -1.f);
+            const float4 a1 = (2 * q + 1 < S) ? lsph[l * S + 2 * q + 1] : make_float4(0.f, 0.f, 0.f, -1.f);
+            const float3 w0 = pose_apply(Tl, make_float3(a0.x, a0.y, a0.z));
+            const float3 w1 = pose_apply(Tl, make_float3(a1.x, a1.y, a1.z));
+            ls.x[q] = make_float2(w0.x, w1.x); ls.y[q] = make_float2(w0.y, w1.y); ls.z[q] = make_float2(w0.z, w1.z);
+            ls.r[q] = make_float2(a0.w < 0.f ? -1e30f : a0.w, a1.w < 0.f ? -1e30f : a1.w);
           }
           have = true;
         }
         float dmin = FLT_MAX;
         int arg = -1;
 #pragma unroll
-        for (int s = 0; s < MAXS; ++s) {
-          if (cr[s] < 0.f) continue;
-          const float d = obstacle_dist<K>(ob, m, make_float3(cx[s], cy[s], cz[s]), cr[s]);
-          if (d < dmin) { dmin = d; arg = s; }
+        for (int q = 0; q < MAXS / 2; ++q) {
+          float2 d;
+          if constexpr (K == 0) {
+            d = ls.sphere_dist2(q, ob.sph[m]);
+          } else if constexpr (K == 2) {
+            d = ls.box_dist2(q, ob.box + 15 * (m - ob.Ms - ob.Mc));
+          } else {
+            d.x = obstacle_dist<K>(ob, m, make_float3(ls.x[q].x, ls.y[q].x, ls.z[q].x), ls.r[q].x);
+            d.y = obstacle_dist<K>(ob, m, make_float3(ls.x[q].y, ls.y[q].y, ls.z[q].y), ls.r[q].y);
+          }
+          if (d.x < dmin) { dmin = d.x; arg = 2 * q; }
+          if (d.y < dmin) { dmin = d.y; arg = 2 * q + 1; }
         }
-        if (arg < 0 || !(dmin < margin)) return;
+        // padded spheres read about 1e30: a link of padding only has no hit
+        if (!(dmin < margin)) return;
         const float v = margin - dmin;
         cw += v * v;
         if (want_grad) {
@@ -156,7 +168,7 @@ __global__ void __launch_bounds__(64 * TG, 8 / TG) traj_cost_kernel(TrajArgs a) 
           float rr = 0.f;
 #pragma unroll
           for (int s = 0; s < MAXS; ++s)
-            if (s == arg) { c = make_float3(cx[s], cy[s], cz[s]); rr = cr[s]; }
+            if (s == arg) { c = make_float3(ls.X(s), ls.Y(s), ls.Z(s)); rr = ls.R(s); }
           obstacle_dist_grad<K>(ob, m, c, rr, g);
           const float k = -2.f * v;  // d(v^2)/dd
           const float3 f = make_float3(k * g.x, k * g.y, k * g.z);
