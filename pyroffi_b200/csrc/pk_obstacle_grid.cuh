@@ -36,11 +36,14 @@ __device__ inline void obstacle_grid_bounds(const float4* ws, int Ms, float reac
 // is scratch.  Called by every thread of the block with block-uniform
 // arguments; `on` (shared) is cleared when the lists would exceed
 // max_entries, and the caller then scans every obstacle instead.  Each
-// cell's list is written by one thread, so the order is deterministic.
+// obstacle adds itself to the cells of its box (shared-memory atomics), and
+// every cell's list is then sorted, so the lists hold increasing obstacle
+// indices whatever the order of the atomics.
 __device__ inline void obstacle_grid_build(const float4* ws, int Ms, float reach, float3 lo, float3 inv, int* obox,
                                            int* cell_start, unsigned short* cell_obs, int max_entries, int& on) {
-  constexpr int G = kObsGrid;
+  constexpr int G = kObsGrid, NC = kObsGridCells;
   const int tid = threadIdx.x, nth = blockDim.x;
+  for (int c = tid; c <= NC; c += nth) cell_start[c] = 0;
   for (int o = tid; o < Ms; o += nth) {
     const float4 O = ws[o];
     const float rho = O.w + reach + 1e-3f;
@@ -54,34 +57,47 @@ __device__ inline void obstacle_grid_build(const float4* ws, int Ms, float reach
     obox[o] = packed;
   }
   __syncthreads();
-  auto inside = [](int b, int ix, int iy, int iz) {
-    return (ix >= (b & 15)) & (ix <= ((b >> 4) & 15)) & (iy >= ((b >> 8) & 15)) & (iy <= ((b >> 12) & 15)) &
-           (iz >= ((b >> 16) & 15)) & (iz <= ((b >> 20) & 15));
+  // calls f(cell) for every cell of obstacle o's box
+  auto cells_of = [&](int o, auto&& f) {
+    const int b = obox[o];
+    for (int ix = b & 15; ix <= ((b >> 4) & 15); ++ix)
+      for (int iy = (b >> 8) & 15; iy <= ((b >> 12) & 15); ++iy)
+        for (int iz = (b >> 16) & 15; iz <= ((b >> 20) & 15); ++iz) f((ix * G + iy) * G + iz);
   };
-  for (int cell = tid; cell < kObsGridCells; cell += nth) {
-    const int ix = cell / (G * G), iy = (cell / G) % G, iz = cell % G;
-    int cnt = 0;
-    for (int o = 0; o < Ms; ++o) cnt += inside(obox[o], ix, iy, iz);
-    cell_start[cell] = cnt;
-  }
+  for (int o = tid; o < Ms; o += nth) cells_of(o, [&](int c) { atomicAdd(&cell_start[c], 1); });
   __syncthreads();
   if (tid == 0) {
     int run = 0;
-    for (int cell = 0; cell < kObsGridCells; ++cell) {
-      const int c = cell_start[cell];
-      cell_start[cell] = run;
-      run += c;
+    for (int c = 0; c < NC; ++c) {
+      const int n = cell_start[c];
+      cell_start[c] = run;
+      run += n;
     }
-    cell_start[kObsGridCells] = run;
+    cell_start[NC] = run;
     if (run > max_entries) on = 0;
   }
   __syncthreads();
   if (on) {
-    for (int cell = tid; cell < kObsGridCells; cell += nth) {
-      const int ix = cell / (G * G), iy = (cell / G) % G, iz = cell % G;
-      int at = cell_start[cell];
-      for (int o = 0; o < Ms; ++o)
-        if (inside(obox[o], ix, iy, iz)) cell_obs[at++] = (unsigned short)o;
+    // fill: cell_start[c] advances to the end of cell c, i.e. the start of c + 1
+    for (int o = tid; o < Ms; o += nth)
+      cells_of(o, [&](int c) { cell_obs[atomicAdd(&cell_start[c], 1)] = (unsigned short)o; });
+    __syncthreads();
+    if (tid == 0) {
+      for (int c = NC - 1; c > 0; --c) cell_start[c] = cell_start[c - 1];
+      cell_start[0] = 0;
+    }
+    __syncthreads();
+    for (int c = tid; c < NC; c += nth) {
+      const int e0 = cell_start[c], e1 = cell_start[c + 1];
+      for (int i = e0 + 1; i < e1; ++i) {
+        const unsigned short v = cell_obs[i];
+        int j = i - 1;
+        while (j >= e0 && cell_obs[j] > v) {
+          cell_obs[j + 1] = cell_obs[j];
+          --j;
+        }
+        cell_obs[j + 1] = v;
+      }
     }
   }
   __syncthreads();
@@ -89,12 +105,12 @@ __device__ inline void obstacle_grid_build(const float4* ws, int Ms, float reach
 
 // Cell of point B, or -1 outside the grid (no obstacle within reach).
 __device__ __forceinline__ int obstacle_grid_cell(float3 lo, float3 inv, float3 B) {
+  constexpr int G = kObsGrid;
   const int ix = __float2int_rd((B.x - lo.x) * inv.x);
   const int iy = __float2int_rd((B.y - lo.y) * inv.y);
   const int iz = __float2int_rd((B.z - lo.z) * inv.z);
-  if ((unsigned)ix >= (unsigned)kObsGrid || (unsigned)iy >= (unsigned)kObsGrid || (unsigned)iz >= (unsigned)kObsGrid)
-    return -1;
-  return (ix * kObsGrid + iy) * kObsGrid + iz;
+  if ((unsigned)ix >= (unsigned)G || (unsigned)iy >= (unsigned)G || (unsigned)iz >= (unsigned)G) return -1;
+  return (ix * G + iy) * G + iz;
 }
 
 }  // namespace pk
