@@ -82,12 +82,13 @@ def test_autograd_adapter():
                                rtol=1e-6, atol=1e-6)
 
 
-@pytest.mark.parametrize("margin", [0.01, 0.3])
-def test_all_obstacle_kinds_match_oracle(margin):
+@pytest.mark.parametrize("margin,n_spheres", [(0.01, 24), (0.3, 23)])
+def test_all_obstacle_kinds_match_oracle(margin, n_spheres):
     """Spheres, capsules, oriented boxes and a halfspace (each kind has its own
-    broad-phase loop); the large margin keeps most (link, obstacle) pairs and
-    puts link bounding centres inside boxes."""
-    w = W.mixed_trajectories(Bt=6, T=12)
+    broad-phase loop; the spheres go two per packed test, so an odd count pads
+    the last pair); the large margin keeps most (link, obstacle) pairs and puts
+    link bounding centres inside boxes."""
+    w = W.mixed_trajectories(Bt=6, T=12, n_spheres=n_spheres)
     tc = TrajectoryCost(w.model, w.spheres, w.world, w.link_pairs, margin=margin, w_smooth=1.0, w_acc=0.5,
                         w_jerk=0.1, w_limits=1.0, w_coll=3.0, device=DEV)
     x = torch.as_tensor(w.traj, device=DEV)
