@@ -147,3 +147,19 @@ def test_solve_matches_oracle_refinement_of_the_same_seeds():
     assert np.mean(ok_gpu) >= 0.5
     assert abs(np.mean(ok_gpu) - np.mean(ok_or)) <= 0.15, (np.mean(ok_gpu), np.mean(ok_or))
     assert np.mean(np.asarray(ok_gpu) == np.asarray(ok_or)) >= 0.8
+
+
+def test_refinement_over_two_seed_chunks_and_empty_batch():
+    """45 refinement seeds: the block walks a chunk of 32 and one of 13; no problems at all."""
+    w, sol, tj, anc, tgt, oc = chain(P=2, S=45, coll=True)
+    noise = np.random.default_rng(11).normal(size=(2, 45, 6, w.model.n_act)).astype(np.float32)
+    cfg, err, stop = sol.refine(t(w.seeds), t(noise), t(w.target_T), max_iter=6, **REF_KW)
+    err = err.cpu().numpy()
+    for p in range(2):
+        _, oe, ostop = ohjcd.lm_refine(w.seeds[p], noise[p], tgt[p:p + 1], w.model.as_dict(), tj, anc,
+                                       w.model.lower, w.model.upper, np.zeros(w.model.n_act, bool), max_iter=6,
+                                       stall_patience=6, eps_pos=1e-8, eps_ori=1e-8, coll=oc, **REF_KW)
+        assert agree(err[p], oe, rtol=1e-2, atol=1e-8) >= 0.85
+        assert int(stop[p]) == int(ostop)
+    c0, e0, s0 = sol.refine(t(w.seeds[:0]), t(noise[:0]), t(w.target_T[:0]), max_iter=6, **REF_KW)
+    assert c0.shape == (0, 45, w.model.n_act) and s0.shape == (0,)

@@ -102,3 +102,17 @@ def test_solve_matches_oracle_on_the_same_seeds():
             acc.append(bool(pe[0] < 1e-3 and re[0] < 1e-2))
     assert np.mean(ok_gpu) >= 0.8
     assert abs(np.mean(ok_gpu) - np.mean(ok_or)) <= 0.15, (np.mean(ok_gpu), np.mean(ok_or))
+
+
+def test_partial_seed_blocks_and_empty_batch():
+    """33 seeds: a full 32-seed block and a block of one; no problems at all."""
+    w, sol, tj, anc, tgt, oc = chain(P=2, S=33, coll=True)
+    cfg, err = sol.run(t(w.seeds), t(w.target_T), max_iter=5, **KW)
+    cfg, err = cfg.cpu().numpy(), err.cpu().numpy()
+    for p in range(2):
+        _, oe = osqp.sqp(w.seeds[p], tgt[p:p + 1], w.model.as_dict(), tj, anc, w.model.lower, w.model.upper,
+                         np.zeros(w.model.n_act, bool), max_iter=5, coll=oc, **OKW)
+        assert agree(err[p], oe) >= 0.85
+        assert np.all(cfg[p] >= w.model.lower - 1e-6) and np.all(cfg[p] <= w.model.upper + 1e-6)
+    c0, e0 = sol.run(t(w.seeds[:0]), t(w.target_T[:0]), max_iter=5, **KW)
+    assert c0.shape == (0, 33, w.model.n_act) and e0.shape == (0, 33)

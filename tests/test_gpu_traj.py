@@ -108,3 +108,27 @@ def test_all_obstacle_kinds_match_oracle(margin, n_spheres):
                                 w.world.arrays(), margin)
     assert np.linalg.norm(ref) > 0
     assert np.linalg.norm(gc - ref) / np.linalg.norm(ref) < 1e-4
+
+
+def test_large_batch_two_lane_path_matches_oracle():
+    """Batches above 2 x SMs run 2 lanes per waypoint (config 3 and the CHOMP
+    line search take that path); smaller ones 4.  Both against the oracle, and
+    against each other on the same trajectories."""
+    w, tc = setup(Bt=320, T=16)
+    x = torch.as_tensor(w.traj, device=DEV)
+    c_big, g_big = tc.cost_and_grad(x)
+    c_small, g_small = tc.cost_and_grad(x[:12].contiguous())
+    np.testing.assert_allclose(c_big[:12].cpu().numpy(), c_small.cpu().numpy(), rtol=1e-5, atol=1e-6)
+    np.testing.assert_allclose(g_big[:12].cpu().numpy(), g_small.cpu().numpy(), rtol=1e-4, atol=1e-5)
+    idx = [0, 5, 77, 150, 233, 319]
+    ref = np.array([oracle_cost(w, w.traj[b].astype(np.float64)) for b in idx])
+    np.testing.assert_allclose(c_big.cpu().numpy()[idx], ref, rtol=1e-4, atol=1e-5)
+    md = w.model.as_dict()
+    for b in (77, 319):
+        xb = w.traj[b].astype(np.float64)
+        ref_g = (w.w_smooth * otr.smoothness_grad(xb, w.w_acc, w.w_jerk)
+                 + w.w_limits * otr.limits_grad(xb, w.model.lower, w.model.upper)
+                 + w.w_collision * otr.collision_grad_fd(xb, md, w.spheres.centers, w.spheres.radii, w.link_pairs,
+                                                         w.world.arrays(), w.margin))
+        rel = np.linalg.norm(g_big[b].cpu().numpy() - ref_g) / max(np.linalg.norm(ref_g), 1e-12)
+        assert rel < 1e-4, (b, rel)
