@@ -184,3 +184,18 @@ def test_invalid_arguments_raise():
     opt = make(w, ScoConfig(m_lbfgs=0))
     with pytest.raises(PkError):
         opt.linearize(torch.as_tensor(w.traj[0], device=DEV))
+
+
+@pytest.mark.parametrize("per_link", [8, 16, 20])
+def test_sphere_count_variants_match_oracle(per_link):
+    """The linearisation is compiled for up to 4, 8, 16 and 32 spheres per link
+    (register pairs); the mixed scene at 8, 16 and 20 spheres per link takes
+    the last three."""
+    w = W.mixed_trajectories(Bt=2, T=8, per_link=per_link)
+    opt = make(w)
+    q = w.traj.reshape(-1, w.traj.shape[-1])
+    d, J, c = opt.linearize(torch.as_tensor(q, device=DEV), want_coll=True)
+    np.testing.assert_allclose(d.cpu().numpy(), osco.group_dists(q, *oracle_args(w), TAU, True), atol=1e-5, rtol=1e-6)
+    np.testing.assert_allclose(c.cpu().numpy(), osco.coll_sum(q, *oracle_args(w), 0.01, True), rtol=1e-5, atol=1e-6)
+    oJ = osco.group_jacobian(q, *oracle_args(w), TAU, True, eps=1e-6)
+    np.testing.assert_allclose(J.cpu().numpy(), oJ, atol=2e-4, rtol=1e-3)

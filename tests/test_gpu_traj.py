@@ -132,3 +132,28 @@ def test_large_batch_two_lane_path_matches_oracle():
                                                          w.world.arrays(), w.margin))
         rel = np.linalg.norm(g_big[b].cpu().numpy() - ref_g) / max(np.linalg.norm(ref_g), 1e-12)
         assert rel < 1e-4, (b, rel)
+
+
+@pytest.mark.parametrize("per_link", [8, 16, 20])
+def test_sphere_count_variants_match_oracle(per_link):
+    """Kernels for up to 8, 16 and 32 spheres per link (register pairs)."""
+    w = W.mixed_trajectories(Bt=3, T=10, per_link=per_link)
+    margin = 0.05
+    tc = TrajectoryCost(w.model, w.spheres, w.world, w.link_pairs, margin=margin, w_smooth=1.0, w_acc=0.5,
+                        w_jerk=0.1, w_limits=1.0, w_coll=3.0, device=DEV)
+    x = torch.as_tensor(w.traj, device=DEV)
+    c = tc.cost(x).cpu().numpy()
+    md = w.model.as_dict()
+    for b in range(3):
+        ref = otr.total_cost(w.traj[b].astype(np.float64), md, w.spheres.centers, w.spheres.radii, w.link_pairs,
+                             w.world.arrays(), margin=margin, w_smooth=1.0, w_acc=0.5, w_jerk=0.1, w_limits=1.0,
+                             w_coll=3.0, lower=w.model.lower, upper=w.model.upper)
+        assert abs(float(c[b]) - ref) <= 1e-4 * abs(ref) + 1e-5, (b, float(c[b]), ref)
+    tcc = TrajectoryCost(w.model, w.spheres, w.world, w.link_pairs, margin=margin, w_smooth=0.0, w_acc=0.0,
+                         w_jerk=0.0, w_limits=0.0, w_coll=1.0, device=DEV)
+    b = int(np.argmax(tcc.waypoint_collision(x).cpu().numpy().sum(1)))
+    g = tcc.grad(x).cpu().numpy()[b].astype(np.float64)
+    ref = otr.collision_grad_fd(w.traj[b].astype(np.float64), md, w.spheres.centers, w.spheres.radii, w.link_pairs,
+                                w.world.arrays(), margin)
+    assert np.linalg.norm(ref) > 0
+    assert np.linalg.norm(g - ref) / np.linalg.norm(ref) < 1e-4
