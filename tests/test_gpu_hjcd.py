@@ -101,8 +101,10 @@ def test_fixed_joints_do_not_move():
     np.testing.assert_array_equal(c2.cpu().numpy()[..., [1, 4]], w.seeds[..., [1, 4]])
 
 
-def test_two_end_effectors_match_oracle():
-    m, sol, tj, anc, tgt, seeds = bimanual()
+@pytest.mark.parametrize("links", [None, (10, 16, 7)])
+def test_two_end_effectors_match_oracle(links):
+    """Two hands (the 2-EE kernels), and the hands plus an elbow (the 4-EE kernels)."""
+    m, sol, tj, anc, tgt, seeds = bimanual(target_links=links)
     _, e0 = sol.coarse(t(seeds), t(tgt), k_max=0)
     cfg, err = sol.coarse(t(seeds), t(tgt), k_max=15)
     noise = np.random.default_rng(3).normal(size=(seeds.shape[0], seeds.shape[1], 8, m.n_act)).astype(np.float32)

@@ -68,9 +68,10 @@ def test_fixed_joints_and_limits():
     assert np.all(cfg >= w.model.lower - 1e-6) and np.all(cfg <= w.model.upper + 1e-6)
 
 
-def test_two_end_effectors_match_oracle():
-    m, _, tj, anc, tgt, seeds = bimanual()
-    sol = SqpSolver(m, W.mixed_classes()[2].target_links, device=DEV)
+@pytest.mark.parametrize("links", [None, (10, 16, 7)])
+def test_two_end_effectors_match_oracle(links):
+    """Two hands (the 2-EE kernel), and the hands plus an elbow (the 4-EE kernel)."""
+    m, sol, tj, anc, tgt, seeds = bimanual(target_links=links, solver=SqpSolver)
     _, e0 = sol.run(t(seeds), t(tgt), max_iter=0, **KW)
     _, e1 = sol.run(t(seeds), t(tgt), max_iter=6, **KW)
     fixed = np.zeros(m.n_act, bool)
