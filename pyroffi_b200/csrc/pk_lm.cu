@@ -849,8 +849,12 @@ __device__ __forceinline__ void lm_seed_groups(const LmArgs& a, unsigned char* s
   }
 }
 
-template <int MAXA, int MAXEE, int TPS>
-__global__ void __launch_bounds__(128, (MAXA <= 8 ? 4 : 2)) lm_kernel(LmArgs a) {
+// MINB: resident blocks per SM the register budget is sized for.  4 caps a
+// thread at 128 registers (a few hundred bytes of spills at MAXA = 8); 2
+// leaves room for the whole seed state, for launches whose shared memory
+// admits only 2 blocks per SM anyway.
+template <int MAXA, int MAXEE, int TPS, int MINB>
+__global__ void __launch_bounds__(128, MINB) lm_kernel(LmArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const LmLayout L = lm_layout(a, TPS);
   const int pb = blockIdx.y;
@@ -873,8 +877,9 @@ struct SeedGroupBatch {
   int* queue;
 };
 
-template <int TPS>
-__global__ void __launch_bounds__(128, 4) lm_batch_kernel(const __grid_constant__ SeedGroupBatch B) {
+// MINB as for lm_kernel.
+template <int TPS, int MINB>
+__global__ void __launch_bounds__(128, MINB) lm_batch_kernel(const __grid_constant__ SeedGroupBatch B) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int s_item;
   __shared__ LmArgs s_args;
@@ -1344,7 +1349,11 @@ static int launch_lm_t(const LmArgs& a0, cudaStream_t st) {
   const int threads = a.spb * TPS;
   const size_t smem = lm_smem_bytes(a, TPS);
   PK_CHECK_CAP(smem <= 220 * 1024, "LM working set (%zu B of shared memory) too large", smem);
-  auto kern = lm_kernel<MAXA, MAXEE, TPS>;
+  // the 4-block register budget only where shared memory admits 3 or more blocks per SM
+  auto kern = lm_kernel<MAXA, MAXEE, TPS, 2>;
+  if constexpr (MAXA <= 8) {
+    if ((228 * 1024) / (smem + 1024) >= 3) kern = lm_kernel<MAXA, MAXEE, TPS, 4>;
+  }
   if (int s = set_smem_limit((const void*)kern, smem)) return s;
   dim3 grid((a.Sd + a.spb - 1) / a.spb, a.P);
   kern<<<grid, threads, smem, st>>>(a);
@@ -1572,7 +1581,8 @@ namespace pk {
 
 template <int TPS>
 static int launch_batch_t(const SeedGroupBatch& B, size_t smem, int threads, int blocks, cudaStream_t st) {
-  auto kern = lm_batch_kernel<TPS>;
+  // the 4-block register budget only where shared memory admits 3 or more blocks per SM
+  auto kern = ((228 * 1024) / (smem + 1024) >= 3) ? lm_batch_kernel<TPS, 4> : lm_batch_kernel<TPS, 2>;
   if (int s = set_smem_limit((const void*)kern, smem)) return s;
   if (blocks <= 0) {
     int dev = 0, sms = 0, per_sm = 0;
