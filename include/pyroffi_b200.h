@@ -341,6 +341,33 @@ int pk_chomp_direction(void* stream, const float* grad, float* dir, int64_t B, i
                        int32_t n_cg_iters, float grad_clip_norm, float smoothness_reg, float cg_tol,
                        int32_t covariant);
 
+/*
+ * CHOMP line search, trial trajectories (no reference counterpart; it fuses
+ * the trial update of chomp_trajopt,
+ * src/pyroffi/optimization_engines/_chomp_optimization.py:282-291):
+ * trials[k, b] = traj[b] + clamp(alphas[k] * dir[b], -max_delta, max_delta)
+ * for k < n_alphas, waypoint 0 set to start[n_act] and waypoint T-1 to goal.
+ * trials is [n_alphas, B, T, n_act]; alphas is a device array.
+ */
+int pk_chomp_line_trials(void* stream, const float* traj, const float* dir, const float* alphas, int32_t n_alphas,
+                         float max_delta, const float* start, const float* goal, float* trials, int64_t B,
+                         int32_t T, int32_t n_act);
+
+/*
+ * CHOMP line search, selection (no reference counterpart; it fuses the
+ * selection and early stop of chomp_trajopt,
+ * src/pyroffi/optimization_engines/_chomp_optimization.py:293-304): per
+ * trajectory, the first minimum over trial_costs[n_alphas, B] and cost[B]
+ * (the zero step); when active[b] and that minimum is below
+ * cost[b] - min_cost_improve, traj[b] takes the winning trial.  An active
+ * trajectory's stall counter resets on improvement and counts otherwise,
+ * and it stays active while stall < early_stop_patience.  traj, active and
+ * stall are updated in place.
+ */
+int pk_chomp_line_select(void* stream, const float* trial_costs, const float* cost, const float* trials, float* traj,
+                         uint8_t* active, int32_t* stall, int32_t n_alphas, float min_cost_improve,
+                         int32_t early_stop_patience, int64_t B, int32_t T, int32_t n_act);
+
 /* SCO trajectory optimisation settings: the fields of ScoTrajOptConfig
  * (src/pyroffi/optimization_engines/_sco_optimization.py:52-104, defaults in
  * brackets) and the reference kernel's fd_eps attribute

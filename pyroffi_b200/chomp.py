@@ -16,10 +16,11 @@ the device:
   in one ``pk_chomp_direction`` launch (a warp per (trajectory, joint)
   timeline);
 * line search over ``step_size * (1, .5, .25, .1, .05, 0)``: the 5B trial
-  trajectories of the non-zero steps are costed in one more launch (the zero
-  step's trial is the current trajectory, costed by the gradient launch), the
-  first minimum wins and is taken when it improves the cost by
-  ``min_cost_improve``;
+  trajectories of the non-zero steps are built by ``pk_chomp_line_trials``
+  and costed in one more launch (the zero step's trial is the current
+  trajectory, costed by the gradient launch); ``pk_chomp_line_select`` takes
+  the first minimum when it improves the cost by ``min_cost_improve`` and
+  updates the stall counters, in place;
 * per-trajectory early stop after ``early_stop_patience`` stalled steps; the
   collision weight grows by ``collision_penalty_scale`` per step up to
   ``w_collision_max``; the final ranking uses ``w_collision_max``.
@@ -103,29 +104,26 @@ class ChompOptimizer:
         B = traj.shape[0]
         dev = traj.device
         alphas = self._alphas(dev)
+        start, goal = f32(start), f32(goal)
         active = torch.ones(B, dtype=torch.bool, device=dev)
         stall = torch.zeros(B, dtype=torch.int32, device=dev)
         w = cfg.w_collision
+        traj = traj.contiguous()
+        K = len(LINE_SEARCH) - 1
+        T, n = int(traj.shape[1]), int(traj.shape[2])
+        trials = torch.empty((K, B, T, n), dtype=torch.float32, device=dev)
+        st = stream_ptr(dev)
         for _ in range(cfg.n_iters):
             c, g = self._costs(traj, w, grad=True)
             d = covariant_direction(g, cfg)
             # the last trial step is 0: that trial is the current trajectory, whose cost
-            # the gradient launch has just produced, so only the others are costed
-            a_nz = alphas[:-1]
-            trials = traj[None] + torch.clamp(a_nz[:, None, None, None] * d[None], -cfg.max_delta_per_step,
-                                              cfg.max_delta_per_step)
-            trials[:, :, 0] = start
-            trials[:, :, -1] = goal
-            tc = self._costs(trials.reshape(-1, *traj.shape[1:]).contiguous(), w).reshape(len(LINE_SEARCH) - 1, B)
-            tc = torch.cat([tc, c[None]], dim=0)
-            trials = torch.cat([trials, traj[None]], dim=0)
-            best_cost, best_idx = torch.min(tc, dim=0)          # first minimum
-            best = trials[best_idx, torch.arange(B, device=dev)]
-            improved = best_cost < (c - cfg.min_cost_improve)
-            take = active & improved
-            traj = torch.where(take[:, None, None], best, traj)
-            stall = torch.where(active, torch.where(improved, torch.zeros_like(stall), stall + 1), stall)
-            active = active & (stall < cfg.early_stop_patience)
+            # the gradient launch has just produced, so only the K others are built and costed
+            _lib.call("pk_chomp_line_trials", st, ptr(traj), ptr(d), ptr(alphas), K, float(cfg.max_delta_per_step),
+                      ptr(start), ptr(goal), ptr(trials), B, T, n)
+            tc = self._costs(trials.view(K * B, T, n), w)
+            # first minimum over the trials and the current cost; step, stall count, early stop (in place)
+            _lib.call("pk_chomp_line_select", st, ptr(tc), ptr(c), ptr(trials), ptr(traj), ptr(active), ptr(stall), K,
+                      float(cfg.min_cost_improve), int(cfg.early_stop_patience), B, T, n)
             w = min(w * cfg.collision_penalty_scale, cfg.w_collision_max)
         final_costs = self._costs(traj, cfg.w_collision_max)
         return traj, final_costs

@@ -19,6 +19,8 @@
 // B200 mapping: one block per trajectory, one warp per joint timeline (the
 // warps loop over the joints); p lives in shared memory for the stencil, the
 // dot products are warp shuffles.
+#include <algorithm>
+
 #include "pk_common.cuh"
 
 namespace pk {
@@ -152,6 +154,68 @@ __global__ void __launch_bounds__(256) chomp_direction_kernel(ChompDirArgs a) {
   }
 }
 
+// Line-search trials: trials[k, b] = traj[b] + clamp(alpha_k dir[b], -max_delta,
+// max_delta) with the ends pinned to start / goal (the reference's trial
+// update, _chomp_optimization.py:282-291, for K step sizes at once).  NaN
+// passes through the clamp, as in torch.clamp.
+__global__ void chomp_trials_kernel(const float* __restrict__ traj, const float* __restrict__ dir,
+                                    const float* __restrict__ alphas, float max_delta, const float* __restrict__ start,
+                                    const float* __restrict__ goal, float* __restrict__ trials, long long per, int T,
+                                    int n, int K) {
+  const long long total = per * K;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(i / per);
+    const long long e = i - (long long)k * per;
+    const int c = (int)(e % n);
+    const int t = (int)((e / n) % T);
+    float v;
+    if (t == 0) {
+      v = start[c];
+    } else if (t == T - 1) {
+      v = goal[c];
+    } else {
+      const float step = alphas[k] * dir[e];
+      v = traj[e] + (step != step ? step : fminf(fmaxf(step, -max_delta), max_delta));
+    }
+    trials[i] = v;
+  }
+}
+
+// Line-search selection, one block per trajectory: the first minimum over
+// the K trial costs and the current cost (as torch.min: a NaN wins), the
+// step taken when the trajectory is active and the minimum improves the
+// current cost by min_improve, the stall counter and the early stop
+// (_chomp_optimization.py:293-304).
+__global__ void chomp_select_kernel(const float* __restrict__ tc, const float* __restrict__ cur,
+                                    const float* __restrict__ trials, float* __restrict__ traj,
+                                    unsigned char* __restrict__ active, int* __restrict__ stall, float min_improve,
+                                    int patience, long long B, long long per_traj, int K) {
+  const long long b = blockIdx.x;
+  __shared__ int take;
+  if (threadIdx.x == 0) {
+    float best = tc[b];
+    int idx = 0;
+    for (int k = 1; k <= K; ++k) {
+      if (best != best) break;
+      const float v = (k < K) ? tc[(long long)k * B + b] : cur[b];
+      if (v != v || v < best) { best = v; idx = k; }
+    }
+    const bool improved = best < cur[b] - min_improve;
+    const bool act = active[b] != 0;
+    take = (act && improved && idx < K) ? idx : -1;
+    int st = stall[b];
+    if (act) st = improved ? 0 : st + 1;
+    stall[b] = st;
+    active[b] = (act && st < patience) ? 1 : 0;
+  }
+  __syncthreads();
+  if (take < 0) return;
+  const float* src = trials + ((long long)take * B + b) * per_traj;
+  float* dst = traj + b * per_traj;
+  for (long long i = threadIdx.x; i < per_traj; i += blockDim.x) dst[i] = src[i];
+}
+
 }  // namespace pk
 
 using namespace pk;
@@ -169,4 +233,32 @@ extern "C" int pk_chomp_direction(void* stream, const float* grad, float* dir, i
   const size_t smem = sizeof(double) * (size_t)warps * ((T > 2 ? T - 2 : 0) + 4);
   chomp_direction_kernel<<<(unsigned)B, 32 * warps, smem, (cudaStream_t)stream>>>(a);
   return cuda_status(cudaGetLastError(), "chomp_direction_kernel launch");
+}
+
+extern "C" int pk_chomp_line_trials(void* stream, const float* traj, const float* dir, const float* alphas,
+                                    int32_t n_alphas, float max_delta, const float* start, const float* goal,
+                                    float* trials, int64_t B, int32_t T, int32_t n_act) {
+  PK_CHECK_ARG(B >= 0 && T >= 0 && n_act >= 0 && n_alphas >= 0, "negative extent");
+  const long long per = (long long)B * T * n_act;
+  if (per == 0 || n_alphas == 0) return PK_OK;
+  PK_CHECK_ARG(traj && dir && alphas && start && goal && trials, "null buffer");
+  const long long total = per * n_alphas;
+  const long long blocks = std::min<long long>((total + 255) / 256, 148LL * 32);
+  chomp_trials_kernel<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(traj, dir, alphas, max_delta, start, goal,
+                                                                           trials, per, T, n_act, n_alphas);
+  return cuda_status(cudaGetLastError(), "chomp_trials_kernel launch");
+}
+
+extern "C" int pk_chomp_line_select(void* stream, const float* trial_costs, const float* cost, const float* trials,
+                                    float* traj, uint8_t* active, int32_t* stall, int32_t n_alphas,
+                                    float min_cost_improve, int32_t early_stop_patience, int64_t B, int32_t T,
+                                    int32_t n_act) {
+  PK_CHECK_ARG(B >= 0 && T >= 0 && n_act >= 0 && n_alphas >= 1, "bad extent");
+  PK_CHECK_CAP(B < (1LL << 31), "batch too large");
+  if (B == 0) return PK_OK;
+  PK_CHECK_ARG(trial_costs && cost && trials && traj && active && stall, "null buffer");
+  chomp_select_kernel<<<(unsigned)B, 128, 0, (cudaStream_t)stream>>>(trial_costs, cost, trials, traj, active, stall,
+                                                                      min_cost_improve, early_stop_patience, B,
+                                                                      (long long)T * n_act, n_alphas);
+  return cuda_status(cudaGetLastError(), "chomp_select_kernel launch");
 }

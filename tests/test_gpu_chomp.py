@@ -84,3 +84,48 @@ def tc_cost_initial(tc, x, cfg):
     xx[:, 0], xx[:, -1] = x[0, 0], x[0, -1]
     tc.opt.w_coll = cfg.w_collision_max
     return tc.cost(xx)
+
+
+def test_line_search_kernels_match_the_tensor_formulation():
+    """pk_chomp_line_trials / pk_chomp_line_select against the same step in
+    torch ops: trials, first minimum, improvement test, stall count, early stop."""
+    from pyroffi_b200 import _lib
+    from pyroffi_b200._tensors import ptr, stream_ptr
+    rng = np.random.default_rng(4)
+    K, B, T, n = 5, 37, 9, 7
+    tr = torch.as_tensor(rng.normal(size=(B, T, n)), dtype=torch.float32, device=DEV)
+    d = torch.as_tensor(rng.normal(size=(B, T, n)) * 2.0, dtype=torch.float32, device=DEV)
+    alphas = torch.tensor([1.0, 0.5, 0.25, 0.1, 0.05], dtype=torch.float32, device=DEV) * 0.7
+    start = torch.as_tensor(rng.normal(size=n), dtype=torch.float32, device=DEV)
+    goal = torch.as_tensor(rng.normal(size=n), dtype=torch.float32, device=DEV)
+    md = 0.3
+    trials = torch.empty((K, B, T, n), dtype=torch.float32, device=DEV)
+    st = stream_ptr(torch.device(DEV))
+    _lib.call("pk_chomp_line_trials", st, ptr(tr), ptr(d), ptr(alphas), K, md, ptr(start), ptr(goal), ptr(trials),
+              B, T, n)
+    ref = tr[None] + torch.clamp(alphas[:, None, None, None] * d[None], -md, md)
+    ref[:, :, 0] = start
+    ref[:, :, -1] = goal
+    assert torch.equal(trials, ref)
+
+    c = torch.as_tensor(rng.uniform(1.0, 2.0, size=B), dtype=torch.float32, device=DEV)
+    tc = torch.as_tensor(rng.uniform(0.9, 2.1, size=(K, B)), dtype=torch.float32, device=DEV)
+    tc[:, :5] = c[:5]                                        # ties with the current cost: no step
+    tc[2, 5:9] = tc[1, 5:9]                                  # ties between trials: the first wins
+    active = torch.as_tensor(rng.uniform(size=B) < 0.8, device=DEV)
+    stall = torch.as_tensor(rng.integers(0, 4, size=B), dtype=torch.int32, device=DEV)
+    mci, pat = 1e-5, 3
+    # torch formulation of the step
+    tcc = torch.cat([tc, c[None]], dim=0)
+    tall = torch.cat([trials, tr[None]], dim=0)
+    best_cost, best_idx = torch.min(tcc, dim=0)
+    best = tall[best_idx, torch.arange(B, device=DEV)]
+    improved = best_cost < (c - mci)
+    want_tr = torch.where((active & improved)[:, None, None], best, tr)
+    want_stall = torch.where(active, torch.where(improved, torch.zeros_like(stall), stall + 1), stall)
+    want_active = active & (want_stall < pat)
+    _lib.call("pk_chomp_line_select", st, ptr(tc), ptr(c), ptr(trials), ptr(tr), ptr(active), ptr(stall), K, mci,
+              pat, B, T, n)
+    assert torch.equal(tr, want_tr)
+    assert torch.equal(stall, want_stall)
+    assert torch.equal(active, want_active)
