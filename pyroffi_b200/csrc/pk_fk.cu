@@ -349,7 +349,12 @@ __device__ __forceinline__ void distance_rows(const FusedArgs& a, const ObsView&
   }
 }
 
-__global__ void __launch_bounds__(256, 3) fk_sphere_collision_kernel(FusedArgs a) {
+// MINB: resident blocks per SM the register budget is sized for.  4 (64
+// registers, small spills) keeps more configurations in flight, which
+// shortens small batches; 3 (80 registers) suits the arithmetic-bound rows of
+// a large world.
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) fk_sphere_collision_kernel(FusedArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   JointTable& jt = *reinterpret_cast<JointTable*>(smem_raw);
   unsigned char* p = smem_raw + sizeof(JointTable);
@@ -549,7 +554,8 @@ extern "C" int pk_fk_sphere_collision(
   while (cpb > 1 && (batch + cpb - 1) / cpb < 4LL * sms) cpb >>= 1;
   PK_CHECK_CAP(smem_for(cpb, stage) <= limit, "robot too large for the fused kernel");
   const size_t smem = smem_for(cpb, stage);
-  if (int st = set_smem_limit((const void*)fk_sphere_collision_kernel, smem)) return st;
+  auto kern = (Ms + Mc + Mb + Mh >= 1024) ? fk_sphere_collision_kernel<3> : fk_sphere_collision_kernel<4>;
+  if (int st = set_smem_limit((const void*)kern, smem)) return st;
   FusedArgs a;
   a.m = ModelArgs{twists, parent_tf, parent_idx, act_idx, mimic_mul, mimic_off, mimic_act_idx,
                   topo_inv, n_joints, n_act};
@@ -568,6 +574,6 @@ extern "C" int pk_fk_sphere_collision(
   a.stage_world = stage ? 1 : 0;
   const long long blocks = (batch + cpb - 1) / cpb;
   PK_CHECK_CAP(blocks < (1LL << 31), "batch too large");
-  fk_sphere_collision_kernel<<<(unsigned)blocks, threads, smem, (cudaStream_t)stream>>>(a);
+  kern<<<(unsigned)blocks, threads, smem, (cudaStream_t)stream>>>(a);
   return cuda_status(cudaGetLastError(), "fk_sphere_collision_kernel launch");
 }
