@@ -368,6 +368,16 @@ int pk_chomp_line_select(void* stream, const float* trial_costs, const float* co
                          uint8_t* active, int32_t* stall, int32_t n_alphas, float min_cost_improve,
                          int32_t early_stop_patience, int64_t B, int32_t T, int32_t n_act);
 
+/*
+ * Health check (no reference counterpart): *count = the number of thread
+ * blocks, since the library was loaded, whose bounded wait for the TMA copy
+ * of the obstacle arrays into shared memory gave up, on the current device.
+ * Such a block counts itself, waits once more and copies the arrays with
+ * plain loads, so its results stay right; a non-zero count means the copy
+ * engine did not complete a copy in time.
+ */
+int pk_stage_wait_timeouts(uint64_t* count);
+
 /* SCO trajectory optimisation settings: the fields of ScoTrajOptConfig
  * (src/pyroffi/optimization_engines/_sco_optimization.py:52-104, defaults in
  * brackets) and the reference kernel's fd_eps attribute

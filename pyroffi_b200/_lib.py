@@ -72,6 +72,7 @@ SIGNATURES: dict[str, list] = {
     "pk_sqp_ik_cuda": [_p] + [_p] * 21 + [_i64, _i64, _f32, _f32, _f32, _f32, _f32, _i64, _f32, _f32, _p, _p]
                       + [_i32] * 10,
     "pk_chomp_direction": [_p, _p, _p, _i64, _i32, _i32, _i32, _f32, _f32, _f32, _i32],
+    "pk_stage_wait_timeouts": [_p],
     "pk_chomp_line_trials": [_p, _p, _p, _p, _i32, _f32, _p, _p, _p, _i64, _i32, _i32],
     "pk_chomp_line_select": [_p, _p, _p, _p, _p, _p, _p, _i32, _f32, _i32, _i64, _i32, _i32],
     "pk_sco_linearize": [_p, C.c_void_p] + [_p] * 20 + [_i64] + [_i32] * 9,

@@ -2,6 +2,8 @@
 #include <stdarg.h>
 #include <stdio.h>
 
+#include <vector>
+
 #include "pk_common.cuh"
 
 namespace {
@@ -29,7 +31,28 @@ int set_smem_limit(const void* kernel, size_t bytes) {
                      "cudaFuncSetAttribute");
 }
 
+// Readers of the per-file counters of bounded waits that gave up, one per
+// source file that stages the world; filled at library load.
+static std::vector<int (*)(unsigned long long*)>& timeout_readers() {
+  static std::vector<int (*)(unsigned long long*)> v;
+  return v;
+}
+
+int register_timeout_reader(int (*reader)(unsigned long long*)) {
+  timeout_readers().push_back(reader);
+  return (int)timeout_readers().size();
+}
+
 }  // namespace pk
+
+extern "C" int pk_stage_wait_timeouts(uint64_t* count) {
+  PK_CHECK_ARG(count != nullptr, "null count");
+  unsigned long long acc = 0;
+  for (auto reader : pk::timeout_readers())
+    if (int s = reader(&acc)) return s;
+  *count = acc;
+  return PK_OK;
+}
 
 extern "C" {
 

@@ -45,14 +45,37 @@ struct ObsView {
   int Ms, Mc, Mb, Mh;
 };
 
+// Blocks whose wait for the TMA copy of stage_world gave up, in the kernels
+// of this source file since the library was loaded (one counter per file;
+// pk_stage_wait_timeouts sums them).  It stays 0 unless the copy engine
+// fails to complete a copy.
+static __device__ unsigned int g_stage_wait_timeouts;
+
+// Host side: adds this file's counter, on the current device, to *acc.
+int register_timeout_reader(int (*reader)(unsigned long long*));
+namespace {
+int read_stage_wait_timeouts(unsigned long long* acc) {
+  unsigned int v = 0;
+  if (int s = cuda_status(cudaMemcpyFromSymbol(&v, g_stage_wait_timeouts, sizeof(v)), "stage wait counter"))
+    return s;
+  *acc += v;
+  return PK_OK;
+}
+[[maybe_unused]] const int kStageWaitReader = register_timeout_reader(read_stage_wait_timeouts);
+}  // namespace
+
 // Copies the obstacle arrays into shared memory at `dst` (16-byte aligned),
 // each array starting on a 16-byte boundary; called by every thread of the
 // block, and the caller synchronises afterwards.  The 16-byte-aligned bulk of
 // each array goes through the TMA bulk-copy engine: one thread issues
 // cp.async.bulk global -> shared with the completion counted in bytes on an
-// mbarrier, and every thread waits on that barrier (the wait is bounded).  An
-// array whose source is not 16-byte aligned, and the bytes past the last
-// 16-byte multiple, are copied with plain loads.
+// mbarrier, and every thread waits on that barrier.  The wait is bounded: a
+// thread that gives up counts the block in g_stage_wait_timeouts (once),
+// waits once more with the same bound for the copy in flight, and then loads
+// the bulk with plain loads itself, so the block's data is right either way
+// (a copy that lands late writes the same bytes).  An array whose source is
+// not 16-byte aligned, and the bytes past the last 16-byte multiple, are
+// copied with plain loads.
 __device__ inline ObsView stage_world(const WorldArgs& w, float* dst) {
   __shared__ __align__(8) unsigned long long s_bar;
   const float* src[4] = {w.spheres, w.capsules, w.boxes, w.halfspaces};
@@ -91,13 +114,23 @@ __device__ inline ObsView stage_world(const WorldArgs& w, float* dst) {
               "l"(src[k]), "r"(bulk[k]), "r"(bar)
               : "memory");
     }
-    unsigned done = 0;
-    for (int it = 0; it < (1 << 22) && !done; ++it)
-      asm volatile(
-          "{\n .reg .pred P;\n mbarrier.try_wait.parity.shared::cta.b64 P, [%1], 0;\n selp.u32 %0, 1, 0, P;\n}"
-          : "=r"(done)
-          : "r"(bar)
-          : "memory");
+    auto wait = [&]() {
+      unsigned done = 0;
+      for (int it = 0; it < (1 << 22) && !done; ++it)
+        asm volatile(
+            "{\n .reg .pred P;\n mbarrier.try_wait.parity.shared::cta.b64 P, [%1], 0;\n selp.u32 %0, 1, 0, P;\n}"
+            : "=r"(done)
+            : "r"(bar)
+            : "memory");
+      return done != 0;
+    };
+    if (!wait()) {
+      if (tid == 0) atomicAdd(&g_stage_wait_timeouts, 1u);
+      wait();
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        for (int i = tid; i < (int)(bulk[k] / 4); i += nth) d[k][i] = src[k][i];
+    }
   }
   ObsView v;
   v.sph = reinterpret_cast<const float4*>(d[0]);

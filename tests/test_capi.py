@@ -138,3 +138,8 @@ def test_trajectory_cost_validates_on_the_host(lib):
     assert call(-1, 64, 8) == _lib.PK_ERR_INVALID
     assert call(4, 64, 8, o=None) == _lib.PK_ERR_INVALID
     assert call(0, 64, 8) == _lib.PK_OK
+
+
+def test_stage_wait_counter_rejects_null(lib):
+    assert lib.pk_stage_wait_timeouts(None) == _lib.PK_ERR_INVALID
+    assert b"null" in lib.pk_last_error()

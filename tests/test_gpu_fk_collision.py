@@ -268,3 +268,22 @@ def test_per_link_rows_identical_with_and_without_per_sphere_rows(case):
     a = fk_sphere_collision(*args, per_sphere=False, per_link=True)
     b = fk_sphere_collision(*args, per_sphere=True, per_link=True)
     assert torch.equal(a.dist_bnm, b.dist_bnm)
+
+
+def test_no_world_staging_wait_gave_up():
+    """Kernels that copy the world into shared memory with the TMA engine wait
+    for it with a bound; a block that gives up is counted.  After staged
+    launches of the fused kernel and the trajectory kernel, the count is 0."""
+    import ctypes as C
+    from pyroffi_b200 import _lib
+    from pyroffi_b200.trajopt import TrajectoryCost
+    w = W.fk_collision(B=256)
+    fk_sphere_collision(DeviceRobot.upload(w.model, DEV), DeviceSpheres.upload(w.spheres, DEV),
+                        DeviceWorld.upload(w.world, DEV), tt(w.cfg), per_sphere=True)
+    wt = W.trajectories(Bt=8, T=16)
+    TrajectoryCost(wt.model, wt.spheres, wt.world, wt.link_pairs, margin=wt.margin, device=DEV).cost_and_grad(
+        torch.as_tensor(wt.traj, device=DEV))
+    torch.cuda.synchronize()
+    n = C.c_uint64(123)
+    assert _lib.load().pk_stage_wait_timeouts(C.byref(n)) == _lib.PK_OK
+    assert n.value == 0
