@@ -554,6 +554,7 @@ extern "C" int pk_fk_sphere_collision(
   while (cpb > 1 && (batch + cpb - 1) / cpb < 4LL * sms) cpb >>= 1;
   PK_CHECK_CAP(smem_for(cpb, stage) <= limit, "robot too large for the fused kernel");
   const size_t smem = smem_for(cpb, stage);
+  // register budget: 4 blocks per SM below 1,024 obstacles, 3 for the arithmetic-bound rows of larger worlds
   auto kern = (Ms + Mc + Mb + Mh >= 1024) ? fk_sphere_collision_kernel<3> : fk_sphere_collision_kernel<4>;
   if (int st = set_smem_limit((const void*)kern, smem)) return st;
   FusedArgs a;
