@@ -35,6 +35,9 @@ extern "C" {
 #define PK_MAX_ACT_ABI 32
 #define PK_MAX_EE_ABI 4
 
+/* Library version string; the calling thread's last error message; the text
+ * of a status code (no reference counterpart: the reference's handlers return
+ * an ffi::Error carrying the message). */
 const char* pk_version(void);
 const char* pk_last_error(void);
 const char* pk_status_string(int status);
@@ -147,7 +150,8 @@ typedef struct pk_lm_options {
 } pk_lm_options;
 
 /*
- * Extended LM IK (a new target, not a drop-in): as pk_ls_ik_cuda plus
+ * Extended LM IK (a new target, not a drop-in; it extends ls_ik_cuda,
+ * src/pyroffi/cuda_kernels/_ls_ik_cuda_kernel.cu:493-529): as pk_ls_ik_cuda plus
  * explicit robot-sphere self-collision pairs (self_i, self_j index
  * robot_spheres_local, hinge-squared with the same margin and weight),
  * configurable damping factors and launch shape.  target_Ts[P, n_ee, 7].
@@ -443,7 +447,8 @@ int pk_sco_inner(void* stream, const pk_sco_options* opt, float* traj, const flo
 int pk_sco_final_cost(void* stream, const pk_sco_options* opt, const float* traj, const float* coll,
                       const float* lower, const float* upper, float* cost, int64_t B, int32_t T, int32_t n_act);
 
-/* Bytes of device workspace pk_sco_trajopt needs for (B, T, n_act). */
+/* Bytes of device workspace pk_sco_trajopt needs for (B, T, n_act) (no
+ * reference counterpart: the reference's XLA call allocates its own). */
 int pk_sco_workspace_bytes(const pk_sco_options* opt, int64_t B, int32_t T, int32_t n_act, size_t* bytes);
 
 /*

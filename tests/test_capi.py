@@ -143,3 +143,23 @@ def test_trajectory_cost_validates_on_the_host(lib):
 def test_stage_wait_counter_rejects_null(lib):
     assert lib.pk_stage_wait_timeouts(None) == _lib.PK_ERR_INVALID
     assert b"null" in lib.pk_last_error()
+
+
+def test_every_declaration_cites_the_reference_or_says_it_has_none():
+    """Each entry point in the header carries a comment that names the
+    reference interface it replaces (file:line) or states that it has no
+    reference counterpart."""
+    import re
+    from pathlib import Path
+    text = (Path(__file__).resolve().parents[1] / "include" / "pyroffi_b200.h").read_text()
+    missing = []
+    for m in re.finditer(r"\n(?:int|const char\*|size_t|void)\s+(pk_\w+)\(", text):
+        before = text[:m.start()]
+        end = before.rfind("*/")
+        comment = before[before.rfind("/*", 0, end):end]
+        between = before[end + 2:]
+        # the comment covers this declaration and any declarations right after it
+        if re.search(r"\n\s*\n", between.strip("\n")) or not re.search(r"\.(cu|cuh|py):\d|counterpart|new target",
+                                                                        comment):
+            missing.append(m.group(1))
+    assert not missing, missing
