@@ -378,7 +378,8 @@ int pk_chomp_line_select(void* stream, const float* trial_costs, const float* co
  * of the obstacle arrays into shared memory gave up, on the current device.
  * Such a block counts itself, waits once more and copies the arrays with
  * plain loads, so its results stay right; a non-zero count means the copy
- * engine did not complete a copy in time.
+ * engine did not complete a copy in time.  The counters are read with
+ * synchronous copies, so call this between workloads, not inside one.
  */
 int pk_stage_wait_timeouts(uint64_t* count);
 
