@@ -143,7 +143,7 @@ typedef struct pk_lm_options {
   int32_t enable_collision;
   float collision_weight;
   float collision_margin;
-  int32_t threads_per_seed; /* 0 = default (2); 1, 2, 4, 8 = lanes sharing one seed; 5 = one lane per line-search
+  int32_t threads_per_seed; /* 0 = default (1); 1, 2, 4, 8 = lanes sharing one seed; 5 = one lane per line-search
                               trial; 16, 32 = warp-per-seed body with that many lanes per seed */
   int32_t seeds_per_block;  /* 0 = choose automatically */
   int32_t lanes_per_wide_seed; /* warp-per-seed body: lanes per seed, 16 (0 = default) or 32 */
@@ -236,13 +236,14 @@ int pk_ik_batch(void* stream, const pk_lm_options* opt, const pk_ik_class* class
  * runs).  No counterpart in the reference.  Same arguments and results as
  * pk_ik_batch without `queue`: the two work-queue counters live in a
  * 256-byte array compiled into the library (it stays on every GPU that
- * loaded the library until the process exits).  The first call on a device
- * looks up that array's device address (cudaGetSymbolAddress), so make it
- * before any stream capture.  Every call shares the array and clears the
- * counters on `stream` before it starts: calls whose kernels overlap on the
- * GPU (different streams, or different host threads) race on the counters
- * and must be serialised by the caller.  A call that would need more
- * counters than the array holds returns PK_ERR_CAPACITY.  Allocates nothing.
+ * loaded the library until the process exits).  Every call looks up that
+ * array's device address in the current context (cudaGetSymbolAddress; the
+ * address is per context, so it is not cached), and the first call in a
+ * context loads the library's device code, so make that first call before
+ * any stream capture.  Every call shares the array and clears the counters
+ * on `stream` before it starts: calls whose kernels overlap on the GPU
+ * (different streams, or different host threads) race on the counters and
+ * must be serialised by the caller.  Allocates nothing.
  */
 int pk_ik_batch_static(void* stream, const pk_lm_options* opt, const pk_ik_class* classes, int32_t n_classes,
                        const float* world_spheres, const float* world_capsules, const float* world_boxes,

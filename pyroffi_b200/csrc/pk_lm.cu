@@ -77,6 +77,7 @@ struct LmShared {
   int fixed[PK_MAX_ACT];
   float4 jb[PK_MAX_JOINTS];        // bounding sphere of each sphere-carrying joint (joint frame)
   int jstart[PK_MAX_JOINTS + 1];   // sphere range per sphere-carrying joint
+  int pjstart[PK_MAX_JOINTS + 1];  // range of sphere pairs (the paired table) per sphere-carrying joint
   int jlist[PK_MAX_JOINTS];        // sorted joint position per sphere-carrying joint
   int n_js;
   int n_rs;                        // valid robot spheres after staging
@@ -105,25 +106,36 @@ __host__ __device__ __forceinline__ int lm_ms_pad(int Ms, int tps) {
   return ((Ms + chunk - 1) / chunk) * chunk;
 }
 
-// Per-seed stride (floats) of the sphere position slots: odd, so the seeds
-// of a warp reading the same sphere hit distinct banks.
+// Self-pair groups per chunk of the warp item list (one lane per seed).
+constexpr int kSelfChunk = 16;
+
 // Trial-lane kernel: float4 positions per seed, padded by one float4 so the
 // 6 seeds of a warp reading the same sphere use different bank groups.
 __host__ __device__ __forceinline__ int lm_pos4_stride(int n_rs) { return n_rs + 1; }
 
-__host__ __device__ __forceinline__ int lm_pos_stride(int n_rs, int n_joints) {
-  return (3 * n_rs + 3 * n_joints) | 1;  // sphere positions, then joint bounding centres
-}
-
 // Byte offsets of the LM block's dynamic shared memory.
 struct LmLayout {
-  size_t rs, ws, pairs, pair4, gjoint, gstart, rsj, rsk, cells, cell_obs, wc, wb, wh, slots, pos, scratch, total;
-  int ms_pad, grid, max_entries, scratch_ints;
+  size_t rs, rsp, ws, pairs, pair4, prec, pgstart, wscr, gjoint, gstart, rsj, rsk, cells, cell_obs, wc, wb, wh, slots, cen, pos, scratch,
+      total;
+  int ms_pad, grid, max_entries, scratch_ints, recs;
 };
 
 __host__ __device__ inline size_t lm_align16(size_t x) { return (x + 15) & ~size_t(15); }
 
-// threads == 0: seed-group kernel (per-seed pose slots and positions);
+// threads == 0: seed-group kernel.  Per seed, the joint pose slots and the
+// bounding-sphere centres, both laid out item-major ([item][spb]: component
+// c of item i of seed g at (i * K + c) * spb + g), so seeds reading the same
+// item hit distinct banks.  Sphere world positions are never stored: world
+// obstacles are moved into joint frames and self pairs go through one
+// relative transform per joint pair.  Both run on packed FP32x2 arithmetic,
+// two spheres or two pairs per operation, from paired tables: each joint's
+// spheres in pairs (float4 (x0, x1, y0, y1), (z0, z1, r0, r1); an odd joint
+// padded with a sphere of radius -1e9), and each self-pair group's pairs in
+// pairs (float4 (-ax0, -ax1, -ay0, -ay1), (-az0, -az1, rr0, rr1),
+// (bx0, bx1, by0, by1), (bz0, bz1, rr0|rr0|, rr1|rr1|) with rr = r_a + r_b +
+// margin; an odd group padded with a pair that never hits).  The staging
+// scratch (self-pair key counts, obstacle boxes) overlays the per-seed area
+// before the seeds run.
 // threads > 0: trial-lane kernel (per-lane pose slots for `threads` lanes,
 // per-seed sphere positions).
 __host__ __device__ inline LmLayout lm_layout(const LmArgs& a, int tps, int threads = 0) {
@@ -131,18 +143,24 @@ __host__ __device__ inline LmLayout lm_layout(const LmArgs& a, int tps, int thre
   size_t o = lm_align16(sizeof(LmShared));
   const int n_rs = a.n_rs, n_self = a.coll ? a.n_self : 0;
   L.ms_pad = lm_ms_pad(a.w.Ms, tps);
-  const int PS = lm_pos_stride(n_rs, a.m.n_joints);
   if (threads == 0) {
-    L.scratch_ints = a.coll ? PS * a.spb : 0;
+    L.scratch_ints = a.coll ? max(a.m.n_joints * a.m.n_joints, a.w.Ms) : 0;
   } else {
     L.scratch_ints = 7 * a.m.n_joints * threads;  // the pose slots double as staging scratch
   }
   L.grid = (a.coll && a.w.Ms >= 32 && a.w.Ms <= 65535 && a.w.Ms <= L.scratch_ints) ? 1 : 0;
   L.max_entries = L.grid ? min(max(48 * a.w.Ms, 1024), 16384) : 0;
   L.rs = o; o = lm_align16(o + 16 * (size_t)n_rs);
+  L.rsp = o; o = lm_align16(o + (threads == 0 ? 16 * (size_t)(n_rs + a.m.n_joints) : 0));
   L.ws = o; o = lm_align16(o + 16 * (size_t)L.ms_pad);
   L.pairs = o; o = lm_align16(o + 8 * (size_t)n_self);
   L.pair4 = o; o = lm_align16(o + (threads > 0 ? 16 * (size_t)n_self : 0));
+  L.prec = o; o = lm_align16(o + (threads == 0 ? 64 * (size_t)n_self : 0));
+  L.pgstart = o; o = lm_align16(o + (threads == 0 ? 4 * (size_t)(n_self + 2) : 0));
+  // one lane per seed: per warp, the self-pair item list (kSelfChunk * 32 u16)
+  // and the item sums (kSelfChunk * 32 floats)
+  L.wscr = o; o = lm_align16(o + ((threads == 0 && tps == 1 && n_self > 0) ? (size_t)(a.spb / 32) * kSelfChunk * 32 * 6 : 0));
+  L.recs = threads == 0 ? 1 : 0;
   L.gjoint = o; o = lm_align16(o + 8 * (size_t)(n_self + 1));
   L.gstart = o; o = lm_align16(o + 4 * (size_t)(n_self + 2));
   L.rsj = o; o = lm_align16(o + 4 * (size_t)n_rs);
@@ -154,12 +172,15 @@ __host__ __device__ inline LmLayout lm_layout(const LmArgs& a, int tps, int thre
   L.wh = o; o = lm_align16(o + 24 * (size_t)a.w.Mh);
   if (threads == 0) {
     L.slots = o; o = lm_align16(o + 28 * (size_t)a.m.n_joints * a.spb);
-    L.pos = o; o = lm_align16(o + 4 * (size_t)L.scratch_ints);
-    L.scratch = L.pos;
+    L.cen = o; o = lm_align16(o + (a.coll ? 12 * (size_t)a.m.n_joints * a.spb : 0));
+    L.scratch = L.slots;
+    L.pos = o;
+    o = max(o, lm_align16(L.scratch + 4 * (size_t)L.scratch_ints));
   } else {
     L.slots = o; o = lm_align16(o + 28 * (size_t)a.m.n_joints * threads);
     L.pos = o; o = lm_align16(o + 16 * (size_t)lm_pos4_stride(n_rs) * a.spb);
     L.scratch = L.slots;
+    L.cen = L.pos;
   }
   L.total = o;
   return L;
@@ -198,7 +219,7 @@ __device__ __forceinline__ float group_sum(float v, unsigned gmask) {
 }
 
 struct PenaltyCtx {
-  const float4* rs;      // robot spheres (x, y, z, r) in their joint frame, grouped by joint
+  const float4* rs;      // robot spheres (x, y, z, r) in their joint frame, grouped by joint slot
   const float4* jb;      // per sphere-carrying joint slot: bounding sphere (x, y, z, R) in its frame
   const int* jstart;     // [n_js + 1] sphere range of each joint slot
   const int* jlist;      // [n_js] sorted joint position of each joint slot
@@ -206,12 +227,15 @@ struct PenaltyCtx {
   const float* wc;
   const float* wb;
   const float* wh;
-  const int2* pairs;     // self pairs in sphere slots, grouped by joint-slot pair
-  const int2* gjoint;    // [n_groups] joint slots (a, b) of each self-pair group
-  const int* gstart;     // [n_groups + 1]
+  const float4* rsp;     // robot spheres in pairs, 2 float4 per pair (the layout's paired sphere table)
+  const int* pjstart;    // [n_js + 1] sphere-pair range of each joint slot
+  const float4* prec;    // self pairs in pairs, 4 float4 per pair of pairs (the layout's paired pair table)
+  const int2* gjoint;    // [n_groups] joint slots (x, y) of each self-pair group
+  const int* pgstart;    // [n_groups + 1] padded pair range of each group (even)
   const int* cell_start; // [G^3 + 1] obstacle grid (null: no grid, scan every obstacle)
   const unsigned short* cell_obs;
-  float* pos;            // this seed: sphere world positions [n_rs][3], then bounding centres [n_js][3]
+  float* cen;            // this seed's bounding centres: component c of slot j at cen[(3 j + c) * cs]
+  int cs;
   float3 glo, ginv;      // grid origin and inverse cell size
   int n_rs, n_js, n_groups, Ms_pad, Mc, Mb, Mh;
   float margin;
@@ -227,116 +251,279 @@ __device__ __forceinline__ void hinge_sq(float d2, float rr, float& pen) {
   }
 }
 
-// Exact hinge terms of the spheres [k0, k1) of one joint against world sphere O.
-__device__ __forceinline__ void narrow_world(const PenaltyCtx& c, int k0, int k1, float4 O, float& pen) {
-  const float* px = c.pos;
-  for (int k = k0; k < k1; ++k) {
-    const float dx = px[3 * k] - O.x, dy = px[3 * k + 1] - O.y, dz = px[3 * k + 2] - O.z;
-    hinge_sq(dx * dx + dy * dy + dz * dz, c.rs[k].w + O.w, pen);
+// p expressed in the frame of pose T: R^T (p - t).
+__device__ __forceinline__ float3 pose_apply_inv(const Pose& T, float3 p) {
+  return quat_rotate(T.w, -T.x, -T.y, -T.z, make_float3(p.x - T.tx, p.y - T.ty, p.z - T.tz));
+}
+
+// Exact hinge terms of the sphere pairs [p0, p1) of a joint against world
+// sphere O (radius already + margin), with the obstacle centre moved into
+// the joint's frame (T) once: |R c_k + t - o| = |c_k - R^T (o - t)|; two
+// spheres per packed FP32x2 operation, terms added in sphere order.
+__device__ __forceinline__ void narrow_world(const PenaltyCtx& c, const Pose& T, int p0, int p1, float4 O,
+                                             float& pen) {
+  const float3 o = pose_apply_inv(T, make_float3(O.x, O.y, O.z));
+  const float2 nx = make_float2(-o.x, -o.x), ny = make_float2(-o.y, -o.y), nz = make_float2(-o.z, -o.z);
+  const float2 ow = make_float2(O.w, O.w);
+  for (int p = p0; p < p1; ++p) {
+    const float4 s0 = c.rsp[2 * p], s1 = c.rsp[2 * p + 1];
+    const float2 dx = __fadd2_rn(make_float2(s0.x, s0.y), nx);
+    const float2 dy = __fadd2_rn(make_float2(s0.z, s0.w), ny);
+    const float2 dz = __fadd2_rn(make_float2(s1.x, s1.y), nz);
+    float2 d2 = __fmul2_rn(dx, dx);
+    d2 = __ffma2_rn(dy, dy, d2);
+    d2 = __ffma2_rn(dz, dz, d2);
+    const float2 rr = __fadd2_rn(make_float2(s1.z, s1.w), ow);
+    hinge_sq(d2.x, rr.x, pen);
+    hinge_sq(d2.y, rr.y, pen);
+  }
+}
+
+// Hinge terms of the pairs of self-pair group gi of one seed (poses in ps),
+// added to pen in pair order: one relative transform T_x^-1 T_y (rotation
+// conj(q_x) q_y as a matrix M, translation u = R_x^T (t_y - t_x)), then per
+// pair |c_a - (M c_b + u)| from the joint-frame records, two pairs per
+// packed FP32x2 operation.
+__device__ __forceinline__ void group_pairs(const PenaltyCtx& c, const PoseSlots& ps, int gi, float& pen) {
+  const int2 ja = c.gjoint[gi];
+  const Pose A = ps.load(c.jlist[ja.x]);
+  const Pose Bp = ps.load(c.jlist[ja.y]);
+  const float qw = A.w * Bp.w + A.x * Bp.x + A.y * Bp.y + A.z * Bp.z;
+  const float qx = A.w * Bp.x - A.x * Bp.w - A.y * Bp.z + A.z * Bp.y;
+  const float qy = A.w * Bp.y + A.x * Bp.z - A.y * Bp.w - A.z * Bp.x;
+  const float qz = A.w * Bp.z - A.x * Bp.y + A.y * Bp.x - A.z * Bp.w;
+  const float3 u = pose_apply_inv(A, make_float3(Bp.tx, Bp.ty, Bp.tz));
+  auto dup = [](float v) { return make_float2(v, v); };
+  const float2 m00 = dup(1.f - 2.f * (qy * qy + qz * qz)), m01 = dup(2.f * (qx * qy - qw * qz)),
+               m02 = dup(2.f * (qx * qz + qw * qy));
+  const float2 m10 = dup(2.f * (qx * qy + qw * qz)), m11 = dup(1.f - 2.f * (qx * qx + qz * qz)),
+               m12 = dup(2.f * (qy * qz - qw * qx));
+  const float2 m20 = dup(2.f * (qx * qz - qw * qy)), m21 = dup(2.f * (qy * qz + qw * qx)),
+               m22 = dup(1.f - 2.f * (qx * qx + qy * qy));
+  const float2 ux = dup(u.x), uy = dup(u.y), uz = dup(u.z);
+  // two pairs per packed FP32x2 operation: e = M c_b + u - c_a
+  const int q1 = c.pgstart[gi + 1];
+  for (int q = c.pgstart[gi]; q < q1; q += 2) {
+    const float4 r0 = c.prec[2 * q], r1 = c.prec[2 * q + 1], r2 = c.prec[2 * q + 2], r3 = c.prec[2 * q + 3];
+    const float2 bx = make_float2(r2.x, r2.y), by = make_float2(r2.z, r2.w), bz = make_float2(r3.x, r3.y);
+    const float2 ex = __ffma2_rn(m00, bx, __ffma2_rn(m01, by, __ffma2_rn(m02, bz, __fadd2_rn(ux, make_float2(r0.x, r0.y)))));
+    const float2 ey = __ffma2_rn(m10, bx, __ffma2_rn(m11, by, __ffma2_rn(m12, bz, __fadd2_rn(uy, make_float2(r0.z, r0.w)))));
+    const float2 ez = __ffma2_rn(m20, bx, __ffma2_rn(m21, by, __ffma2_rn(m22, bz, __fadd2_rn(uz, make_float2(r1.x, r1.y)))));
+    float2 d2 = __fmul2_rn(ex, ex);
+    d2 = __ffma2_rn(ey, ey, d2);
+    d2 = __ffma2_rn(ez, ez, d2);
+    if (d2.x < r3.z) { const float e = sqrtf(d2.x) - r1.z; pen += e * e; }
+    if (d2.y < r3.w) { const float e = sqrtf(d2.y) - r1.w; pen += e * e; }
+  }
+}
+
+// Self pairs of one seed, split over its TPS lanes (TPS > 1): the
+// bounding-sphere culls of the joint-slot groups into a mask of this lane's
+// surviving groups (survivors go round-robin to the seed's lanes), then the
+// pairs of those groups in increasing group order.
+template <int TPS>
+__device__ __forceinline__ void self_share(const PenaltyCtx& c, const PoseSlots& ps, int t, float& pen) {
+  const float* const cen = c.cen;
+  const int cs = c.cs;
+  int turn = 0;  // surviving groups seen so far (the same count on every lane of the seed)
+  for (int g0 = 0; g0 < c.n_groups; g0 += 32) {
+    unsigned mask = 0u;
+    for (int i = 0; i < 32 && g0 + i < c.n_groups; ++i) {
+      const int2 ja = c.gjoint[g0 + i];
+      const float dx = cen[(3 * ja.x) * cs] - cen[(3 * ja.y) * cs];
+      const float dy = cen[(3 * ja.x + 1) * cs] - cen[(3 * ja.y + 1) * cs];
+      const float dz = cen[(3 * ja.x + 2) * cs] - cen[(3 * ja.y + 2) * cs];
+      const float rr = c.jb[ja.x].w + c.jb[ja.y].w + c.margin;
+      if (!(dx * dx + dy * dy + dz * dz < rr * fabsf(rr))) continue;
+      if ((turn++ & (TPS - 1)) == t) mask |= 1u << i;
+    }
+    while (mask) {
+      const int gi = g0 + __ffs(mask) - 1;
+      mask &= mask - 1u;
+      group_pairs(c, ps, gi, pen);
+    }
+  }
+}
+
+// Self pairs of the 32 seeds of a warp (TPS == 1), all 32 lanes together.
+// Per chunk of kSelfChunk groups, each lane culls the groups for its own
+// seed (none when !need); the surviving (seed, group) items go into the
+// warp's list in (group, lane) order; lane l takes items l, l + 32, ... and
+// writes each item's sum (its pairs in pair order) to res[group][seed]; then
+// each lane adds its own surviving groups' sums in group order.  The result
+// does not depend on which lane took which item, and the work of a chunk is
+// spread over the warp instead of following the seed with the most
+// surviving groups.  slots_w: the pose slots of the warp's first seed.
+__device__ __forceinline__ void self_warp(const PenaltyCtx& c, float* slots_w, int spb, bool need, float& pen,
+                                          unsigned short* list, float* res) {
+  const int lane = threadIdx.x & 31;
+  const float* const cen = c.cen;
+  const int cs = c.cs;
+  for (int g0 = 0; g0 < c.n_groups; g0 += kSelfChunk) {
+    const int nc = min(kSelfChunk, c.n_groups - g0);
+    unsigned mine = 0u;
+    int n_items = 0;
+    for (int i = 0; i < nc; ++i) {
+      bool sv = false;
+      if (need) {
+        const int2 ja = c.gjoint[g0 + i];
+        const float dx = cen[(3 * ja.x) * cs] - cen[(3 * ja.y) * cs];
+        const float dy = cen[(3 * ja.x + 1) * cs] - cen[(3 * ja.y + 1) * cs];
+        const float dz = cen[(3 * ja.x + 2) * cs] - cen[(3 * ja.y + 2) * cs];
+        const float rr = c.jb[ja.x].w + c.jb[ja.y].w + c.margin;
+        sv = dx * dx + dy * dy + dz * dz < rr * fabsf(rr);
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, sv);
+      if (sv) {
+        list[n_items + __popc(m & ((1u << lane) - 1u))] = (unsigned short)((lane << 8) | i);
+        mine |= 1u << i;
+      }
+      n_items += __popc(m);
+    }
+    __syncwarp();
+    for (int k = lane; k < n_items; k += 32) {
+      const int item = list[k];
+      const int o = item >> 8, i = item & 255;
+      float part = 0.f;
+      group_pairs(c, PoseSlots{slots_w + o, spb}, g0 + i, part);
+      res[i * 32 + o] = part;
+    }
+    __syncwarp();
+    while (mine) {
+      const int i = __ffs(mine) - 1;
+      mine &= mine - 1u;
+      pen += res[i * 32 + lane];
+    }
+    __syncwarp();  // the next chunk reuses list and res
   }
 }
 
 // Partial hinge penalty of lane t of a TPS-group (not weighted, not summed).
-//  1. per sphere-carrying joint, the joint's bounding-sphere centre (lane 0)
-//     and lane t's share of its spheres go to this seed's shared slots;
+//  1. lane t puts the bounding-sphere centres of joint slots t, t+TPS, ...
+//     (world frame) into this seed's shared slots;
 //  2. world spheres: conservative culls before any sphere-level test.  The
 //     joint's bounding sphere (centre B, radius R) can only reach obstacle o
 //     if |B - o| < R + r_o + margin.  With the obstacle grid, only the
 //     obstacles registered in B's cell (every obstacle whose ball of radius
 //     r_o + margin + max R covers part of that cell) are candidates; lane t
 //     takes candidates t, t+TPS, ...  Without it, lane t scans obstacles
-//     t, t+TPS, ... into a 32-bit survivor mask.
-//  3. capsules / boxes / halfspaces: exact test of lane t's spheres;
+//     t, t+TPS, ... into a 32-bit survivor mask.  A surviving obstacle is
+//     moved into the joint's frame and tested against the joint's spheres;
+//  3. capsules / boxes / halfspaces: lane t takes joint slots t, t+TPS, ...;
+//     a joint whose bounding ball is margin clear of a capsule or box (both
+//     distances are 1-Lipschitz in the point, so no sphere inside the ball
+//     is closer) is skipped for it, else its spheres are tested in the world
+//     frame;
 //  4. self pairs by joint-slot group: a group is skipped when the two
-//     joints' bounding spheres are margin apart; otherwise lane t tests
-//     its pairs t, t+TPS, ... of the group.
+//     joints' bounding spheres are margin apart; the surviving groups go
+//     round-robin to the group's lanes, and a lane takes each of its groups
+//     whole: one relative transform T_x^-1 T_y (as a rotation matrix), then
+//     per pair |c_a - (M c_b + u)| from the joint-frame records.
+//
+// TPS == 1: every lane of the warp calls it (need == false: the lane adds
+// nothing but takes part in the warp's self-pair items, self_warp); TPS > 1:
+// the seed's lanes call it when the seed needs it.
 template <int TPS>
-__device__ float penalty_share(const PenaltyCtx& c, const PoseSlots& ps, int t, unsigned gmask) {
+__device__ float penalty_share(const PenaltyCtx& c, const PoseSlots& ps, int t, unsigned gmask, bool need,
+                               float* slots_w, int spb, unsigned short* wlist, float* wres) {
   float pen = 0.f;
-  float* const px = c.pos;
-  float* const pb = c.pos + 3 * c.n_rs;
-  for (int j = 0; j < c.n_js; ++j) {
-    const Pose T = ps.load(c.jlist[j]);
-    if (t == 0) {
+  float* const cen = c.cen;
+  const int cs = c.cs;
+  if (need) {
+    for (int j = t; j < c.n_js; j += TPS) {
+      const Pose T = ps.load(c.jlist[j]);
       const float4 bl = c.jb[j];
       const float3 B = pose_apply(T, make_float3(bl.x, bl.y, bl.z));
-      pb[3 * j] = B.x; pb[3 * j + 1] = B.y; pb[3 * j + 2] = B.z;
+      cen[(3 * j) * cs] = B.x; cen[(3 * j + 1) * cs] = B.y; cen[(3 * j + 2) * cs] = B.z;
     }
-    for (int k = c.jstart[j] + t; k < c.jstart[j + 1]; k += TPS) {
-      const float4 s = c.rs[k];
-      const float3 w = pose_apply(T, make_float3(s.x, s.y, s.z));
-      px[3 * k] = w.x; px[3 * k + 1] = w.y; px[3 * k + 2] = w.z;
-    }
-  }
-  __syncwarp(gmask);
+    if (TPS > 1) __syncwarp(gmask);
 
-  for (int j = 0; j < c.n_js && c.Ms_pad > 0; ++j) {
-    const float R = c.jb[j].w;
-    const float Bx = pb[3 * j], By = pb[3 * j + 1], Bz = pb[3 * j + 2];
-    const int k0 = c.jstart[j], k1 = c.jstart[j + 1];
-    if (c.cell_start) {
-      const int cell = obstacle_grid_cell(c.glo, c.ginv, make_float3(Bx, By, Bz));
-      if (cell < 0) continue;  // outside the grid no obstacle is within reach of this joint
-      const int e1 = c.cell_start[cell + 1];
-      for (int e = c.cell_start[cell] + t; e < e1; e += TPS) {
-        const float4 O = c.ws[c.cell_obs[e]];
-        const float rr = R + O.w;
-        const float dx = Bx - O.x, dy = By - O.y, dz = Bz - O.z;
-        if (dx * dx + dy * dy + dz * dz < rr * fabsf(rr)) narrow_world(c, k0, k1, O, pen);
-      }
-    } else {
-      for (int ob = t; ob < c.Ms_pad; ob += 32 * TPS) {
-        unsigned mask = 0u;
-#pragma unroll
-        for (int i = 0; i < 32; ++i) {
-          const float4 O = c.ws[ob + i * TPS];
-          const float rr = R + O.w;
-          const float dx = Bx - O.x, dy = By - O.y, dz = Bz - O.z;
-          if (dx * dx + dy * dy + dz * dz < rr * fabsf(rr)) mask |= 1u << i;
+    for (int j = 0; j < c.n_js && c.Ms_pad > 0; ++j) {
+      const float R = c.jb[j].w;
+      const float Bx = cen[(3 * j) * cs], By = cen[(3 * j + 1) * cs], Bz = cen[(3 * j + 2) * cs];
+      const int p0 = c.pjstart[j], p1 = c.pjstart[j + 1];
+      if (c.cell_start) {
+        const int cell = obstacle_grid_cell(c.glo, c.ginv, make_float3(Bx, By, Bz));
+        if (cell < 0) continue;  // outside the grid no obstacle is within reach of this joint
+        const int e1 = c.cell_start[cell + 1];
+        // the lane's candidates in chunks of 32: bounding tests into a survivor
+        // mask first, then the narrow tests of the survivors, so a warp runs
+        // the narrow loop max-over-lanes times per chunk instead of once per
+        // candidate slot in which any lane has a survivor
+        for (int e0 = c.cell_start[cell] + t; e0 < e1; e0 += 32 * TPS) {
+          unsigned mask = 0u;
+          for (int i = 0; i < 32 && e0 + i * TPS < e1; ++i) {
+            const float4 O = c.ws[c.cell_obs[e0 + i * TPS]];
+            const float rr = R + O.w;
+            const float dx = Bx - O.x, dy = By - O.y, dz = Bz - O.z;
+            if (dx * dx + dy * dy + dz * dz < rr * fabsf(rr)) mask |= 1u << i;
+          }
+          if (mask) {
+            const Pose T = ps.load(c.jlist[j]);
+            while (mask) {
+              const int i = __ffs(mask) - 1;
+              mask &= mask - 1u;
+              narrow_world(c, T, p0, p1, c.ws[c.cell_obs[e0 + i * TPS]], pen);
+            }
+          }
         }
-        while (mask) {
-          const int i = __ffs(mask) - 1;
-          mask &= mask - 1u;
-          narrow_world(c, k0, k1, c.ws[ob + i * TPS], pen);
+      } else {
+        for (int ob = t; ob < c.Ms_pad; ob += 32 * TPS) {
+          unsigned mask = 0u;
+  #pragma unroll
+          for (int i = 0; i < 32; ++i) {
+            const float4 O = c.ws[ob + i * TPS];
+            const float rr = R + O.w;
+            const float dx = Bx - O.x, dy = By - O.y, dz = Bz - O.z;
+            if (dx * dx + dy * dy + dz * dz < rr * fabsf(rr)) mask |= 1u << i;
+          }
+          if (mask) {
+            const Pose T = ps.load(c.jlist[j]);
+            while (mask) {
+              const int i = __ffs(mask) - 1;
+              mask &= mask - 1u;
+              narrow_world(c, T, p0, p1, c.ws[ob + i * TPS], pen);
+            }
+          }
         }
       }
     }
-  }
 
-  if (c.Mc + c.Mb + c.Mh > 0) {
-    for (int k = t; k < c.n_rs; k += TPS) {
-      const float3 p = make_float3(px[3 * k], px[3 * k + 1], px[3 * k + 2]);
-      const float r = c.rs[k].w;
-      for (int m = 0; m < c.Mc; ++m) {
-        const float d = d_sphere_capsule(p, r, c.wc + 7 * m);
-        if (d < c.margin) { const float e = d - c.margin; pen += e * e; }
-      }
-      for (int m = 0; m < c.Mb; ++m) {
-        const float d = d_sphere_box(p, r, c.wb + 15 * m);
-        if (d < c.margin) { const float e = d - c.margin; pen += e * e; }
-      }
-      for (int m = 0; m < c.Mh; ++m) {
-        const float d = d_sphere_halfspace(p, r, c.wh + 6 * m);
-        if (d < c.margin) { const float e = d - c.margin; pen += e * e; }
+    if (c.Mc + c.Mb + c.Mh > 0) {
+      for (int j = t; j < c.n_js; j += TPS) {
+        const float3 B = make_float3(cen[(3 * j) * cs], cen[(3 * j + 1) * cs], cen[(3 * j + 2) * cs]);
+        const float R = c.jb[j].w;
+        const int k0 = c.jstart[j], k1 = c.jstart[j + 1];
+        const Pose T = ps.load(c.jlist[j]);
+        for (int m = 0; m < c.Mc; ++m) {
+          if (!(d_sphere_capsule(B, R, c.wc + 7 * m) < c.margin)) continue;
+          for (int k = k0; k < k1; ++k) {
+            const float4 s = c.rs[k];
+            const float d = d_sphere_capsule(pose_apply(T, make_float3(s.x, s.y, s.z)), s.w, c.wc + 7 * m);
+            if (d < c.margin) { const float e = d - c.margin; pen += e * e; }
+          }
+        }
+        for (int m = 0; m < c.Mb; ++m) {
+          if (!(d_sphere_box(B, R, c.wb + 15 * m) < c.margin)) continue;
+          for (int k = k0; k < k1; ++k) {
+            const float4 s = c.rs[k];
+            const float d = d_sphere_box(pose_apply(T, make_float3(s.x, s.y, s.z)), s.w, c.wb + 15 * m);
+            if (d < c.margin) { const float e = d - c.margin; pen += e * e; }
+          }
+        }
+        for (int m = 0; m < c.Mh; ++m) {  // no cull: a normal need not be unit length
+          for (int k = k0; k < k1; ++k) {
+            const float4 s = c.rs[k];
+            const float d = d_sphere_halfspace(pose_apply(T, make_float3(s.x, s.y, s.z)), s.w, c.wh + 6 * m);
+            if (d < c.margin) { const float e = d - c.margin; pen += e * e; }
+          }
+        }
       }
     }
-  }
 
-  for (int gi = 0; gi < c.n_groups; ++gi) {
-    const int2 ja = c.gjoint[gi];
-    const float dx = pb[3 * ja.x] - pb[3 * ja.y];
-    const float dy = pb[3 * ja.x + 1] - pb[3 * ja.y + 1];
-    const float dz = pb[3 * ja.x + 2] - pb[3 * ja.y + 2];
-    const float rr = c.jb[ja.x].w + c.jb[ja.y].w + c.margin;
-    if (!(dx * dx + dy * dy + dz * dz < rr * fabsf(rr))) continue;
-    for (int q = c.gstart[gi] + t; q < c.gstart[gi + 1]; q += TPS) {
-      const int2 pr = c.pairs[q];
-      const float ex = px[3 * pr.x] - px[3 * pr.y];
-      const float ey = px[3 * pr.x + 1] - px[3 * pr.y + 1];
-      const float ez = px[3 * pr.x + 2] - px[3 * pr.y + 2];
-      hinge_sq(ex * ex + ey * ey + ez * ez, c.rs[pr.x].w + c.rs[pr.y].w + c.margin, pen);
-    }
+    if (TPS > 1) self_share<TPS>(c, ps, t, pen);
   }
+  if (TPS == 1 && c.n_groups > 0) self_warp(c, slots_w, spb, need, pen, wlist, wres);
   __syncwarp(gmask);
   return pen;
 }
@@ -531,6 +718,7 @@ __device__ void lm_stage(const LmArgs& a, unsigned char* smem_raw, const LmLayou
   float4* rs4 = reinterpret_cast<float4*>(smem_raw + L.rs);
   float4* ws4 = reinterpret_cast<float4*>(smem_raw + L.ws);
   int2* pairs = reinterpret_cast<int2*>(smem_raw + L.pairs);
+  float4* prec = reinterpret_cast<float4*>(smem_raw + L.prec);
   int2* gjoint = reinterpret_cast<int2*>(smem_raw + L.gjoint);
   int* gstart = reinterpret_cast<int*>(smem_raw + L.gstart);
   int* rsj = reinterpret_cast<int*>(smem_raw + L.rsj);
@@ -622,15 +810,34 @@ __device__ void lm_stage(const LmArgs& a, unsigned char* smem_raw, const LmLayou
       sh.jb[q] = make_float4(cx, cy, cz, R);
       rmax = fmaxf(rmax, R);
     }
+    if (L.recs) {
+      // the paired sphere table: joint slot q's spheres from pair pjstart[q]
+      float* rf = reinterpret_cast<float*>(smem_raw + L.rsp);
+      int run = 0;
+      for (int q = 0; q < n_js; ++q) {
+        sh.pjstart[q] = run;
+        const int k0 = sh.jstart[q], n = sh.jstart[q + 1] - k0;
+        for (int i = 0; i < n + (n & 1); ++i) {
+          const int h = i & 1;
+          float* f = rf + 8 * (run + (i >> 1));
+          const float4 v = (i < n) ? rs4[k0 + i] : make_float4(0.f, 0.f, 0.f, -1e9f);
+          f[h] = v.x; f[2 + h] = v.y; f[4 + h] = v.z; f[6 + h] = v.w;
+        }
+        run += (n + 1) >> 1;
+      }
+      sh.pjstart[n_js] = run;
+    }
     // self pairs in grouped sphere slots, grouped by (joint slot, joint slot)
+    // with a counting sort on the key x_slot * n_js + y_slot; the layout
+    // sizes the scratch for n_joints^2 >= n_js^2 keys, so every group holds
+    // the pairs of one joint pair (x_slot <= y_slot).  The seed-group layout
+    // also gets each pair as a joint-frame record: (c_a, r_a + r_b + margin)
+    // in slot x's frame, (c_b, 0) in slot y's frame.
     int n_groups = 0;
     if (a.coll && a.n_self > 0 && n_js > 0) {
       const int NK = n_js * n_js;
-      const bool by_key = NK <= L.scratch_ints;
       int* kc = scratch;
-      if (by_key)
-        for (int i = 0; i < NK; ++i) kc[i] = 0;
-      int n_valid = 0;
+      for (int i = 0; i < NK; ++i) kc[i] = 0;
       for (int pass = 0; pass < 2; ++pass) {
         for (int q = 0; q < a.n_self; ++q) {
           int x = a.self_i[q], y = a.self_j[q];
@@ -638,36 +845,52 @@ __device__ void lm_stage(const LmArgs& a, unsigned char* smem_raw, const LmLayou
           x = rsk[x]; y = rsk[y];
           if (x < 0 || y < 0) continue;
           if (rsj[x] > rsj[y]) { const int tmp = x; x = y; y = tmp; }
-          const int key = by_key ? rsj[x] * n_js + rsj[y] : 0;
+          const int key = rsj[x] * n_js + rsj[y];
           if (pass == 0) {
-            if (by_key) kc[key]++;
-            ++n_valid;
+            kc[key]++;
           } else {
-            pairs[by_key ? kc[key]++ : n_valid++] = make_int2(x, y);
+            pairs[kc[key]++] = make_int2(x, y);
           }
         }
         if (pass == 0) {
-          if (by_key) {
-            int run = 0;
-            for (int key = 0; key < NK; ++key) {
-              if (kc[key] == 0) continue;
-              gjoint[n_groups] = make_int2(key / n_js, key % n_js);
-              gstart[n_groups] = run;
-              const int c0 = kc[key];
-              kc[key] = run;
-              run += c0;
-              ++n_groups;
-            }
+          int run = 0;
+          for (int key = 0; key < NK; ++key) {
+            if (kc[key] == 0) continue;
+            gjoint[n_groups] = make_int2(key / n_js, key % n_js);
             gstart[n_groups] = run;
-          } else if (n_valid > 0) {
-            // too many joint slots for the key table: one group that is never culled
-            gjoint[0] = make_int2(0, 0);
-            gstart[0] = 0;
-            gstart[1] = n_valid;
-            n_groups = 1;
+            const int c0 = kc[key];
+            kc[key] = run;
+            run += c0;
+            ++n_groups;
           }
-          n_valid = 0;
+          gstart[n_groups] = run;
         }
+      }
+      if (L.recs) {
+        // the paired pair table: group g's pairs from padded index pgstart[g]
+        int* pgstart = reinterpret_cast<int*>(smem_raw + L.pgstart);
+        float* pf = reinterpret_cast<float*>(prec);
+        int run = 0;
+        for (int g = 0; g < n_groups; ++g) {
+          pgstart[g] = run;
+          const int n = gstart[g + 1] - gstart[g];
+          for (int i = 0; i < n + (n & 1); ++i) {
+            const int pq = run + i, h = pq & 1;
+            float* f = pf + 16 * (pq >> 1);
+            if (i < n) {
+              const int2 pr = pairs[gstart[g] + i];
+              const float4 A = rs4[pr.x], Bs = rs4[pr.y];
+              const float rr = A.w + Bs.w + a.margin;
+              f[h] = -A.x; f[2 + h] = -A.y; f[4 + h] = -A.z; f[6 + h] = rr;
+              f[8 + h] = Bs.x; f[10 + h] = Bs.y; f[12 + h] = Bs.z; f[14 + h] = rr * fabsf(rr);
+            } else {  // padding: |u|^2 >= 0 is never below -1
+              f[h] = 0.f; f[2 + h] = 0.f; f[4 + h] = 0.f; f[6 + h] = -1.f;
+              f[8 + h] = 0.f; f[10 + h] = 0.f; f[12 + h] = 0.f; f[14 + h] = -1.f;
+            }
+          }
+          run += n + (n & 1);
+        }
+        pgstart[n_groups] = run;
       }
     }
     sh.n_groups = n_groups;
@@ -688,15 +911,17 @@ __device__ void lm_stage(const LmArgs& a, unsigned char* smem_raw, const LmLayou
 
 // `count` seeds of problem pb, with the block's shared memory already
 // staged for (a, pb) by lm_stage; seed group g reads and writes flat seed
-// index gs_base + g.  A group past `count` does nothing
-// (the body has no block-wide barrier).
+// index gs_base + g.  Every lane of the warp stays in the iteration loop
+// until all of the warp's seeds are done (converged, out of iterations, or
+// past `count`, which reads and writes nothing): a done seed's lanes run
+// along without changing its state, so the warp's collective steps
+// (self_warp) always see all 32 lanes.  No block-wide barrier.
 template <int MAXA, int MAXEE, int TPS>
 __device__ __forceinline__ void lm_seed_groups(const LmArgs& a, unsigned char* smem_raw, const LmLayout& L, int pb,
                                                int count, size_t gs_base) {
   LmShared& sh = *reinterpret_cast<LmShared*>(smem_raw);
   float4* rs4 = reinterpret_cast<float4*>(smem_raw + L.rs);
   float4* ws4 = reinterpret_cast<float4*>(smem_raw + L.ws);
-  int2* pairs = reinterpret_cast<int2*>(smem_raw + L.pairs);
   int2* gjoint = reinterpret_cast<int2*>(smem_raw + L.gjoint);
   int* gstart = reinterpret_cast<int*>(smem_raw + L.gstart);
   int* cell_start = reinterpret_cast<int*>(smem_raw + L.cells);
@@ -705,14 +930,14 @@ __device__ __forceinline__ void lm_seed_groups(const LmArgs& a, unsigned char* s
   float* wb = reinterpret_cast<float*>(smem_raw + L.wb);
   float* wh = reinterpret_cast<float*>(smem_raw + L.wh);
   float* slots = reinterpret_cast<float*>(smem_raw + L.slots);
-  float* pos = reinterpret_cast<float*>(smem_raw + L.pos);
-  const int PS = lm_pos_stride(a.n_rs, a.m.n_joints);
+  float* cen = reinterpret_cast<float*>(smem_raw + L.cen);
+  const float4* prec = reinterpret_cast<const float4*>(smem_raw + L.prec);
   const int tid = threadIdx.x;
   const int g = tid / TPS, t = tid - g * TPS;
   const int lane = tid & 31;
   const unsigned gmask = (TPS == 32) ? 0xffffffffu : (((1u << TPS) - 1u) << (lane & ~(TPS - 1)));
-  if (g >= count) return;
-  const size_t gs = gs_base + g;
+  const bool valid = g < count;
+  const size_t gs = gs_base + (valid ? g : 0);
   (void)pb;
 
   const JointTable& jt = sh.jt;
@@ -722,9 +947,11 @@ __device__ __forceinline__ void lm_seed_groups(const LmArgs& a, unsigned char* s
   const bool use_coll = a.coll && (sh.n_rs > 0);
   PenaltyCtx pc;
   pc.rs = rs4; pc.jb = sh.jb; pc.jstart = sh.jstart; pc.jlist = sh.jlist;
-  pc.ws = ws4; pc.wc = wc; pc.wb = wb; pc.wh = wh; pc.pairs = pairs; pc.gjoint = gjoint; pc.gstart = gstart;
+  pc.rsp = reinterpret_cast<const float4*>(smem_raw + L.rsp); pc.pjstart = sh.pjstart;
+  pc.ws = ws4; pc.wc = wc; pc.wb = wb; pc.wh = wh; pc.prec = prec; pc.gjoint = gjoint;
+  pc.pgstart = reinterpret_cast<const int*>(smem_raw + L.pgstart);
   pc.cell_start = sh.grid_on ? cell_start : nullptr; pc.cell_obs = cell_obs;
-  pc.pos = pos + (size_t)g * PS; pc.glo = sh.glo; pc.ginv = sh.ginv;
+  pc.cen = cen + g; pc.cs = a.spb; pc.glo = sh.glo; pc.ginv = sh.ginv;
   pc.n_rs = sh.n_rs; pc.n_js = sh.n_js; pc.n_groups = sh.n_groups; pc.Ms_pad = L.ms_pad;
   pc.Mc = a.w.Mc; pc.Mb = a.w.Mb; pc.Mh = a.w.Mh; pc.margin = a.margin;
 
@@ -733,13 +960,20 @@ __device__ __forceinline__ void lm_seed_groups(const LmArgs& a, unsigned char* s
   float cfg[MAXA], best[MAXA];
 #pragma unroll
   for (int i = 0; i < MAXA; ++i) {
-    cfg[i] = (i < a.n_act) ? a.seeds[gs * a.n_act + i] : 0.f;
+    cfg[i] = (valid && i < a.n_act) ? a.seeds[gs * a.n_act + i] : 0.f;
     best[i] = cfg[i];
   }
+  float* const slots_w = slots + (g & ~31);  // one lane per seed: the pose slots of the warp's first seed
+  unsigned short* const wlist =
+      reinterpret_cast<unsigned short*>(smem_raw + L.wscr) + (size_t)(tid >> 5) * kSelfChunk * 32 * 3;
+  float* const wres = reinterpret_cast<float*>(wlist + kSelfChunk * 32);
 
-  auto penalty = [&]() -> float {
+  // TPS == 1: called by every lane (collective); TPS > 1: by the lanes of
+  // seeds that need it
+  auto penalty = [&](bool need) -> float {
     if (!use_coll) return 0.f;
-    const float share = penalty_share<TPS>(pc, ps, t, gmask);
+    if (TPS > 1 && !need) return 0.f;
+    const float share = penalty_share<TPS>(pc, ps, t, gmask, need, slots_w, a.spb, wlist, wres);
     return a.coll_w * group_sum<TPS>(share, gmask);
   };
   // Every lane of the group computes the FK (same values); lane 0 stores it.
@@ -770,9 +1004,12 @@ __device__ __forceinline__ void lm_seed_groups(const LmArgs& a, unsigned char* s
   float best_a_err = 1e30f, best_a_pen = 0.f;
   int best_a = 0;
   int it = 0, ev = -1;
+  bool done = !valid;
 #pragma unroll
   for (int c = 0; c < MAXA; ++c) delta[c] = 0.f;
-  while (true) {
+  // ev runs the same schedule on every lane of the warp; `done` only stops
+  // a seed's state from changing
+  while (!__all_sync(0xffffffffu, done)) {
     float q[MAXA];
 #pragma unroll
     for (int c = 0; c < MAXA; ++c)
@@ -781,23 +1018,28 @@ __device__ __forceinline__ void lm_seed_groups(const LmArgs& a, unsigned char* s
     ee_residual<MAXEE>(sh, ps, a.n_ee, r, pee);
 
     if (ev == 0) {
-      bool all_conv = true;
-      float max_p = 0.f, max_o = 0.f;
+      if (!done) {
+        bool all_conv = true;
+        float max_p = 0.f, max_o = 0.f;
 #pragma unroll
-      for (int e = 0; e < MAXEE; ++e) {
-        if (e < a.n_ee) {
-          const float np = sqrtf(r[6 * e] * r[6 * e] + r[6 * e + 1] * r[6 * e + 1] + r[6 * e + 2] * r[6 * e + 2]);
-          const float no = sqrtf(r[6 * e + 3] * r[6 * e + 3] + r[6 * e + 4] * r[6 * e + 4] + r[6 * e + 5] * r[6 * e + 5]);
-          if (np >= a.eps_pos || no >= a.eps_ori) all_conv = false;
-          max_p = fmaxf(max_p, np);
-          max_o = fmaxf(max_o, no);
+        for (int e = 0; e < MAXEE; ++e) {
+          if (e < a.n_ee) {
+            const float np = sqrtf(r[6 * e] * r[6 * e] + r[6 * e + 1] * r[6 * e + 1] + r[6 * e + 2] * r[6 * e + 2]);
+            const float no = sqrtf(r[6 * e + 3] * r[6 * e + 3] + r[6 * e + 4] * r[6 * e + 4] + r[6 * e + 5] * r[6 * e + 5]);
+            if (np >= a.eps_pos || no >= a.eps_ori) all_conv = false;
+            max_p = fmaxf(max_p, np);
+            max_o = fmaxf(max_o, no);
+          }
+        }
+        if (all_conv) {
+          done = true;
+        } else {
+          curr = lm_direction<MAXA, MAXEE>(sh, ps, a.n_ee, W, r, pee, lam, max_p, max_o, delta) + pen_cur;
+          best_a_err = 1e30f;
+          best_a_pen = pen_cur;
+          best_a = 0;
         }
       }
-      if (all_conv) break;
-      curr = lm_direction<MAXA, MAXEE>(sh, ps, a.n_ee, W, r, pee, lam, max_p, max_o, delta) + pen_cur;
-      best_a_err = 1e30f;
-      best_a_pen = pen_cur;
-      best_a = 0;
       ev = 1;
       continue;
     }
@@ -807,41 +1049,42 @@ __device__ __forceinline__ void lm_seed_groups(const LmArgs& a, unsigned char* s
     // penalty is skipped, which leaves every decision and output unchanged.
     // (The test is uniform across the seed's lanes.)
     const float wsq = weighted_sq(r);
-    const float pen = (ev < 0 || wsq < best_a_err) ? penalty() : 0.f;
-    const float err = wsq + pen;
-    if (ev < 0) {
-      pen_cur = pen;
-      best_err = err;
-      if (a.max_iter <= 0) break;
-      ev = 0;
-      continue;
-    }
-    if (err < best_a_err) { best_a_err = err; best_a = ev - 1; best_a_pen = pen; }
-    if (ev < 5) { ++ev; continue; }
-
-    // accept / reject the damped step, track the all-time best
-    const float alpha = line_alpha(best_a);
-    float trial[MAXA];
+    const float pen = penalty(!done && (ev < 0 || wsq < best_a_err));
+    if (!done) {
+      const float err = wsq + pen;
+      if (ev < 0) {
+        pen_cur = pen;
+        best_err = err;
+        if (a.max_iter <= 0) done = true;
+      } else {
+        if (err < best_a_err) { best_a_err = err; best_a = ev - 1; best_a_pen = pen; }
+        if (ev == 5) {
+          // accept / reject the damped step, track the all-time best
+          const float alpha = line_alpha(best_a);
+          float trial[MAXA];
 #pragma unroll
-    for (int c = 0; c < MAXA; ++c) trial[c] = fmaxf(sh.lo[c], fminf(sh.hi[c], cfg[c] + alpha * delta[c]));
-    if (best_a_err < curr * (1.0f - 1e-4f)) {
+          for (int c = 0; c < MAXA; ++c) trial[c] = fmaxf(sh.lo[c], fminf(sh.hi[c], cfg[c] + alpha * delta[c]));
+          if (best_a_err < curr * (1.0f - 1e-4f)) {
 #pragma unroll
-      for (int c = 0; c < MAXA; ++c) cfg[c] = trial[c];
-      pen_cur = best_a_pen;
-      lam = fmaxf(lam * a.lam_down, 1e-10f);
-    } else {
-      lam = fminf(lam * a.lam_up, 1e6f);
-    }
-    if (best_a_err < best_err) {
-      best_err = best_a_err;
+            for (int c = 0; c < MAXA; ++c) cfg[c] = trial[c];
+            pen_cur = best_a_pen;
+            lam = fmaxf(lam * a.lam_down, 1e-10f);
+          } else {
+            lam = fminf(lam * a.lam_up, 1e6f);
+          }
+          if (best_a_err < best_err) {
+            best_err = best_a_err;
 #pragma unroll
-      for (int c = 0; c < MAXA; ++c) best[c] = trial[c];
+            for (int c = 0; c < MAXA; ++c) best[c] = trial[c];
+          }
+          if (++it >= a.max_iter) done = true;
+        }
+      }
     }
-    if (++it >= a.max_iter) break;
-    ev = 0;
+    ev = (ev < 0 || ev == 5) ? 0 : ev + 1;
   }
 
-  if (t == 0) {
+  if (t == 0 && valid) {
 #pragma unroll
     for (int c = 0; c < MAXA; ++c)
       if (c < a.n_act) a.out_cfg[gs * a.n_act + c] = best[c];
@@ -1349,13 +1592,17 @@ static int launch_lm_t(const LmArgs& a0, cudaStream_t st) {
   const int threads = a.spb * TPS;
   const size_t smem = lm_smem_bytes(a, TPS);
   PK_CHECK_CAP(smem <= 220 * 1024, "LM working set (%zu B of shared memory) too large", smem);
-  // the 4-block register budget only where shared memory admits 3 or more blocks per SM
+  dim3 grid((a.Sd + a.spb - 1) / a.spb, a.P);
+  // The 4-block register budget (spills) only where shared memory admits 3
+  // or more blocks per SM and the grid needs more than 2 blocks per SM.
   auto kern = lm_kernel<MAXA, MAXEE, TPS, 2>;
   if constexpr (MAXA <= 8) {
-    if ((228 * 1024) / (smem + 1024) >= 3) kern = lm_kernel<MAXA, MAXEE, TPS, 4>;
+    int dev = 0, sms = 0;
+    if (int s = cuda_status(cudaGetDevice(&dev), "cudaGetDevice")) return s;
+    if (int s = cuda_status(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attribute")) return s;
+    if ((228 * 1024) / (smem + 1024) >= 3 && (long long)grid.x * grid.y > 2LL * sms) kern = lm_kernel<MAXA, MAXEE, TPS, 4>;
   }
   if (int s = set_smem_limit((const void*)kern, smem)) return s;
-  dim3 grid((a.Sd + a.spb - 1) / a.spb, a.P);
   kern<<<grid, threads, smem, st>>>(a);
   return cuda_status(cudaGetLastError(), "lm_kernel launch");
 }
@@ -1401,11 +1648,11 @@ static int launch_lm(LmArgs a, int tps, int spb, cudaStream_t st) {
   // threads_per_seed 5: the trial-lane kernel (5 lanes per seed, one
   // line-search trial each); 1, 2, 4, 8: the seed-group kernel with the
   // collision penalty split across that many lanes; 0: the fastest measured
-  // default, 2 lanes x 64 seeds per block.  (16 and 32, the warp-per-seed
+  // default, 1 lane x 128 seeds per block.  (16 and 32, the warp-per-seed
   // body, are routed by lm_common.)
   if (tps <= 0) {
-    tps = 2;
-    if (spb <= 0) spb = 64;
+    tps = 1;
+    if (spb <= 0) spb = 128;
   }
   if (tps == 5) {
     if (a.n_act <= 8 && a.n_ee <= 1) return launch_lm_trial<8, 1>(a, st);
@@ -1598,7 +1845,7 @@ static int launch_batch_t(const SeedGroupBatch& B, size_t smem, int threads, int
 
 int launch_seed_group_batch(const BatchCall& b, cudaStream_t st, int* launched) {
   int tps = b.opt.threads_per_seed, spb = b.opt.seeds_per_block;
-  if (tps <= 0) { tps = 2; if (spb <= 0) spb = 64; }
+  if (tps <= 0) { tps = 1; if (spb <= 0) spb = 128; }
   if (spb <= 0) spb = 128 / tps;
   SeedGroupBatch B{};
   bool any = false;
@@ -1692,8 +1939,6 @@ extern "C" int pk_ik_batch(void* stream, const pk_lm_options* opt, const pk_ik_c
 // image, so the call needs no allocation at all.
 // ---------------------------------------------------------------------------
 
-#include <mutex>
-
 #define PK_STATIC_QUEUE_INTS 64  // 256 bytes; one call needs 2
 
 namespace {
@@ -1701,23 +1946,20 @@ namespace {
 // Loaded with the library on every GPU that runs it and kept until exit.
 static __device__ __align__(256) int32_t g_static_queue[PK_STATIC_QUEUE_INTS];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_static_mutex;
-int32_t* g_static_ptr[kMaxDevices] = {};
+constexpr int kStaticQueueNeeded = 2;  // item counters of the two persistent kernels
+static_assert(kStaticQueueNeeded <= PK_STATIC_QUEUE_INTS, "the static queue area is too small");
 
-// Device address of g_static_queue on the current device, looked up once per
-// device (host code only sees a stand-in for the symbol, never its address).
+// Device address of g_static_queue in the current context.  Host code only
+// sees a stand-in for the symbol, so the address is looked up with
+// cudaGetSymbolAddress, which allocates nothing.  It is looked up on every
+// call rather than cached: the module is loaded once per context, so after
+// cudaDeviceReset, or in another context on the same device, the array sits
+// at another address.  The first call in a context loads the module, which
+// is why that call should come before any stream capture.
 int static_queue_address(int32_t** out) {
-  int dev = 0;
-  if (int s = cuda_status(cudaGetDevice(&dev), "cudaGetDevice")) return s;
-  PK_CHECK_CAP(dev >= 0 && dev < kMaxDevices, "device %d beyond the %d devices this entry supports", dev, kMaxDevices);
-  std::lock_guard<std::mutex> lock(g_static_mutex);
-  if (!g_static_ptr[dev]) {
-    void* p = nullptr;
-    if (int s = cuda_status(cudaGetSymbolAddress(&p, g_static_queue), "cudaGetSymbolAddress")) return s;
-    g_static_ptr[dev] = static_cast<int32_t*>(p);
-  }
-  *out = g_static_ptr[dev];
+  void* p = nullptr;
+  if (int s = cuda_status(cudaGetSymbolAddress(&p, g_static_queue), "cudaGetSymbolAddress")) return s;
+  *out = static_cast<int32_t*>(p);
   return PK_OK;
 }
 
@@ -1727,9 +1969,6 @@ extern "C" int pk_ik_batch_static(void* stream, const pk_lm_options* opt, const 
                                   int32_t n_classes, const float* world_spheres, const float* world_capsules,
                                   const float* world_boxes, const float* world_halfspaces, int32_t Ms, int32_t Mc,
                                   int32_t Mb, int32_t Mh, const int32_t* items, int32_t n_items, int32_t blocks) {
-  const int needed = 2;  // item counters of the two persistent kernels
-  PK_CHECK_CAP(needed <= PK_STATIC_QUEUE_INTS, "the call needs %d queue counters, the static area holds %d", needed,
-               PK_STATIC_QUEUE_INTS);
   int32_t* queue = nullptr;
   if (int s = static_queue_address(&queue)) return s;
   // pk_ik_batch clears the counters with an async memset on `stream` before its launches

@@ -4,6 +4,7 @@ three times and synchronises, so a profiler can skip the first launches and
 capture one warm launch.
 
     python -m pyroffi_b200.profile_cases lm          # seed-group LM, 256 x 128 seeds, 30 iterations
+    python -m pyroffi_b200.profile_cases lm 1 128    # the same with 1 lane per seed, 128 seeds per block
     python -m pyroffi_b200.profile_cases fkc1        # fused FK + collision, 65,536 configs, [B, K, M] output
     python -m pyroffi_b200.profile_cases fkc5        # fused FK + collision, 4,096 configs of the sweep robot, [B, N, M]
     python -m pyroffi_b200.profile_cases wide        # warp-per-seed LM, 15-DOF bimanual, 64 problems x 64 seeds
@@ -26,14 +27,15 @@ import torch
 from . import workloads as W
 
 
-def _lm():
+def _lm(tps=0, spb=0):
     from .ik import BatchIkSolver
     w = W.ik(P=256, Sd=128)
     dev = torch.device("cuda:0")
     s = BatchIkSolver(w.model, w.target_link, spheres=w.spheres, world=w.world, self_pairs=w.self_pairs,
                       max_iter=w.max_iter, lambda_init=w.lambda_init, lambda_down=w.lambda_down,
                       lambda_up=w.lambda_up, collision_weight=w.collision_weight,
-                      collision_margin=w.collision_margin, device=dev)
+                      collision_margin=w.collision_margin, threads_per_seed=tps, seeds_per_block=spb,
+                      device=dev)
     tg, sd = torch.as_tensor(w.target_T, device=dev), torch.as_tensor(w.seeds, device=dev)
     return lambda: s.run_lm(tg, sd)
 
@@ -137,10 +139,10 @@ CASES = {"lm": _lm, "fkc1": lambda: _fkc(65536, False), "fkc5": lambda: _fkc(409
 
 def main(argv=None) -> int:
     argv = sys.argv[1:] if argv is None else argv
-    if len(argv) != 1 or argv[0] not in CASES:
+    if not argv or argv[0] not in CASES or (len(argv) > 1 and argv[0] != "lm") or len(argv) > 3:
         print(__doc__)
         return 2
-    fn = CASES[argv[0]]()
+    fn = CASES[argv[0]](*map(int, argv[1:]))
     for _ in range(3):
         fn()
     torch.cuda.synchronize()

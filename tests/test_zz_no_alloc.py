@@ -66,7 +66,10 @@ def test_static_scratch_entry_matches_regular_entry_twice():
             torch.testing.assert_close(b.out_err[c], ref_err[c], rtol=0, atol=0)
 
 
-def test_static_scratch_entry_rejects_bad_arguments():
+def test_static_scratch_entry_forwards_argument_checks():
+    """The entry validates its arguments as pk_ik_batch does: 9 classes (more
+    than the batch supports) is refused before any launch, and the outputs
+    stay untouched."""
     w = W.mixed_ik(n_problems=8, seeds_range=(4, 8))
     b = MixedIkBatch(w.classes, w.world, device=DEV)
     b.prepare(w.problem_class, w.n_seeds)
