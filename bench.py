@@ -359,7 +359,7 @@ def run_ours(args):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": LM_DRAM_BYTES_PER_LAUNCH,
-                         "traffic_unit": "bytes per launch (ncu dram__bytes_read+write, profiles/lm_kernel_ik_256x128.md)",
+                         "traffic_unit": "bytes per launch (ncu dram__bytes_read+write, one capture of this kernel)",
                          "kernel": "lm_kernel<8,1,2,2>",
                          "peak_source": "measured FP32 FMA microbenchmark (pk_fp32_fma_peak), this run",
                          "flop_per_seed_iter": FLOP_PER_SEED_ITER,

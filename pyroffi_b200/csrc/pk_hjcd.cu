@@ -25,10 +25,12 @@
 //
 // B200 mapping.  Coarse: one thread per seed, grid (seed blocks, problems),
 // robot, limits, world and robot spheres in shared memory, joint poses in
-// per-thread shared slots.  Refinement: one warp per problem, one lane per
-// refinement seed (32 at a time); the problem's stop flag is a warp vote, so
-// every seed of a problem stops at the same iteration and results do not
-// depend on scheduling (the reference polls a global flag across blocks).
+// per-thread shared slots.  Refinement: one 128-thread block per problem,
+// four lanes per refinement seed (32 seeds at a time; the four lanes split
+// the collision penalty); the problem's stop flag is a block vote
+// (__syncthreads_or), so every seed of a problem stops at the same iteration
+// and results do not depend on scheduling (the reference polls a global flag
+// across blocks).
 #include "pk_seed_ik.cuh"
 
 namespace pk {

@@ -17,6 +17,7 @@ HERE = Path(__file__).resolve().parent
 sys.path.insert(0, str(HERE.parent.parent))
 
 from pyroffi_b200.urdf import load_urdf  # noqa: E402
+from oracle.refpath import reference_root  # noqa: E402
 
 FIELDS = ("twists", "parent_tf", "parent_idx", "act_idx", "mimic_mul", "mimic_off", "mimic_act_idx",
           "parent_joint_indices", "lower", "upper", "topo_inv")
@@ -35,7 +36,10 @@ def panda_arrays(ref: Path) -> dict:
 
 
 def main(argv) -> int:
-    ref = Path(argv[1]) if len(argv) > 1 else Path("/root/reference")
+    ref = Path(argv[1]) if len(argv) > 1 else reference_root()
+    if ref is None:
+        print("reference checkout not found: pass its root or set PYROFFI_REF", file=sys.stderr)
+        return 1
     np.savez_compressed(HERE / "robots" / "panda.npz", **panda_arrays(ref))
     print("wrote", HERE / "robots" / "panda.npz")
     return 0

@@ -14,9 +14,11 @@ import pytest
 from scipy.spatial.transform import Rotation
 
 from oracle import kinematics as okin
+from oracle.refpath import reference_root
 from pyroffi_b200.urdf import load_urdf, read_srdf_disabled_pairs
 
-RES = Path("/root/reference/resources")
+_REF = reference_root()
+RES = _REF / "resources" if _REF is not None else Path("/nonexistent")
 pytestmark = pytest.mark.skipif(not RES.is_dir(), reason="the reference checkout's resources are not present")
 ROBOTS = sorted(str(p) for p in RES.glob("*/*_spherized*.urdf") if "ridgeback" not in p.name) if RES.is_dir() else []
 
