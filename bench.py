@@ -71,61 +71,22 @@ def dist_env():
 # ---------------------------------------------------------------------------
 
 def cpu_port_lib():
-    import ctypes as C
+    from oracle import cpu_port
 
-    so = ROOT / "oracle" / "_build" / "libpk_cpu.so"
-    if not so.exists():
-        subprocess.run(["make", "-C", str(ROOT / "oracle"), "cpu"], check=True, capture_output=True)
-    lib = C.CDLL(str(so))
-    lib.pk_cpu_max_threads.restype = C.c_int
-    return lib
+    return cpu_port.load()
 
 
 def cpu_solve(lib, w, p0, n_prob, n_threads):
     """Run the CPU port on problems [p0, p0+n_prob); returns (seconds, cfgs, errs)."""
-    import ctypes as C
+    from oracle import cpu_port
 
-    m = w.model
-    fp = lambda a: np.ascontiguousarray(a).ctypes.data_as(C.c_void_p)  # noqa: E731
-    keep = []
-
-    def arr(a, dt):
-        a = np.ascontiguousarray(a, dtype=dt)
-        keep.append(a)
-        return a.ctypes.data_as(C.c_void_p)
-
-    seeds = np.ascontiguousarray(w.seeds[p0:p0 + n_prob])
-    tgt = np.ascontiguousarray(w.target_T[p0:p0 + n_prob, None, :])
-    out_cfg = np.zeros_like(seeds)
-    out_err = np.zeros(seeds.shape[:2], np.float32)
-    tj = np.asarray([m.link_joint(w.target_link)], np.int32)
-    anc = m.ancestor_mask(w.target_link)[None]
-    f32, i32 = np.float32, np.int32
-    t0 = time.perf_counter()
-    st = lib.pk_cpu_ls_ik(
-        fp(seeds), arr(m.twists, f32), arr(m.parent_tf, f32), arr(m.parent_idx, i32), arr(m.act_idx, i32),
-        arr(m.mimic_mul, f32), arr(m.mimic_off, f32), arr(m.mimic_act_idx, i32), arr(m.topo_inv, i32),
-        arr(tj, i32), arr(anc, i32), fp(tgt), arr(w.spheres_local, f32), arr(w.sphere_joint, i32),
-        arr(w.world.spheres, f32), arr(w.self_pairs[:, 0], i32), arr(w.self_pairs[:, 1], i32),
-        arr(m.lower, f32), arr(m.upper, f32), arr(np.zeros(m.n_act), i32), fp(out_cfg), fp(out_err),
-        C.c_int(n_prob), C.c_int(seeds.shape[1]), C.c_int(m.n_act), C.c_int(m.n_joints), C.c_int(1),
-        C.c_int(len(w.spheres_local)), C.c_int(len(w.world.spheres)), C.c_int(len(w.self_pairs)),
-        C.c_int(w.max_iter), C.c_float(w.pos_weight), C.c_float(w.ori_weight), C.c_float(w.lambda_init),
-        C.c_float(w.lambda_down), C.c_float(w.lambda_up), C.c_float(1e-8), C.c_float(1e-8), C.c_int(1),
-        C.c_float(w.collision_weight), C.c_float(w.collision_margin), C.c_int(n_threads))
-    dt = time.perf_counter() - t0
-    if st != 0:
-        raise RuntimeError(f"pk_cpu_ls_ik failed ({st})")
-    return dt, out_cfg, out_err
+    return cpu_port.ls_ik(lib, w, p0, n_prob, n_threads)
 
 
 def cpu_success(w, p0, cfgs, errs):
-    from oracle import lm as olm
+    from oracle import cpu_port
 
-    win, _ = olm.select_winner(cfgs.astype(np.float64), errs)
-    pe, re = olm.pose_errors(win, w.target_T[p0:p0 + len(cfgs)].astype(np.float64), w.model.as_dict(),
-                             w.model.link_joint(w.target_link))
-    return float(np.mean((pe < w.pos_tol) & (re < w.rot_tol)))
+    return float(np.mean(cpu_port.success(w, p0, cfgs, errs)))
 
 
 def run_reference(args):

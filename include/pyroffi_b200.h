@@ -147,6 +147,10 @@ typedef struct pk_lm_options {
                               trial; 16, 32 = warp-per-seed body with that many lanes per seed */
   int32_t seeds_per_block;  /* 0 = choose automatically */
   int32_t lanes_per_wide_seed; /* warp-per-seed body: lanes per seed, 16 (0 = default) or 32 */
+  int32_t fp32_solve;       /* 0 = FP64 normal equations and Cholesky (as the reference); 1 = FP32, with one FP64
+                              iterative-refinement step when the squared ratio of the largest to the smallest
+                              Cholesky pivot exceeds 1e6 (seed-group kernel: n_act <= 16, n_ee <= 2,
+                              threads_per_seed 0 or 1; PK_ERR_INVALID elsewhere, pk_ik_batch included) */
 } pk_lm_options;
 
 /*
@@ -283,7 +287,10 @@ int pk_ik_verify_select(void* stream, const float* cfgs, const float* errs, cons
  *   dist_bkm[B, K, M]    per-sphere distances with K = S*N, k = s*N + n, in
  *                        the layout of pk_collision_world_sphere,
  *   dist_bnm[B, N, M]    per-link minimum over the link's spheres, in the
- *                        layout of pk_collision_world_sphere_reduced.
+ *                        layout of pk_collision_world_sphere_reduced,
+ *   sphere_centers[B, K, 4]  each sphere's world centre and radius (the
+ *                        output of at_config), k = s*N + n as in dist_bkm,
+ *                        16-byte aligned; padded spheres keep r < 0.
  */
 int pk_fk_sphere_collision(void* stream, const float* cfg, const float* twists,
                            const float* parent_tf, const int32_t* parent_idx,
@@ -293,7 +300,7 @@ int pk_fk_sphere_collision(void* stream, const float* cfg, const float* twists,
                            const float* world_spheres, const float* world_capsules,
                            const float* world_boxes, const float* world_halfspaces,
                            float* min_dist, float* link_poses, float* dist_bkm, float* dist_bnm,
-                           int64_t batch,
+                           float* sphere_centers, int64_t batch,
                            int32_t n_act, int32_t n_joints, int32_t n_links, int32_t S, int32_t Ms,
                            int32_t Mc, int32_t Mb, int32_t Mh);
 
@@ -374,15 +381,36 @@ int pk_chomp_line_select(void* stream, const float* trial_costs, const float* co
                          int32_t early_stop_patience, int64_t B, int32_t T, int32_t n_act);
 
 /*
- * Health check (no reference counterpart): *count = the number of thread
- * blocks, since the library was loaded, whose bounded wait for the TMA copy
- * of the obstacle arrays into shared memory gave up, on the current device.
- * Such a block counts itself, waits once more and copies the arrays with
- * plain loads, so its results stay right; a non-zero count means the copy
- * engine did not complete a copy in time.  The counters are read with
- * synchronous copies, so call this between workloads, not inside one.
+ * Health check (no reference counterpart; the reference's kernels do not wait
+ * on the copy engine).  *count = the number of thread blocks, since the
+ * library was loaded or since pk_stage_wait_reset, whose bounded wait for the
+ * TMA copy of the obstacle arrays into shared memory ran out of time, on the
+ * current device.  Returns PK_OK when that number is 0 and PK_ERR_TIMEOUT
+ * otherwise.  Such a block counts itself, waits once more and copies the
+ * arrays with plain loads, so its own results stay right; if that second
+ * wait runs out too, the block finishes with the copy possibly in flight,
+ * the copy may land in a later block's shared memory, and pk_last_error()
+ * then says that outputs since then are untrusted.  Each wait is limited by
+ * the GPU's global timer (1 s unless pk_stage_wait_configure says otherwise).
+ * The counters are read with synchronous copies, so call this between
+ * workloads, not inside one.
  */
 int pk_stage_wait_timeouts(uint64_t* count);
+
+/* Zeroes the counters behind pk_stage_wait_timeouts on the current device
+ * (synchronous; no reference counterpart). */
+int pk_stage_wait_reset(void);
+
+/*
+ * Test hook and time limit of the bounded wait (no reference counterpart).
+ * force_timeout = 1 makes every block of the kernels that stage the obstacle
+ * arrays skip the TMA copy, wait out the limit and take the plain-load path
+ * (nothing is then in flight, so results equal the normal path's bit for
+ * bit); 0 restores the copy.  limit_ns bounds each wait by the GPU's global
+ * timer (<= 0: 1 s).  Synchronous; affects later launches on the current
+ * device, in every thread.
+ */
+int pk_stage_wait_configure(int32_t force_timeout, int64_t limit_ns);
 
 /* SCO trajectory optimisation settings: the fields of ScoTrajOptConfig
  * (src/pyroffi/optimization_engines/_sco_optimization.py:52-104, defaults in

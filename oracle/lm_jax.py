@@ -61,14 +61,39 @@ def body_log_residual(T_joints, target_jnts, target_T):
 
 def collision_constraint(model, spheres_local, sphere_joint, ws=None, self_i=None, self_j=None, margin=0.02):
     """c(q) = sqrt(sum of hinge² terms) [S]: with weight w_c, ``w_c * c²`` is the
-    CUDA variant's penalty ``w_c * sum hinge²`` on the same spheres and pairs."""
+    CUDA variant's penalty ``w_c * sum hinge²`` (``collision.lm_penalty``) on
+    the same robot spheres, world spheres and sphere pairs, evaluated with
+    sphere-only arithmetic (the world here holds spheres only)."""
     ws = np.zeros((0, 4)) if ws is None else np.asarray(ws, np.float64)
-    z7, z15, z6 = np.zeros((0, 7)), np.zeros((0, 15)), np.zeros((0, 6))
+    sl = np.asarray(spheres_local, np.float64)
+    sj = np.asarray(sphere_joint)
+    valid = (sj >= 0) & (sj < model["n_joints"])
+    r_all = sl[:, 3]
+    si = None if self_i is None or len(self_i) == 0 else np.asarray(self_i)
+    sjj = None if si is None else np.asarray(self_j)
+    wo = np.ascontiguousarray(ws[:, :3])
+    o2 = np.sum(wo * wo, axis=-1)
+    rsum = r_all[valid][:, None] + ws[None, :, 3]                   # [n_valid, Ms]
+    reach2 = np.where(rsum + margin > 0, (rsum + margin) ** 2 * (1 + 1e-9) + 1e-12, 0.0)
 
     def c(q):
         Tj = _fk(q, model)
-        pen = collision.lm_penalty(Tj, spheres_local, sphere_joint, ws, z7, z15, z6, margin, 1.0, self_i, self_j)
-        return np.sqrt(np.maximum(pen, 0.0))
+        P = collision.robot_sphere_world(Tj, sl, np.where(valid, sj, 0))        # [S, n_rs, 3]
+        pen = np.zeros(P.shape[0])
+        if len(ws):
+            Pv = P[:, valid]
+            # |p - o|^2 = |p|^2 + |o|^2 - 2 p.o, the cross term as one matrix product
+            d2 = np.sum(Pv * Pv, axis=-1)[..., None] + o2[None, None, :] - 2.0 * (Pv @ wo.T)
+            # only pairs closer than r + r_o + margin have a non-zero hinge
+            s_idx, k_idx, m_idx = np.nonzero(d2 < reach2[None])
+            d = np.sqrt(np.maximum(d2[s_idx, k_idx, m_idx], 0.0)) - rsum[k_idx, m_idx]
+            h = np.minimum(d - margin, 0.0)
+            pen += np.bincount(s_idx, weights=h * h, minlength=P.shape[0])
+        if si is not None:
+            d = np.sqrt(np.sum((P[:, si] - P[:, sjj]) ** 2, axis=-1)) - (r_all[si] + r_all[sjj])
+            h = np.minimum(d - margin, 0.0)
+            pen += np.sum(h * h, axis=-1)
+        return np.sqrt(pen)
     return c
 
 

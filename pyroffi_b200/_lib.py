@@ -46,6 +46,7 @@ class LmOptions(C.Structure):
         ("threads_per_seed", _i32),
         ("seeds_per_block", _i32),
         ("lanes_per_wide_seed", _i32),
+        ("fp32_solve", _i32),
     ]
 
 
@@ -61,7 +62,7 @@ SIGNATURES: dict[str, list] = {
     + [_i32] * 10,
     "pk_ls_ik_ex": [_p, C.POINTER(LmOptions)] + [_p] * 25 + [_i32] * 11,
     "pk_ik_verify_select": [_p] * 4 + [_f32] + [_p] * 10 + [_f32, _f32] + [_p] * 4 + [_i32] * 5,
-    "pk_fk_sphere_collision": [_p] * 20 + [_i64] + [_i32] * 8,
+    "pk_fk_sphere_collision": [_p] * 21 + [_i64] + [_i32] * 8,
     "pk_ik_batch": [_p, C.POINTER(LmOptions), C.c_void_p, _i32] + [_p] * 4 + [_i32] * 4 + [_p, _i32, _p, _i32],
     "pk_ik_batch_static": [_p, C.POINTER(LmOptions), C.c_void_p, _i32] + [_p] * 4 + [_i32] * 4 + [_p, _i32, _i32],
     "pk_fp32_fma_peak": [_p, _p, _i32, _i32],
@@ -73,6 +74,8 @@ SIGNATURES: dict[str, list] = {
                       + [_i32] * 10,
     "pk_chomp_direction": [_p, _p, _p, _i64, _i32, _i32, _i32, _f32, _f32, _f32, _i32],
     "pk_stage_wait_timeouts": [_p],
+    "pk_stage_wait_reset": [],
+    "pk_stage_wait_configure": [_i32, _i64],
     "pk_chomp_line_trials": [_p, _p, _p, _p, _i32, _f32, _p, _p, _p, _i64, _i32, _i32],
     "pk_chomp_line_select": [_p, _p, _p, _p, _p, _p, _p, _i32, _f32, _i32, _i64, _i32, _i32],
     "pk_sco_linearize": [_p, C.c_void_p] + [_p] * 20 + [_i64] + [_i32] * 9,

@@ -25,11 +25,12 @@ class FkCollisionResult:
     link_poses: torch.Tensor | None   # [B, N, 7]
     dist_bkm: torch.Tensor | None     # [B, S*N, M]
     dist_bnm: torch.Tensor | None = None  # [B, N, M]
+    sphere_centers: torch.Tensor | None = None  # [B, S*N, 4] world centre + radius
 
 
 def fk_sphere_collision(robot: DeviceRobot, spheres: DeviceSpheres, world: DeviceWorld,
                         cfg: torch.Tensor, *, min_dist: bool = True, link_poses: bool = True,
-                        per_sphere: bool = False, per_link: bool = False,
+                        per_sphere: bool = False, per_link: bool = False, sphere_centers: bool = False,
                         out: FkCollisionResult | None = None) -> FkCollisionResult:
     dev = cfg.device
     c = f32(cfg)
@@ -42,10 +43,11 @@ def fk_sphere_collision(robot: DeviceRobot, spheres: DeviceSpheres, world: Devic
             torch.empty(B, dtype=torch.float32, device=dev) if min_dist else None,
             torch.empty((B, N, 7), dtype=torch.float32, device=dev) if link_poses else None,
             torch.empty((B, S * N, M), dtype=torch.float32, device=dev) if per_sphere else None,
-            torch.empty((B, N, M), dtype=torch.float32, device=dev) if per_link else None)
+            torch.empty((B, N, M), dtype=torch.float32, device=dev) if per_link else None,
+            torch.empty((B, S * N, 4), dtype=torch.float32, device=dev) if sphere_centers else None)
     _lib.call("pk_fk_sphere_collision", stream_ptr(dev), ptr(c), *[ptr(t) for t in robot.fk_args()],
               ptr(robot.parent_joint_indices), ptr(spheres.link_spheres),
               *[ptr(t) for t in world.arrays()], ptr(out.min_dist), ptr(out.link_poses),
-              ptr(out.dist_bkm), ptr(out.dist_bnm), B, robot.model.n_act, robot.model.n_joints, N, S,
+              ptr(out.dist_bkm), ptr(out.dist_bnm), ptr(out.sphere_centers), B, robot.model.n_act, robot.model.n_joints, N, S,
               Ms, Mc, Mb, Mh)
     return out

@@ -31,26 +31,44 @@ int set_smem_limit(const void* kernel, size_t bytes) {
                      "cudaFuncSetAttribute");
 }
 
-// Readers of the per-file counters of bounded waits that gave up, one per
-// source file that stages the world; filled at library load.
-static std::vector<int (*)(unsigned long long*)>& timeout_readers() {
-  static std::vector<int (*)(unsigned long long*)> v;
+// The bounded-wait hooks of every source file that stages the world; filled
+// at library load.
+static std::vector<StageWaitHooks>& stage_wait_hooks() {
+  static std::vector<StageWaitHooks> v;
   return v;
 }
 
-int register_timeout_reader(int (*reader)(unsigned long long*)) {
-  timeout_readers().push_back(reader);
-  return (int)timeout_readers().size();
+int register_stage_wait_hooks(StageWaitHooks h) {
+  stage_wait_hooks().push_back(h);
+  return (int)stage_wait_hooks().size();
 }
 
 }  // namespace pk
 
 extern "C" int pk_stage_wait_timeouts(uint64_t* count) {
   PK_CHECK_ARG(count != nullptr, "null count");
-  unsigned long long acc = 0;
-  for (auto reader : pk::timeout_readers())
-    if (int s = reader(&acc)) return s;
-  *count = acc;
+  unsigned long long gave_up = 0, abandoned = 0;
+  for (const auto& h : pk::stage_wait_hooks())
+    if (int s = h.read(&gave_up, &abandoned)) return s;
+  *count = gave_up;
+  if (gave_up == 0) return PK_OK;
+  pk::set_error("%llu block(s) gave up waiting for the TMA copy of the obstacle arrays and loaded them plainly; "
+                "%llu of them finished with the copy possibly in flight%s",
+                gave_up, abandoned, abandoned ? ": outputs since then are untrusted" : "");
+  return PK_ERR_TIMEOUT;
+}
+
+extern "C" int pk_stage_wait_reset(void) {
+  for (const auto& h : pk::stage_wait_hooks())
+    if (int s = h.reset()) return s;
+  return PK_OK;
+}
+
+extern "C" int pk_stage_wait_configure(int32_t force_timeout, int64_t limit_ns) {
+  PK_CHECK_ARG(force_timeout == 0 || force_timeout == 1, "force_timeout must be 0 or 1");
+  const unsigned long long lim = limit_ns > 0 ? (unsigned long long)limit_ns : 1000000000ull;
+  for (const auto& h : pk::stage_wait_hooks())
+    if (int s = h.set((unsigned)force_timeout, lim)) return s;
   return PK_OK;
 }
 

@@ -386,6 +386,15 @@ int cuda_status(cudaError_t e, const char* where);
 // Raises the kernel's dynamic shared-memory limit when `bytes` exceeds the
 // 48 KB default (on the current device).
 int set_smem_limit(const void* kernel, size_t bytes);
+// Host hooks of the bounded wait in the obstacle staging of one source file
+// (pk_obstacles.cuh): read its counters (adding to the sums), zero them, set
+// the test hook and the time limit; each on the current device.
+struct StageWaitHooks {
+  int (*read)(unsigned long long* gave_up, unsigned long long* abandoned);
+  int (*reset)();
+  int (*set)(unsigned int force, unsigned long long limit_ns);
+};
+int register_stage_wait_hooks(StageWaitHooks h);
 }  // namespace pk
 
 #define PK_CHECK_ARG(cond, ...)                 \

@@ -63,6 +63,7 @@ struct FusedArgs {
   float* link_poses;        // [B, N, 7] or null
   float* dist_bkm;          // [B, K, M] or null
   float* dist_bnm;          // [B, N, M] or null (min over each link's spheres)
+  float* centres_out;       // [B, K, 4] or null (world centre and radius, k = s*N + n)
   long long batch;
   int N, S;
   int cpb;                  // configurations per block
@@ -430,6 +431,14 @@ __global__ void __launch_bounds__(256, MINB) fk_sphere_collision_kernel(FusedArg
       d[h] = w.x; d[2 + h] = w.y; d[4 + h] = w.z; d[6 + h] = -w.w;
     }
   };
+  if (a.centres_out) {
+    float4* dst = reinterpret_cast<float4*>(a.centres_out) + b0 * K;
+    for (int g = tid; g < nc * K; g += T) {
+      const int c = g / K, k = g - c * K;
+      const int s = k / N, n = k - s * N;
+      __stcs(dst + g, world_centre(c, n, s));
+    }
+  }
   const bool per_link = a.dist_bnm || !a.dist_bkm;
   if (per_link)
     for (int n = tid; n < N; n += T) {
@@ -513,7 +522,8 @@ extern "C" int pk_fk_sphere_collision(
     const float* mimic_off, const int32_t* mimic_act_idx, const int32_t* topo_inv,
     const int32_t* parent_joint_indices, const float* link_spheres, const float* world_spheres,
     const float* world_capsules, const float* world_boxes, const float* world_halfspaces,
-    float* min_dist, float* link_poses, float* dist_bkm, float* dist_bnm, int64_t batch, int32_t n_act,
+    float* min_dist, float* link_poses, float* dist_bkm, float* dist_bnm, float* sphere_centers, int64_t batch,
+    int32_t n_act,
     int32_t n_joints, int32_t n_links, int32_t S, int32_t Ms, int32_t Mc, int32_t Mb,
     int32_t Mh) {
   PK_CHECK_ARG(batch >= 0 && n_links >= 0 && S >= 0 && Ms >= 0 && Mc >= 0 && Mb >= 0 && Mh >= 0,
@@ -529,6 +539,8 @@ extern "C" int pk_fk_sphere_collision(
                "null world buffer");
   PK_CHECK_ARG(link_spheres == nullptr || (reinterpret_cast<uintptr_t>(link_spheres) & 15) == 0,
                "link_spheres must be 16-byte aligned");
+  PK_CHECK_ARG(sphere_centers == nullptr || (reinterpret_cast<uintptr_t>(sphere_centers) & 15) == 0,
+               "sphere_centers must be 16-byte aligned");
   WorldArgs w{world_spheres, world_capsules, world_boxes, world_halfspaces, Ms, Mc, Mb, Mh};
   const int K = n_links * S;
   const int threads = 256;
@@ -568,6 +580,7 @@ extern "C" int pk_fk_sphere_collision(
   a.link_poses = link_poses;
   a.dist_bkm = dist_bkm;
   a.dist_bnm = dist_bnm;
+  a.centres_out = sphere_centers;
   a.batch = batch;
   a.N = n_links;
   a.S = S;

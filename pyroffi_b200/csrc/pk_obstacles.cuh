@@ -45,37 +45,70 @@ struct ObsView {
   int Ms, Mc, Mb, Mh;
 };
 
-// Blocks whose wait for the TMA copy of stage_world gave up, in the kernels
-// of this source file since the library was loaded (one counter per file;
-// pk_stage_wait_timeouts sums them).  It stays 0 unless the copy engine
-// fails to complete a copy.
-static __device__ unsigned int g_stage_wait_timeouts;
+// State of the bounded wait of stage_world in the kernels of this source
+// file (one copy per file; the pk_stage_wait_* entry points visit them all):
+//   gave_up    blocks whose first wait for the TMA copy ran out of time;
+//   abandoned  of those, blocks whose second wait ran out too, so that they
+//              finished with a copy possibly still in flight;
+//   force      test hook: when set, no copy is issued and every wait runs out;
+//   limit_ns   the time limit of each wait, by %globaltimer (default 1 s).
+struct StageWaitState {
+  unsigned int gave_up;
+  unsigned int abandoned;
+  unsigned int force;
+  unsigned int pad;
+  unsigned long long limit_ns;
+};
+static __device__ StageWaitState g_stage_wait = {0u, 0u, 0u, 0u, 1000000000ull};
 
-// Host side: adds this file's counter, on the current device, to *acc.
-int register_timeout_reader(int (*reader)(unsigned long long*));
+// Host side: this file's hooks (StageWaitHooks) for its own g_stage_wait.
 namespace {
-int read_stage_wait_timeouts(unsigned long long* acc) {
-  unsigned int v = 0;
-  if (int s = cuda_status(cudaMemcpyFromSymbol(&v, g_stage_wait_timeouts, sizeof(v)), "stage wait counter"))
-    return s;
-  *acc += v;
+int stage_wait_read(unsigned long long* gave_up, unsigned long long* abandoned) {
+  StageWaitState v{};
+  if (int s = cuda_status(cudaMemcpyFromSymbol(&v, g_stage_wait, sizeof(v)), "stage wait state")) return s;
+  *gave_up += v.gave_up;
+  *abandoned += v.abandoned;
   return PK_OK;
 }
-[[maybe_unused]] const int kStageWaitReader = register_timeout_reader(read_stage_wait_timeouts);
+int stage_wait_reset() {
+  const unsigned int z[2] = {0u, 0u};
+  return cuda_status(cudaMemcpyToSymbol(g_stage_wait, z, sizeof(z)), "stage wait reset");
+}
+int stage_wait_set(unsigned int force, unsigned long long limit_ns) {
+  if (int s = cuda_status(cudaMemcpyToSymbol(g_stage_wait, &force, sizeof(force),
+                                             offsetof(StageWaitState, force)), "stage wait force"))
+    return s;
+  return cuda_status(cudaMemcpyToSymbol(g_stage_wait, &limit_ns, sizeof(limit_ns),
+                                        offsetof(StageWaitState, limit_ns)), "stage wait limit");
+}
+[[maybe_unused]] const int kStageWaitHooks =
+    register_stage_wait_hooks(StageWaitHooks{stage_wait_read, stage_wait_reset, stage_wait_set});
 }  // namespace
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 // Copies the obstacle arrays into shared memory at `dst` (16-byte aligned),
 // each array starting on a 16-byte boundary; called by every thread of the
 // block, and the caller synchronises afterwards.  The 16-byte-aligned bulk of
 // each array goes through the TMA bulk-copy engine: one thread issues
 // cp.async.bulk global -> shared with the completion counted in bytes on an
-// mbarrier, and every thread waits on that barrier.  The wait is bounded: a
-// thread that gives up counts the block in g_stage_wait_timeouts (once),
-// waits once more with the same bound for the copy in flight, and then loads
-// the bulk with plain loads itself, so the block's data is right either way
-// (a copy that lands late writes the same bytes).  An array whose source is
-// not 16-byte aligned, and the bytes past the last 16-byte multiple, are
-// copied with plain loads.
+// mbarrier, and every thread waits on that barrier for at most
+// g_stage_wait.limit_ns.  A thread whose wait runs out counts the block in
+// gave_up (thread 0 does), waits once more with the same limit, and then
+// loads the bulk with plain loads itself, so this block's data is right
+// either way (a copy that lands late writes the same bytes).  If the second
+// wait runs out too, the block counts itself in `abandoned` and finishes
+// with the copy possibly still in flight, which may then land in the shared
+// memory of a later block: pk_stage_wait_timeouts reports PK_ERR_TIMEOUT,
+// and the outputs of that launch and of later ones on the device are not to
+// be trusted.  With g_stage_wait.force set, no copy is issued (nothing is in
+// flight), the first wait runs out, and the block takes the plain-load path
+// without the second wait.  An array whose source is not 16-byte aligned,
+// and the bytes past the last 16-byte multiple, are copied with plain loads.
 __device__ inline ObsView stage_world(const WorldArgs& w, float* dst) {
   __shared__ __align__(8) unsigned long long s_bar;
   const float* src[4] = {w.spheres, w.capsules, w.boxes, w.halfspaces};
@@ -98,12 +131,14 @@ __device__ inline ObsView stage_world(const WorldArgs& w, float* dst) {
     for (int i = (int)(bulk[k] / 4) + tid; i < nf[k]; i += nth) d[k][i] = src[k][i];
   if (total > 0) {
     const unsigned bar = (unsigned)__cvta_generic_to_shared(&s_bar);
+    const bool force = *(volatile const unsigned int*)&g_stage_wait.force != 0u;
+    const unsigned long long limit = *(volatile const unsigned long long*)&g_stage_wait.limit_ns;
     if (tid == 0) {
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    if (tid == 0) {
+    if (tid == 0 && !force) {
       asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(total) : "memory");
 #pragma unroll
       for (int k = 0; k < 4; ++k)
@@ -116,17 +151,20 @@ __device__ inline ObsView stage_world(const WorldArgs& w, float* dst) {
     }
     auto wait = [&]() {
       unsigned done = 0;
-      for (int it = 0; it < (1 << 22) && !done; ++it)
+      const unsigned long long t0 = global_ns();
+      for (;;) {
         asm volatile(
             "{\n .reg .pred P;\n mbarrier.try_wait.parity.shared::cta.b64 P, [%1], 0;\n selp.u32 %0, 1, 0, P;\n}"
             : "=r"(done)
             : "r"(bar)
             : "memory");
+        if (done || global_ns() - t0 > limit) break;
+      }
       return done != 0;
     };
     if (!wait()) {
-      if (tid == 0) atomicAdd(&g_stage_wait_timeouts, 1u);
-      wait();
+      if (tid == 0) atomicAdd(&g_stage_wait.gave_up, 1u);
+      if (!force && !wait() && tid == 0) atomicAdd(&g_stage_wait.abandoned, 1u);
 #pragma unroll
       for (int k = 0; k < 4; ++k)
         for (int i = tid; i < (int)(bulk[k] / 4); i += nth) d[k][i] = src[k][i];

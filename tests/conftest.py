@@ -6,6 +6,7 @@ import pytest
 
 ROOT = Path(__file__).resolve().parents[1]
 sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "tests"))
 
 
 def pytest_configure(config):
@@ -19,6 +20,12 @@ def _has_gpu() -> bool:
         return torch.cuda.is_available()
     except Exception:
         return False
+
+
+def pytest_sessionfinish(session, exitstatus):
+    from error_report import write_if_requested
+
+    write_if_requested()
 
 
 def pytest_collection_modifyitems(config, items):

@@ -143,6 +143,8 @@ def test_trajectory_cost_validates_on_the_host(lib):
 def test_stage_wait_counter_rejects_null(lib):
     assert lib.pk_stage_wait_timeouts(None) == _lib.PK_ERR_INVALID
     assert b"null" in lib.pk_last_error()
+    assert lib.pk_stage_wait_configure(2, 0) == _lib.PK_ERR_INVALID
+    assert b"force_timeout" in lib.pk_last_error()
 
 
 def test_every_declaration_cites_the_reference_or_says_it_has_none():

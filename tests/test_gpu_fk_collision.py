@@ -1,6 +1,7 @@
 """GPU parity: FK, collision drop-ins and the fused FK->collision kernel
-against the FP64 oracle (tolerances: FK 1e-5 m / 1e-5 rad, distances 1e-5 m
-plus FP32 rounding of the inputs' magnitude)."""
+against the FP64 oracle (tolerances: FK 1e-5 m / 1e-5 rad, sphere centres
+1e-5 m, distances 1e-5 m).  Each test records the largest error it saw
+(``error_report``)."""
 
 import numpy as np
 import pytest
@@ -16,6 +17,7 @@ from pyroffi_b200.cuda_kernels import (collision_self_capsule, collision_self_sp
                                        collision_world_capsule, collision_world_sphere,
                                        collision_world_sphere_reduced, fk_cuda)
 from pyroffi_b200.device import DeviceRobot, DeviceSpheres, DeviceWorld
+from error_report import assert_distances, record
 
 pytestmark = pytest.mark.gpu
 DEV = "cuda:0"
@@ -57,8 +59,11 @@ def test_fk_cuda_matches_oracle(golden, name, B):
     out = run_fk(g, cfg)
     ref = oracle_fk(g, cfg)
     assert out.shape == ref.shape
-    assert np.abs(out[..., 4:] - ref[..., 4:]).max() < POS_TOL
-    assert rot_angle(out[..., :4], ref[..., :4]).max() < ROT_TOL
+    pe, re = np.abs(out[..., 4:] - ref[..., 4:]).max(), rot_angle(out[..., :4], ref[..., :4]).max()
+    record("FK joint position (fk_cuda)", pe, f"{name} B={B}", "m")
+    record("FK joint rotation (fk_cuda)", re, f"{name} B={B}", "rad")
+    assert pe < POS_TOL
+    assert re < ROT_TOL
 
 
 def test_fk_cuda_reproduces_reference_golden(golden):
@@ -128,12 +133,12 @@ def test_world_sphere_and_reduced(world_kind):
     out = collision_world_sphere(tt(centers), tt(radii), *wt).cpu().numpy()
     ref = oc.world_sphere(c_bsn.reshape(B, K, 3).astype(np.float64), radii, *[x.astype(np.float64) for x in world])
     assert out.shape == ref.shape
-    np.testing.assert_allclose(out, ref, atol=2e-5, rtol=1e-6)
+    assert_distances(out, ref, quantity="signed distance (collision_world_sphere)", case=world_kind)
     red = collision_world_sphere_reduced(tt(centers), tt(radii), *wt, n=N).cpu().numpy()
     rref = oc.world_sphere_reduced(c_bsn.reshape(B, K, 3).astype(np.float64), radii,
                                    *[x.astype(np.float64) for x in world], N)
     assert red.shape == rref.shape
-    np.testing.assert_allclose(red, rref, atol=2e-5, rtol=1e-6)
+    assert_distances(red, rref, quantity="signed distance (collision_world_sphere_reduced)", case=world_kind)
 
 
 def test_world_capsule_robot():
@@ -151,7 +156,7 @@ def test_world_capsule_robot():
         oc.capsule_capsule(c[..., 0:3], c[..., 3:6], c[..., 6], wc[:, 0:3], wc[:, 3:6], wc[:, 6]),
         oc.capsule_box(c[..., 0:3], c[..., 3:6], c[..., 6], wb),
         oc.capsule_halfspace(c[..., 0:3], c[..., 3:6], c[..., 6], wh)], axis=-1)
-    np.testing.assert_allclose(out, ref, atol=3e-5, rtol=1e-5)
+    assert_distances(out, ref, quantity="signed distance (collision_world_capsule)")
 
 
 def test_self_sphere_and_capsule():
@@ -161,13 +166,13 @@ def test_self_sphere_and_capsule():
     pairs = np.array([(i, j) for i in range(N) for j in range(i)], np.int32)
     out = collision_self_sphere(tt(c), tt(r), tt(pairs[:, 0], torch.int32), tt(pairs[:, 1], torch.int32)).cpu().numpy()
     ref = oc.self_sphere_full(c.astype(np.float64), r.astype(np.float64), pairs[:, 0], pairs[:, 1])
-    np.testing.assert_allclose(out, ref, atol=2e-5, rtol=1e-6)
+    assert_distances(out, ref, quantity="signed distance (collision_self_sphere)")
     caps = np.concatenate([rng.uniform(-1, 1, (B, N, 6)), rng.uniform(0.02, 0.1, (B, N, 1))], -1).astype(np.float32)
     out = collision_self_capsule(tt(caps), tt(pairs[:, 0], torch.int32), tt(pairs[:, 1], torch.int32)).cpu().numpy()
     c64 = caps.astype(np.float64)
     ref = oc.capsule_capsule(c64[:, pairs[:, 0], 0:3], c64[:, pairs[:, 0], 3:6], c64[:, pairs[:, 0], 6],
                              c64[:, pairs[:, 1], 0:3], c64[:, pairs[:, 1], 3:6], c64[:, pairs[:, 1], 6])
-    np.testing.assert_allclose(out, ref, atol=3e-5, rtol=1e-5)
+    assert_distances(out, ref, quantity="signed distance (collision_self_capsule)")
     empty = collision_self_sphere(tt(c), tt(r), tt(np.zeros(0), torch.int32), tt(np.zeros(0), torch.int32))
     assert empty.shape == (B, 0)
 
@@ -203,13 +208,25 @@ def test_fused_fk_sphere_collision(case):
         world.spheres, world.capsules, world.boxes, world.halfspaces = mixed_world(rng, Ms=21, Mc=3, Mb=4, Mh=2)
         cfg = model.random_cfgs(rng, 77)
     res = fk_sphere_collision(DeviceRobot.upload(model, DEV), DeviceSpheres.upload(spheres, DEV),
-                              DeviceWorld.upload(world, DEV), tt(cfg), per_sphere=True)
+                              DeviceWorld.upload(world, DEV), tt(cfg), per_sphere=True, sphere_centers=True)
     links, bkm, dmin = fused_reference(model, spheres, world, cfg)
     lp = res.link_poses.cpu().numpy()
-    assert np.abs(lp[..., 4:] - links[..., 4:]).max() < POS_TOL
-    assert rot_angle(lp[..., :4], links[..., :4]).max() < ROT_TOL
-    np.testing.assert_allclose(res.dist_bkm.cpu().numpy(), bkm, atol=2e-5, rtol=1e-6)
-    np.testing.assert_allclose(res.min_dist.cpu().numpy(), dmin, atol=2e-5)
+    pe, re = np.abs(lp[..., 4:] - links[..., 4:]).max(), rot_angle(lp[..., :4], links[..., :4]).max()
+    record("FK link position (fused)", pe, case, "m")
+    record("FK link rotation (fused)", re, case, "rad")
+    assert pe < POS_TOL
+    assert re < ROT_TOL
+    # sphere centres (at_config), k = s*N + n, compared directly
+    c = se3.apply(links[:, :, None, :], spheres.centers.astype(np.float64))     # [B,N,S,3]
+    B, N, S = c.shape[:3]
+    ck = np.swapaxes(c, 1, 2).reshape(B, S * N, 3)
+    sc = res.sphere_centers.cpu().numpy()
+    cerr = np.abs(sc[..., :3] - ck).max()
+    record("sphere centre (fused, at_config)", cerr, case, "m")
+    assert cerr < POS_TOL
+    np.testing.assert_array_equal(sc[..., 3], np.broadcast_to(spheres.radii.T.reshape(-1), (B, S * N)))
+    assert_distances(res.dist_bkm.cpu().numpy(), bkm, quantity="signed distance (fused, per sphere)", case=case)
+    assert_distances(res.min_dist.cpu().numpy(), dmin, quantity="signed distance (fused, minimum)", case=case)
 
 
 def test_fused_large_batch_min_only():
@@ -218,7 +235,8 @@ def test_fused_large_batch_min_only():
                               DeviceWorld.upload(w.world, DEV), tt(w.cfg), link_poses=False)
     idx = np.random.default_rng(0).choice(len(w.cfg), 512, replace=False)
     _, _, dmin = fused_reference(w.model, w.spheres, w.world, w.cfg[idx])
-    np.testing.assert_allclose(res.min_dist.cpu().numpy()[idx], dmin, atol=2e-5)
+    assert_distances(res.min_dist.cpu().numpy()[idx], dmin, quantity="signed distance (fused, minimum)",
+                     case="65553 configs")
 
 
 @pytest.mark.parametrize("both", [False, True])
@@ -242,10 +260,10 @@ def test_fused_per_link_rows(case, both):
     r_k = np.broadcast_to(spheres.radii.T.reshape(-1), (B, S * N))
     d = np.where(r_k[..., None] < 0, np.inf, bkm).reshape(B, S, N, -1).min(axis=1)
     bnm = np.where(np.isinf(d), 1e9, d)
-    np.testing.assert_allclose(res.dist_bnm.cpu().numpy(), bnm, atol=2e-5, rtol=1e-6)
-    np.testing.assert_allclose(res.min_dist.cpu().numpy(), dmin, atol=2e-5)
+    assert_distances(res.dist_bnm.cpu().numpy(), bnm, quantity="signed distance (fused, per link)", case=case)
+    assert_distances(res.min_dist.cpu().numpy(), dmin, quantity="signed distance (fused, minimum)", case=case)
     if both:
-        np.testing.assert_allclose(res.dist_bkm.cpu().numpy(), bkm, atol=2e-5, rtol=1e-6)
+        assert_distances(res.dist_bkm.cpu().numpy(), bkm, quantity="signed distance (fused, per sphere)", case=case)
 
 
 @pytest.mark.parametrize("case", ["sweep", "padded"])
@@ -287,3 +305,48 @@ def test_no_world_staging_wait_gave_up():
     n = C.c_uint64(123)
     assert _lib.load().pk_stage_wait_timeouts(C.byref(n)) == _lib.PK_OK
     assert n.value == 0
+
+
+def test_forced_staging_timeout_is_reported_and_results_are_unchanged():
+    """The bounded wait's test hook: with force_timeout set, no TMA copy is
+    issued, every staging block waits out a 0.2 ms limit (by the GPU's global
+    timer), counts itself and loads the obstacle arrays plainly.  The host
+    then reads PK_ERR_TIMEOUT, and the outputs equal the normal path's bit
+    for bit.  Nothing is in flight at any point, and the hook is switched off
+    again whatever happens."""
+    import ctypes as C
+    from pyroffi_b200 import _lib
+    from pyroffi_b200.trajopt import TrajectoryCost
+    lib = _lib.load()
+    w = W.fk_collision(B=300)
+    args = (DeviceRobot.upload(w.model, DEV), DeviceSpheres.upload(w.spheres, DEV),
+            DeviceWorld.upload(w.world, DEV), tt(w.cfg))
+    wt = W.trajectories(Bt=8, T=16)
+    tc = TrajectoryCost(wt.model, wt.spheres, wt.world, wt.link_pairs, margin=wt.margin, device=DEV)
+    x = torch.as_tensor(wt.traj, device=DEV)
+
+    def run():
+        r = fk_sphere_collision(*args, per_sphere=True)
+        c, g = tc.cost_and_grad(x)
+        torch.cuda.synchronize()
+        return r.min_dist.clone(), r.dist_bkm.clone(), c.clone(), g.clone()
+
+    n = C.c_uint64(0)
+    assert lib.pk_stage_wait_reset() == _lib.PK_OK
+    normal = run()
+    assert lib.pk_stage_wait_timeouts(C.byref(n)) == _lib.PK_OK and n.value == 0
+    try:
+        assert lib.pk_stage_wait_configure(1, 200_000) == _lib.PK_OK
+        forced = run()
+    finally:
+        assert lib.pk_stage_wait_configure(0, 0) == _lib.PK_OK
+    assert lib.pk_stage_wait_timeouts(C.byref(n)) == _lib.PK_ERR_TIMEOUT
+    assert n.value >= 2, n.value              # at least one block of each kernel
+    assert b"gave up" in lib.pk_last_error() and b"untrusted" not in lib.pk_last_error()
+    for a, b in zip(normal, forced):
+        assert torch.equal(a, b)
+    assert lib.pk_stage_wait_reset() == _lib.PK_OK
+    after = run()
+    assert lib.pk_stage_wait_timeouts(C.byref(n)) == _lib.PK_OK and n.value == 0
+    for a, b in zip(normal, after):
+        assert torch.equal(a, b)

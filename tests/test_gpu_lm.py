@@ -11,6 +11,7 @@ import numpy as np
 import pytest
 import torch
 
+from error_report import record
 from oracle import kinematics as okin
 from oracle import lm as olm
 from pyroffi_b200 import robot as R
@@ -67,6 +68,59 @@ def test_lm_few_iterations_seed_by_seed(tps, max_iter):
         ok += close.sum()
     # decisions on the edge of the accept test may flip between FP32 and FP64
     assert ok >= 0.95 * 3 * 40, ok
+
+
+@pytest.mark.parametrize("tps", [0, 2])
+def test_lm_thirty_iterations_seed_by_seed(tps):
+    """A whole 30-iteration solve, seed by seed, against the FP64 oracle: the
+    FP64 normal equations keep the FP32 kernel on the oracle's path."""
+    w = small_ik(P=3, Sd=40)
+    s = solver_for(w, threads_per_seed=tps)
+    cfgs, errs = s.run_lm(tt(w.target_T), tt(w.seeds))
+    cfgs, errs = cfgs.cpu().numpy(), errs.cpu().numpy()
+    ok = 0
+    for p in range(3):
+        oc_, oe = oracle_run(w, p, w.max_iter)
+        close = (np.abs(cfgs[p] - oc_).max(axis=1) < 2e-4) & (np.abs(errs[p] - oe) <= 1e-3 * np.abs(oe) + 1e-4)
+        ok += close.sum()
+    record("IK seed disagreement with the FP64 oracle after 30 iterations (fraction)", 1.0 - ok / 120.0,
+           f"3 x 40 seeds, threads_per_seed {tps}")
+    assert ok >= 0.95 * 3 * 40, ok
+
+
+@pytest.mark.parametrize("max_iter", [0, 1, 2])
+def test_lm_fp32_solve_seed_by_seed(max_iter):
+    """FP32 normal equations + Cholesky with the conditional FP64 refinement
+    step, against the FP64 oracle: the same agreement bar as the FP64 solve
+    over the first iterations.  (Once the damping falls below about 1e-6 the
+    7-DOF chain's 6 x 7 system is conditioned beyond FP32, one refinement
+    step leaves steps a fraction of a percent apart, and seeds part ways.)"""
+    w = small_ik(P=3, Sd=40)
+    s = solver_for(w, max_iter=max_iter, fp32_solve=True)
+    cfgs, errs = s.run_lm(tt(w.target_T), tt(w.seeds))
+    cfgs, errs = cfgs.cpu().numpy(), errs.cpu().numpy()
+    ok = 0
+    for p in range(3):
+        oc_, oe = oracle_run(w, p, max_iter)
+        close = (np.abs(cfgs[p] - oc_).max(axis=1) < 2e-4) & (np.abs(errs[p] - oe) <= 1e-3 * np.abs(oe) + 1e-4)
+        ok += close.sum()
+    assert ok >= 0.95 * 3 * 40, ok
+
+
+def test_lm_fp32_solve_success_matches_fp64_solve():
+    """30 iterations on 32 problems x 128 seeds: the FP32 solve finds as many
+    solutions (1 mm / 0.01 rad, FP64-verified) as the FP64 solve, within 2."""
+    w = small_ik(P=32, Sd=128)
+    r64 = solver_for(w).solve(tt(w.target_T), tt(w.seeds))
+    r32 = solver_for(w, fp32_solve=True).solve(tt(w.target_T), tt(w.seeds))
+    n64, n32 = int(r64.success.sum()), int(r32.success.sum())
+    assert n32 >= n64 - 2, (n32, n64)
+
+
+def test_lm_fp32_solve_rejects_other_mappings():
+    w = small_ik(P=1, Sd=8)
+    with pytest.raises(Exception, match="fp32_solve"):
+        solver_for(w, fp32_solve=True, threads_per_seed=2).run_lm(tt(w.target_T), tt(w.seeds))
 
 
 def test_lm_initial_error_matches_oracle_exactly_enough():

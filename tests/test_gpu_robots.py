@@ -22,6 +22,7 @@ from pyroffi_b200.ik import BatchIkSolver
 from pyroffi_b200.sqp import SqpSolver
 from pyroffi_b200.trajopt import TrajectoryCost
 
+from error_report import assert_distances
 from robot_fixtures import load_robot
 
 pytestmark = pytest.mark.gpu
@@ -61,7 +62,7 @@ def test_self_distances_of_the_srdf_pairs(panda):
     got = collision_self_sphere(t(c_bsn3), t(r_bsn), t(pairs[:, 0], torch.int32),
                                 t(pairs[:, 1], torch.int32)).cpu().numpy()
     want = ocoll.self_sphere_full(c_bsn3, r_bsn, pairs[:, 0], pairs[:, 1])
-    np.testing.assert_allclose(got, want, atol=2e-5)
+    assert_distances(got, want, quantity="signed distance (collision_self_sphere)", case="panda SRDF pairs")
 
 
 def test_fused_world_distances(panda):
@@ -79,9 +80,9 @@ def test_fused_world_distances(panda):
     d = np.where(sp.radii[None, :, :, None] < 0, np.inf, d).min(axis=2)                        # [B, N, M]
     got = r.dist_bnm.cpu().numpy()
     fin = np.isfinite(d)
-    np.testing.assert_allclose(got[fin], d[fin], atol=2e-5)
-    np.testing.assert_allclose(r.min_dist.cpu().numpy(), np.where(fin, d, np.inf).reshape(256, -1).min(axis=1),
-                               atol=2e-5)
+    assert_distances(got[fin], d[fin], quantity="signed distance (fused, per link)", case="panda")
+    assert_distances(r.min_dist.cpu().numpy(), np.where(fin, d, np.inf).reshape(256, -1).min(axis=1),
+                     quantity="signed distance (fused, minimum)", case="panda")
 
 
 def test_trajectory_cost_and_gradient(panda):

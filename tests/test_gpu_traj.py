@@ -7,6 +7,7 @@ import numpy as np
 import pytest
 import torch
 
+from error_report import record
 from oracle import traj as otr
 from pyroffi_b200 import workloads as W
 from pyroffi_b200.trajopt import TrajectoryCost, TrajectoryCostFn
@@ -32,6 +33,7 @@ def test_cost_matches_oracle():
     w, tc = setup(Bt=16, T=32)
     c = tc.cost(torch.as_tensor(w.traj, device=DEV)).cpu().numpy()
     ref = np.array([oracle_cost(w, w.traj[b].astype(np.float64)) for b in range(16)])
+    record("trajectory cost (relative)", np.abs(c - ref) / np.abs(ref), "16 x 32 x 7")
     np.testing.assert_allclose(c, ref, rtol=1e-4, atol=1e-5)
     wp = tc.waypoint_collision(torch.as_tensor(w.traj, device=DEV)).cpu().numpy()
     assert (wp > 0).any(), "the workload should touch obstacles"
@@ -50,6 +52,7 @@ def test_gradient_matches_finite_differences():
                + w.w_collision * otr.collision_grad_fd(xb, md, w.spheres.centers, w.spheres.radii, w.link_pairs,
                                                        w.world.arrays(), w.margin))
         rel = np.linalg.norm(g[b] - ref) / max(np.linalg.norm(ref), 1e-12)
+        record("trajectory gradient vs FP64 finite differences (relative)", rel, "3 x 12 x 7, full cost")
         assert rel < 1e-4, (b, rel)
     # the fused launch and the separate ones agree
     np.testing.assert_allclose(tc.cost(x).cpu().numpy(), c.cpu().numpy(), rtol=0, atol=0)
@@ -69,6 +72,7 @@ def test_collision_gradient_alone_matches_fd():
     ref = otr.collision_grad_fd(w.traj[b].astype(np.float64), w.model.as_dict(), w.spheres.centers,
                                 w.spheres.radii, w.link_pairs, w.world.arrays(), w.margin)
     rel = np.linalg.norm(g - ref) / np.linalg.norm(ref)
+    record("trajectory gradient vs FP64 finite differences (relative)", rel, "8 x 8 x 7, collision only")
     assert rel < 1e-4, rel
 
 

@@ -8,6 +8,7 @@ import torch
 from oracle import kinematics as okin
 from oracle import lm as olm
 from oracle import se3
+from error_report import assert_distances
 from pyroffi_b200 import workloads as W
 from pyroffi_b200.collision import fk_sphere_collision
 from pyroffi_b200.device import DeviceRobot, DeviceSpheres, DeviceWorld
@@ -43,7 +44,8 @@ def test_fused_kernel_on_urdf_robot():
     d = d - r.spheres.radii[None, :, :, None] - world.spheres[None, None, None, :, 3]
     d = np.where(r.spheres.radii[None, :, :, None] < 0, np.inf, d).min(axis=2)
     want = np.where(np.isinf(d), 1e9, d)
-    np.testing.assert_allclose(res.dist_bnm.cpu().numpy(), want, atol=2e-5, rtol=1e-6)
+    assert_distances(res.dist_bnm.cpu().numpy(), want, quantity="signed distance (fused, per link)",
+                     case="URDF robot")
 
 
 @pytest.mark.parametrize("max_iter", [1, 2])
