@@ -34,17 +34,35 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-METRIC = "IK solves/s @1mm/0.01rad (256 targets x 128 seeds, 30 LM iters, 100 obstacle spheres + 200 self pairs)"
-UNIT = "solves/s"
+METRIC = "IK solves/s @1mm/0.01rad (problems/s, solved or not; 256 targets x 128 seeds x 30 LM iters)"
+UNIT = "problems/s"
 P_PER_GPU, SEEDS, ITERS = 256, 128, 30
 # algorithmic FLOP per seed-iteration: 6 error evaluations of
 # (FK 130*7 + residual 60 + sphere transforms 33*56 + world pairs 12*56*100 + self pairs 12*200)
 # + Jacobian 45*7 + normal equations and Cholesky ~800
 FLOP_PER_SEED_ITER = 6 * (130 * 7 + 60 + 33 * 56 + 12 * 56 * 100 + 12 * 200) + 45 * 7 + 800
 L2_FLUSH_BYTES = 256 << 20
-# DRAM bytes (read + write) of one launch of the LM kernel on this workload, from one ncu capture
-# (the ~1 MB of outputs were still in L2 when that launch ended, so the write side is small)
-LM_DRAM_BYTES_PER_LAUNCH = 1113344 + 3072
+# From one ncu capture of one launch of the LM kernel on this workload (python -m
+# pyroffi_b200.profile_cases lm): DRAM bytes read + written (the ~1 MB of outputs were still in L2
+# when the launch ended), and the FP32 work the kernel executed, 2 FLOP per FFMA, 1 per FADD / FMUL,
+# twice that for the packed FFMA2 / FADD2 / FMUL2, summed over threads; the FMA pipe's active share.
+LM_DRAM_BYTES_PER_LAUNCH = 1092352 + 1792
+LM_EXECUTED_FLOP_PER_LAUNCH = 29415151114
+LM_FMA_PIPE_PCT = 15.3
+
+
+def r4(x):
+    """x rounded to 4 significant digits (keeps the JSON line short)."""
+    if x is None:
+        return None
+    return float(f"{x:.4g}")
+
+
+def ik_config():
+    """The workload's config block, the same on both arms."""
+    return {"workload": "ik_lm_collision", "problems_per_gpu": P_PER_GPU, "seeds": SEEDS, "iters": ITERS,
+            "robot": "7-DOF chain, 56 spheres", "obstacles": 100, "self_pairs": 200, "lambda": "1e-2 x0.1/x10",
+            "l2": "flushed between steps"}
 
 
 def parse():
@@ -114,8 +132,7 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "ik_lm_collision", "problems": P_PER_GPU, "seeds": SEEDS, "iters": ITERS,
-                   "robot": "7-DOF revolute chain", "obstacles": 100, "self_pairs": 200},
+        "config": ik_config(),
         "success_rate": float(np.mean(succ)),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -298,36 +315,40 @@ def run_ours(args):
         flops = FLOP_PER_SEED_ITER * P_PER_GPU * SEEDS * ITERS
         achieved = flops / lm_avg_s / 1e12
         peak = fp32_peak_tflops(torch, _lib.call, lambda: stream.cuda_stream)
+        ok_gpu = res_w[3].cpu().numpy().astype(bool)
         cpu = None
         if not args.no_cpu_baseline:
             lib = cpu_port_lib()
             threads = lib.pk_cpu_max_threads()
             cpu_solve(lib, w, 0, 1, threads)
             dt, cfgs_c, errs_c = cpu_solve(lib, w, 0, args.cpu_sample, threads)
-            cpu = {"value": args.cpu_sample / dt, "unit": UNIT, "cores": threads, "kind": "port",
-                   "sample": f"{args.cpu_sample} problems x 128 seeds x 30 iterations (C port, OpenMP)",
-                   "success_rate": cpu_success(w, 0, cfgs_c, errs_c)}
+            cpu = {"value": r4(args.cpu_sample / dt), "unit": UNIT, "cores": threads, "kind": "port",
+                   "sample": f"problems 0-{args.cpu_sample - 1}, all seeds (C port, OpenMP)",
+                   "success_rate": cpu_success(w, 0, cfgs_c, errs_c),
+                   "gpu_success_rate_same_problems": float(ok_gpu[:args.cpu_sample].mean())}
+        executed = None
+        if LM_EXECUTED_FLOP_PER_LAUNCH:
+            ex = LM_EXECUTED_FLOP_PER_LAUNCH / lm_avg_s / 1e12
+            executed = {"achieved": r4(ex), "frac": r4(ex / peak), "fma_pipe_pct": LM_FMA_PIPE_PCT,
+                        "basis": "ncu FP32 SASS counts / event time"}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "ik_lm_collision", "problems_per_gpu": P_PER_GPU, "seeds": SEEDS,
-                       "iters": ITERS, "robot": "7-DOF revolute chain, 56 spheres", "obstacles": 100,
-                       "self_pairs": 200, "lambda": "1e-2, x0.1 accept / x10 reject",
-                       "l2": "flushed (256 MB write) between timed steps"},
+            "config": ik_config(),
             "success_rate": success,
+            "successful_solves_per_s": value * success,
             "gpu_launches": 2 * args.steps,
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": LM_DRAM_BYTES_PER_LAUNCH,
-                         "traffic_unit": "bytes per launch (ncu dram__bytes_read+write, one capture of this kernel)",
-                         "kernel": "lm_kernel<8,1,2,2>",
-                         "peak_source": "measured FP32 FMA microbenchmark (pk_fp32_fma_peak), this run",
-                         "flop_per_seed_iter": FLOP_PER_SEED_ITER,
-                         "flop_basis": "algorithmic count of the dense evaluation (6 evaluations per iteration, every "
-                                       "sphere-obstacle and self pair); the kernel culls pairs exactly by bounding "
-                                       "spheres, so this is dense-equivalent throughput"},
-            "kernel_ms": {"lm": statistics.mean(lm_ms), "verify_select": statistics.mean(step_ms) - statistics.mean(lm_ms)},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "successful_solves_per_s": e2e_value * success},
+            "roofline": {"bound": "fp32", "achieved": r4(achieved), "peak": r4(peak), "unit": "TFLOP/s",
+                         "frac": r4(achieved / peak), "traffic": LM_DRAM_BYTES_PER_LAUNCH,
+                         "kernel": "lm_kernel<8,1,1,2>",
+                         "peak_source": "pk_fp32_fma_peak, this run",
+                         "basis": f"dense-equivalent, {FLOP_PER_SEED_ITER} FLOP/seed-iter",
+                         "executed": executed},
+            "kernel_ms": {"lm": r4(statistics.mean(lm_ms)),
+                          "verify_select": r4(statistics.mean(step_ms) - statistics.mean(lm_ms))},
             "clocks": clock_summary,
             "cpu_baseline": cpu,
         }
@@ -370,9 +391,11 @@ def _cpu_rate(fn, units):
 
 
 def secondary_metrics(torch, dev, fp32_peak, cpu=True):
-    """Configs 1 (FK + sphere collision), 3 (trajectory cost + adjoint), 4
-    (mixed persistent batch IK) and 5 (FK + collision bandwidth sweep),
-    each against its roofline.  Seeded synthetic inputs, resident in HBM."""
+    """Configs 1 (FK + sphere collision), 3 (trajectory cost + adjoint, CHOMP,
+    SCO), HJCD / SQP on config 2's problems, 4 (mixed persistent batch IK) and
+    5 (FK + collision bandwidth sweep), each against its roofline, as numbers
+    only (units in the key names; workloads are described in the design
+    notes).  Seeded synthetic inputs, resident in HBM; L2 flushed between reps."""
     from pyroffi_b200 import workloads as W
     from pyroffi_b200.batch_ik import MixedIkBatch
     from pyroffi_b200.collision import FkCollisionResult, fk_sphere_collision
@@ -396,16 +419,20 @@ def secondary_metrics(torch, dev, fp32_peak, cpu=True):
     r2 = fk_sphere_collision(R, S, Wd, cfg, per_sphere=True)
     ms_bkm = _timed_ms(torch, lambda: fk_sphere_collision(R, S, Wd, cfg, per_sphere=True, out=r2), flush)
     n_valid = int((w.spheres.radii >= 0).sum())
+    # bytes per configuration: cfg in, min + 7-float poses of the N links out, and the [K, M] rows;
+    # K counts the base link's 8 padded rows (the output layout), K56 only the 56 real spheres
     bytes_cfg = 4 * w.model.n_act + 4 + 4 * 7 * N + 4 * K * M
+    bytes_k56 = 4 * w.model.n_act + 4 + 4 * 7 * N + 4 * n_valid * M
     flop_cfg = 130 * w.model.n_act + 33 * n_valid + 12 * n_valid * M
-    out["fk_collision_config1"] = {
-        "workload": "7-DOF chain, 8 spheres/link, 64 obstacle spheres; min distance + link poses",
-        "B1024_us_per_call": 1e3 * ms_1024, "B1024_configs_per_s": 1024 / (ms_1024 * 1e-3),
-        "B65536_bkm_ms": ms_bkm, "B65536_bkm_configs_per_s": 65536 / (ms_bkm * 1e-3),
-        "roofline": {"bound": "hbm", "achieved": 65536 * bytes_cfg / (ms_bkm * 1e-3) / 1e9, "peak": hbm,
-                     "unit": "GB/s", "frac": 65536 * bytes_cfg / (ms_bkm * 1e-3) / 1e9 / hbm,
-                     "bytes_per_config": bytes_cfg, "layout": f"[B, K={K}, M={M}] f32 + min + poses",
-                     "fp32_tflops": 65536 * flop_cfg / (ms_bkm * 1e-3) / 1e12, "kernel": "fk_sphere_collision_kernel"},
+    gbs = 65536 * bytes_cfg / (ms_bkm * 1e-3) / 1e9
+    gbs56 = 65536 * bytes_k56 / (ms_bkm * 1e-3) / 1e9
+    out["c1"] = {
+        "us_B1024": r4(1e3 * ms_1024), "configs_per_s_B1024": r4(1024 / (ms_1024 * 1e-3)),
+        "ms_B65536_bkm": r4(ms_bkm), "configs_per_s_B65536": r4(65536 / (ms_bkm * 1e-3)),
+        "roofline": {"bound": "hbm", "achieved": r4(gbs), "peak": hbm, "unit": "GB/s", "frac": r4(gbs / hbm),
+                     "bytes_per_config": bytes_cfg, f"K{K}": K,
+                     "frac_K56": r4(gbs56 / hbm), "bytes_per_config_K56": bytes_k56,
+                     "fp32_tflops": r4(65536 * flop_cfg / (ms_bkm * 1e-3) / 1e12)},
     }
     del r2
     if cpu:
@@ -418,9 +445,8 @@ def secondary_metrics(torch, dev, fp32_peak, cpu=True):
             cen = ocoll.transform_points(links[:, :, None, :], w.spheres.centers.astype(np.float64)[None])
             d = ocoll.point_vs_world(cen, np.broadcast_to(w.spheres.radii, cen.shape[:-1]), *w.world.arrays())
             return np.where(w.spheres.radii[None, :, :, None] < 0, np.inf, d).reshape(len(cs), -1).min(axis=1)
-        out["fk_collision_config1"]["cpu_baseline"] = {
-            "value": _cpu_rate(fkc_oracle, len(cs)), "unit": "configs/s", "cores": 1, "kind": "port",
-            "sample": "256 configurations, FP64 numpy oracle (FK, sphere centres, all sphere-obstacle distances, min)"}
+        out["c1"]["cpu_baseline"] = {"value": r4(_cpu_rate(fkc_oracle, len(cs))), "unit": "configs/s",
+                                     "cores": 1, "kind": "port", "sample": "256 configs, FP64 oracle"}
 
     # config 3: 512 trajectories x 64 waypoints x 7 DOF, 256 spheres + 32 boxes
     wt = W.trajectories()
@@ -430,19 +456,14 @@ def secondary_metrics(torch, dev, fp32_peak, cpu=True):
     ms_b = _timed_ms(torch, lambda: tc.grad(x), flush)
     ms_fb = _timed_ms(torch, lambda: tc.cost_and_grad(x), flush)
     Bt, T = wt.traj.shape[:2]
-    f_fwd, f_bwd = 296646, 459326
-    out["traj_config3"] = {
-        "workload": "512 x 64 x 7 CHOMP cost + hand-written adjoint, 256 spheres + 32 boxes",
-        "forward_ms": ms_f, "backward_recompute_ms": ms_b, "fused_fwd_bwd_ms": ms_fb,
-        "fwd_bwd_traj_per_s": Bt / (ms_fb * 1e-3),
-        "roofline": {"bound": "fp32", "achieved": Bt * T * f_bwd / (ms_fb * 1e-3) / 1e12, "peak": fp32_peak,
-                     "unit": "TFLOP/s", "frac": Bt * T * f_bwd / (ms_fb * 1e-3) / 1e12 / fp32_peak,
-                     "flop_per_waypoint": f_bwd, "kernel": "traj_cost_kernel",
-                     "flop_basis": "dense evaluation (every link sphere against every obstacle); the kernel skips "
-                                   "(link, obstacle) pairs beyond the margin, so this is dense-equivalent throughput "
-                                   "and frac can pass 1"},
+    f_bwd = 459326
+    tf = Bt * T * f_bwd / (ms_fb * 1e-3) / 1e12
+    out["c3"] = {
+        "ms_fwd": r4(ms_f), "ms_bwd_recompute": r4(ms_b), "ms_fused_fwd_bwd": r4(ms_fb),
+        "fwd_bwd_traj_per_s": r4(Bt / (ms_fb * 1e-3)),
+        "roofline": {"bound": "fp32", "achieved": r4(tf), "peak": r4(fp32_peak), "unit": "TFLOP/s",
+                     "frac": r4(tf / fp32_peak), "basis": "dense-equivalent"},
     }
-
     if cpu:
         from oracle import traj as otraj
         md = wt.model.as_dict()
@@ -452,9 +473,8 @@ def secondary_metrics(torch, dev, fp32_peak, cpu=True):
                 otraj.total_cost(wt.traj[b], md, wt.spheres.centers, wt.spheres.radii, wt.link_pairs,
                                  wt.world.arrays(), margin=wt.margin, w_smooth=1.0, w_acc=0.5, w_jerk=0.1,
                                  w_limits=1.0, w_coll=3.0, lower=wt.model.lower, upper=wt.model.upper)
-        out["traj_config3"]["cpu_baseline"] = {
-            "value": _cpu_rate(traj_oracle, 2), "unit": "trajectory costs/s (forward only)", "cores": 1,
-            "kind": "port", "sample": "2 trajectories x 64 waypoints, FP64 numpy oracle cost (no gradient)"}
+        out["c3"]["cpu_baseline"] = {"value": r4(_cpu_rate(traj_oracle, 2)), "unit": "traj costs/s (fwd)",
+                                     "cores": 1, "kind": "port", "sample": "2 traj, FP64 oracle"}
 
     # CHOMP optimiser on the adjoint: the config-3 trajectories, 100 iterations, one CUDA graph
     from pyroffi_b200.chomp import ChompConfig, ChompOptimizer
@@ -464,42 +484,19 @@ def secondary_metrics(torch, dev, fp32_peak, cpu=True):
     s0, g0 = x[0, 0].clone(), x[0, -1].clone()
     opt.run(x, s0, g0, graph=True)
     ms_chomp = _timed_ms(torch, lambda: opt.run(x, s0, g0, graph=True), flush, reps=3, warm=1)
-    _, cc, _ = opt.run(x, s0, g0, graph=True)
-    out["chomp_config3"] = {
-        "workload": "CHOMP, 512 x 64 x 7 trajectories, 100 iterations (cost+gradient, truncated-CG covariant step, "
-                    "6-point line search per iteration), one CUDA graph",
-        "ms_per_run": ms_chomp, "iterations_per_s": ccfg.n_iters / (ms_chomp * 1e-3),
-        "trajectory_iterations_per_s": Bt * ccfg.n_iters / (ms_chomp * 1e-3),
-        "final_cost_mean": float(cc.mean()),
-    }
+    out["chomp"] = {"ms_100_iters": r4(ms_chomp), "traj_iters_per_s": r4(Bt * ccfg.n_iters / (ms_chomp * 1e-3))}
 
-    # SCO optimiser: the config-3 trajectories, 10 outer x 30 inner L-BFGS iterations, one CUDA graph;
-    # its stages timed alone, and the reference's central-difference Jacobians for comparison
+    # SCO optimiser: 10 outer x 30 inner L-BFGS iterations, one CUDA graph
     from pyroffi_b200.sco import ScoConfig, ScoOptimizer
     scfg = ScoConfig()
     sco = ScoOptimizer(wt.model, wt.spheres, wt.world, wt.link_pairs, scfg, device=dev)
     sco.run(x, s0, g0, graph=True)
     ms_sco = _timed_ms(torch, lambda: sco.run(x, s0, g0, graph=True), flush, reps=3, warm=1)
-    _, sc, _ = sco.run(x, s0, g0, graph=True)
-    ms_lin = _timed_ms(torch, lambda: sco.linearize(x), flush)
-    dl, Jl, _ = sco.linearize(x)
-    ms_inner = _timed_ms(torch, lambda: sco.inner(x, dl, Jl, scfg.w_collision, s0, g0), flush)
-    sco_fd = ScoOptimizer(wt.model, wt.spheres, wt.world, wt.link_pairs, scfg, fd_eps=1e-4, device=dev)
-    sco_fd.run(x, s0, g0, graph=True)
-    ms_sco_fd = _timed_ms(torch, lambda: sco_fd.run(x, s0, g0, graph=True), flush, reps=2, warm=1)
-    out["sco_config3"] = {
-        "workload": "SCO, 512 x 64 x 7 trajectories, 10 outer (analytic smooth-min linearisation) x 30 inner "
-                    "L-BFGS iterations, one CUDA graph",
-        "ms_per_run": ms_sco, "trajectories_per_s": Bt / (ms_sco * 1e-3),
-        "linearize_ms": ms_lin, "inner_solve_ms": ms_inner,
-        "ms_per_run_fd_jacobian": ms_sco_fd,
-        "final_cost_mean": float(sc.mean()),
-    }
+    out["sco"] = {"ms_per_run": r4(ms_sco), "traj_per_s": r4(Bt / (ms_sco * 1e-3))}
 
-    # HJCD-IK on config 2's problems (collision-aware, 100 obstacle spheres): 32 coarse seeds x 20
-    # coordinate-descent steps, 30 refinement seeds x 40 LM iterations (the reference benchmark's
-    # HJCD settings), FP64 verification of the winners
+    # HJCD-IK and SQP-IK on config 2's problems (collision on), the reference benchmark's settings
     from pyroffi_b200.hjcd import HjcdSolver
+    from pyroffi_b200.sqp import SqpSolver
     wi = W.ik()
     hj = HjcdSolver(wi.model, wi.target_link, spheres=wi.spheres, world=wi.world, enable_collision=True, device=dev)
     vs = BatchIkSolver(wi.model, wi.target_link, device=dev)
@@ -515,16 +512,8 @@ def secondary_metrics(torch, dev, fp32_peak, cpu=True):
     _, _, parts_h = hj.solve(tgt_h, prev_h, return_all=True, **hkw)
     _, _, _, ok_h = vs.verify_select(parts_h[5], parts_h[6], tgt_h)
     P_h = wi.target_T.shape[0]
-    out["hjcd_config2"] = {
-        "workload": f"HJCD-IK, {P_h} problems of config 2 (7-DOF chain, 100 obstacle spheres, collision on), "
-                    "32 coarse seeds x 20 steps, 30 refinement seeds x 40 LM iterations",
-        "ms_per_solve_batch": ms_hj, "solves_per_s": P_h / (ms_hj * 1e-3),
-        "success_rate": float(ok_h.float().mean()),
-    }
-
-    # SQP-IK on the same problems: 32 seeds x 60 iterations, 2 active-set re-solves (the reference
-    # benchmark's SQP settings)
-    from pyroffi_b200.sqp import SqpSolver
+    out["hjcd"] = {"ms": r4(ms_hj), "problems_per_s": r4(P_h / (ms_hj * 1e-3)),
+                   "success_rate": float(ok_h.float().mean())}
     sq = SqpSolver(wi.model, wi.target_link, spheres=wi.spheres, world=wi.world, enable_collision=True, device=dev)
     skw = dict(num_seeds=32, max_iter=60, n_inner_iters=2, pos_weight=50.0, ori_weight=10.0, lambda_init=5e-3,
                generator=gen_h)
@@ -534,14 +523,11 @@ def secondary_metrics(torch, dev, fp32_peak, cpu=True):
     gen_h.manual_seed(0)
     _, _, parts_s = sq.solve(tgt_h, prev_h, return_all=True, **skw)
     _, _, _, ok_s = vs.verify_select(parts_s[1], parts_s[2], tgt_h)
-    out["sqp_config2"] = {
-        "workload": f"SQP-IK, {P_h} problems of config 2 (collision on), 32 seeds x 60 iterations, "
-                    "2 active-set re-solves per step",
-        "ms_per_solve_batch": ms_sq, "solves_per_s": P_h / (ms_sq * 1e-3),
-        "success_rate": float(ok_s.float().mean()),
-    }
+    out["sqp"] = {"ms": r4(ms_sq), "problems_per_s": r4(P_h / (ms_sq * 1e-3)),
+                  "success_rate": float(ok_s.float().mean())}
 
-    # config 4: 4096 mixed IK problems in one persistent batch (CUDA graph)
+    # config 4: 4096 mixed IK problems in one persistent batch (CUDA graph), against the same kernels
+    # called per class (problems padded to the class's largest seed count) and per problem
     wm = W.mixed_ik()
     o = dict(max_iter=wm.max_iter, lambda_init=wm.lambda_init, lambda_down=wm.lambda_down, lambda_up=wm.lambda_up,
              collision_weight=wm.collision_weight, collision_margin=wm.collision_margin, pos_tol=wm.pos_tol,
@@ -553,24 +539,38 @@ def secondary_metrics(torch, dev, fp32_peak, cpu=True):
     ms_batch = _timed_ms(torch, b.solve, flush, reps=3, warm=1)
     res = b.solve()
     torch.cuda.synchronize()
-    succ = sum(int(r.success.sum()) for r in res) / len(wm.problem_class)
-    plain = 0.0
-    for c, cl in enumerate(wm.classes):
-        s = BatchIkSolver(cl.model, cl.target_links, spheres=cl.spheres, world=wm.world, device=dev, **o)
-        tg, sd = torch.as_tensor(wm.target_T[c], device=dev), torch.as_tensor(wm.seeds[c], device=dev)
-        plain += _timed_ms(torch, lambda: s.solve(tg, sd), flush, reps=2, warm=1)
     n_p = len(wm.problem_class)
-    out["batch_ik_config4"] = {
-        "workload": "4096 problems (40% 7-DOF, 30% 6-DOF, 20% 15-DOF bimanual, 10% 29-DOF humanoid), "
-                    "32-256 seeds, 500 obstacle spheres, 30 LM iterations",
-        "solves_per_s": n_p / (ms_batch * 1e-3), "ms_per_batch": ms_batch, "success_rate": succ,
-        "success_per_class": [float(r.success.float().mean()) for r in res],
-        "plain_per_class_padded_ms": plain, "speedup_vs_per_class_padded": plain / ms_batch,
-        "kernel_launches_per_batch": b.launches_per_solve(),
+    succ = sum(int(r.success.sum()) for r in res) / n_p
+    plain, per_problem, ok_pp = 0.0, 0.0, 0
+    for c, cl in enumerate(wm.classes):
+        s_c = BatchIkSolver(cl.model, cl.target_links, spheres=cl.spheres, world=wm.world, device=dev, **o)
+        tg, sd = torch.as_tensor(wm.target_T[c], device=dev), torch.as_tensor(wm.seeds[c], device=dev)
+        plain += _timed_ms(torch, lambda: s_c.solve(tg, sd), flush, reps=2, warm=1)
+        # per problem: one solve call per problem with its own seed count (the plain drop-in pattern)
+        idx = np.nonzero(wm.problem_class == c)[0]
+        ns = [int(wm.n_seeds[i]) for i in idx]
+        views = [(tg[j:j + 1], sd[j:j + 1, :ns[j]].contiguous()) for j in range(len(idx))]
+        s_c.solve(*views[0])
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        flush.fill_(1.0)
+        e0.record()
+        rs = [s_c.solve(t_, s_) for t_, s_ in views]
+        e1.record()
+        e1.synchronize()
+        per_problem += e0.elapsed_time(e1)
+        ok_pp += sum(int(r_.success.sum()) for r_ in rs)
+    out["c4"] = {
+        "ms_batch": r4(ms_batch), "problems_per_s": r4(n_p / (ms_batch * 1e-3)), "success_rate": succ,
+        "success_per_class": [round(float(r.success.float().mean()), 4) for r in res],
+        "ms_per_class_padded": r4(plain), "speedup_vs_per_class": r4(plain / ms_batch),
+        "ms_per_problem_calls": r4(per_problem), "success_rate_per_problem_calls": ok_pp / n_p,
+        "speedup_vs_per_problem_calls": r4(per_problem / ms_batch),
+        "launches_per_batch": b.launches_per_solve(),
     }
     del b
 
-    # config 5: 16 spheres/link vs 4096 spheres + 256 oriented boxes, B = 1024 ... 262144
+    # config 5: 16 spheres/link vs 4096 spheres + 256 oriented boxes, B = 1024 ... 262144, [B, N, M] rows
     ws = W.sweep(B=262144)
     R5, S5, W5 = DeviceRobot.upload(ws.model, dev), DeviceSpheres.upload(ws.spheres, dev), DeviceWorld.upload(ws.world, dev)
     N5, M5 = ws.spheres.n_links, sum(W5.counts())
@@ -587,20 +587,19 @@ def secondary_metrics(torch, dev, fp32_peak, cpu=True):
         rb = FkCollisionResult(mind[:B], None, None, bnm[:B])
         ms = _timed_ms(torch, lambda: fk_sphere_collision(R5, S5, W5, cb, link_poses=False, per_link=True, out=rb),
                        flush, reps=3)
-        sweep[str(B)] = {"ms": ms, "configs_per_s": B / (ms * 1e-3), "hbm_gbs": B * bytes5 / (ms * 1e-3) / 1e9,
-                         "fp32_tflops": B * flop5 / (ms * 1e-3) / 1e12,
-                         "fp32_frac": B * flop5 / (ms * 1e-3) / 1e12 / fp32_peak}
+        sweep[str(B)] = [r4(ms), r4(B / (ms * 1e-3)), r4(B * bytes5 / (ms * 1e-3) / 1e9),
+                         r4(B * flop5 / (ms * 1e-3) / 1e12 / fp32_peak)]
     del bnm
     pairs5 = W.active_link_pairs(ws.model, ws.spheres)
     tc5 = TrajectoryCost(ws.model, ws.spheres, ws.world, pairs5, device=dev)
     x5 = cfg5[:65536].reshape(1024, 64, -1).contiguous()
     ms_fb5 = _timed_ms(torch, lambda: tc5.cost_and_grad(x5), flush, reps=3)
-    out["sweep_config5"] = {
-        "workload": "7-DOF chain, 16 spheres/link (112) vs 4096 spheres + 256 oriented boxes; [B, N, M] per-link rows",
-        "bytes_per_config": bytes5, "flop_per_config": flop5, "by_batch": sweep,
-        "roofline": {"bound": "fp32", "achieved": sweep["262144"]["fp32_tflops"], "peak": fp32_peak,
-                     "unit": "TFLOP/s", "frac": sweep["262144"]["fp32_frac"], "kernel": "fk_sphere_collision_kernel"},
-        "fwd_bwd_65536_configs_ms": ms_fb5,
+    t262 = 262144 * flop5 / (sweep["262144"][0] * 1e-3) / 1e12
+    out["c5"] = {
+        "by_batch_ms_cfgps_gbs_fp32frac": sweep,
+        "roofline": {"bound": "fp32", "achieved": r4(t262), "peak": r4(fp32_peak), "unit": "TFLOP/s",
+                     "frac": r4(t262 / fp32_peak), "B": 262144},
+        "ms_fwd_bwd_65536": r4(ms_fb5),
     }
     return out
 

@@ -2019,6 +2019,7 @@ extern "C" int pk_ik_batch(void* stream, const pk_lm_options* opt, const pk_ik_c
                            const float* world_halfspaces, int32_t Ms, int32_t Mc, int32_t Mb, int32_t Mh,
                            const int32_t* items, int32_t n_items, int32_t* queue, int32_t blocks) {
   PK_CHECK_ARG(opt != nullptr && classes != nullptr, "null options or classes");
+  PK_CHECK_ARG(!opt->fp32_solve, "fp32_solve is not offered by the batched kernels");
   PK_CHECK_ARG(n_classes >= 1, "at least one class is required");
   PK_CHECK_CAP(n_classes <= PK_MAX_CLASSES, "n_classes=%d exceeds %d", n_classes, PK_MAX_CLASSES);
   PK_CHECK_ARG(n_items >= 0 && Ms >= 0 && Mc >= 0 && Mb >= 0 && Mh >= 0, "negative extent");
