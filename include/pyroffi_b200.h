@@ -182,7 +182,9 @@ int pk_ls_ik_ex(void* stream, const pk_lm_options* opt, const float* seeds, cons
  *   body 0: seed-group kernel (n_act <= 8, n_ee == 1; lanes per seed and
  *           seeds per block from pk_lm_options);
  *   body 1: one warp per seed with its state in shared memory
- *           (n_act <= 32, n_ee <= 4).
+ *           (n_act <= 32, n_ee <= 4);
+ *   body 2: seed-group kernel, one lane per seed, 128 seeds per block
+ *           (n_act <= 16, n_ee <= 2).
  */
 typedef struct pk_ik_class {
   const float* twists;
@@ -221,10 +223,12 @@ typedef struct pk_ik_class {
  * counterpart): the persistent form of pk_ls_ik_ex.  items[n_items][4] =
  * (class, problem, first seed, seed count) in device memory, in the order
  * blocks should take them (longest first balances the tail); a body-0 item
- * holds at most seeds_per_block seeds.  Each body runs one persistent kernel
- * whose blocks take items from a device counter in queue[2] (caller-owned
- * device memory; cleared here with an async memset on `stream` before the
- * launch, so one queue serves one call in flight at a time).  blocks = 0
+ * holds at most seeds_per_block seeds (128 when that is 0 and
+ * threads_per_seed is 0 or 1), a body-2 item at most 128.  Each body runs
+ * one persistent kernel whose blocks take items from a device counter in
+ * queue[2] (caller-owned device memory; cleared here with async memsets on
+ * `stream` before the launches, so one queue serves one call in flight at
+ * a time; bodies 0 and 2 use queue[0] one after the other).  blocks = 0
  * sizes each grid to one full wave on the current device.  Same per-seed
  * iteration and outputs as pk_ls_ik_ex with opt.
  */

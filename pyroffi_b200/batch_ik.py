@@ -32,7 +32,7 @@ from . import _lib
 from ._tensors import f32, ptr, stream_ptr
 from .ik import BatchIkSolver
 
-BODY_SEED_GROUP, BODY_WARP = 0, 1
+BODY_SEED_GROUP, BODY_WARP, BODY_SEED_GROUP16 = 0, 1, 2
 
 
 @dataclass
@@ -44,7 +44,14 @@ class ClassResult:
 
 
 def default_body(n_act: int, n_ee: int) -> int:
-    return BODY_SEED_GROUP if (n_act <= 8 and n_ee == 1) else BODY_WARP
+    """Register kernels where they fit: the 8-wide seed-group body for small
+    single-EE robots, the 16-wide one-lane body up to 16 DOF and 2 EEs, the
+    warp-per-seed body beyond."""
+    if n_act <= 8 and n_ee == 1:
+        return BODY_SEED_GROUP
+    if n_act <= 16 and n_ee <= 2:
+        return BODY_SEED_GROUP16
+    return BODY_WARP
 
 
 class MixedIkBatch:
@@ -108,10 +115,15 @@ class MixedIkBatch:
         self._graph = None
 
     def _chunk(self, c: int) -> int:
+        """Seeds per item: one block's seeds for the seed-group bodies (the
+        library's defaults: one lane x 128 seeds), 64 for the warp body."""
         if self.bodies[c] == BODY_SEED_GROUP:
-            tps = self.opt.threads_per_seed if self.opt.threads_per_seed > 0 else 2
-            spb = self.opt.seeds_per_block if self.opt.seeds_per_block > 0 else (64 if tps == 2 else 128 // tps)
-            return spb
+            tps = self.opt.threads_per_seed if self.opt.threads_per_seed > 0 else 1
+            if self.opt.seeds_per_block > 0:
+                return self.opt.seeds_per_block
+            return 128 if self.opt.threads_per_seed <= 0 else 128 // tps
+        if self.bodies[c] == BODY_SEED_GROUP16:
+            return 128
         return 64
 
     def _cost_per_seed(self, c: int) -> float:
@@ -119,7 +131,7 @@ class MixedIkBatch:
         sphere tests and the solve size."""
         s, m = self.solvers[c], self.classes[c].model
         n_rs = int(s.spheres_local.shape[0])
-        return m.n_joints * 8 + n_rs * 6 + m.n_act ** 2 + (200 if self.bodies[c] == BODY_WARP else 0)
+        return m.n_joints * 8 + n_rs * 6 + m.n_act ** 2 + (200 if self.bodies[c] != BODY_SEED_GROUP else 0)
 
     def _build_items(self) -> None:
         items, cost = [], []
@@ -197,6 +209,8 @@ class MixedIkBatch:
         return self.verify()
 
     def launches_per_solve(self) -> int:
+        """Kernels per solve: one persistent launch per body in use, one
+        verification per class."""
         bodies = {self.bodies[c] for c in range(len(self.classes)) if self.counts[c]}
         return len(bodies) + sum(1 for c in range(len(self.classes)) if self.counts[c])
 

@@ -1,5 +1,5 @@
-// Internal interface of the batched (work-queue) IK launchers: the
-// seed-group body (pk_lm.cu) and the warp-per-seed body (pk_lm_wide.cu)
+// Internal interface of the batched (work-queue) IK launchers: the two
+// seed-group bodies (pk_lm.cu) and the warp-per-seed body (pk_lm_wide.cu)
 // each run one persistent kernel over the items of their robot classes.
 #pragma once
 
@@ -11,8 +11,9 @@ namespace pk {
 constexpr int PK_MAX_CLASSES = 8;
 
 // body selector of a class (pk_ik_class.body)
-constexpr int kBodySeedGroup = 0;  // TPS lanes per seed, registers (n_act <= 8, one EE)
-constexpr int kBodyWarp = 1;       // one warp per seed, shared-memory state (n_act <= 32)
+constexpr int kBodySeedGroup = 0;    // TPS lanes per seed, registers (n_act <= 8, one EE)
+constexpr int kBodyWarp = 1;         // one warp per seed, shared-memory state (n_act <= 32)
+constexpr int kBodySeedGroup16 = 2;  // one lane per seed, registers (n_act <= 16, n_ee <= 2)
 
 struct BatchCall {
   const pk_ik_class* cls;  // host array, n_classes entries

@@ -1225,9 +1225,12 @@ struct SeedGroupBatch {
   int* queue;
 };
 
-// MINB as for lm_kernel.
-template <int TPS, int MINB>
+// MINB as for lm_kernel.  MAXA / MAXEE select the body: <8, 1> serves the
+// classes of body kBodySeedGroup, <16, 2> (one lane per seed) those of
+// kBodySeedGroup16; items of other bodies are skipped.
+template <int MAXA, int MAXEE, int TPS, int MINB>
 __global__ void __launch_bounds__(128, MINB) lm_batch_kernel(const __grid_constant__ SeedGroupBatch B) {
+  constexpr int kMyBody = (MAXA <= 8 && MAXEE == 1) ? kBodySeedGroup : kBodySeedGroup16;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int s_item;
   __shared__ LmArgs s_args;
@@ -1241,15 +1244,15 @@ __global__ void __launch_bounds__(128, MINB) lm_batch_kernel(const __grid_consta
     if (item.x < 0 || item.x >= B.n_classes) continue;
     int body;
     pick_class(B.body, item.x, body);
-    if (body != kBodySeedGroup) continue;
+    if (body != kMyBody) continue;
     if (threadIdx.x == 0) pick_class(B.cls, item.x, s_args);
     __syncthreads();
     const LmArgs& a = s_args;
     if (item.y < 0 || item.y >= a.P || item.z < 0 || item.w <= 0 || item.z + item.w > a.Sd || item.w > a.spb)
       continue;  // malformed item: nothing is read or written for it
     const LmLayout L = lm_layout(a, TPS);
-    lm_stage<8>(a, smem_raw, L, item.y);
-    lm_seed_groups<8, 1, TPS>(a, smem_raw, L, item.y, item.w, (size_t)item.y * a.Sd + item.z);
+    lm_stage<MAXA>(a, smem_raw, L, item.y);
+    lm_seed_groups<MAXA, MAXEE, TPS>(a, smem_raw, L, item.y, item.w, (size_t)item.y * a.Sd + item.z);
     __syncthreads();
   }
 }
@@ -1937,10 +1940,12 @@ extern "C" int pk_ik_verify_select(void* stream, const float* cfgs, const float*
 
 namespace pk {
 
-template <int TPS>
+template <int MAXA, int MAXEE, int TPS>
 static int launch_batch_t(const SeedGroupBatch& B, size_t smem, int threads, int blocks, cudaStream_t st) {
-  // the 4-block register budget only where shared memory admits 3 or more blocks per SM
-  auto kern = ((228 * 1024) / (smem + 1024) >= 3) ? lm_batch_kernel<TPS, 4> : lm_batch_kernel<TPS, 2>;
+  // the 4-block register budget only where shared memory admits 3 or more blocks per SM (8-wide body)
+  auto kern = lm_batch_kernel<MAXA, MAXEE, TPS, 2>;
+  if constexpr (MAXA <= 8)
+    if ((228 * 1024) / (smem + 1024) >= 3) kern = lm_batch_kernel<MAXA, MAXEE, TPS, 4>;
   if (int s = set_smem_limit((const void*)kern, smem)) return s;
   if (blocks <= 0) {
     int dev = 0, sms = 0, per_sm = 0;
@@ -1954,8 +1959,15 @@ static int launch_batch_t(const SeedGroupBatch& B, size_t smem, int threads, int
   return cuda_status(cudaGetLastError(), "lm_batch_kernel launch");
 }
 
-int launch_seed_group_batch(const BatchCall& b, cudaStream_t st, int* launched) {
+// One persistent launch over the items of the classes of `body`
+// (kBodySeedGroup: 8-wide, lanes and seeds per block from the options;
+// kBodySeedGroup16: 16-wide, one lane per seed, 128 seeds per block).
+static int launch_seed_group_body(const BatchCall& b, int body, cudaStream_t st, bool& queue_used, int& count) {
   int tps = b.opt.threads_per_seed, spb = b.opt.seeds_per_block;
+  if (body == kBodySeedGroup16) {
+    tps = 1;
+    spb = 128;
+  }
   if (tps <= 0) { tps = 1; if (spb <= 0) spb = 128; }
   if (spb <= 0) spb = 128 / tps;
   SeedGroupBatch B{};
@@ -1964,13 +1976,17 @@ int launch_seed_group_batch(const BatchCall& b, cudaStream_t st, int* launched) 
   for (int c = 0; c < b.n_classes; ++c) {
     const pk_ik_class& k = b.cls[c];
     B.body[c] = k.body;
-    if (k.body != kBodySeedGroup) continue;
+    if (k.body != body) continue;
     PK_CHECK_ARG(tps == 1 || tps == 2 || tps == 4 || tps == 8,
                  "seed-group classes take threads_per_seed 0, 1, 2, 4 or 8 (got %d)", tps);
     PK_CHECK_ARG(spb * tps <= 128 && (spb * tps) % 32 == 0,
                  "seeds_per_block * threads_per_seed must be a multiple of 32 and at most 128");
-    PK_CHECK_CAP(k.n_act <= 8 && k.n_ee == 1, "seed-group classes need n_act <= 8 and one EE (class %d: %d, %d)",
-                 c, k.n_act, k.n_ee);
+    if (body == kBodySeedGroup)
+      PK_CHECK_CAP(k.n_act <= 8 && k.n_ee == 1, "body-0 classes need n_act <= 8 and one EE (class %d: %d, %d)",
+                   c, k.n_act, k.n_ee);
+    else
+      PK_CHECK_CAP(k.n_act <= 16 && k.n_ee <= 2, "body-2 classes need n_act <= 16 and n_ee <= 2 (class %d: %d, %d)",
+                   c, k.n_act, k.n_ee);
     LmArgs a{};
     a.m = ModelArgs{k.twists, k.parent_tf, k.parent_idx, k.act_idx, k.mimic_mul, k.mimic_off, k.mimic_act_idx,
                     k.topo_inv, k.n_joints, k.n_act};
@@ -2001,15 +2017,36 @@ int launch_seed_group_batch(const BatchCall& b, cudaStream_t st, int* launched) 
   B.n_items = b.n_items;
   B.queue = b.queue;
   const int threads = spb * tps;
-  int s;
-  switch (tps) {
-    case 1: s = launch_batch_t<1>(B, smem, threads, b.blocks, st); break;
-    case 2: s = launch_batch_t<2>(B, smem, threads, b.blocks, st); break;
-    case 4: s = launch_batch_t<4>(B, smem, threads, b.blocks, st); break;
-    default: s = launch_batch_t<8>(B, smem, threads, b.blocks, st); break;
+  // the item counter queue[0] serves both seed-group launches: the second
+  // one starts from a counter cleared on the stream after the first
+  if (queue_used) {
+    if (int s = cuda_status(cudaMemsetAsync(b.queue, 0, sizeof(int32_t), st), "queue reset")) return s;
   }
-  if (s == PK_OK && launched) ++*launched;
+  int s;
+  if (body == kBodySeedGroup16) {
+    s = launch_batch_t<16, 2, 1>(B, smem, threads, b.blocks, st);
+  } else {
+    switch (tps) {
+      case 1: s = launch_batch_t<8, 1, 1>(B, smem, threads, b.blocks, st); break;
+      case 2: s = launch_batch_t<8, 1, 2>(B, smem, threads, b.blocks, st); break;
+      case 4: s = launch_batch_t<8, 1, 4>(B, smem, threads, b.blocks, st); break;
+      default: s = launch_batch_t<8, 1, 8>(B, smem, threads, b.blocks, st); break;
+    }
+  }
+  if (s == PK_OK) {
+    queue_used = true;
+    ++count;
+  }
   return s;
+}
+
+int launch_seed_group_batch(const BatchCall& b, cudaStream_t st, int* launched) {
+  bool queue_used = false;
+  int n = 0;
+  if (int s = launch_seed_group_body(b, kBodySeedGroup, st, queue_used, n)) return s;
+  if (int s = launch_seed_group_body(b, kBodySeedGroup16, st, queue_used, n)) return s;
+  if (launched) *launched += n;
+  return PK_OK;
 }
 
 }  // namespace pk
@@ -2030,7 +2067,9 @@ extern "C" int pk_ik_batch(void* stream, const pk_lm_options* opt, const pk_ik_c
   PK_CHECK_ARG(items && queue, "null items or queue");
   PK_CHECK_ARG((reinterpret_cast<uintptr_t>(items) & 15) == 0, "items must be 16-byte aligned");
   for (int c = 0; c < n_classes; ++c)
-    PK_CHECK_ARG(classes[c].body == kBodySeedGroup || classes[c].body == kBodyWarp, "class %d: body must be 0 or 1", c);
+    PK_CHECK_ARG(classes[c].body == kBodySeedGroup || classes[c].body == kBodyWarp ||
+                     classes[c].body == kBodySeedGroup16,
+                 "class %d: body must be 0, 1 or 2", c);
   const cudaStream_t st = (cudaStream_t)stream;
   if (int s = cuda_status(cudaMemsetAsync(queue, 0, 2 * sizeof(int32_t), st), "queue reset")) return s;
   BatchCall b{classes, n_classes, WorldArgs{world_spheres, world_capsules, world_boxes, world_halfspaces, Ms, Mc, Mb, Mh},

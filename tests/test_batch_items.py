@@ -5,7 +5,7 @@ longest first; the mixed workload has the configured class mix."""
 import numpy as np
 
 from pyroffi_b200 import workloads as W
-from pyroffi_b200.batch_ik import BODY_SEED_GROUP, BODY_WARP, MixedIkBatch
+from pyroffi_b200.batch_ik import BODY_SEED_GROUP, BODY_SEED_GROUP16, BODY_WARP, MixedIkBatch
 
 
 def test_mixed_workload_shape():
@@ -24,7 +24,7 @@ def test_mixed_workload_shape():
 def test_items_cover_every_seed_once():
     w = W.mixed_ik(n_problems=60, seeds_range=(1, 150))
     b = MixedIkBatch(w.classes, w.world, device="cpu")
-    assert b.bodies == [BODY_SEED_GROUP, BODY_SEED_GROUP, BODY_WARP, BODY_WARP]
+    assert b.bodies == [BODY_SEED_GROUP, BODY_SEED_GROUP, BODY_SEED_GROUP16, BODY_WARP]
     b.prepare(w.problem_class, w.n_seeds)
     items = b.items.numpy()
     seen = {c: np.zeros((b.counts[c], b.strides[c]), int) for c in range(4)}

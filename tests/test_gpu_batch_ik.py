@@ -16,7 +16,7 @@ import torch
 
 from oracle import lm as olm
 from pyroffi_b200 import workloads as W
-from pyroffi_b200.batch_ik import BODY_SEED_GROUP, BODY_WARP, MixedIkBatch
+from pyroffi_b200.batch_ik import BODY_SEED_GROUP, BODY_SEED_GROUP16, BODY_WARP, MixedIkBatch
 from pyroffi_b200.ik import BatchIkSolver
 
 pytestmark = pytest.mark.gpu
@@ -91,7 +91,9 @@ def per_class_reference(w, b):
         if b.counts[c] == 0:
             out.append(None)
             continue
-        tps = 2 if b.bodies[c] == BODY_SEED_GROUP else 16
+        # the same kernels as the batch's bodies: 2 lanes x 64 seeds (body 0: lanes per seed change only the
+        # lane that sums each penalty term, the sum order is fixed), one lane per seed (body 2), warp body (1)
+        tps = {BODY_SEED_GROUP: 2, BODY_SEED_GROUP16: 0, BODY_WARP: 16}[b.bodies[c]]
         s = BatchIkSolver(cl.model, cl.target_links, spheres=cl.spheres, world=w.world, device=DEV,
                           **opts(w, threads_per_seed=tps, seeds_per_block=64 if tps == 2 else 0))
         out.append(s.run_lm(b.targets[c], b.seeds[c]))
@@ -115,7 +117,7 @@ def make_batch(w, **kw):
 def test_batch_equals_per_class_launches(mixed):
     w = mixed
     b = make_batch(w)
-    assert b.bodies == [BODY_SEED_GROUP, BODY_SEED_GROUP, BODY_WARP, BODY_WARP]
+    assert b.bodies == [BODY_SEED_GROUP, BODY_SEED_GROUP, BODY_SEED_GROUP16, BODY_WARP]
     b.run_lm()
     ref = per_class_reference(w, b)
     for c in range(len(w.classes)):

@@ -83,10 +83,12 @@ def test_config2_against_the_port_on_all_problems(config2):
                            w.self_pairs[:, 0], w.self_pairs[:, 1])
     e64 = np.sum((res * Wt) ** 2, axis=-1) + pen
     e32 = err_g[np.arange(256), np.argmin(err_g, axis=1)]
-    # The FP32 residual of a pose near its target is a difference of ~0.5 m
-    # coordinates, good to about 6e-8 m (3e-6 after the weight of 50), so the
-    # squared error carries an absolute error of about 2 * 3e-6 * sqrt(e)
-    # on top of the FP32 relative rounding of the sums.
+    # Each term of the weighted error is (w * r)^2 with w = 50 for position,
+    # 10 for rotation and sqrt(1e4) = 100 for a hinge of the collision
+    # penalty; r comes from FP32 poses and sphere centres good to about 1e-6 m
+    # (the measured FK and centre errors), so e carries an absolute error of
+    # about 2 * sqrt(e) * 100 * 1e-6 on top of the FP32 relative rounding of
+    # the sums.
     diff = np.abs(e32 - e64)
     rel = diff / np.maximum(np.abs(e64), 1e-12)
     big = e64 > 1e-2
@@ -94,7 +96,7 @@ def test_config2_against_the_port_on_all_problems(config2):
            "256 x 128 x 30")
     record("IK weighted error of the winner, FP32 kernel vs FP64 (absolute, errors <= 1e-2)", diff[~big],
            "256 x 128 x 30")
-    assert np.all(diff <= 1e-4 * e64 + 2e-5 * np.sqrt(e64) + 1e-9), float(np.max(diff - 1e-4 * e64))
+    assert np.all(diff <= 1e-4 * e64 + 2e-4 * np.sqrt(e64) + 1e-9), float(np.max(diff - 1e-4 * e64))
     record("IK final position error of solved problems (FP64)", r.pos_err.cpu().numpy()[succ_g], "256 x 128 x 30",
            "m")
     record("IK final rotation error of solved problems (FP64)", r.rot_err.cpu().numpy()[succ_g], "256 x 128 x 30",
