@@ -151,6 +151,13 @@ typedef struct pk_lm_options {
                               iterative-refinement step when the squared ratio of the largest to the smallest
                               Cholesky pivot exceeds 1e6 (seed-group kernel: n_act <= 16, n_ee <= 2,
                               threads_per_seed 0 or 1; PK_ERR_INVALID elsewhere, pk_ik_batch included) */
+  int32_t obstacle_grid;    /* the LM kernels' obstacle tile: the world spheres are binned into a uniform grid of
+                              this many cells per axis, built per block in shared memory, and each joint's
+                              bounding sphere tests only its cell's list; 0 = default (8), 1..16 = that many,
+                              -1 = no grid (every obstacle takes the bounding test).  The seed-group kernels'
+                              results do not depend on it (each joint's hinge terms are summed in increasing
+                              obstacle order); the warp-per-seed body spreads its candidates over lanes by list
+                              position, so its sums may round differently */
 } pk_lm_options;
 
 /*

@@ -12,7 +12,8 @@ a device counter until the list is empty.  The per-class FP64 verification
 and winner selection (``pk_ik_verify_select``) follow on the same stream.
 The whole solve can be captured once in a CUDA graph and replayed; an
 autotuner picks the seed-group kernel's lanes per seed and seeds per block
-and the warp body's lanes per seed by timing the actual batch.
+the warp body's lanes per seed and the obstacle tile (the per-block obstacle
+grid's cells per axis) by timing the actual batch.
 
 It is the persistent form of calling ``ls_ik_solve_cuda_batch``
 (``src/pyroffi/optimization_engines/_ls_ik.py:1002-1172``) once per robot
@@ -228,12 +229,15 @@ class MixedIkBatch:
         self._graph = g
 
     # -- autotuning ---------------------------------------------------------
-    def autotune(self, candidates=((2, 64), (4, 32), (1, 128), (8, 16)), wide_lanes=(16, 32), reps: int = 2):
+    def autotune(self, candidates=((1, 128), (1, 64), (2, 64), (4, 32)), wide_lanes=(16, 32), grids=(0, 4, 6),
+                 reps: int = 2):
         """Time the prepared batch for each (threads_per_seed, seeds_per_block)
-        of the seed-group body and each lane count per seed of the warp body
-        (the item list is rebuilt for each, since a seed-group item holds one
-        block's seeds) and keep the fastest.  Returns
-        {(threads_per_seed, seeds_per_block, lanes_per_wide_seed): ms}."""
+        of the 8-wide seed-group body, each lane count per seed of the warp
+        body and each obstacle tile (``obstacle_grid``: the cells per axis of
+        the per-block obstacle grid, 0 = the default 8, -1 = none), and keep
+        the fastest.  The item list is rebuilt for each, since a seed-group
+        item holds one block's seeds.  Returns {(threads_per_seed,
+        seeds_per_block, lanes_per_wide_seed, obstacle_grid): ms}."""
         used = {b for c, b in enumerate(self.bodies) if self.counts[c]}
         if BODY_SEED_GROUP not in used:
             candidates = ((self.opt.threads_per_seed, self.opt.seeds_per_block),)
@@ -242,20 +246,22 @@ class MixedIkBatch:
         results = {}
         for tps, spb in candidates:
             for lanes in wide_lanes:
-                self.opt.threads_per_seed, self.opt.seeds_per_block = tps, spb
-                self.opt.lanes_per_wide_seed = lanes
-                self._build_items()
-                self.run_lm()
-                torch.cuda.synchronize(self.device)
-                ts = []
-                for _ in range(reps):
-                    t0 = time.perf_counter()
+                for grid in grids:
+                    self.opt.threads_per_seed, self.opt.seeds_per_block = tps, spb
+                    self.opt.lanes_per_wide_seed, self.opt.obstacle_grid = lanes, grid
+                    self._build_items()
                     self.run_lm()
                     torch.cuda.synchronize(self.device)
-                    ts.append(time.perf_counter() - t0)
-                results[(tps, spb, lanes)] = 1e3 * min(ts)
-        tps, spb, lanes = min(results, key=results.get)
-        self.opt.threads_per_seed, self.opt.seeds_per_block, self.opt.lanes_per_wide_seed = tps, spb, lanes
+                    ts = []
+                    for _ in range(reps):
+                        t0 = time.perf_counter()
+                        self.run_lm()
+                        torch.cuda.synchronize(self.device)
+                        ts.append(time.perf_counter() - t0)
+                    results[(tps, spb, lanes, grid)] = 1e3 * min(ts)
+        tps, spb, lanes, grid = min(results, key=results.get)
+        self.opt.threads_per_seed, self.opt.seeds_per_block = tps, spb
+        self.opt.lanes_per_wide_seed, self.opt.obstacle_grid = lanes, grid
         self._build_items()
         self._graph = None
         return results

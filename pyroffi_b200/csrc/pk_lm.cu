@@ -66,6 +66,7 @@ struct LmArgs {
   float coll_w, margin;
   int spb;
   int f32_solve;  // FP32 normal equations + conditional FP64 refinement (seed-group kernel, one lane per seed)
+  int grid_n;     // obstacle grid cells per axis (0: no grid, every obstacle takes the bounding test)
 };
 
 // Shared-memory layout of one LM block.
@@ -84,6 +85,7 @@ struct LmShared {
   int n_rs;                        // valid robot spheres after staging
   int n_groups;                    // self-pair groups
   int grid_on;
+  int grid_n;                      // cells per axis of the grid in use
   float3 glo, ginv;                // obstacle grid origin, inverse cell size
   float rmax;                      // largest joint bounding radius
 };
@@ -149,7 +151,7 @@ __host__ __device__ inline LmLayout lm_layout(const LmArgs& a, int tps, int thre
   } else {
     L.scratch_ints = 7 * a.m.n_joints * threads;  // the pose slots double as staging scratch
   }
-  L.grid = (a.coll && a.w.Ms >= 32 && a.w.Ms <= 65535 && a.w.Ms <= L.scratch_ints) ? 1 : 0;
+  L.grid = (a.grid_n > 0 && a.coll && a.w.Ms >= 32 && a.w.Ms <= 65535 && a.w.Ms <= L.scratch_ints) ? 1 : 0;
   L.max_entries = L.grid ? min(max(48 * a.w.Ms, 1024), 16384) : 0;
   L.rs = o; o = lm_align16(o + 16 * (size_t)n_rs);
   L.rsp = o; o = lm_align16(o + (threads == 0 ? 16 * (size_t)(n_rs + a.m.n_joints) : 0));
@@ -166,7 +168,7 @@ __host__ __device__ inline LmLayout lm_layout(const LmArgs& a, int tps, int thre
   L.gstart = o; o = lm_align16(o + 4 * (size_t)(n_self + 2));
   L.rsj = o; o = lm_align16(o + 4 * (size_t)n_rs);
   L.rsk = o; o = lm_align16(o + 4 * (size_t)n_rs);
-  L.cells = o; o = lm_align16(o + (L.grid ? 4 * (size_t)(kObsGridCells + 1) : 0));
+  L.cells = o; o = lm_align16(o + (L.grid ? 4 * (size_t)(obstacle_grid_cells(a.grid_n) + 1) : 0));
   L.cell_obs = o; o = lm_align16(o + 2 * (size_t)L.max_entries);
   L.wc = o; o = lm_align16(o + 28 * (size_t)a.w.Mc);
   L.wb = o; o = lm_align16(o + 60 * (size_t)a.w.Mb);
@@ -238,6 +240,7 @@ struct PenaltyCtx {
   float* cen;            // this seed's bounding centres: component c of slot j at cen[(3 j + c) * cs]
   int cs;
   float3 glo, ginv;      // grid origin and inverse cell size
+  int gn;                // grid cells per axis
   int n_rs, n_js, n_groups, Ms_pad, Mc, Mb, Mh;
   float margin;
 };
@@ -444,7 +447,7 @@ __device__ float penalty_share(const PenaltyCtx& c, const PoseSlots& ps, int t, 
       const float Bx = cen[(3 * j) * cs], By = cen[(3 * j + 1) * cs], Bz = cen[(3 * j + 2) * cs];
       const int p0 = c.pjstart[j], p1 = c.pjstart[j + 1];
       if (c.cell_start) {
-        const int cell = obstacle_grid_cell(c.glo, c.ginv, make_float3(Bx, By, Bz));
+        const int cell = obstacle_grid_cell(c.glo, c.ginv, c.gn, make_float3(Bx, By, Bz));
         if (cell < 0) continue;  // outside the grid no obstacle is within reach of this joint
         const int e1 = c.cell_start[cell + 1];
         // the lane's candidates in chunks of 32: bounding tests into a survivor
@@ -1001,8 +1004,9 @@ __device__ void lm_stage(const LmArgs& a, unsigned char* smem_raw, const LmLayou
     sh.n_groups = n_groups;
     // obstacle-grid bounds (world radii already carry the margin)
     sh.grid_on = 0;
+    sh.grid_n = a.grid_n;
     if (L.grid && n_js > 0) {
-      obstacle_grid_bounds(ws4, a.w.Ms, rmax, sh.glo, sh.ginv);
+      obstacle_grid_bounds(ws4, a.w.Ms, rmax, a.grid_n, sh.glo, sh.ginv);
       sh.rmax = rmax;
       sh.grid_on = 1;
     }
@@ -1010,8 +1014,8 @@ __device__ void lm_stage(const LmArgs& a, unsigned char* smem_raw, const LmLayou
   __syncthreads();
 
   if (sh.grid_on)
-    obstacle_grid_build(ws4, a.w.Ms, sh.rmax, sh.glo, sh.ginv, scratch, cell_start, cell_obs, L.max_entries,
-                        sh.grid_on);
+    obstacle_grid_build(ws4, a.w.Ms, sh.rmax, sh.grid_n, sh.glo, sh.ginv, scratch, cell_start, cell_obs,
+                        L.max_entries, sh.grid_on);
 }
 
 // `count` seeds of problem pb, with the block's shared memory already
@@ -1056,7 +1060,7 @@ __device__ __forceinline__ void lm_seed_groups(const LmArgs& a, unsigned char* s
   pc.ws = ws4; pc.wc = wc; pc.wb = wb; pc.wh = wh; pc.prec = prec; pc.gjoint = gjoint;
   pc.pgstart = reinterpret_cast<const int*>(smem_raw + L.pgstart);
   pc.cell_start = sh.grid_on ? cell_start : nullptr; pc.cell_obs = cell_obs;
-  pc.cen = cen + g; pc.cs = a.spb; pc.glo = sh.glo; pc.ginv = sh.ginv;
+  pc.cen = cen + g; pc.cs = a.spb; pc.glo = sh.glo; pc.ginv = sh.ginv; pc.gn = sh.grid_n;
   pc.n_rs = sh.n_rs; pc.n_js = sh.n_js; pc.n_groups = sh.n_groups; pc.Ms_pad = L.ms_pad;
   pc.Mc = a.w.Mc; pc.Mb = a.w.Mb; pc.Mh = a.w.Mh; pc.margin = a.margin;
 
@@ -1290,6 +1294,7 @@ struct CoopCtx {
   const unsigned short* cell_obs;
   float4* pos;           // this seed's sphere world positions and radii [n_rs]
   float3 glo, ginv;
+  int gn;
   int n_rs, n_js, Ms, Mc, Mb, Mh;
   float margin;
 };
@@ -1317,7 +1322,7 @@ __device__ float coop_penalty(const CoopCtx& c, const PoseSlots& psk, int t, uns
     int e0 = 0, e1 = c.Ms;
     const unsigned short* list = nullptr;
     if (c.cell_start) {
-      const int cell = obstacle_grid_cell(c.glo, c.ginv, B);
+      const int cell = obstacle_grid_cell(c.glo, c.ginv, c.gn, B);
       if (cell < 0) continue;
       e0 = c.cell_start[cell];
       e1 = c.cell_start[cell + 1];
@@ -1421,7 +1426,7 @@ __global__ void __launch_bounds__(128, 4) lm_trial_kernel(LmArgs a) {
   cc.cell_start = sh.grid_on ? reinterpret_cast<const int*>(smem_raw + L.cells) : nullptr;
   cc.cell_obs = reinterpret_cast<const unsigned short*>(smem_raw + L.cell_obs);
   cc.pos = reinterpret_cast<float4*>(smem_raw + L.pos) + (size_t)(wid * 6 + gw) * lm_pos4_stride(a.n_rs);
-  cc.glo = sh.glo; cc.ginv = sh.ginv;
+  cc.glo = sh.glo; cc.ginv = sh.ginv; cc.gn = sh.grid_n;
   cc.n_rs = sh.n_rs; cc.n_js = sh.n_js; cc.Ms = a.w.Ms;
   cc.Mc = a.w.Mc; cc.Mb = a.w.Mb; cc.Mh = a.w.Mh; cc.margin = a.margin;
   const bool use_coll = a.coll && (sh.n_rs > 0);
@@ -1825,6 +1830,9 @@ static int lm_common(void* stream, const pk_lm_options& o, const float* seeds, c
   a.eps_pos = o.eps_pos; a.eps_ori = o.eps_ori;
   a.coll = o.enable_collision ? 1 : 0; a.coll_w = o.collision_weight; a.margin = o.collision_margin;
   a.f32_solve = o.fp32_solve ? 1 : 0;
+  PK_CHECK_ARG(o.obstacle_grid >= -1 && o.obstacle_grid <= kObsGridMax,
+               "obstacle_grid must be -1 (none), 0 (default) or 1..%d cells per axis", kObsGridMax);
+  a.grid_n = obstacle_grid_option(o.obstacle_grid);
   if (int s = validate_lm(a)) return s;
   if (P == 0 || Sd == 0) return PK_OK;
   PK_CHECK_ARG(seeds && twists && parent_tf && parent_idx && act_idx && mimic_mul && mimic_off &&
@@ -2003,6 +2011,7 @@ static int launch_seed_group_body(const BatchCall& b, int body, cudaStream_t st,
     a.coll = o.enable_collision ? 1 : 0; a.coll_w = o.collision_weight; a.margin = o.collision_margin;
     if (!a.coll) a.n_self = 0;
     a.spb = spb;
+    a.grid_n = obstacle_grid_option(o.obstacle_grid);
     if (int s = validate_lm(a)) return s;
     PK_CHECK_ARG(k.seeds && k.out_cfg && k.out_err && k.target_Ts && k.lower && k.upper && k.fixed_mask,
                  "null buffer in class %d", c);
@@ -2057,6 +2066,8 @@ extern "C" int pk_ik_batch(void* stream, const pk_lm_options* opt, const pk_ik_c
                            const int32_t* items, int32_t n_items, int32_t* queue, int32_t blocks) {
   PK_CHECK_ARG(opt != nullptr && classes != nullptr, "null options or classes");
   PK_CHECK_ARG(!opt->fp32_solve, "fp32_solve is not offered by the batched kernels");
+  PK_CHECK_ARG(opt->obstacle_grid >= -1 && opt->obstacle_grid <= kObsGridMax,
+               "obstacle_grid must be -1 (none), 0 (default) or 1..%d cells per axis", kObsGridMax);
   PK_CHECK_ARG(n_classes >= 1, "at least one class is required");
   PK_CHECK_CAP(n_classes <= PK_MAX_CLASSES, "n_classes=%d exceeds %d", n_classes, PK_MAX_CLASSES);
   PK_CHECK_ARG(n_items >= 0 && Ms >= 0 && Mc >= 0 && Mb >= 0 && Mh >= 0, "negative extent");

@@ -63,6 +63,7 @@ struct WideLayout {
   size_t rs, rsj, rsk, pairs, ws, wc, wb, wh, cells, cell_obs, obox, warps, warp_bytes, total;
   size_t w_cfg, w_best, w_dact, w_trial, w_dcol, w_cs, w_r, w_fw, w_pee, w_T, w_J, w_A, w_y, w_pos, w_slot;
   int max_rs, max_self, max_joints, max_act, max_rows, max_entries, nwarps;
+  int grid_n;  // obstacle grid cells per axis (0: no grid)
 };
 
 struct WideLaunch {
@@ -78,6 +79,7 @@ struct WideLaunch {
   int n_items;
   int* queue;         // persistent: item counter; null: grid launch (problem blockIdx.y, seed block blockIdx.x)
   int grid_chunk;     // grid launch: seeds per block
+  int grid_n;         // obstacle grid cells per axis (0: no grid)
   WideLayout L;
 };
 
@@ -108,11 +110,12 @@ struct WideShared {
 __host__ __device__ inline size_t w_align16(size_t x) { return (x + 15) & ~size_t(15); }
 
 __host__ inline WideLayout wide_layout(int max_rs, int max_self, int max_joints, int max_act, int max_ee,
-                                       const WorldArgs& w, int nwarps) {
+                                       const WorldArgs& w, int nwarps, int grid_n) {
   WideLayout L{};
   L.max_rs = max_rs; L.max_self = max_self; L.max_joints = max_joints; L.max_act = max_act;
   L.max_rows = 6 * max_ee; L.nwarps = nwarps;
-  L.max_entries = (w.Ms >= 32 && w.Ms <= 65535) ? std::min(std::max(16 * w.Ms, 1024), 8192) : 0;
+  L.grid_n = grid_n;
+  L.max_entries = (grid_n > 0 && w.Ms >= 32 && w.Ms <= 65535) ? std::min(std::max(16 * w.Ms, 1024), 8192) : 0;
   size_t o = w_align16(sizeof(WideShared));
   L.rs = o; o = w_align16(o + 16 * (size_t)max_rs);
   L.rsj = o; o = w_align16(o + 4 * (size_t)max_rs);
@@ -122,7 +125,7 @@ __host__ inline WideLayout wide_layout(int max_rs, int max_self, int max_joints,
   L.wc = o; o = w_align16(o + 28 * (size_t)w.Mc);
   L.wb = o; o = w_align16(o + 60 * (size_t)w.Mb);
   L.wh = o; o = w_align16(o + 24 * (size_t)w.Mh);
-  L.cells = o; o = w_align16(o + (L.max_entries ? 4 * (size_t)(kObsGridCells + 1) : 0));
+  L.cells = o; o = w_align16(o + (L.max_entries ? 4 * (size_t)(obstacle_grid_cells(grid_n) + 1) : 0));
   L.cell_obs = o; o = w_align16(o + 2 * (size_t)L.max_entries);
   L.obox = o; o = w_align16(o + (L.max_entries ? 4 * (size_t)w.Ms : 0));
   // one warp's area
@@ -305,14 +308,15 @@ __device__ void wide_stage_class(const WideLaunch& P, const WideArgs& A, unsigne
     // obstacle-grid bounds (world radii already carry the margin)
     sh.grid_on = 0;
     if (L.max_entries > 0 && n_js > 0 && P.coll) {
-      obstacle_grid_bounds(ws4, w.Ms, rmax, sh.glo, sh.ginv);
+      obstacle_grid_bounds(ws4, w.Ms, rmax, L.grid_n, sh.glo, sh.ginv);
       sh.grid_on = 1;
     }
   }
   __syncthreads();
 
   if (sh.grid_on)
-    obstacle_grid_build(ws4, w.Ms, sh.rmax, sh.glo, sh.ginv, obox, cell_start, cell_obs, L.max_entries, sh.grid_on);
+    obstacle_grid_build(ws4, w.Ms, sh.rmax, L.grid_n, sh.glo, sh.ginv, obox, cell_start, cell_obs, L.max_entries,
+                        sh.grid_on);
 }
 
 // Targets of problem pb (threads < n_ee); the caller synchronises.
@@ -435,7 +439,7 @@ __device__ __noinline__ float w_penalty(const WideLaunch& P, const WideShared& s
       const float3 B = pose_apply(w_load(W.T, sh.js_joint[j]), make_float3(bl.x, bl.y, bl.z));
       int e0 = 0, n = Ms;
       if (sh.grid_on) {
-        const int cell = obstacle_grid_cell(sh.glo, sh.ginv, B);
+        const int cell = obstacle_grid_cell(sh.glo, sh.ginv, P.L.grid_n, B);
         // outside the grid no obstacle is within reach of this joint
         if (cell < 0) {
           n = 0;
@@ -834,6 +838,7 @@ static void wide_options(WideLaunch& P, const pk_lm_options& o) {
   P.max_iter = o.max_iter; P.pos_w = o.pos_weight; P.ori_w = o.ori_weight; P.lam0 = o.lambda_init;
   P.lam_down = o.lambda_down; P.lam_up = o.lambda_up; P.eps_pos = o.eps_pos; P.eps_ori = o.eps_ori;
   P.coll = o.enable_collision ? 1 : 0; P.coll_w = o.collision_weight; P.margin = o.collision_margin;
+  P.grid_n = obstacle_grid_option(o.obstacle_grid);
 }
 
 static int wide_group(const pk_lm_options& o) { return o.lanes_per_wide_seed == 32 ? 32 : 16; }
@@ -872,7 +877,7 @@ static int run_warp_t(WideLaunch& P, const WideMax& mx, int grid_seeds, int grid
   int best_threads = 0, best_per_sm = 0, best_groups = -1;
   WideLayout best{};
   for (int threads = 256; threads >= 64 && threads >= G; threads >>= 1) {
-    const WideLayout L = wide_layout(mx.rs, mx.self, mx.joints, mx.act, mx.ee, P.w, threads / G);
+    const WideLayout L = wide_layout(mx.rs, mx.self, mx.joints, mx.act, mx.ee, P.w, threads / G, P.grid_n);
     if (L.total > (size_t)max_smem) continue;
     if (int s = set_smem_limit((const void*)kern, L.total)) return s;
     int per_sm = 0;

@@ -14,11 +14,16 @@
 
 namespace pk {
 
-constexpr int kObsGrid = 8;                                      // cells per axis (indices packed in 4 bits)
-constexpr int kObsGridCells = kObsGrid * kObsGrid * kObsGrid;
+// Cells per axis G: a launch option (the obstacle tile of the IK kernels),
+// 8 by default, at most 16 (cell indices are packed in 4 bits).
+constexpr int kObsGridDefault = 8;
+constexpr int kObsGridMax = 16;
+__host__ __device__ __forceinline__ int obstacle_grid_cells(int G) { return G * G * G; }
+// pk_lm_options.obstacle_grid -> cells per axis: 0 the default, -1 no grid (0 here)
+__host__ __device__ __forceinline__ int obstacle_grid_option(int v) { return v == 0 ? kObsGridDefault : (v < 0 ? 0 : v); }
 
 // Origin and inverse cell size of the grid (one thread).
-__device__ inline void obstacle_grid_bounds(const float4* ws, int Ms, float reach, float3& lo, float3& inv) {
+__device__ inline void obstacle_grid_bounds(const float4* ws, int Ms, float reach, int G, float3& lo, float3& inv) {
   float l[3] = {3e38f, 3e38f, 3e38f}, h[3] = {-3e38f, -3e38f, -3e38f};
   for (int o = 0; o < Ms; ++o) {
     const float4 O = ws[o];
@@ -28,20 +33,20 @@ __device__ inline void obstacle_grid_bounds(const float4* ws, int Ms, float reac
     l[2] = fminf(l[2], O.z - rho); h[2] = fmaxf(h[2], O.z + rho);
   }
   lo = make_float3(l[0], l[1], l[2]);
-  inv = make_float3(kObsGrid / fmaxf(h[0] - l[0], 1e-6f), kObsGrid / fmaxf(h[1] - l[1], 1e-6f),
-                    kObsGrid / fmaxf(h[2] - l[2], 1e-6f));
+  inv = make_float3(G / fmaxf(h[0] - l[0], 1e-6f), G / fmaxf(h[1] - l[1], 1e-6f), G / fmaxf(h[2] - l[2], 1e-6f));
 }
 
-// Cell lists: cell_start[kObsGridCells + 1] offsets into cell_obs; obox[Ms]
+// Cell lists: cell_start[G^3 + 1] offsets into cell_obs; obox[Ms]
 // is scratch.  Called by every thread of the block with block-uniform
 // arguments; `on` (shared) is cleared when the lists would exceed
 // max_entries, and the caller then scans every obstacle instead.  Each
 // obstacle adds itself to the cells of its box (shared-memory atomics), and
 // every cell's list is then sorted, so the lists hold increasing obstacle
 // indices whatever the order of the atomics.
-__device__ inline void obstacle_grid_build(const float4* ws, int Ms, float reach, float3 lo, float3 inv, int* obox,
-                                           int* cell_start, unsigned short* cell_obs, int max_entries, int& on) {
-  constexpr int G = kObsGrid, NC = kObsGridCells;
+__device__ inline void obstacle_grid_build(const float4* ws, int Ms, float reach, int G, float3 lo, float3 inv,
+                                           int* obox, int* cell_start, unsigned short* cell_obs, int max_entries,
+                                           int& on) {
+  const int NC = obstacle_grid_cells(G);
   const int tid = threadIdx.x, nth = blockDim.x;
   for (int c = tid; c <= NC; c += nth) cell_start[c] = 0;
   for (int o = tid; o < Ms; o += nth) {
@@ -104,8 +109,7 @@ __device__ inline void obstacle_grid_build(const float4* ws, int Ms, float reach
 }
 
 // Cell of point B, or -1 outside the grid (no obstacle within reach).
-__device__ __forceinline__ int obstacle_grid_cell(float3 lo, float3 inv, float3 B) {
-  constexpr int G = kObsGrid;
+__device__ __forceinline__ int obstacle_grid_cell(float3 lo, float3 inv, int G, float3 B) {
   const int ix = __float2int_rd((B.x - lo.x) * inv.x);
   const int iy = __float2int_rd((B.y - lo.y) * inv.y);
   const int iz = __float2int_rd((B.z - lo.z) * inv.z);

@@ -79,7 +79,7 @@ __host__ __device__ inline size_t seed_ik_grid_offset(const SeedIkArgs& a) {
 }
 __host__ __device__ inline size_t seed_ik_grid_bytes(const SeedIkArgs& a) {
   if (!a.grid_entries) return 0;
-  return seed_ik_align16(sizeof(int) * (kObsGridCells + 1)) + seed_ik_align16(2 * (size_t)a.grid_entries) +
+  return seed_ik_align16(sizeof(int) * (obstacle_grid_cells(kObsGridDefault) + 1)) + seed_ik_align16(2 * (size_t)a.grid_entries) +
          seed_ik_align16(sizeof(int) * (size_t)a.w.Ms);
 }
 __host__ __device__ inline size_t seed_ik_slots_offset(const SeedIkArgs& a) {
@@ -186,18 +186,18 @@ __device__ inline void seed_ik_stage(const SeedIkArgs& a, SeedIkShared& sh, Robo
     unsigned char* g = reinterpret_cast<unsigned char*>(world_dst) + (seed_ik_grid_offset(a) - seed_ik_world_offset(a));
     int* cell_start = reinterpret_cast<int*>(g);
     unsigned short* cell_obs =
-        reinterpret_cast<unsigned short*>(g + seed_ik_align16(sizeof(int) * (kObsGridCells + 1)));
+        reinterpret_cast<unsigned short*>(g + seed_ik_align16(sizeof(int) * (obstacle_grid_cells(kObsGridDefault) + 1)));
     int* obox = reinterpret_cast<int*>(reinterpret_cast<unsigned char*>(cell_obs) +
                                        seed_ik_align16(2 * (size_t)a.grid_entries));
     float reach = 0.f;
     for (int k = 0; k < R.ng; ++k) reach = fmaxf(reach, R.bound[k].w);
     reach += a.collision_margin;
     if (tid == 0) {
-      obstacle_grid_bounds(ob.sph, ob.Ms, reach, sh.glo, sh.ginv);
+      obstacle_grid_bounds(ob.sph, ob.Ms, reach, kObsGridDefault, sh.glo, sh.ginv);
       sh.grid_on = 1;
     }
     __syncthreads();
-    obstacle_grid_build(ob.sph, ob.Ms, reach, sh.glo, sh.ginv, obox, cell_start, cell_obs, a.grid_entries,
+    obstacle_grid_build(ob.sph, ob.Ms, reach, kObsGridDefault, sh.glo, sh.ginv, obox, cell_start, cell_obs, a.grid_entries,
                         sh.grid_on);
     if (sh.grid_on) {
       R.cell_start = cell_start;
@@ -313,7 +313,7 @@ __device__ __forceinline__ float seed_ik_penalty(const SeedIkArgs& a, const Pose
     };
     int m0 = 0;
     if (R.cell_start) {
-      const int cell = obstacle_grid_cell(R.glo, R.ginv, B);
+      const int cell = obstacle_grid_cell(R.glo, R.ginv, kObsGridDefault, B);
       if (cell >= 0) {
         const int e1 = R.cell_start[cell + 1];
         for (int e = R.cell_start[cell] + gl; e < e1; e += TPS) {

@@ -157,8 +157,8 @@ def test_batch_autotune_keeps_results(mixed):
     b = make_batch(w)
     b.run_lm()
     base = [e.clone() for e in b.out_err]
-    res = b.autotune(candidates=((2, 64), (4, 32)), wide_lanes=(16, 32), reps=1)
-    assert set(res) == {(2, 64, 16), (2, 64, 32), (4, 32, 16), (4, 32, 32)}
+    res = b.autotune(candidates=((2, 64), (4, 32)), wide_lanes=(16, 32), grids=(0, -1), reps=1)
+    assert set(res) == {(t, s, l, g) for t, s in ((2, 64), (4, 32)) for l in (16, 32) for g in (0, -1)}
     b.run_lm()
     # lanes per seed change the order of the penalty sum only; an accept test
     # on the edge may flip for a few seeds
@@ -192,3 +192,27 @@ def test_batch_success_vs_oracle_small(mixed):
             or_ok += int(max(pe_all) < w.pos_tol and max(re_all) < w.rot_tol)
         gpu_ok = int(res[c].success.cpu().numpy()[[int(w.index_in_class[p]) for p in probs]].sum())
         assert gpu_ok >= or_ok - 1, (c, gpu_ok, or_ok)
+
+
+@pytest.mark.parametrize("grid", [4, 12, 16, -1])
+def test_obstacle_tile_leaves_results_unchanged(mixed, grid):
+    """The obstacle tile (cells per axis of the per-block grid, or none) only
+    changes which obstacles take the bounding test.  The seed-group bodies
+    still sum the hinge terms of each joint in increasing obstacle order, so
+    their outputs are the same bits as with the default grid; the warp body
+    spreads the (joint, candidate) pairs over its lanes by list position, so
+    its sums may change order (rounding only)."""
+    w = mixed
+    b = make_batch(w)
+    b.run_lm()
+    base = [(c.clone(), e.clone()) for c, e in zip(b.out_cfg, b.out_err)]
+    b.opt.obstacle_grid = grid
+    b.run_lm()
+    for c in range(len(w.classes)):
+        m = torch.as_tensor(used_mask(b, c), device=DEV)
+        if b.bodies[c] != BODY_WARP:
+            assert torch.equal(b.out_err[c][m], base[c][1][m]), c
+            assert torch.equal(b.out_cfg[c][m], base[c][0][m]), c
+        else:
+            a, e = b.out_err[c][m].cpu().numpy(), base[c][1][m].cpu().numpy()
+            assert np.mean(np.abs(a - e) <= 1e-4 * np.abs(e) + 1e-5) >= 0.95
