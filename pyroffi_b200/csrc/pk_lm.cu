@@ -667,12 +667,14 @@ __device__ __forceinline__ void lm_solve_f32(const LmShared& sh, const float (&J
 // scaling, normal equations (Js^T Js + lam I) p = -Js^T fw with fixed and
 // padded joints masked, Cholesky solve (p = 0 on a non-positive pivot),
 // unscaling and the trust-region clip.  Writes `delta`, returns ||fw||^2.
-// F32S false: the normal equations and the Cholesky in FP64, as the
-// reference.  F32S true: both in FP32, and when the squared ratio of the
-// largest to the smallest Cholesky pivot exceeds 1e6, one step of iterative
-// refinement: the residual b - A x in FP64 (A applied as Js^T (Js x) + lam x
-// from the FP32 Jacobian entries, which FP64 holds exactly), the correction
-// solved with the FP32 factor.
+// F32S false: the damped system solved in FP64 through its R x R dual form
+// (R = 6 MAXEE residual rows; the reference solves the MAXA x MAXA normal
+// equations in FP64, the same step in exact arithmetic).  F32S true: the
+// MAXA x MAXA normal equations and their Cholesky in FP32, and when the
+// squared ratio of the largest to the smallest Cholesky pivot exceeds 1e6,
+// one step of iterative refinement: the residual b - A x in FP64 (A applied
+// as Js^T (Js x) + lam x from the FP32 Jacobian entries, which FP64 holds
+// exactly), the correction solved with the FP32 factor.
 template <int MAXA, int MAXEE, bool F32S = false>
 __device__ __forceinline__ float lm_direction(const LmShared& sh, const PoseSlots& ps, int n_ee, const float (&W)[6],
                                               const float (&r)[6 * MAXEE], const float (&pee)[3 * MAXEE],
@@ -740,62 +742,69 @@ __device__ __forceinline__ float lm_direction(const LmShared& sh, const PoseSlot
   if constexpr (F32S) {
     lm_solve_f32<MAXA, MAXEE>(sh, J, fw, lam, col_s, delta);
   } else {
-  // FP64 normal equations (lower triangle, packed) + masking
-  double A[MAXA * (MAXA + 1) / 2];
-  double rhs[MAXA];
+  // FP64, through the push-through identity
+  //   (Js^T Js + lam I)^-1 Js^T = Js^T (Js Js^T + lam I)^-1,
+  // so p = -Js^T y with (Js Js^T + lam I) y = fw: an R x R system (R = 6
+  // MAXEE rows) instead of MAXA x MAXA, the same step in exact arithmetic.
+  // Fixed and padded joints enter as zero columns of Js, which gives them a
+  // zero step and the other joints the step of the reduced system, as the
+  // masked MAXA x MAXA system does (lam > 0 keeps both positive definite).
+  constexpr int R = 6 * MAXEE;
+  double A[R * (R + 1) / 2];
+  double y[R];
 #pragma unroll
-  for (int i = 0; i < MAXA; ++i) {
-    const bool fi = sh.fixed[i];
+  for (int i = 0; i < R; ++i) {
 #pragma unroll
     for (int j = 0; j <= i; ++j) {
-      double acc = 0.0;
+      double acc = (i == j) ? (double)lam : 0.0;
 #pragma unroll
-      for (int k = 0; k < 6 * MAXEE; ++k) acc += (double)J[k][i] * (double)J[k][j];
-      if (i == j) acc += (double)lam;
-      const bool fj = sh.fixed[j];
-      A[i * (i + 1) / 2 + j] = (fi || fj) ? ((i == j) ? 1.0 : 0.0) : acc;
+      for (int c = 0; c < MAXA; ++c)
+        if (!sh.fixed[c]) acc = fma((double)J[i][c], (double)J[j][c], acc);
+      A[i * (i + 1) / 2 + j] = acc;
     }
-    double rb = 0.0;
-#pragma unroll
-    for (int k = 0; k < 6 * MAXEE; ++k) rb += (double)J[k][i] * (double)fw[k];
-    rhs[i] = fi ? 0.0 : -rb;
+    y[i] = (double)fw[i];
   }
   // Cholesky A = L L^T in place; a non-positive pivot zeroes the step
   bool ok = true;
 #pragma unroll
-  for (int k = 0; k < MAXA; ++k) {
+  for (int k = 0; k < R; ++k) {
     double s2 = A[k * (k + 1) / 2 + k];
 #pragma unroll
     for (int q = 0; q < k; ++q) s2 -= A[k * (k + 1) / 2 + q] * A[k * (k + 1) / 2 + q];
     if (!(s2 > 0.0)) ok = false;
     const double lkk = sqrt(ok ? s2 : 1.0);
     const double inv = 1.0 / lkk;
-    A[k * (k + 1) / 2 + k] = lkk;
+    A[k * (k + 1) / 2 + k] = inv;
 #pragma unroll
-    for (int i = k + 1; i < MAXA; ++i) {
+    for (int i = k + 1; i < R; ++i) {
       double tt = A[i * (i + 1) / 2 + k];
 #pragma unroll
       for (int q = 0; q < k; ++q) tt -= A[i * (i + 1) / 2 + q] * A[k * (k + 1) / 2 + q];
       A[i * (i + 1) / 2 + k] = tt * inv;
     }
   }
-  // forward / backward substitution
+  // forward / backward substitution (the diagonal holds reciprocals)
 #pragma unroll
-  for (int i = 0; i < MAXA; ++i) {
-    double s2 = rhs[i];
+  for (int i = 0; i < R; ++i) {
+    double s2 = y[i];
 #pragma unroll
-    for (int q = 0; q < i; ++q) s2 -= A[i * (i + 1) / 2 + q] * rhs[q];
-    rhs[i] = s2 / A[i * (i + 1) / 2 + i];
+    for (int q = 0; q < i; ++q) s2 -= A[i * (i + 1) / 2 + q] * y[q];
+    y[i] = s2 * A[i * (i + 1) / 2 + i];
   }
 #pragma unroll
-  for (int i = MAXA - 1; i >= 0; --i) {
-    double s2 = rhs[i];
+  for (int i = R - 1; i >= 0; --i) {
+    double s2 = y[i];
 #pragma unroll
-    for (int q = i + 1; q < MAXA; ++q) s2 -= A[q * (q + 1) / 2 + i] * rhs[q];
-    rhs[i] = s2 / A[i * (i + 1) / 2 + i];
+    for (int q = i + 1; q < R; ++q) s2 -= A[q * (q + 1) / 2 + i] * y[q];
+    y[i] = s2 * A[i * (i + 1) / 2 + i];
   }
 #pragma unroll
-  for (int c = 0; c < MAXA; ++c) delta[c] = ok ? (float)rhs[c] / col_s[c] : 0.f;
+  for (int c = 0; c < MAXA; ++c) {
+    double pc = 0.0;
+#pragma unroll
+    for (int k = 0; k < R; ++k) pc = fma((double)J[k][c], y[k], pc);
+    delta[c] = (ok && !sh.fixed[c]) ? (float)(-pc) / col_s[c] : 0.f;
+  }
   }
   float dn2 = 0.f;
 #pragma unroll
