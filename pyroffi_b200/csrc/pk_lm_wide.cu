@@ -574,38 +574,51 @@ __device__ __noinline__ float w_direction(const WideShared& sh, int n_act, int n
   float fw2 = 0.f;
   for (int k = 0; k < rows; ++k) fw2 += W.fw[k] * W.fw[k];
 
-  // FP64 normal equations, packed lower triangle: lanes take the entries
-  // e = i (i + 1) / 2 + j in turn
+  // FP64 damped system, packed lower triangle: lanes take the entries
+  // e = i (i + 1) / 2 + j in turn.  With fewer residual rows than active
+  // columns it is the dual form (Js Js^T + lam I) y = fw, p = -Js^T y (the
+  // push-through identity: the same step as (Js^T Js + lam I) p = -Js^T fw,
+  // on a rows x rows system); otherwise the normal equations themselves.
+  const bool dual = rows < ncol;
+  const int n = dual ? rows : ncol;
   {
-    const int ne = ncol * (ncol + 1) / 2;
+    const int ne = n * (n + 1) / 2;
     int i = 0, j = gl;
-    while (i < ncol && j > i) { j -= i + 1; ++i; }
+    while (i < n && j > i) { j -= i + 1; ++i; }
     for (int e = gl; e < ne; e += G) {
       double acc = 0.0;
-      for (int k = 0; k < rows; ++k) acc += (double)W.J[i * rows + k] * (double)W.J[j * rows + k];
+      if (dual) {
+        for (int c = 0; c < ncol; ++c) acc += (double)W.J[c * rows + i] * (double)W.J[c * rows + j];
+      } else {
+        for (int k = 0; k < rows; ++k) acc += (double)W.J[i * rows + k] * (double)W.J[j * rows + k];
+      }
       if (i == j) acc += (double)lam;
       W.A[e] = acc;
       j += G;
-      while (i < ncol && j > i) { j -= i + 1; ++i; }
+      while (i < n && j > i) { j -= i + 1; ++i; }
     }
   }
-  for (int i = gl; i < ncol; i += G) {
-    double rb = 0.0;
-    for (int k = 0; k < rows; ++k) rb += (double)W.J[i * rows + k] * (double)W.fw[k];
-    W.y[i] = -rb;
+  if (dual) {
+    for (int i = gl; i < rows; i += G) W.y[i] = (double)W.fw[i];
+  } else {
+    for (int i = gl; i < ncol; i += G) {
+      double rb = 0.0;
+      for (int k = 0; k < rows; ++k) rb += (double)W.J[i * rows + k] * (double)W.fw[k];
+      W.y[i] = -rb;
+    }
   }
   __syncwarp(gm);
 
   // Cholesky A = L L^T, left-looking; a non-positive pivot zeroes the step.
   // The diagonal keeps 1 / L[k][k] (every later use multiplies by it).
   bool ok = true;
-  for (int k = 0; k < ncol; ++k) {
+  for (int k = 0; k < n; ++k) {
     const int kk = k * (k + 1) / 2;
     double s2 = W.A[kk + k];
     for (int q = 0; q < k; ++q) s2 -= W.A[kk + q] * W.A[kk + q];
     if (!(s2 > 0.0)) ok = false;
     const double inv = 1.0 / sqrt(ok ? s2 : 1.0);
-    for (int i = k + 1 + gl; i < ncol; i += G) {
+    for (int i = k + 1 + gl; i < n; i += G) {
       const int ii = i * (i + 1) / 2;
       double tt = W.A[ii + k];
       for (int q = 0; q < k; ++q) tt -= W.A[ii + q] * W.A[kk + q];
@@ -616,14 +629,14 @@ __device__ __noinline__ float w_direction(const WideShared& sh, int n_act, int n
     __syncwarp(gm);
   }
   // L y = b, then L^T x = y (column by column; x overwrites y)
-  for (int i = 0; i < ncol; ++i) {
+  for (int i = 0; i < n; ++i) {
     const double yi = W.y[i] * W.A[i * (i + 1) / 2 + i];
-    for (int j = i + 1 + gl; j < ncol; j += G) W.y[j] -= W.A[j * (j + 1) / 2 + i] * yi;
+    for (int j = i + 1 + gl; j < n; j += G) W.y[j] -= W.A[j * (j + 1) / 2 + i] * yi;
     __syncwarp(gm);
     if (gl == 0) W.y[i] = yi;
     __syncwarp(gm);
   }
-  for (int i = ncol - 1; i >= 0; --i) {
+  for (int i = n - 1; i >= 0; --i) {
     const int ii = i * (i + 1) / 2;
     const double xi = W.y[i] * W.A[ii + i];
     for (int j = gl; j < i; j += G) W.y[j] -= W.A[ii + j] * xi;
@@ -631,7 +644,15 @@ __device__ __noinline__ float w_direction(const WideShared& sh, int n_act, int n
     if (gl == 0) W.y[i] = xi;
     __syncwarp(gm);
   }
-  for (int c = gl; c < ncol; c += G) W.dcol[c] = ok ? (float)W.y[c] / W.cs[c] : 0.f;
+  if (dual) {
+    for (int c = gl; c < ncol; c += G) {
+      double pc = 0.0;
+      for (int k = 0; k < rows; ++k) pc += (double)W.J[c * rows + k] * W.y[k];
+      W.dcol[c] = ok ? (float)(-pc) / W.cs[c] : 0.f;
+    }
+  } else {
+    for (int c = gl; c < ncol; c += G) W.dcol[c] = ok ? (float)W.y[c] / W.cs[c] : 0.f;
+  }
   __syncwarp(gm);
   float dn2 = 0.f;
   for (int c = 0; c < ncol; ++c) dn2 += W.dcol[c] * W.dcol[c];
