@@ -143,7 +143,8 @@ typedef struct pk_lm_options {
   int32_t enable_collision;
   float collision_weight;
   float collision_margin;
-  int32_t threads_per_seed; /* 0 = default (1); 1, 2, 4, 8 = lanes sharing one seed; 5 = one lane per line-search
+  int32_t threads_per_seed; /* 0 = default (1 lane; 128 seeds per block up to 8 DOF / 1 EE, 96 up to 16 DOF /
+                              2 EEs); 1, 2, 4, 8 = lanes sharing one seed; 5 = one lane per line-search
                               trial; 16, 32 = warp-per-seed body with that many lanes per seed */
   int32_t seeds_per_block;  /* 0 = choose automatically */
   int32_t lanes_per_wide_seed; /* warp-per-seed body: lanes per seed, 16 (0 = default) or 32 */
@@ -190,7 +191,7 @@ int pk_ls_ik_ex(void* stream, const pk_lm_options* opt, const float* seeds, cons
  *           seeds per block from pk_lm_options);
  *   body 1: one warp per seed with its state in shared memory
  *           (n_act <= 32, n_ee <= 4);
- *   body 2: seed-group kernel, one lane per seed, 128 seeds per block
+ *   body 2: seed-group kernel, one lane per seed, 96 seeds per block
  *           (n_act <= 16, n_ee <= 2).
  */
 typedef struct pk_ik_class {
@@ -231,7 +232,7 @@ typedef struct pk_ik_class {
  * (class, problem, first seed, seed count) in device memory, in the order
  * blocks should take them (longest first balances the tail); a body-0 item
  * holds at most seeds_per_block seeds (128 when that is 0 and
- * threads_per_seed is 0 or 1), a body-2 item at most 128.  Each body runs
+ * threads_per_seed is 0 or 1), a body-2 item at most 96.  Each body runs
  * one persistent kernel whose blocks take items from a device counter in
  * queue[2] (caller-owned device memory; cleared here with async memsets on
  * `stream` before the launches, so one queue serves one call in flight at

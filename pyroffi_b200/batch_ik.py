@@ -117,14 +117,15 @@ class MixedIkBatch:
 
     def _chunk(self, c: int) -> int:
         """Seeds per item: one block's seeds for the seed-group bodies (the
-        library's defaults: one lane x 128 seeds), 64 for the warp body."""
+        library's defaults: one lane x 128 seeds for the 8-wide body, one
+        lane x 96 seeds for the 16-wide body), 64 for the warp body."""
         if self.bodies[c] == BODY_SEED_GROUP:
             tps = self.opt.threads_per_seed if self.opt.threads_per_seed > 0 else 1
             if self.opt.seeds_per_block > 0:
                 return self.opt.seeds_per_block
             return 128 if self.opt.threads_per_seed <= 0 else 128 // tps
         if self.bodies[c] == BODY_SEED_GROUP16:
-            return 128
+            return 96
         return 64
 
     def _cost_per_seed(self, c: int) -> float:

@@ -112,6 +112,12 @@ __host__ __device__ __forceinline__ int lm_ms_pad(int Ms, int tps) {
 // Self-pair groups per chunk of the warp item list (one lane per seed).
 constexpr int kSelfChunk = 16;
 
+// Seeds per block of the 16-wide one-lane kernel by default: the 16-DOF /
+// 2-EE register state takes the whole register file at 2 blocks of 128
+// threads, and a 128-seed block's per-seed pose slots push a 500-obstacle
+// world's block past half of the SM's shared memory; 96 keeps 2 blocks.
+constexpr int kSeedsPerBlock16 = 96;
+
 // Trial-lane kernel: float4 positions per seed, padded by one float4 so the
 // 6 seeds of a warp reading the same sphere use different bank groups.
 __host__ __device__ __forceinline__ int lm_pos4_stride(int n_rs) { return n_rs + 1; }
@@ -175,7 +181,9 @@ __host__ __device__ inline LmLayout lm_layout(const LmArgs& a, int tps, int thre
   L.wh = o; o = lm_align16(o + 24 * (size_t)a.w.Mh);
   if (threads == 0) {
     L.slots = o; o = lm_align16(o + 28 * (size_t)a.m.n_joints * a.spb);
-    L.cen = o; o = lm_align16(o + (a.coll ? 12 * (size_t)a.m.n_joints * a.spb : 0));
+    // bounding centres are kept per seed only where other lanes read them:
+    // lanes sharing a seed (tps > 1) or the warp-shared self-pair items
+    L.cen = o; o = lm_align16(o + ((a.coll && (tps > 1 || n_self > 0)) ? 12 * (size_t)a.m.n_joints * a.spb : 0));
     L.scratch = L.slots;
     L.pos = o;
     o = max(o, lm_align16(L.scratch + 4 * (size_t)L.scratch_ints));
@@ -238,6 +246,7 @@ struct PenaltyCtx {
   const int* cell_start; // [G^3 + 1] obstacle grid (null: no grid, scan every obstacle)
   const unsigned short* cell_obs;
   float* cen;            // this seed's bounding centres: component c of slot j at cen[(3 j + c) * cs]
+                         // (null: not kept; each lane computes its seed's centres where it needs them)
   int cs;
   float3 glo, ginv;      // grid origin and inverse cell size
   int gn;                // grid cells per axis
@@ -433,18 +442,27 @@ __device__ float penalty_share(const PenaltyCtx& c, const PoseSlots& ps, int t, 
   float pen = 0.f;
   float* const cen = c.cen;
   const int cs = c.cs;
+  // bounding centre of joint slot j: kept per seed, or computed here
+  auto centre = [&](int j) {
+    if (cen) return make_float3(cen[(3 * j) * cs], cen[(3 * j + 1) * cs], cen[(3 * j + 2) * cs]);
+    const float4 bl = c.jb[j];
+    return pose_apply(ps.load(c.jlist[j]), make_float3(bl.x, bl.y, bl.z));
+  };
   if (need) {
-    for (int j = t; j < c.n_js; j += TPS) {
-      const Pose T = ps.load(c.jlist[j]);
-      const float4 bl = c.jb[j];
-      const float3 B = pose_apply(T, make_float3(bl.x, bl.y, bl.z));
-      cen[(3 * j) * cs] = B.x; cen[(3 * j + 1) * cs] = B.y; cen[(3 * j + 2) * cs] = B.z;
+    if (cen) {
+      for (int j = t; j < c.n_js; j += TPS) {
+        const Pose T = ps.load(c.jlist[j]);
+        const float4 bl = c.jb[j];
+        const float3 B = pose_apply(T, make_float3(bl.x, bl.y, bl.z));
+        cen[(3 * j) * cs] = B.x; cen[(3 * j + 1) * cs] = B.y; cen[(3 * j + 2) * cs] = B.z;
+      }
+      if (TPS > 1) __syncwarp(gmask);
     }
-    if (TPS > 1) __syncwarp(gmask);
 
     for (int j = 0; j < c.n_js && c.Ms_pad > 0; ++j) {
       const float R = c.jb[j].w;
-      const float Bx = cen[(3 * j) * cs], By = cen[(3 * j + 1) * cs], Bz = cen[(3 * j + 2) * cs];
+      const float3 Bj = centre(j);
+      const float Bx = Bj.x, By = Bj.y, Bz = Bj.z;
       const int p0 = c.pjstart[j], p1 = c.pjstart[j + 1];
       if (c.cell_start) {
         const int cell = obstacle_grid_cell(c.glo, c.ginv, c.gn, make_float3(Bx, By, Bz));
@@ -495,7 +513,7 @@ __device__ float penalty_share(const PenaltyCtx& c, const PoseSlots& ps, int t, 
 
     if (c.Mc + c.Mb + c.Mh > 0) {
       for (int j = t; j < c.n_js; j += TPS) {
-        const float3 B = make_float3(cen[(3 * j) * cs], cen[(3 * j + 1) * cs], cen[(3 * j + 2) * cs]);
+        const float3 B = centre(j);
         const float R = c.jb[j].w;
         const int k0 = c.jstart[j], k1 = c.jstart[j + 1];
         const Pose T = ps.load(c.jlist[j]);
@@ -1069,7 +1087,7 @@ __device__ __forceinline__ void lm_seed_groups(const LmArgs& a, unsigned char* s
   pc.ws = ws4; pc.wc = wc; pc.wb = wb; pc.wh = wh; pc.prec = prec; pc.gjoint = gjoint;
   pc.pgstart = reinterpret_cast<const int*>(smem_raw + L.pgstart);
   pc.cell_start = sh.grid_on ? cell_start : nullptr; pc.cell_obs = cell_obs;
-  pc.cen = cen + g; pc.cs = a.spb; pc.glo = sh.glo; pc.ginv = sh.ginv; pc.gn = sh.grid_n;
+  pc.cen = (TPS > 1 || (a.coll && a.n_self > 0)) ? cen + g : nullptr; pc.cs = a.spb; pc.glo = sh.glo; pc.ginv = sh.ginv; pc.gn = sh.grid_n;
   pc.n_rs = sh.n_rs; pc.n_js = sh.n_js; pc.n_groups = sh.n_groups; pc.Ms_pad = L.ms_pad;
   pc.Mc = a.w.Mc; pc.Mb = a.w.Mb; pc.Mh = a.w.Mh; pc.margin = a.margin;
 
@@ -1775,7 +1793,7 @@ static int launch_lm(LmArgs a, int tps, int spb, cudaStream_t st) {
   // body, are routed by lm_common.)
   if (tps <= 0) {
     tps = 1;
-    if (spb <= 0) spb = 128;
+    if (spb <= 0) spb = (a.n_act <= 8 && a.n_ee <= 1) ? 128 : kSeedsPerBlock16;
   }
   if (tps == 5) {
     PK_CHECK_ARG(!a.f32_solve, "fp32_solve runs with threads_per_seed 0 or 1");
@@ -1978,12 +1996,12 @@ static int launch_batch_t(const SeedGroupBatch& B, size_t smem, int threads, int
 
 // One persistent launch over the items of the classes of `body`
 // (kBodySeedGroup: 8-wide, lanes and seeds per block from the options;
-// kBodySeedGroup16: 16-wide, one lane per seed, 128 seeds per block).
+// kBodySeedGroup16: 16-wide, one lane per seed, kSeedsPerBlock16 seeds per block).
 static int launch_seed_group_body(const BatchCall& b, int body, cudaStream_t st, bool& queue_used, int& count) {
   int tps = b.opt.threads_per_seed, spb = b.opt.seeds_per_block;
   if (body == kBodySeedGroup16) {
     tps = 1;
-    spb = 128;
+    spb = kSeedsPerBlock16;
   }
   if (tps <= 0) { tps = 1; if (spb <= 0) spb = 128; }
   if (spb <= 0) spb = 128 / tps;
