@@ -161,7 +161,12 @@ __host__ __device__ inline LmLayout lm_layout(const LmArgs& a, int tps, int thre
   L.max_entries = L.grid ? min(max(48 * a.w.Ms, 1024), 16384) : 0;
   L.rs = o; o = lm_align16(o + 16 * (size_t)n_rs);
   L.rsp = o; o = lm_align16(o + (threads == 0 ? 16 * (size_t)(n_rs + a.m.n_joints) : 0));
+  // the world, in stage_world's layout: spheres in ms_pad float4 slots, then
+  // capsules, boxes, halfspaces, each on a 16-byte boundary
   L.ws = o; o = lm_align16(o + 16 * (size_t)L.ms_pad);
+  L.wc = o; o = lm_align16(o + 28 * (size_t)a.w.Mc);
+  L.wb = o; o = lm_align16(o + 60 * (size_t)a.w.Mb);
+  L.wh = o; o = lm_align16(o + 24 * (size_t)a.w.Mh);
   L.pairs = o; o = lm_align16(o + 8 * (size_t)n_self);
   L.pair4 = o; o = lm_align16(o + (threads > 0 ? 16 * (size_t)n_self : 0));
   L.prec = o; o = lm_align16(o + (threads == 0 ? 64 * (size_t)n_self : 0));
@@ -176,9 +181,6 @@ __host__ __device__ inline LmLayout lm_layout(const LmArgs& a, int tps, int thre
   L.rsk = o; o = lm_align16(o + 4 * (size_t)n_rs);
   L.cells = o; o = lm_align16(o + (L.grid ? 4 * (size_t)(obstacle_grid_cells(a.grid_n) + 1) : 0));
   L.cell_obs = o; o = lm_align16(o + 2 * (size_t)L.max_entries);
-  L.wc = o; o = lm_align16(o + 28 * (size_t)a.w.Mc);
-  L.wb = o; o = lm_align16(o + 60 * (size_t)a.w.Mb);
-  L.wh = o; o = lm_align16(o + 24 * (size_t)a.w.Mh);
   if (threads == 0) {
     L.slots = o; o = lm_align16(o + 28 * (size_t)a.m.n_joints * a.spb);
     // bounding centres are kept per seed only where other lanes read them:
@@ -882,13 +884,17 @@ __device__ void lm_stage(const LmArgs& a, unsigned char* smem_raw, const LmLayou
     sh.hi[i] = real ? a.upper[i] : 0.f;
     sh.fixed[i] = real ? (a.fixed_mask[i] != 0) : 1;
   }
-  for (int i = tid; i < L.ms_pad; i += blockDim.x)
-    ws4[i] = (i < a.w.Ms) ? make_float4(a.w.spheres[4 * i], a.w.spheres[4 * i + 1], a.w.spheres[4 * i + 2],
-                                        a.w.spheres[4 * i + 3] + a.margin)
-                          : make_float4(1e18f, 1e18f, 1e18f, 0.f);  // padding: never within reach
-  for (int i = tid; i < a.w.Mc * 7; i += blockDim.x) wc[i] = a.w.capsules[i];
-  for (int i = tid; i < a.w.Mb * 15; i += blockDim.x) wb[i] = a.w.boxes[i];
-  for (int i = tid; i < a.w.Mh * 6; i += blockDim.x) wh[i] = a.w.halfspaces[i];
+  // the world by the TMA bulk-copy engine (stage_world: bounded wait,
+  // plain-load fallback), then the margin folded into the sphere radii and
+  // the padding slots set, in place
+  (void)wc; (void)wb; (void)wh;
+  stage_world(a.w, reinterpret_cast<float*>(ws4), L.ms_pad);
+  __syncthreads();
+  for (int i = tid; i < L.ms_pad; i += blockDim.x) {
+    if (i < a.w.Ms) ws4[i].w = ws4[i].w + a.margin;
+    else ws4[i] = make_float4(1e18f, 1e18f, 1e18f, 0.f);  // padding: never within reach
+  }
+  __syncthreads();
 
   // Thread 0 (a few hundred serial steps, once per block): robot spheres
   // grouped by joint in topological order (invalid joint indices dropped, as

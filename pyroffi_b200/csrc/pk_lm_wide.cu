@@ -194,11 +194,13 @@ __device__ void wide_stage_class(const WideLaunch& P, const WideArgs& A, unsigne
     sh.lo[i] = real ? A.lower[i] : 0.f;
     sh.hi[i] = real ? A.upper[i] : 0.f;
   }
-  for (int i = tid; i < w.Ms; i += blockDim.x)
-    ws4[i] = make_float4(w.spheres[4 * i], w.spheres[4 * i + 1], w.spheres[4 * i + 2], w.spheres[4 * i + 3] + P.margin);
-  for (int i = tid; i < w.Mc * 7; i += blockDim.x) wc[i] = w.capsules[i];
-  for (int i = tid; i < w.Mb * 15; i += blockDim.x) wb[i] = w.boxes[i];
-  for (int i = tid; i < w.Mh * 6; i += blockDim.x) wh[i] = w.halfspaces[i];
+  // the world by the TMA bulk-copy engine (stage_world: bounded wait,
+  // plain-load fallback; its layout is this one's), then the margin folded
+  // into the sphere radii in place
+  (void)wc; (void)wb; (void)wh;
+  stage_world(w, reinterpret_cast<float*>(ws4));
+  __syncthreads();
+  for (int i = tid; i < w.Ms; i += blockDim.x) ws4[i].w = ws4[i].w + P.margin;
   __syncthreads();
 
   // Thread 0: active columns and their joint lists, FK levels, spheres

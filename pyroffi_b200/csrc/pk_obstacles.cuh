@@ -109,7 +109,9 @@ __device__ __forceinline__ unsigned long long global_ns() {
 // flight), the first wait runs out, and the block takes the plain-load path
 // without the second wait.  An array whose source is not 16-byte aligned,
 // and the bytes past the last 16-byte multiple, are copied with plain loads.
-__device__ inline ObsView stage_world(const WorldArgs& w, float* dst) {
+// sphere_slots (>= Ms; -1: Ms) float4 slots are reserved for the spheres,
+// so a caller can pad them; the other arrays follow the reserved slots.
+__device__ inline ObsView stage_world(const WorldArgs& w, float* dst, int sphere_slots = -1) {
   __shared__ __align__(8) unsigned long long s_bar;
   const float* src[4] = {w.spheres, w.capsules, w.boxes, w.halfspaces};
   const int nf[4] = {w.Ms * 4, w.Mc * 7, w.Mb * 15, w.Mh * 6};
@@ -120,7 +122,7 @@ __device__ inline ObsView stage_world(const WorldArgs& w, float* dst) {
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     d[k] = q;
-    q += WorldArgs::round4((size_t)nf[k]);
+    q += (k == 0 && sphere_slots > w.Ms) ? 4 * (size_t)sphere_slots : WorldArgs::round4((size_t)nf[k]);
     const bool aligned = nf[k] > 0 && (reinterpret_cast<uintptr_t>(src[k]) & 15) == 0;
     bulk[k] = aligned ? ((unsigned)nf[k] * 4u) & ~15u : 0u;
     total += bulk[k];

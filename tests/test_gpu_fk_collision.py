@@ -311,9 +311,10 @@ def test_forced_staging_timeout_is_reported_and_results_are_unchanged():
     """The bounded wait's test hook: with force_timeout set, no TMA copy is
     issued, every staging block waits out a 0.2 ms limit (by the GPU's global
     timer), counts itself and loads the obstacle arrays plainly.  The host
-    then reads PK_ERR_TIMEOUT, and the outputs equal the normal path's bit
-    for bit.  Nothing is in flight at any point, and the hook is switched off
-    again whatever happens."""
+    then reads PK_ERR_TIMEOUT, and the outputs (fused collision, trajectory
+    cost and gradient, LM IK) equal the normal path's bit for bit.  Nothing
+    is in flight at any point, and the hook is switched off again whatever
+    happens."""
     import ctypes as C
     from pyroffi_b200 import _lib
     from pyroffi_b200.trajopt import TrajectoryCost
@@ -324,12 +325,19 @@ def test_forced_staging_timeout_is_reported_and_results_are_unchanged():
     wt = W.trajectories(Bt=8, T=16)
     tc = TrajectoryCost(wt.model, wt.spheres, wt.world, wt.link_pairs, margin=wt.margin, device=DEV)
     x = torch.as_tensor(wt.traj, device=DEV)
+    from pyroffi_b200.ik import BatchIkSolver
+    wi = W.ik(P=4, Sd=64)
+    lm = BatchIkSolver(wi.model, wi.target_link, spheres=wi.spheres, world=wi.world, self_pairs=wi.self_pairs,
+                       max_iter=3, lambda_init=wi.lambda_init, lambda_down=wi.lambda_down, lambda_up=wi.lambda_up,
+                       device=DEV)
+    tg, sd = tt(wi.target_T), tt(wi.seeds)
 
     def run():
         r = fk_sphere_collision(*args, per_sphere=True)
         c, g = tc.cost_and_grad(x)
+        q, e = lm.run_lm(tg, sd)
         torch.cuda.synchronize()
-        return r.min_dist.clone(), r.dist_bkm.clone(), c.clone(), g.clone()
+        return r.min_dist.clone(), r.dist_bkm.clone(), c.clone(), g.clone(), q.clone(), e.clone()
 
     n = C.c_uint64(0)
     assert lib.pk_stage_wait_reset() == _lib.PK_OK
