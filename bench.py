@@ -46,9 +46,16 @@ L2_FLUSH_BYTES = 256 << 20
 # pyroffi_b200.profile_cases lm): DRAM bytes read + written (the ~1 MB of outputs were still in L2
 # when the launch ended), and the FP32 work the kernel executed, 2 FLOP per FFMA, 1 per FADD / FMUL,
 # twice that for the packed FFMA2 / FADD2 / FMUL2, summed over threads; the FMA pipe's active share.
-LM_DRAM_BYTES_PER_LAUNCH = 1092352 + 1792
-LM_EXECUTED_FLOP_PER_LAUNCH = 29415151114
-LM_FMA_PIPE_PCT = 15.3
+LM_DRAM_BYTES_PER_LAUNCH = 1145856 + 768
+LM_EXECUTED_FLOP_PER_LAUNCH = 29373823588
+LM_FMA_PIPE_PCT = 15.8
+# The same counts for the trajectory kernel's fused forward + backward launch on the 512 x 64 x 7 workload
+# (python -m pyroffi_b200.profile_cases traj) and for the fused FK + collision kernel on the sweep robot's
+# per-link rows (python -m pyroffi_b200.profile_cases fkc5, 4,096 configurations; per configuration).
+TRAJ_EXECUTED_FLOP_PER_LAUNCH = 1339234465
+TRAJ_FMA_PIPE_PCT = 29.9
+SWEEP_EXECUTED_FLOP_PER_CONFIG = 27802706944 / 4096
+SWEEP_FMA_PIPE_PCT = 60.4
 
 
 def r4(x):
@@ -462,7 +469,10 @@ def secondary_metrics(torch, dev, fp32_peak, cpu=True):
         "ms_fwd": r4(ms_f), "ms_bwd_recompute": r4(ms_b), "ms_fused_fwd_bwd": r4(ms_fb),
         "fwd_bwd_traj_per_s": r4(Bt / (ms_fb * 1e-3)),
         "roofline": {"bound": "fp32", "achieved": r4(tf), "peak": r4(fp32_peak), "unit": "TFLOP/s",
-                     "frac": r4(tf / fp32_peak), "basis": "dense-equivalent"},
+                     "frac": r4(tf / fp32_peak), "basis": "dense-equivalent",
+                     "executed": {"achieved": r4(TRAJ_EXECUTED_FLOP_PER_LAUNCH / (ms_fb * 1e-3) / 1e12),
+                                  "frac": r4(TRAJ_EXECUTED_FLOP_PER_LAUNCH / (ms_fb * 1e-3) / 1e12 / fp32_peak),
+                                  "fma_pipe_pct": TRAJ_FMA_PIPE_PCT}},
     }
     if cpu:
         from oracle import traj as otraj
@@ -598,7 +608,12 @@ def secondary_metrics(torch, dev, fp32_peak, cpu=True):
     out["c5"] = {
         "by_batch_ms_cfgps_gbs_fp32frac": sweep,
         "roofline": {"bound": "fp32", "achieved": r4(t262), "peak": r4(fp32_peak), "unit": "TFLOP/s",
-                     "frac": r4(t262 / fp32_peak), "B": 262144},
+                     "frac": r4(t262 / fp32_peak), "B": 262144,
+                     "executed": {"achieved": r4(262144 * SWEEP_EXECUTED_FLOP_PER_CONFIG / (sweep["262144"][0] * 1e-3)
+                                                 / 1e12),
+                                  "frac": r4(262144 * SWEEP_EXECUTED_FLOP_PER_CONFIG / (sweep["262144"][0] * 1e-3)
+                                             / 1e12 / fp32_peak),
+                                  "fma_pipe_pct": SWEEP_FMA_PIPE_PCT}},
         "ms_fwd_bwd_65536": r4(ms_fb5),
     }
     return out
