@@ -47,6 +47,11 @@ __device__ __forceinline__ float3 pose_apply(const Pose& T, float3 p) {
   return make_float3(r.x + T.tx, r.y + T.ty, r.z + T.tz);
 }
 
+// p expressed in the frame of pose T: R^T (p - t).
+__device__ __forceinline__ float3 pose_apply_inv(const Pose& T, float3 p) {
+  return quat_rotate(T.w, -T.x, -T.y, -T.z, make_float3(p.x - T.tx, p.y - T.ty, p.z - T.tz));
+}
+
 __device__ __forceinline__ Pose pose_compose(const Pose& a, const Pose& b) {
   Pose o;
   o.w = a.w * b.w - a.x * b.x - a.y * b.y - a.z * b.z;

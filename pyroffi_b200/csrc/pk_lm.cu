@@ -266,11 +266,6 @@ __device__ __forceinline__ void hinge_sq(float d2, float rr, float& pen) {
   }
 }
 
-// p expressed in the frame of pose T: R^T (p - t).
-__device__ __forceinline__ float3 pose_apply_inv(const Pose& T, float3 p) {
-  return quat_rotate(T.w, -T.x, -T.y, -T.z, make_float3(p.x - T.tx, p.y - T.ty, p.z - T.tz));
-}
-
 // Exact hinge terms of the sphere pairs [p0, p1) of a joint against world
 // sphere O (radius already + margin), with the obstacle centre moved into
 // the joint's frame (T) once: |R c_k + t - o| = |c_k - R^T (o - t)|; two

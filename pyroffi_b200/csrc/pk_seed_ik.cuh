@@ -287,7 +287,9 @@ __device__ __forceinline__ void seed_ik_jacobian(const SeedIkShared& sh, const P
 // obstacle at least the margin from a joint group's bounding sphere adds
 // exactly 0 for every sphere of the group and is skipped; with the grid, the
 // world spheres tested are those listed in the cell of the group's bounding
-// centre.
+// centre.  A world sphere that passes is moved into the joint's frame once
+// and tested against the group's spheres there on squared distances (a
+// square root only for a hit); the other kinds are tested in the world frame.
 template <int TPS>
 __device__ __forceinline__ float seed_ik_penalty(const SeedIkArgs& a, const PoseSlots& ps, const RobotSpheresS& R,
                                               const ObsView& ob, int gl, unsigned gmask) {
@@ -311,19 +313,35 @@ __device__ __forceinline__ float seed_ik_penalty(const SeedIkArgs& a, const Pose
         }
       }
     };
-    int m0 = 0;
+    // world sphere m against the group's spheres, in the joint's frame
+    auto narrow_sphere = [&](int m) {
+      const float4 O = ob.sph[m];
+      const float3 o = pose_apply_inv(Tj, make_float3(O.x, O.y, O.z));
+      for (int i = R.gstart[k]; i < R.gstart[k + 1]; ++i) {
+        const float4 q = R.sph[i];
+        const float dx = q.x - o.x, dy = q.y - o.y, dz = q.z - o.z;
+        const float d2 = dx * dx + dy * dy + dz * dz;
+        const float rr = q.w + O.w + margin;
+        if (d2 < rr * fabsf(rr)) {
+          const float e = sqrtf(d2) - rr;
+          pen += e * e;
+        }
+      }
+    };
     if (R.cell_start) {
       const int cell = obstacle_grid_cell(R.glo, R.ginv, kObsGridDefault, B);
       if (cell >= 0) {
         const int e1 = R.cell_start[cell + 1];
         for (int e = R.cell_start[cell] + gl; e < e1; e += TPS) {
           const int m = R.cell_obs[e];
-          if (obstacle_near<0>(ob, m, B, jb.w, margin)) narrow(m, ObsKind<0>());
+          if (obstacle_near<0>(ob, m, B, jb.w, margin)) narrow_sphere(m);
         }
       }
-      m0 = ob.Ms;  // the other kinds are scanned
+    } else {
+      for (int m = gl; m < ob.Ms; m += TPS)
+        if (obstacle_near<0>(ob, m, B, jb.w, margin)) narrow_sphere(m);
     }
-    for (int m = m0 + gl; m < M; m += TPS)
+    for (int m = ob.Ms + gl; m < M; m += TPS)
       if (obstacle_near(ob, m, B, jb.w, margin)) narrow(m, ObsKind<-1>());
   }
 #pragma unroll
