@@ -426,10 +426,14 @@ __device__ __noinline__ float w_penalty(const WideLaunch& P, const WideShared& s
   const int* cell_start = reinterpret_cast<const int*>(smem + L.cells);
   const unsigned short* cell_obs = reinterpret_cast<const unsigned short*>(smem + L.cell_obs);
   const int n_rs = sh.n_rs;
-  for (int k = gl; k < n_rs; k += G) {
-    const float4 s = rs4[k];
-    const float3 p = pose_apply(w_load(W.T, sh.js_joint[rsj[k]]), make_float3(s.x, s.y, s.z));
-    W.pos[k] = make_float4(p.x, p.y, p.z, s.w);
+  // sphere world positions: for the self pairs and the capsule / box /
+  // halfspace tests (world spheres are tested in the joint's frame)
+  if (sh.n_pairs > 0 || P.w.Mc + P.w.Mb + P.w.Mh > 0) {
+    for (int k = gl; k < n_rs; k += G) {
+      const float4 s = rs4[k];
+      const float3 p = pose_apply(w_load(W.T, sh.js_joint[rsj[k]]), make_float3(s.x, s.y, s.z));
+      W.pos[k] = make_float4(p.x, p.y, p.z, s.w);
+    }
   }
   __syncwarp(gm);
   float pen = 0.f;
@@ -475,10 +479,12 @@ __device__ __noinline__ float w_penalty(const WideLaunch& P, const WideShared& s
       const float rr = Bj.w + O.w;
       const float dx = Bj.x - O.x, dy = Bj.y - O.y, dz = Bj.z - O.z;
       if (dx * dx + dy * dy + dz * dz < rr * fabsf(rr)) {
+        // the obstacle in the joint's frame, against the joint's spheres there
+        const float3 o = pose_apply_inv(w_load(W.T, sh.js_joint[j]), make_float3(O.x, O.y, O.z));
         for (int k = sh.jstart[j]; k < sh.jstart[j + 1]; ++k) {
-          const float4 p = W.pos[k];
-          const float ex = p.x - O.x, ey = p.y - O.y, ez = p.z - O.z;
-          w_hinge(ex * ex + ey * ey + ez * ez, p.w + O.w, pen);
+          const float4 q = rs4[k];
+          const float ex = q.x - o.x, ey = q.y - o.y, ez = q.z - o.z;
+          w_hinge(ex * ex + ey * ey + ez * ez, q.w + O.w, pen);
         }
       }
     }
