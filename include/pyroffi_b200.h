@@ -326,6 +326,10 @@ typedef struct pk_traj_options {
   float w_jerk;
   float w_limits;
   float w_coll;
+  const uint8_t* active;   /* optional (NULL: every trajectory): trajectory b is evaluated only when
+                              active[b % active_period] != 0, and its outputs are left as they were otherwise
+                              (an optimiser's finished trajectories, its trial copies included) */
+  int64_t active_period;
 } pk_traj_options;
 
 /*
@@ -359,11 +363,13 @@ int pk_traj_cost_grad(void* stream, const pk_traj_options* opt, const float* tra
  * grad_clip_norm <= 0), ends set to 0, then dir = -M^-1 g on every joint's
  * interior timeline by n_cg_iters truncated FP64 CG steps (relative
  * tolerance cg_tol) on M x = 6x + reg x - 4(x[t-1] + x[t+1]) + x[t-2] + x[t+2];
- * covariant = 0 gives dir = -g.  At most 128 interior waypoints.
+ * covariant = 0 gives dir = -g.  At most 128 interior waypoints.  active[B]
+ * (optional, NULL = all): trajectories with active[b] == 0 are skipped and
+ * their dir rows left as they were.
  */
 int pk_chomp_direction(void* stream, const float* grad, float* dir, int64_t B, int32_t T, int32_t n_act,
                        int32_t n_cg_iters, float grad_clip_norm, float smoothness_reg, float cg_tol,
-                       int32_t covariant);
+                       int32_t covariant, const uint8_t* active);
 
 /*
  * CHOMP line search, trial trajectories (no reference counterpart; it fuses
@@ -371,11 +377,13 @@ int pk_chomp_direction(void* stream, const float* grad, float* dir, int64_t B, i
  * src/pyroffi/optimization_engines/_chomp_optimization.py:282-291):
  * trials[k, b] = traj[b] + clamp(alphas[k] * dir[b], -max_delta, max_delta)
  * for k < n_alphas, waypoint 0 set to start[n_act] and waypoint T-1 to goal.
- * trials is [n_alphas, B, T, n_act]; alphas is a device array.
+ * trials is [n_alphas, B, T, n_act]; alphas is a device array.  active[B]
+ * (optional, NULL = all): the trials of trajectories with active[b] == 0
+ * are not written.
  */
 int pk_chomp_line_trials(void* stream, const float* traj, const float* dir, const float* alphas, int32_t n_alphas,
                          float max_delta, const float* start, const float* goal, float* trials, int64_t B,
-                         int32_t T, int32_t n_act);
+                         int32_t T, int32_t n_act, const uint8_t* active);
 
 /*
  * CHOMP line search, selection (no reference counterpart; it fuses the

@@ -73,11 +73,11 @@ SIGNATURES: dict[str, list] = {
                                               _p] + [_i32] * 10,
     "pk_sqp_ik_cuda": [_p] + [_p] * 21 + [_i64, _i64, _f32, _f32, _f32, _f32, _f32, _i64, _f32, _f32, _p, _p]
                       + [_i32] * 10,
-    "pk_chomp_direction": [_p, _p, _p, _i64, _i32, _i32, _i32, _f32, _f32, _f32, _i32],
+    "pk_chomp_direction": [_p, _p, _p, _i64, _i32, _i32, _i32, _f32, _f32, _f32, _i32, _p],
     "pk_stage_wait_timeouts": [_p],
     "pk_stage_wait_reset": [],
     "pk_stage_wait_configure": [_i32, _i64],
-    "pk_chomp_line_trials": [_p, _p, _p, _p, _i32, _f32, _p, _p, _p, _i64, _i32, _i32],
+    "pk_chomp_line_trials": [_p, _p, _p, _p, _i32, _f32, _p, _p, _p, _i64, _i32, _i32, _p],
     "pk_chomp_line_select": [_p, _p, _p, _p, _p, _p, _p, _i32, _f32, _i32, _i64, _i32, _i32],
     "pk_sco_linearize": [_p, C.c_void_p] + [_p] * 20 + [_i64] + [_i32] * 9,
     "pk_sco_inner": [_p, C.c_void_p] + [_p] * 8 + [_f32, _i64, _i32, _i32],
@@ -106,7 +106,7 @@ class TrajOptions(C.Structure):
     """``pk_traj_options`` of the C-ABI."""
 
     _fields_ = [("margin", _f32), ("w_smooth", _f32), ("w_acc", _f32), ("w_jerk", _f32),
-                ("w_limits", _f32), ("w_coll", _f32)]
+                ("w_limits", _f32), ("w_coll", _f32), ("active", C.c_void_p), ("active_period", _i64)]
 
 
 class ScoOptions(C.Structure):

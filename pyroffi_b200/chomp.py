@@ -66,24 +66,31 @@ class ChompConfig:
 LINE_SEARCH = (1.0, 0.5, 0.25, 0.1, 0.05, 0.0)
 
 
-def covariant_direction(grad: torch.Tensor, cfg: ChompConfig) -> torch.Tensor:
+def covariant_direction(grad: torch.Tensor, cfg: ChompConfig, active=None) -> torch.Tensor:
     """Clipped, endpoint-pinned descent direction [B, T, n]: -M^-1 g on each
     joint's interior timeline by the truncated FP64 CG, or -g without the
-    covariant update (one ``pk_chomp_direction`` launch)."""
+    covariant update (one ``pk_chomp_direction`` launch).  With ``active``
+    (uint8/bool [B] on the device), only those trajectories' rows are set."""
     g = f32(grad)
     B, T, n = (int(v) for v in g.shape)
     d = torch.empty_like(g)
     _lib.call("pk_chomp_direction", stream_ptr(g.device), ptr(g), ptr(d), B, T, n, int(cfg.n_cg_iters),
               float(cfg.grad_clip_norm), float(cfg.smoothness_reg), float(cfg.cg_tol),
-              int(bool(cfg.use_covariant_update)))
+              int(bool(cfg.use_covariant_update)), ptr(active))
     return d
 
 
 class ChompOptimizer:
-    """``run(init_trajs, start, goal)`` -> (best_traj [T, n], costs [B], final_trajs [B, T, n])."""
+    """``run(init_trajs, start, goal)`` -> (best_traj [T, n], costs [B], final_trajs [B, T, n]).
 
-    def __init__(self, cost: TrajectoryCost, cfg: ChompConfig = ChompConfig()):
+    skip_finished: a trajectory that has early-stopped no longer changes, so
+    its cost, gradient, direction and line-search trials are skipped from
+    then on (the kernels take the ``active`` mask); the results are the same
+    bits as without the skip."""
+
+    def __init__(self, cost: TrajectoryCost, cfg: ChompConfig = ChompConfig(), skip_finished: bool = True):
         self.cost, self.cfg = cost, cfg
+        self.skip_finished = skip_finished
         o = cost.opt
         o.w_smooth, o.w_acc, o.w_jerk, o.w_limits = cfg.w_smooth, cfg.w_acc, cfg.w_jerk, cfg.w_limits
         o.margin = cfg.collision_margin
@@ -95,9 +102,9 @@ class ChompOptimizer:
             self._alpha_t = torch.tensor(LINE_SEARCH, dtype=torch.float32, device=dev) * self.cfg.step_size
         return self._alpha_t
 
-    def _costs(self, trajs, w_coll, grad=False):
+    def _costs(self, trajs, w_coll, grad=False, active=None):
         self.cost.opt.w_coll = float(w_coll)
-        return self.cost.cost_and_grad(trajs) if grad else self.cost.cost(trajs)
+        return self.cost.cost_and_grad(trajs, active) if grad else self.cost.cost(trajs, active)
 
     def _iterate(self, traj, start, goal):
         cfg = self.cfg
@@ -113,14 +120,16 @@ class ChompOptimizer:
         T, n = int(traj.shape[1]), int(traj.shape[2])
         trials = torch.empty((K, B, T, n), dtype=torch.float32, device=dev)
         st = stream_ptr(dev)
+        # finished (early-stopped) trajectories are skipped: the selection reads nothing of theirs
+        act = active if self.skip_finished else None
         for _ in range(cfg.n_iters):
-            c, g = self._costs(traj, w, grad=True)
-            d = covariant_direction(g, cfg)
+            c, g = self._costs(traj, w, grad=True, active=act)
+            d = covariant_direction(g, cfg, act)
             # the last trial step is 0: that trial is the current trajectory, whose cost
             # the gradient launch has just produced, so only the K others are built and costed
             _lib.call("pk_chomp_line_trials", st, ptr(traj), ptr(d), ptr(alphas), K, float(cfg.max_delta_per_step),
-                      ptr(start), ptr(goal), ptr(trials), B, T, n)
-            tc = self._costs(trials.view(K * B, T, n), w)
+                      ptr(start), ptr(goal), ptr(trials), B, T, n, ptr(act))
+            tc = self._costs(trials.view(K * B, T, n), w, active=act)
             # first minimum over the trials and the current cost; step, stall count, early stop (in place)
             _lib.call("pk_chomp_line_select", st, ptr(tc), ptr(c), ptr(trials), ptr(traj), ptr(active), ptr(stall), K,
                       float(cfg.min_cost_improve), int(cfg.early_stop_patience), B, T, n)

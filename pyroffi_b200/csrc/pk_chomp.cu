@@ -31,6 +31,7 @@ struct ChompDirArgs {
   int T, n, iters;
   float clip, reg, tol;
   int covariant;
+  const unsigned char* active;  // null, or only trajectories with active[b] != 0 are processed
 };
 
 __device__ __forceinline__ double warp_sum_d(double v) {
@@ -46,6 +47,7 @@ __global__ void __launch_bounds__(256) chomp_direction_kernel(ChompDirArgs a) {
   const int T = a.T, n = a.n, Tn = T * n, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int nw = blockDim.x >> 5;
   const long long b = blockIdx.x;
+  if (a.active && !a.active[b]) return;  // block-uniform
   const float* g = a.grad + b * Tn;
   float* d = a.dir + b * Tn;
   // global-norm clip (FP32, as the reference's jnp.linalg.norm of the gradient)
@@ -161,7 +163,7 @@ __global__ void __launch_bounds__(256) chomp_direction_kernel(ChompDirArgs a) {
 __global__ void chomp_trials_kernel(const float* __restrict__ traj, const float* __restrict__ dir,
                                     const float* __restrict__ alphas, float max_delta, const float* __restrict__ start,
                                     const float* __restrict__ goal, float* __restrict__ trials, long long per, int T,
-                                    int n, int K) {
+                                    int n, int K, const unsigned char* __restrict__ active) {
   const long long total = per * K;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
        i += (long long)gridDim.x * blockDim.x) {
@@ -169,6 +171,7 @@ __global__ void chomp_trials_kernel(const float* __restrict__ traj, const float*
     const long long e = i - (long long)k * per;
     const int c = (int)(e % n);
     const int t = (int)((e / n) % T);
+    if (active && !active[e / ((long long)T * n)]) continue;  // a finished trajectory: its trials are not read
     float v;
     if (t == 0) {
       v = start[c];
@@ -222,13 +225,13 @@ using namespace pk;
 
 extern "C" int pk_chomp_direction(void* stream, const float* grad, float* dir, int64_t B, int32_t T, int32_t n_act,
                                   int32_t n_cg_iters, float grad_clip_norm, float smoothness_reg, float cg_tol,
-                                  int32_t covariant) {
+                                  int32_t covariant, const uint8_t* active) {
   PK_CHECK_ARG(B >= 0 && T >= 0 && n_act >= 0 && n_cg_iters >= 0, "negative extent");
   PK_CHECK_CAP(T <= 130, "the CG solve takes at most 128 interior waypoints (T=%d)", T);
   PK_CHECK_CAP(B < (1LL << 31), "batch too large");
   if (B == 0 || T == 0 || n_act == 0) return PK_OK;
   PK_CHECK_ARG(grad && dir, "null buffer");
-  ChompDirArgs a{grad, dir, T, n_act, n_cg_iters, grad_clip_norm, smoothness_reg, cg_tol, covariant ? 1 : 0};
+  ChompDirArgs a{grad, dir, T, n_act, n_cg_iters, grad_clip_norm, smoothness_reg, cg_tol, covariant ? 1 : 0, active};
   int warps = n_act < 8 ? n_act : 8;
   const size_t smem = sizeof(double) * (size_t)warps * ((T > 2 ? T - 2 : 0) + 4);
   chomp_direction_kernel<<<(unsigned)B, 32 * warps, smem, (cudaStream_t)stream>>>(a);
@@ -237,7 +240,7 @@ extern "C" int pk_chomp_direction(void* stream, const float* grad, float* dir, i
 
 extern "C" int pk_chomp_line_trials(void* stream, const float* traj, const float* dir, const float* alphas,
                                     int32_t n_alphas, float max_delta, const float* start, const float* goal,
-                                    float* trials, int64_t B, int32_t T, int32_t n_act) {
+                                    float* trials, int64_t B, int32_t T, int32_t n_act, const uint8_t* active) {
   PK_CHECK_ARG(B >= 0 && T >= 0 && n_act >= 0 && n_alphas >= 0, "negative extent");
   const long long per = (long long)B * T * n_act;
   if (per == 0 || n_alphas == 0) return PK_OK;
@@ -245,7 +248,7 @@ extern "C" int pk_chomp_line_trials(void* stream, const float* traj, const float
   const long long total = per * n_alphas;
   const long long blocks = std::min<long long>((total + 255) / 256, 148LL * 32);
   chomp_trials_kernel<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(traj, dir, alphas, max_delta, start, goal,
-                                                                           trials, per, T, n_act, n_alphas);
+                                                                           trials, per, T, n_act, n_alphas, active);
   return cuda_status(cudaGetLastError(), "chomp_trials_kernel launch");
 }
 

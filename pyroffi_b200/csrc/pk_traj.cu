@@ -44,6 +44,8 @@ struct TrajArgs {
   long long B;
   int T, N, S, P;
   float margin, w_smooth, w_acc, w_jerk, w_limits, w_coll;
+  const unsigned char* active;  // null, or trajectory b runs only when active[b % active_period]
+  long long active_period;
 };
 
 // Lanes per waypoint: the world (link, obstacle) pairs and the self pairs of
@@ -52,6 +54,7 @@ struct TrajArgs {
 template <int MAXS, int TG>
 __global__ void __launch_bounds__(64 * TG, 8 / TG) traj_cost_kernel(TrajArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  if (a.active && !a.active[blockIdx.x % a.active_period]) return;  // block-uniform: nothing is written
   JointTable& jt = *reinterpret_cast<JointTable*>(smem_raw);
   unsigned char* p = smem_raw + sizeof(JointTable);
   const int N = a.N, S = a.S, T = a.T, n = a.m.n_act, nj = a.m.n_joints;
@@ -400,6 +403,9 @@ extern "C" int pk_traj_cost_grad(void* stream, const pk_traj_options* opt, const
   a.B = B; a.T = T; a.N = n_links; a.S = S; a.P = P;
   a.margin = opt->margin; a.w_smooth = opt->w_smooth; a.w_acc = opt->w_acc; a.w_jerk = opt->w_jerk;
   a.w_limits = opt->w_limits; a.w_coll = opt->w_coll;
+  PK_CHECK_ARG(opt->active == nullptr || opt->active_period > 0, "active_period must be positive with an active mask");
+  a.active = opt->active;
+  a.active_period = opt->active ? opt->active_period : 1;
   // lanes per waypoint: 4 when a waypoint has much world to test or the
   // batch is too small to fill the GPU with 2-lane blocks, else 2
   int dev = 0, sms = 148;

@@ -45,9 +45,17 @@ class TrajectoryCost:
         self.pair_j = torch.as_tensor(np.ascontiguousarray(lp[:, 1]), device=self.device)
         self.opt = _lib.TrajOptions(margin, w_smooth, w_acc, w_jerk, w_limits, w_coll)
 
-    def _run(self, traj: torch.Tensor, want_cost: bool, want_grad: bool, want_wp: bool = False):
+    def _run(self, traj: torch.Tensor, want_cost: bool, want_grad: bool, want_wp: bool = False, active=None):
+        """``active`` (optional, uint8/bool [P] on the device): trajectory b is
+        evaluated only when active[b % P]; the rows of the others in the
+        returned tensors are then left unset (for an optimiser that reads
+        only its unfinished trajectories)."""
         x = f32(traj)
         B, T, n = (int(v) for v in x.shape)
+        if active is not None:
+            self.opt.active, self.opt.active_period = active.data_ptr(), int(active.numel())
+        else:
+            self.opt.active, self.opt.active_period = None, 0
         cost = torch.empty(B, dtype=torch.float32, device=self.device) if want_cost else None
         grad = torch.empty((B, T, n), dtype=torch.float32, device=self.device) if want_grad else None
         wp = torch.empty((B, T), dtype=torch.float32, device=self.device) if want_wp else None
@@ -60,14 +68,14 @@ class TrajectoryCost:
                   int(self.pair_i.shape[0]), Ms, Mc, Mb, Mh)
         return cost, grad, wp
 
-    def cost(self, traj):
-        return self._run(traj, True, False)[0]
+    def cost(self, traj, active=None):
+        return self._run(traj, True, False, active=active)[0]
 
-    def grad(self, traj):
-        return self._run(traj, False, True)[1]
+    def grad(self, traj, active=None):
+        return self._run(traj, False, True, active=active)[1]
 
-    def cost_and_grad(self, traj):
-        c, g, _ = self._run(traj, True, True)
+    def cost_and_grad(self, traj, active=None):
+        c, g, _ = self._run(traj, True, True, active=active)
         return c, g
 
     def waypoint_collision(self, traj):

@@ -121,10 +121,10 @@ def test_hjcd_refinement_validates_on_the_host(lib):
 
 def test_chomp_direction_validates_on_the_host(lib):
     d = C.c_void_p(16)
-    assert lib.pk_chomp_direction(None, d, d, -1, 64, 7, 24, 10.0, 1.0, 1e-6, 1) == _lib.PK_ERR_INVALID
-    assert lib.pk_chomp_direction(None, d, d, 4, 131, 7, 24, 10.0, 1.0, 1e-6, 1) == _lib.PK_ERR_CAPACITY
-    assert lib.pk_chomp_direction(None, d, d, 0, 64, 7, 24, 10.0, 1.0, 1e-6, 1) == _lib.PK_OK
-    assert lib.pk_chomp_direction(None, None, None, 4, 64, 7, 24, 10.0, 1.0, 1e-6, 1) == _lib.PK_ERR_INVALID
+    assert lib.pk_chomp_direction(None, d, d, -1, 64, 7, 24, 10.0, 1.0, 1e-6, 1, None) == _lib.PK_ERR_INVALID
+    assert lib.pk_chomp_direction(None, d, d, 4, 131, 7, 24, 10.0, 1.0, 1e-6, 1, None) == _lib.PK_ERR_CAPACITY
+    assert lib.pk_chomp_direction(None, d, d, 0, 64, 7, 24, 10.0, 1.0, 1e-6, 1, None) == _lib.PK_OK
+    assert lib.pk_chomp_direction(None, None, None, 4, 64, 7, 24, 10.0, 1.0, 1e-6, 1, None) == _lib.PK_ERR_INVALID
 
 
 def test_trajectory_cost_validates_on_the_host(lib):

@@ -102,7 +102,7 @@ def test_line_search_kernels_match_the_tensor_formulation():
     trials = torch.empty((K, B, T, n), dtype=torch.float32, device=DEV)
     st = stream_ptr(torch.device(DEV))
     _lib.call("pk_chomp_line_trials", st, ptr(tr), ptr(d), ptr(alphas), K, md, ptr(start), ptr(goal), ptr(trials),
-              B, T, n)
+              B, T, n, None)
     ref = tr[None] + torch.clamp(alphas[:, None, None, None] * d[None], -md, md)
     ref[:, :, 0] = start
     ref[:, :, -1] = goal
@@ -129,3 +129,46 @@ def test_line_search_kernels_match_the_tensor_formulation():
     assert torch.equal(tr, want_tr)
     assert torch.equal(stall, want_stall)
     assert torch.equal(active, want_active)
+
+
+def test_skipping_finished_trajectories_leaves_results_unchanged():
+    """Early-stopped trajectories no longer change, so the cost, gradient,
+    direction and trial launches skip them (the kernels' active masks); on
+    the config-3 trajectories, where most stop within 100 iterations, the
+    final trajectories and costs are the same bits with and without the skip."""
+    wt = W.trajectories(Bt=64, T=64)
+    cfg = ChompConfig()
+    x = torch.as_tensor(wt.traj, device=DEV)
+    s0, g0 = x[0, 0].clone(), x[0, -1].clone()
+    out = []
+    for skip in (True, False):
+        tc = TrajectoryCost(wt.model, wt.spheres, wt.world, wt.link_pairs, margin=cfg.collision_margin, device=DEV)
+        _, costs, final = ChompOptimizer(tc, cfg, skip_finished=skip).run(x, s0, g0)
+        out.append((costs.clone(), final.clone()))
+    assert torch.equal(out[0][0], out[1][0])
+    assert torch.equal(out[0][1], out[1][1])
+
+
+def test_masked_kernels_write_only_active_rows():
+    from pyroffi_b200 import _lib
+    from pyroffi_b200._tensors import ptr, stream_ptr
+    rng = np.random.default_rng(3)
+    K, B, T, n = 2, 9, 8, 5
+    tr = torch.as_tensor(rng.normal(size=(B, T, n)), dtype=torch.float32, device=DEV)
+    d = torch.as_tensor(rng.normal(size=(B, T, n)), dtype=torch.float32, device=DEV)
+    alphas = torch.tensor([1.0, 0.5], dtype=torch.float32, device=DEV)
+    start, goal = tr[0, 0].clone(), tr[0, -1].clone()
+    active = torch.as_tensor(np.arange(B) % 3 != 1, device=DEV)
+    trials = torch.full((K, B, T, n), 7.0, dtype=torch.float32, device=DEV)
+    _lib.call("pk_chomp_line_trials", stream_ptr(torch.device(DEV)), ptr(tr), ptr(d), ptr(alphas), K, 0.3,
+              ptr(start), ptr(goal), ptr(trials), B, T, n, ptr(active))
+    ref = torch.full_like(trials, 7.0)
+    _lib.call("pk_chomp_line_trials", stream_ptr(torch.device(DEV)), ptr(tr), ptr(d), ptr(alphas), K, 0.3,
+              ptr(start), ptr(goal), ptr(ref), B, T, n, None)
+    a = active.cpu().numpy()
+    assert torch.equal(trials[:, a], ref[:, a])
+    assert torch.all(trials[:, ~a] == 7.0)
+    g = torch.as_tensor(rng.normal(size=(B, 12, n)), dtype=torch.float32, device=DEV)
+    full = covariant_direction(g, ChompConfig())
+    part = covariant_direction(g, ChompConfig(), active)
+    assert torch.equal(part[a], full[a])
