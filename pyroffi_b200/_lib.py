@@ -9,6 +9,7 @@ library's message.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import threading
 from pathlib import Path
 
@@ -145,9 +146,23 @@ def load() -> C.CDLL:
         return lib
 
 
+# PK_NVTX=1: every entry-point call is an NVTX range named after the entry
+# point, so a timeline profiler shows the library's launches by name.
+_NVTX = os.environ.get("PK_NVTX", "") not in ("", "0")
+
+
 def call(name: str, *args) -> None:
     lib = load()
-    st = getattr(lib, name)(*args)
+    if _NVTX:
+        import torch
+
+        torch.cuda.nvtx.range_push(name)
+        try:
+            st = getattr(lib, name)(*args)
+        finally:
+            torch.cuda.nvtx.range_pop()
+    else:
+        st = getattr(lib, name)(*args)
     if st != PK_OK:
         raise PkError(st, name, lib.pk_last_error().decode(errors="replace"))
 

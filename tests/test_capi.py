@@ -178,3 +178,15 @@ def test_fp32_solve_is_rejected_where_it_is_not_offered(lib):
     opt.threads_per_seed = 2
     st = lib.pk_ls_ik_ex(None, C.byref(opt), *([d] * 25), 1, 8, 7, 7, 1, 0, 0, 0, 0, 0, 0)
     assert st == _lib.PK_ERR_INVALID and b"fp32_solve" in lib.pk_last_error()
+
+
+def test_nvtx_ranges_wrap_calls_when_asked(monkeypatch):
+    """PK_NVTX=1 wraps each entry-point call in an NVTX range named after it
+    (here with torch's NVTX calls recorded instead of sent)."""
+    import torch
+    pushed = []
+    monkeypatch.setattr(_lib, "_NVTX", True)
+    monkeypatch.setattr(torch.cuda.nvtx, "range_push", lambda name: pushed.append(name))
+    monkeypatch.setattr(torch.cuda.nvtx, "range_pop", lambda: pushed.append("pop"))
+    _lib.call("pk_chomp_line_select", None, None, None, None, None, None, None, 1, 0.0, 1, 0, 4, 7)
+    assert pushed == ["pk_chomp_line_select", "pop"]
