@@ -148,10 +148,13 @@ typedef struct pk_lm_options {
                               trial; 16, 32 = warp-per-seed body with that many lanes per seed */
   int32_t seeds_per_block;  /* 0 = choose automatically */
   int32_t lanes_per_wide_seed; /* warp-per-seed body: lanes per seed, 16 (0 = default) or 32 */
-  int32_t fp32_solve;       /* 0 = FP64 normal equations and Cholesky (as the reference); 1 = FP32, with one FP64
-                              iterative-refinement step when the squared ratio of the largest to the smallest
-                              Cholesky pivot exceeds 1e6 (seed-group kernel: n_act <= 16, n_ee <= 2,
-                              threads_per_seed 0 or 1; PK_ERR_INVALID elsewhere, pk_ik_batch included) */
+  int32_t fp64_solve;       /* the damped step is solved through its 6 n_ee x 6 n_ee dual system
+                              (Js Js^T + lambda I) y = fw, p = -Js^T y.  0 = FP32 system and Cholesky, with one
+                              FP64 iterative-refinement step when the squared ratio of the largest to the
+                              smallest pivot exceeds 1e6 (default); 1 = FP64, the precision of the reference's
+                              normal equations (seed-group kernel: n_act <= 16, n_ee <= 2, threads_per_seed 0 or
+                              1; PK_ERR_INVALID elsewhere, pk_ik_batch included).  The warp-per-seed body (more
+                              than 16 DOF or 2 EEs) solves in FP64 */
   int32_t obstacle_grid;    /* the LM kernels' obstacle tile: the world spheres are binned into a uniform grid of
                               this many cells per axis, built per block in shared memory, and each joint's
                               bounding sphere tests only its cell's list; 0 = default (8), 1..16 = that many,

@@ -47,7 +47,7 @@ class LmOptions(C.Structure):
         ("threads_per_seed", _i32),
         ("seeds_per_block", _i32),
         ("lanes_per_wide_seed", _i32),
-        ("fp32_solve", _i32),
+        ("fp64_solve", _i32),
         ("obstacle_grid", _i32),
     ]
 

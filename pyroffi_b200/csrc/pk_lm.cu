@@ -65,7 +65,7 @@ struct LmArgs {
   int coll;
   float coll_w, margin;
   int spb;
-  int f32_solve;  // FP32 normal equations + conditional FP64 refinement (seed-group kernel, one lane per seed)
+  int f64_solve;  // the damped step's system in FP64 (seed-group kernel, one lane per seed); else FP32
   int grid_n;     // obstacle grid cells per axis (0: no grid, every obstacle takes the bounding test)
 };
 
@@ -582,99 +582,106 @@ __device__ __forceinline__ void ee_residual(const LmShared& sh, const PoseSlots&
   }
 }
 
-// FP32 normal equations and Cholesky with one conditional FP64 refinement
-// step (the F32S form of lm_direction).  J is the column-scaled weighted
+// FP32 damped step with one conditional FP64 refinement step (the default
+// form of lm_direction), on the same R x R dual system as the FP64 form:
+// (Js Js^T + lam I) y = fw, p = -Js^T y (R = 6 MAXEE), fixed and padded
+// joints as zero columns.  Its eigenvalues are sigma_i(Js)^2 + lam: unlike
+// the MAXA x MAXA normal equations of a redundant arm, whose null space puts
+// an eigenvalue at lam itself, it is only ill-conditioned near singular
+// configurations.  The system and its Cholesky are FP32; when the squared
+// ratio of the largest to the smallest pivot exceeds 1e6, one step of
+// iterative refinement follows: the residual fw - (Js Js^T + lam I) y in
+// FP64 (from the FP32 Jacobian entries, which FP64 holds exactly), the
+// correction solved with the FP32 factor.  J is the column-scaled weighted
 // Jacobian, fw the weighted residual; writes the unscaled step into delta
 // (zero on a non-positive pivot).
 template <int MAXA, int MAXEE>
 __device__ __forceinline__ void lm_solve_f32(const LmShared& sh, const float (&J)[6 * MAXEE][MAXA],
                                              const float (&fw)[6 * MAXEE], float lam, const float (&col_s)[MAXA],
                                              float (&delta)[MAXA]) {
-  float A[MAXA * (MAXA + 1) / 2];
-  float b[MAXA];
+  constexpr int R = 6 * MAXEE;
+  float A[R * (R + 1) / 2];
 #pragma unroll
-  for (int i = 0; i < MAXA; ++i) {
-    const bool fi = sh.fixed[i];
+  for (int i = 0; i < R; ++i) {
 #pragma unroll
     for (int j = 0; j <= i; ++j) {
-      float acc = 0.f;
+      float acc = (i == j) ? lam : 0.f;
 #pragma unroll
-      for (int k = 0; k < 6 * MAXEE; ++k) acc = fmaf(J[k][i], J[k][j], acc);
-      if (i == j) acc += lam;
-      const bool fj = sh.fixed[j];
-      A[i * (i + 1) / 2 + j] = (fi || fj) ? ((i == j) ? 1.f : 0.f) : acc;
+      for (int c = 0; c < MAXA; ++c)
+        if (!sh.fixed[c]) acc = fmaf(J[i][c], J[j][c], acc);
+      A[i * (i + 1) / 2 + j] = acc;
     }
-    float rb = 0.f;
-#pragma unroll
-    for (int k = 0; k < 6 * MAXEE; ++k) rb = fmaf(J[k][i], fw[k], rb);
-    b[i] = fi ? 0.f : -rb;
   }
   // Cholesky A = L L^T in place, diagonal kept as its reciprocal
   bool ok = true;
   float pmax = 0.f, pmin = 3.4e38f;
 #pragma unroll
-  for (int k = 0; k < MAXA; ++k) {
+  for (int k = 0; k < R; ++k) {
     float s2 = A[k * (k + 1) / 2 + k];
 #pragma unroll
     for (int q = 0; q < k; ++q) s2 = fmaf(-A[k * (k + 1) / 2 + q], A[k * (k + 1) / 2 + q], s2);
     if (!(s2 > 0.f)) ok = false;
     pmax = fmaxf(pmax, s2);
     pmin = fminf(pmin, s2);
-    const float inv = rsqrtf(ok ? s2 : 1.f);
+    const float inv = 1.f / sqrtf(ok ? s2 : 1.f);
     A[k * (k + 1) / 2 + k] = inv;
 #pragma unroll
-    for (int i = k + 1; i < MAXA; ++i) {
+    for (int i = k + 1; i < R; ++i) {
       float tt = A[i * (i + 1) / 2 + k];
 #pragma unroll
       for (int q = 0; q < k; ++q) tt = fmaf(-A[i * (i + 1) / 2 + q], A[k * (k + 1) / 2 + q], tt);
       A[i * (i + 1) / 2 + k] = tt * inv;
     }
   }
-  auto solve = [&](float (&v)[MAXA]) {
+  auto solve = [&](float (&v)[R]) {
 #pragma unroll
-    for (int i = 0; i < MAXA; ++i) {
+    for (int i = 0; i < R; ++i) {
       float s2 = v[i];
 #pragma unroll
       for (int q = 0; q < i; ++q) s2 = fmaf(-A[i * (i + 1) / 2 + q], v[q], s2);
       v[i] = s2 * A[i * (i + 1) / 2 + i];
     }
 #pragma unroll
-    for (int i = MAXA - 1; i >= 0; --i) {
+    for (int i = R - 1; i >= 0; --i) {
       float s2 = v[i];
 #pragma unroll
-      for (int q = i + 1; q < MAXA; ++q) s2 = fmaf(-A[q * (q + 1) / 2 + i], v[q], s2);
+      for (int q = i + 1; q < R; ++q) s2 = fmaf(-A[q * (q + 1) / 2 + i], v[q], s2);
       v[i] = s2 * A[i * (i + 1) / 2 + i];
     }
   };
-  float x[MAXA];
+  float y[R];
 #pragma unroll
-  for (int i = 0; i < MAXA; ++i) x[i] = b[i];
-  solve(x);
+  for (int i = 0; i < R; ++i) y[i] = fw[i];
+  solve(y);
   if (ok && pmax > 1e6f * pmin) {
-    // r = b - A x in FP64: b = -Js^T fw and A x = Js^T (Js x) + lam x over the
-    // free joints (fixed rows are identity rows with b = 0)
-    double u[6 * MAXEE];
+    // r = fw - (Js Js^T + lam I) y in FP64 over the free columns
+    double u[MAXA];
 #pragma unroll
-    for (int k = 0; k < 6 * MAXEE; ++k) {
+    for (int c = 0; c < MAXA; ++c) {
       double acc = 0.0;
 #pragma unroll
-      for (int c = 0; c < MAXA; ++c) acc = fma((double)J[k][c], sh.fixed[c] ? 0.0 : (double)x[c], acc);
-      u[k] = acc;
+      for (int k = 0; k < R; ++k) acc = fma((double)J[k][c], (double)y[k], acc);
+      u[c] = sh.fixed[c] ? 0.0 : acc;
     }
-    float d[MAXA];
+    float d[R];
 #pragma unroll
-    for (int i = 0; i < MAXA; ++i) {
-      double acc = (double)lam * (double)x[i];
+    for (int i = 0; i < R; ++i) {
+      double acc = (double)lam * (double)y[i];
 #pragma unroll
-      for (int k = 0; k < 6 * MAXEE; ++k) acc = fma((double)J[k][i], u[k] + (double)fw[k], acc);
-      d[i] = sh.fixed[i] ? -x[i] : (float)(-acc);
+      for (int c = 0; c < MAXA; ++c) acc = fma((double)J[i][c], u[c], acc);
+      d[i] = (float)((double)fw[i] - acc);
     }
     solve(d);
 #pragma unroll
-    for (int i = 0; i < MAXA; ++i) x[i] = (float)((double)x[i] + (double)d[i]);
+    for (int i = 0; i < R; ++i) y[i] = (float)((double)y[i] + (double)d[i]);
   }
 #pragma unroll
-  for (int c = 0; c < MAXA; ++c) delta[c] = ok ? x[c] / col_s[c] : 0.f;
+  for (int c = 0; c < MAXA; ++c) {
+    float pc = 0.f;
+#pragma unroll
+    for (int k = 0; k < R; ++k) pc = fmaf(J[k][c], y[k], pc);
+    delta[c] = (ok && !sh.fixed[c]) ? -pc / col_s[c] : 0.f;
+  }
 }
 
 // Damped Gauss-Newton step of the current point (_ls_ik_cuda_kernel.cu:257-335):
@@ -682,15 +689,12 @@ __device__ __forceinline__ void lm_solve_f32(const LmShared& sh, const float (&J
 // scaling, normal equations (Js^T Js + lam I) p = -Js^T fw with fixed and
 // padded joints masked, Cholesky solve (p = 0 on a non-positive pivot),
 // unscaling and the trust-region clip.  Writes `delta`, returns ||fw||^2.
-// F32S false: the damped system solved in FP64 through its R x R dual form
-// (R = 6 MAXEE residual rows; the reference solves the MAXA x MAXA normal
-// equations in FP64, the same step in exact arithmetic).  F32S true: the
-// MAXA x MAXA normal equations and their Cholesky in FP32, and when the
-// squared ratio of the largest to the smallest Cholesky pivot exceeds 1e6,
-// one step of iterative refinement: the residual b - A x in FP64 (A applied
-// as Js^T (Js x) + lam x from the FP32 Jacobian entries, which FP64 holds
-// exactly), the correction solved with the FP32 factor.
-template <int MAXA, int MAXEE, bool F32S = false>
+// The damped system is solved through its R x R dual form (R = 6 MAXEE
+// residual rows; the reference solves the MAXA x MAXA normal equations in
+// FP64, the same step in exact arithmetic).  F64S false (the default): the
+// dual system and its Cholesky in FP32, with one FP64 refinement step when
+// the squared pivot ratio exceeds 1e6 (lm_solve_f32).  F64S true: in FP64.
+template <int MAXA, int MAXEE, bool F64S = false>
 __device__ __forceinline__ float lm_direction(const LmShared& sh, const PoseSlots& ps, int n_ee, const float (&W)[6],
                                               const float (&r)[6 * MAXEE], const float (&pee)[3 * MAXEE],
                                               float lam, float max_p, float max_o, float (&delta)[MAXA]) {
@@ -754,7 +758,7 @@ __device__ __forceinline__ float lm_direction(const LmShared& sh, const PoseSlot
 #pragma unroll
     for (int c = 0; c < MAXA; ++c) J[k][c] = J[k][c] / col_s[c];
 
-  if constexpr (F32S) {
+  if constexpr (!F64S) {
     lm_solve_f32<MAXA, MAXEE>(sh, J, fw, lam, col_s, delta);
   } else {
   // FP64, through the push-through identity
@@ -1053,7 +1057,7 @@ __device__ void lm_stage(const LmArgs& a, unsigned char* smem_raw, const LmLayou
 // past `count`, which reads and writes nothing): a done seed's lanes run
 // along without changing its state, so the warp's collective steps
 // (self_warp) always see all 32 lanes.  No block-wide barrier.
-template <int MAXA, int MAXEE, int TPS, bool F32S = false>
+template <int MAXA, int MAXEE, int TPS, bool F64S = false>
 __device__ __forceinline__ void lm_seed_groups(const LmArgs& a, unsigned char* smem_raw, const LmLayout& L, int pb,
                                                int count, size_t gs_base) {
   LmShared& sh = *reinterpret_cast<LmShared*>(smem_raw);
@@ -1171,7 +1175,7 @@ __device__ __forceinline__ void lm_seed_groups(const LmArgs& a, unsigned char* s
         if (all_conv) {
           done = true;
         } else {
-          curr = lm_direction<MAXA, MAXEE, F32S>(sh, ps, a.n_ee, W, r, pee, lam, max_p, max_o, delta) + pen_cur;
+          curr = lm_direction<MAXA, MAXEE, F64S>(sh, ps, a.n_ee, W, r, pee, lam, max_p, max_o, delta) + pen_cur;
           best_a_err = 1e30f;
           best_a_pen = pen_cur;
           best_a = 0;
@@ -1233,7 +1237,7 @@ __device__ __forceinline__ void lm_seed_groups(const LmArgs& a, unsigned char* s
 // thread at 128 registers (a few hundred bytes of spills at MAXA = 8); 2
 // leaves room for the whole seed state, for launches whose shared memory
 // admits only 2 blocks per SM anyway.
-template <int MAXA, int MAXEE, int TPS, int MINB, bool F32S = false>
+template <int MAXA, int MAXEE, int TPS, int MINB, bool F64S = false>
 __global__ void __launch_bounds__(128, MINB) lm_kernel(LmArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const LmLayout L = lm_layout(a, TPS);
@@ -1241,7 +1245,7 @@ __global__ void __launch_bounds__(128, MINB) lm_kernel(LmArgs a) {
   lm_stage<MAXA>(a, smem_raw, L, pb);
   const int s_first = blockIdx.x * a.spb;
   const int count = min(a.spb, a.Sd - s_first);
-  lm_seed_groups<MAXA, MAXEE, TPS, F32S>(a, smem_raw, L, pb, count, (size_t)pb * a.Sd + s_first);
+  lm_seed_groups<MAXA, MAXEE, TPS, F64S>(a, smem_raw, L, pb, count, (size_t)pb * a.Sd + s_first);
 }
 
 // Persistent seed-group kernel of pk_ik_batch: blocks take items (class,
@@ -1727,7 +1731,7 @@ __global__ void __launch_bounds__(128) verify_select_kernel(VerifyArgs a) {
 
 static size_t lm_smem_bytes(const LmArgs& a, int tps) { return lm_layout(a, tps).total; }
 
-template <int MAXA, int MAXEE, int TPS, bool F32S = false>
+template <int MAXA, int MAXEE, int TPS, bool F64S = false>
 static int launch_lm_t(const LmArgs& a0, cudaStream_t st) {
   LmArgs a = a0;
   const int threads = a.spb * TPS;
@@ -1736,12 +1740,12 @@ static int launch_lm_t(const LmArgs& a0, cudaStream_t st) {
   dim3 grid((a.Sd + a.spb - 1) / a.spb, a.P);
   // The 4-block register budget (spills) only where shared memory admits 3
   // or more blocks per SM and the grid needs more than 2 blocks per SM.
-  auto kern = lm_kernel<MAXA, MAXEE, TPS, 2, F32S>;
+  auto kern = lm_kernel<MAXA, MAXEE, TPS, 2, F64S>;
   if constexpr (MAXA <= 8) {
     int dev = 0, sms = 0;
     if (int s = cuda_status(cudaGetDevice(&dev), "cudaGetDevice")) return s;
     if (int s = cuda_status(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attribute")) return s;
-    if ((228 * 1024) / (smem + 1024) >= 3 && (long long)grid.x * grid.y > 2LL * sms) kern = lm_kernel<MAXA, MAXEE, TPS, 4, F32S>;
+    if ((228 * 1024) / (smem + 1024) >= 3 && (long long)grid.x * grid.y > 2LL * sms) kern = lm_kernel<MAXA, MAXEE, TPS, 4, F64S>;
   }
   if (int s = set_smem_limit((const void*)kern, smem)) return s;
   kern<<<grid, threads, smem, st>>>(a);
@@ -1750,7 +1754,7 @@ static int launch_lm_t(const LmArgs& a0, cudaStream_t st) {
 
 template <int MAXA, int MAXEE>
 static int launch_lm_tps(const LmArgs& a, int tps, cudaStream_t st) {
-  if (a.f32_solve) return launch_lm_t<MAXA, MAXEE, 1, true>(a, st);
+  if (a.f64_solve) return launch_lm_t<MAXA, MAXEE, 1, true>(a, st);
   switch (tps) {
     case 1: return launch_lm_t<MAXA, MAXEE, 1>(a, st);
     case 2: return launch_lm_t<MAXA, MAXEE, 2>(a, st);
@@ -1797,14 +1801,14 @@ static int launch_lm(LmArgs a, int tps, int spb, cudaStream_t st) {
     if (spb <= 0) spb = (a.n_act <= 8 && a.n_ee <= 1) ? 128 : kSeedsPerBlock16;
   }
   if (tps == 5) {
-    PK_CHECK_ARG(!a.f32_solve, "fp32_solve runs with threads_per_seed 0 or 1");
+    PK_CHECK_ARG(!a.f64_solve, "fp64_solve runs with threads_per_seed 0 or 1");
     if (a.n_act <= 8 && a.n_ee <= 1) return launch_lm_trial<8, 1>(a, st);
     if (a.n_act <= 16 && a.n_ee <= 2) return launch_lm_trial<16, 2>(a, st);
     set_error("the LM kernel supports n_act <= 16 with n_ee <= 2 (got n_act=%d, n_ee=%d)", a.n_act, a.n_ee);
     return PK_ERR_CAPACITY;
   }
   PK_CHECK_ARG(tps == 1 || tps == 2 || tps == 4 || tps == 8, "threads_per_seed must be 0, 1, 2, 4, 5, 8, 16 or 32");
-  PK_CHECK_ARG(!a.f32_solve || tps == 1, "fp32_solve runs with threads_per_seed 0 or 1");
+  PK_CHECK_ARG(!a.f64_solve || tps == 1, "fp64_solve runs with threads_per_seed 0 or 1");
   if (spb <= 0) spb = 128 / tps;
   PK_CHECK_ARG(spb * tps <= 128 && (spb * tps) % 32 == 0,
                "seeds_per_block * threads_per_seed must be a multiple of 32 and at most 128");
@@ -1857,7 +1861,7 @@ static int lm_common(void* stream, const pk_lm_options& o, const float* seeds, c
   a.lam0 = o.lambda_init; a.lam_down = o.lambda_down; a.lam_up = o.lambda_up;
   a.eps_pos = o.eps_pos; a.eps_ori = o.eps_ori;
   a.coll = o.enable_collision ? 1 : 0; a.coll_w = o.collision_weight; a.margin = o.collision_margin;
-  a.f32_solve = o.fp32_solve ? 1 : 0;
+  a.f64_solve = o.fp64_solve ? 1 : 0;
   PK_CHECK_ARG(o.obstacle_grid >= -1 && o.obstacle_grid <= kObsGridMax,
                "obstacle_grid must be -1 (none), 0 (default) or 1..%d cells per axis", kObsGridMax);
   a.grid_n = obstacle_grid_option(o.obstacle_grid);
@@ -1876,7 +1880,7 @@ static int lm_common(void* stream, const pk_lm_options& o, const float* seeds, c
   // that many lanes per seed; robots beyond the seed-group kernel's buckets
   // (n_act > 16 or n_ee > 2) take it too
   if (o.threads_per_seed == 16 || o.threads_per_seed == 32 || a.n_act > 16 || a.n_ee > 2) {
-    PK_CHECK_ARG(!a.f32_solve, "fp32_solve runs in the seed-group kernel (n_act <= 16, n_ee <= 2, "
+    PK_CHECK_ARG(!a.f64_solve, "fp64_solve runs in the seed-group kernel (n_act <= 16, n_ee <= 2, "
                  "threads_per_seed 0 or 1)");
     pk_lm_options ow = o;
     if (o.threads_per_seed == 16 || o.threads_per_seed == 32) ow.lanes_per_wide_seed = o.threads_per_seed;
@@ -2093,7 +2097,7 @@ extern "C" int pk_ik_batch(void* stream, const pk_lm_options* opt, const pk_ik_c
                            const float* world_halfspaces, int32_t Ms, int32_t Mc, int32_t Mb, int32_t Mh,
                            const int32_t* items, int32_t n_items, int32_t* queue, int32_t blocks) {
   PK_CHECK_ARG(opt != nullptr && classes != nullptr, "null options or classes");
-  PK_CHECK_ARG(!opt->fp32_solve, "fp32_solve is not offered by the batched kernels");
+  PK_CHECK_ARG(!opt->fp64_solve, "fp64_solve is not offered by the batched kernels");
   PK_CHECK_ARG(opt->obstacle_grid >= -1 && opt->obstacle_grid <= kObsGridMax,
                "obstacle_grid must be -1 (none), 0 (default) or 1..%d cells per axis", kObsGridMax);
   PK_CHECK_ARG(n_classes >= 1, "at least one class is required");

@@ -43,7 +43,7 @@ class BatchIkSolver:
                  lambda_down: float = 0.5, lambda_up: float = 3.0, eps_pos: float = 1e-8,
                  eps_ori: float = 1e-8, collision_weight: float = 1e4,
                  collision_margin: float = 0.02, pos_tol: float = 1e-3, rot_tol: float = 1e-2,
-                 threads_per_seed: int = 0, seeds_per_block: int = 0, fp32_solve: bool = False, device="cuda"):
+                 threads_per_seed: int = 0, seeds_per_block: int = 0, fp64_solve: bool = False, device="cuda"):
         self.device = torch.device(device)
         self.model = model
         self.robot = DeviceRobot.upload(model, self.device)
@@ -68,7 +68,7 @@ class BatchIkSolver:
         coll = (rs.shape[0] > 0) and (sum(self.world.counts()) > 0 or sp.shape[0] > 0)
         self.opt = _lib.LmOptions(max_iter, pos_weight, ori_weight, lambda_init, lambda_down, lambda_up,
                                   eps_pos, eps_ori, int(coll), collision_weight, collision_margin,
-                                  threads_per_seed, seeds_per_block, 0, int(fp32_solve))
+                                  threads_per_seed, seeds_per_block, 0, int(fp64_solve))
         self.pos_tol, self.rot_tol = pos_tol, rot_tol
 
     def set_fixed_mask(self, mask) -> None:

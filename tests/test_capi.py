@@ -167,17 +167,17 @@ def test_every_declaration_cites_the_reference_or_says_it_has_none():
     assert not missing, missing
 
 
-def test_fp32_solve_is_rejected_where_it_is_not_offered(lib):
-    """fp32_solve runs in the seed-group kernel only: the batched entry and the
+def test_fp64_solve_is_rejected_where_it_is_not_offered(lib):
+    """fp64_solve runs in the seed-group kernel only: the batched entry and the
     other lane mappings refuse it on the host, before any launch."""
     d = C.c_void_p(16)
     opt = _lib.LmOptions(30, 50.0, 10.0, 1e-2, 0.1, 10.0, 1e-8, 1e-8, 0, 1e4, 0.02, 0, 0, 0, 1)
     cls = _lib.IkClass()
     st = lib.pk_ik_batch(None, C.byref(opt), C.byref(cls), 1, None, None, None, None, 0, 0, 0, 0, d, 1, d, 0)
-    assert st == _lib.PK_ERR_INVALID and b"fp32_solve" in lib.pk_last_error()
+    assert st == _lib.PK_ERR_INVALID and b"fp64_solve" in lib.pk_last_error()
     opt.threads_per_seed = 2
     st = lib.pk_ls_ik_ex(None, C.byref(opt), *([d] * 25), 1, 8, 7, 7, 1, 0, 0, 0, 0, 0, 0)
-    assert st == _lib.PK_ERR_INVALID and b"fp32_solve" in lib.pk_last_error()
+    assert st == _lib.PK_ERR_INVALID and b"fp64_solve" in lib.pk_last_error()
 
 
 def test_nvtx_ranges_wrap_calls_when_asked(monkeypatch):

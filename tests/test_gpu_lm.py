@@ -88,15 +88,12 @@ def test_lm_thirty_iterations_seed_by_seed(tps):
     assert ok >= 0.95 * 3 * 40, ok
 
 
-@pytest.mark.parametrize("max_iter", [0, 1, 2])
-def test_lm_fp32_solve_seed_by_seed(max_iter):
-    """FP32 normal equations + Cholesky with the conditional FP64 refinement
-    step, against the FP64 oracle: the same agreement bar as the FP64 solve
-    over the first iterations.  (Once the damping falls below about 1e-6 the
-    7-DOF chain's 6 x 7 system is conditioned beyond FP32, one refinement
-    step leaves steps a fraction of a percent apart, and seeds part ways.)"""
+@pytest.mark.parametrize("max_iter", [0, 1, 2, 30])
+def test_lm_fp64_solve_seed_by_seed(max_iter):
+    """The FP64 option of the damped step (the precision of the reference's
+    normal equations) against the FP64 oracle, seed by seed."""
     w = small_ik(P=3, Sd=40)
-    s = solver_for(w, max_iter=max_iter, fp32_solve=True)
+    s = solver_for(w, max_iter=max_iter, fp64_solve=True)
     cfgs, errs = s.run_lm(tt(w.target_T), tt(w.seeds))
     cfgs, errs = cfgs.cpu().numpy(), errs.cpu().numpy()
     ok = 0
@@ -107,20 +104,21 @@ def test_lm_fp32_solve_seed_by_seed(max_iter):
     assert ok >= 0.95 * 3 * 40, ok
 
 
-def test_lm_fp32_solve_success_matches_fp64_solve():
-    """30 iterations on 32 problems x 128 seeds: the FP32 solve finds as many
-    solutions (1 mm / 0.01 rad, FP64-verified) as the FP64 solve, within 2."""
+def test_lm_fp32_default_success_matches_fp64_solve():
+    """30 iterations on 32 problems x 128 seeds: the default FP32 dual solve
+    (with its conditional FP64 refinement) finds as many solutions (1 mm /
+    0.01 rad, FP64-verified) as the FP64 solve, within 2."""
     w = small_ik(P=32, Sd=128)
-    r64 = solver_for(w).solve(tt(w.target_T), tt(w.seeds))
-    r32 = solver_for(w, fp32_solve=True).solve(tt(w.target_T), tt(w.seeds))
+    r64 = solver_for(w, fp64_solve=True).solve(tt(w.target_T), tt(w.seeds))
+    r32 = solver_for(w).solve(tt(w.target_T), tt(w.seeds))
     n64, n32 = int(r64.success.sum()), int(r32.success.sum())
     assert n32 >= n64 - 2, (n32, n64)
 
 
-def test_lm_fp32_solve_rejects_other_mappings():
+def test_lm_fp64_solve_rejects_other_mappings():
     w = small_ik(P=1, Sd=8)
-    with pytest.raises(Exception, match="fp32_solve"):
-        solver_for(w, fp32_solve=True, threads_per_seed=2).run_lm(tt(w.target_T), tt(w.seeds))
+    with pytest.raises(Exception, match="fp64_solve"):
+        solver_for(w, fp64_solve=True, threads_per_seed=2).run_lm(tt(w.target_T), tt(w.seeds))
 
 
 def test_lm_initial_error_matches_oracle_exactly_enough():
