@@ -153,12 +153,16 @@ typedef struct pk_lm_options {
                               FP64 iterative-refinement step when the squared ratio of the largest to the
                               smallest pivot exceeds 1e6 (default); 1 = FP64, the precision of the reference's
                               normal equations (seed-group kernel: n_act <= 16, n_ee <= 2, threads_per_seed 0 or
-                              1; PK_ERR_INVALID elsewhere, pk_ik_batch included).  The warp-per-seed body (more
-                              than 16 DOF or 2 EEs) solves in FP64 */
+                              1; PK_ERR_INVALID elsewhere, pk_ik_batch included).  With fewer free columns than
+                              6 n_ee rows (fixed joints) the n_act x n_act primal system is solved instead, in the
+                              same precision.  The warp-per-seed body (more than 16 DOF or 2 EEs) always takes
+                              the FP32 form */
   int32_t obstacle_grid;    /* the LM kernels' obstacle tile: the world spheres are binned into a uniform grid of
                               this many cells per axis, built per block in shared memory, and each joint's
-                              bounding sphere tests only its cell's list; 0 = default (8), 1..16 = that many,
-                              -1 = no grid (every obstacle takes the bounding test).  The seed-group kernels'
+                              bounding sphere tests only its cell's list; 0 = default (seed-group kernels: 14
+                              for up to 160 world spheres, else 8; warp-per-seed body: 8), 1..16 = that many,
+                              -1 = no grid (every obstacle takes the bounding test).  A seed-group grid finer
+                              than 8 whose lists overflow their capacity falls back to 8 cells per axis.  The seed-group kernels'
                               results do not depend on it (each joint's hinge terms are summed in increasing
                               obstacle order); the warp-per-seed body spreads its candidates over lanes by list
                               position, so its sums may round differently */

@@ -235,7 +235,7 @@ class MixedIkBatch:
         """Time the prepared batch for each (threads_per_seed, seeds_per_block)
         of the 8-wide seed-group body, each lane count per seed of the warp
         body and each obstacle tile (``obstacle_grid``: the cells per axis of
-        the per-block obstacle grid, 0 = the default 8, -1 = none), and keep
+        the per-block obstacle grid, 0 = the default, -1 = none), and keep
         the fastest.  The item list is rebuilt for each, since a seed-group
         item holds one block's seeds.  Returns {(threads_per_seed,
         seeds_per_block, lanes_per_wide_seed, obstacle_grid): ms}."""

@@ -13,9 +13,10 @@
 // penalty.
 //
 // Refinement (:324-695), per seed, max_iter iterations: the same adaptive row
-// weights (without gating), Jacobi column scaling, FP64 normal equations with
-// LM damping and the soft joint-limit prior lpw / h^2 (q - mid), fixed joints
-// masked, Cholesky (a non-positive pivot gives a zero step), the trust-region
+// weights (without gating), Jacobi column scaling, normal equations (FP64 in
+// the reference) with LM damping and the soft joint-limit prior
+// lpw / h^2 (q - mid), fixed joints masked, Cholesky (a non-positive pivot
+// gives a zero step), the trust-region
 // clip, a 5-point line search on the unweighted error (the first trial that
 // is a new minimum and a sufficient decrease ends it), accept with lambda
 // x0.5 / reject x3, all-time best tracking, and a Gaussian kick from the
@@ -31,6 +32,7 @@
 // (__syncthreads_or), so every seed of a problem stops at the same iteration
 // and results do not depend on scheduling (the reference polls a global flag
 // across blocks).
+#include "pk_damped_step.cuh"
 #include "pk_seed_ik.cuh"
 
 namespace pk {
@@ -128,9 +130,10 @@ __device__ __forceinline__ float hjcd_error(const SeedIkArgs& a, const SeedIkSha
 }
 
 // LM step of the current point: adaptive row weights, Jacobi column scaling,
-// FP64 normal equations with damping and the joint-limit prior, fixed and
-// padding columns masked, Cholesky (zero step on a non-positive pivot),
-// unscaling and the trust-region clip.
+// the damped system with the joint-limit prior, fixed and padding columns
+// masked, solved in FP32 with one conditional FP64 refinement step
+// (damped_step_f32: its dual form for one or two EEs; zero step on a
+// non-positive pivot), unscaling and the trust-region clip.
 template <int MAXA, int MAXEE>
 __device__ __forceinline__ void hjcd_direction(const SeedIkArgs& a, const SeedIkShared& sh, const PoseSlots& ps,
                                                const float (&r)[6 * MAXEE], const float (&pee)[3 * MAXEE],
@@ -166,68 +169,25 @@ __device__ __forceinline__ void hjcd_direction(const SeedIkArgs& a, const SeedIk
   for (int k = 0; k < 6 * MAXEE; ++k)
 #pragma unroll
     for (int c = 0; c < MAXA; ++c) J[k][c] = J[k][c] / cs[c];
-  double A[MAXA * (MAXA + 1) / 2];
-  double rhs[MAXA];
+  // the joint-limit prior w / h^2 (q - mid) in scaled columns: diagonal
+  // w / (h^2 s^2), right-hand side w (q - mid) / (h^2 s)
+  bool fr[MAXA];
+  float pd[MAXA], v[MAXA], zero[MAXA], x[MAXA];
 #pragma unroll
   for (int i = 0; i < MAXA; ++i) {
-    const bool fi = sh.fixed[i];
-#pragma unroll
-    for (int j = 0; j <= i; ++j) {
-      double acc = 0.0;
-#pragma unroll
-      for (int k = 0; k < 6 * MAXEE; ++k) acc += (double)J[k][i] * (double)J[k][j];
-      const bool fj = sh.fixed[j];
-      A[i * (i + 1) / 2 + j] = (fi || fj) ? ((i == j) ? 1.0 : 0.0) : acc;
-    }
-    double rb = 0.0;
-#pragma unroll
-    for (int k = 0; k < 6 * MAXEE; ++k) rb += (double)J[k][i] * (double)fw[k];
-    if (fi) {
-      rhs[i] = 0.0;
-    } else {
-      const double hr = (double)((sh.hi[i] - sh.lo[i]) * 0.5f + 1e-8f);
-      const double mid = (double)((sh.lo[i] + sh.hi[i]) * 0.5f);
-      const double dpr = (double)a.limit_prior_weight / (hr * hr);
-      A[i * (i + 1) / 2 + i] += (double)lam + dpr / ((double)cs[i] * (double)cs[i]);
-      rhs[i] = -(rb + dpr * (double)(cfg[i] - (float)mid) / (double)cs[i]);
-    }
+    fr[i] = !sh.fixed[i];
+    zero[i] = 0.f;
+    const float hr = (sh.hi[i] - sh.lo[i]) * 0.5f + 1e-8f;
+    const float mid = (sh.lo[i] + sh.hi[i]) * 0.5f;
+    const float dpr = a.limit_prior_weight / (hr * hr);
+    pd[i] = fr[i] ? dpr / (cs[i] * cs[i]) : 0.f;
+    v[i] = fr[i] ? dpr * (cfg[i] - mid) / cs[i] : 0.f;
   }
-  bool ok = true;
-#pragma unroll
-  for (int k = 0; k < MAXA; ++k) {
-    double s2 = A[k * (k + 1) / 2 + k];
-#pragma unroll
-    for (int q = 0; q < k; ++q) s2 -= A[k * (k + 1) / 2 + q] * A[k * (k + 1) / 2 + q];
-    if (!(s2 > 0.0)) ok = false;
-    const double lkk = sqrt(ok ? s2 : 1.0);
-    const double inv = 1.0 / lkk;
-    A[k * (k + 1) / 2 + k] = lkk;
-#pragma unroll
-    for (int i = k + 1; i < MAXA; ++i) {
-      double tt = A[i * (i + 1) / 2 + k];
-#pragma unroll
-      for (int q = 0; q < k; ++q) tt -= A[i * (i + 1) / 2 + q] * A[k * (k + 1) / 2 + q];
-      A[i * (i + 1) / 2 + k] = tt * inv;
-    }
-  }
-#pragma unroll
-  for (int i = 0; i < MAXA; ++i) {
-    double s2 = rhs[i];
-#pragma unroll
-    for (int q = 0; q < i; ++q) s2 -= A[i * (i + 1) / 2 + q] * rhs[q];
-    rhs[i] = s2 / A[i * (i + 1) / 2 + i];
-  }
-#pragma unroll
-  for (int i = MAXA - 1; i >= 0; --i) {
-    double s2 = rhs[i];
-#pragma unroll
-    for (int q = i + 1; q < MAXA; ++q) s2 -= A[q * (q + 1) / 2 + i] * rhs[q];
-    rhs[i] = s2 / A[i * (i + 1) / 2 + i];
-  }
+  const bool ok = damped_step_f32<6 * MAXEE, MAXA>(J, fw, 6 * n_ee, lam, pd, fr, zero, v, x);
   float dn2 = 0.f;
 #pragma unroll
   for (int c = 0; c < MAXA; ++c) {
-    delta[c] = ok ? (float)rhs[c] / cs[c] : 0.f;
+    delta[c] = ok ? x[c] / cs[c] : 0.f;
     dn2 += delta[c] * delta[c];
   }
   float R;

@@ -39,6 +39,7 @@
 #include <algorithm>
 
 #include "pk_batch.cuh"
+#include "pk_damped_step.cuh"
 #include "pk_obstacle_grid.cuh"
 
 namespace pk {
@@ -67,6 +68,7 @@ struct LmArgs {
   int spb;
   int f64_solve;  // the damped step's system in FP64 (seed-group kernel, one lane per seed); else FP32
   int grid_n;     // obstacle grid cells per axis (0: no grid, every obstacle takes the bounding test)
+  int grid_auto;  // grid_n is the default resolution (the launch may coarsen it; see lm_fit_grid)
 };
 
 // Shared-memory layout of one LM block.
@@ -158,7 +160,8 @@ __host__ __device__ inline LmLayout lm_layout(const LmArgs& a, int tps, int thre
     L.scratch_ints = 7 * a.m.n_joints * threads;  // the pose slots double as staging scratch
   }
   L.grid = (a.grid_n > 0 && a.coll && a.w.Ms >= 32 && a.w.Ms <= 65535 && a.w.Ms <= L.scratch_ints) ? 1 : 0;
-  L.max_entries = L.grid ? min(max(48 * a.w.Ms, 1024), 16384) : 0;
+  // list capacity: a finer grid lists each obstacle in more cells
+  L.max_entries = L.grid ? min(max((a.grid_n > kObsGridDefault ? 80 : 48) * a.w.Ms, 1024), 16384) : 0;
   L.rs = o; o = lm_align16(o + 16 * (size_t)n_rs);
   L.rsp = o; o = lm_align16(o + (threads == 0 ? 16 * (size_t)(n_rs + a.m.n_joints) : 0));
   // the world, in stage_world's layout: spheres in ms_pad float4 slots, then
@@ -589,17 +592,41 @@ __device__ __forceinline__ void ee_residual(const LmShared& sh, const PoseSlots&
 // the MAXA x MAXA normal equations of a redundant arm, whose null space puts
 // an eigenvalue at lam itself, it is only ill-conditioned near singular
 // configurations.  The system and its Cholesky are FP32; when the squared
-// ratio of the largest to the smallest pivot exceeds 1e6, one step of
-// iterative refinement follows: the residual fw - (Js Js^T + lam I) y in
-// FP64 (from the FP32 Jacobian entries, which FP64 holds exactly), the
-// correction solved with the FP32 factor.  J is the column-scaled weighted
+// ratio of the largest to the smallest pivot (over the live rows) exceeds
+// 1e6, one step of iterative refinement follows: the residual
+// fw - (Js Js^T + lam I) y in FP64 (from the FP32 Jacobian entries, which
+// FP64 holds exactly), the correction solved with the FP32 factor.  With
+// fewer free columns than live rows the primal system is solved instead, in
+// the same way (damped_step_primal).  J is the column-scaled weighted
 // Jacobian, fw the weighted residual; writes the unscaled step into delta
 // (zero on a non-positive pivot).
 template <int MAXA, int MAXEE>
 __device__ __forceinline__ void lm_solve_f32(const LmShared& sh, const float (&J)[6 * MAXEE][MAXA],
-                                             const float (&fw)[6 * MAXEE], float lam, const float (&col_s)[MAXA],
-                                             float (&delta)[MAXA]) {
+                                             const float (&fw)[6 * MAXEE], int rows, float lam,
+                                             const float (&col_s)[MAXA], float (&delta)[MAXA]) {
   constexpr int R = 6 * MAXEE;
+  {
+    // fewer free columns than live rows (fixed joints): the dual system
+    // would carry the null space of Js^T as eigenvalues lam, so the primal
+    // system (of full column rank then) is solved instead; block-uniform
+    bool fr[MAXA];
+    float zero[MAXA], x[MAXA];
+    int nf = 0;
+#pragma unroll
+    for (int c = 0; c < MAXA; ++c) {
+      fr[c] = !sh.fixed[c];
+      zero[c] = 0.f;
+      nf += fr[c] ? 1 : 0;
+    }
+    if (nf < rows) {
+      bool ok;
+      if constexpr (MAXA <= 8) ok = damped_step_primal<R, MAXA>(J, fw, lam, zero, fr, zero, zero, x);
+      else ok = damped_step_primal_ool<R, MAXA>(J, fw, lam, zero, fr, zero, zero, x);
+#pragma unroll
+      for (int c = 0; c < MAXA; ++c) delta[c] = (ok && fr[c]) ? x[c] / col_s[c] : 0.f;
+      return;
+    }
+  }
   float A[R * (R + 1) / 2];
 #pragma unroll
   for (int i = 0; i < R; ++i) {
@@ -621,8 +648,10 @@ __device__ __forceinline__ void lm_solve_f32(const LmShared& sh, const float (&J
 #pragma unroll
     for (int q = 0; q < k; ++q) s2 = fmaf(-A[k * (k + 1) / 2 + q], A[k * (k + 1) / 2 + q], s2);
     if (!(s2 > 0.f)) ok = false;
-    pmax = fmaxf(pmax, s2);
-    pmin = fminf(pmin, s2);
+    if (k < rows) {  // padding rows of absent EEs hold lam alone
+      pmax = fmaxf(pmax, s2);
+      pmin = fminf(pmin, s2);
+    }
     const float inv = 1.f / sqrtf(ok ? s2 : 1.f);
     A[k * (k + 1) / 2 + k] = inv;
 #pragma unroll
@@ -759,7 +788,7 @@ __device__ __forceinline__ float lm_direction(const LmShared& sh, const PoseSlot
     for (int c = 0; c < MAXA; ++c) J[k][c] = J[k][c] / col_s[c];
 
   if constexpr (!F64S) {
-    lm_solve_f32<MAXA, MAXEE>(sh, J, fw, lam, col_s, delta);
+    lm_solve_f32<MAXA, MAXEE>(sh, J, fw, 6 * n_ee, lam, col_s, delta);
   } else {
   // FP64, through the push-through identity
   //   (Js^T Js + lam I)^-1 Js^T = Js^T (Js Js^T + lam I)^-1,
@@ -1045,9 +1074,23 @@ __device__ void lm_stage(const LmArgs& a, unsigned char* smem_raw, const LmLayou
   }
   __syncthreads();
 
-  if (sh.grid_on)
+  if (sh.grid_on) {
     obstacle_grid_build(ws4, a.w.Ms, sh.rmax, sh.grid_n, sh.glo, sh.ginv, scratch, cell_start, cell_obs,
                         L.max_entries, sh.grid_on);
+    // a fine grid whose lists overflow the capacity falls back to the default
+    // resolution (fewer, longer lists) before going without a grid
+    if (!sh.grid_on && sh.grid_n > kObsGridDefault) {
+      __syncthreads();
+      if (tid == 0) {
+        sh.grid_n = kObsGridDefault;
+        obstacle_grid_bounds(ws4, a.w.Ms, sh.rmax, sh.grid_n, sh.glo, sh.ginv);
+        sh.grid_on = 1;
+      }
+      __syncthreads();
+      obstacle_grid_build(ws4, a.w.Ms, sh.rmax, sh.grid_n, sh.glo, sh.ginv, scratch, cell_start, cell_obs,
+                          L.max_entries, sh.grid_on);
+    }
+  }
 }
 
 // `count` seeds of problem pb, with the block's shared memory already
@@ -1731,9 +1774,25 @@ __global__ void __launch_bounds__(128) verify_select_kernel(VerifyArgs a) {
 
 static size_t lm_smem_bytes(const LmArgs& a, int tps) { return lm_layout(a, tps).total; }
 
+// Blocks per SM that shared memory admits (at most the 4 of the small
+// register budget).
+static int lm_blocks_per_sm(size_t smem) { return (int)std::min<size_t>(4, (228 * 1024) / (smem + 1024)); }
+
+// The fine default grid (lm_grid_option) only where its larger cell lists
+// keep the blocks per SM that the default resolution admits; else the
+// default resolution.  `threads` as for lm_layout.
+static void lm_fit_grid(LmArgs& a, int tps, int threads = 0) {
+  if (!a.grid_auto || a.grid_n <= kObsGridDefault) return;
+  LmArgs b = a;
+  b.grid_n = kObsGridDefault;
+  if (lm_blocks_per_sm(lm_layout(a, tps, threads).total) < lm_blocks_per_sm(lm_layout(b, tps, threads).total))
+    a.grid_n = kObsGridDefault;
+}
+
 template <int MAXA, int MAXEE, int TPS, bool F64S = false>
 static int launch_lm_t(const LmArgs& a0, cudaStream_t st) {
   LmArgs a = a0;
+  lm_fit_grid(a, TPS);
   const int threads = a.spb * TPS;
   const size_t smem = lm_smem_bytes(a, TPS);
   PK_CHECK_CAP(smem <= 220 * 1024, "LM working set (%zu B of shared memory) too large", smem);
@@ -1767,6 +1826,7 @@ template <int MAXA, int MAXEE>
 static int launch_lm_trial(LmArgs a, cudaStream_t st) {
   const int threads = 128;
   a.spb = 6 * (threads / 32);  // 6 groups of 5 lanes per warp
+  lm_fit_grid(a, 1, threads);
   const size_t smem = lm_layout(a, 1, threads).total;
   PK_CHECK_CAP(smem <= 220 * 1024, "LM working set (%zu B of shared memory) too large", smem);
   auto kern = lm_trial_kernel<MAXA, MAXEE>;
@@ -1864,7 +1924,8 @@ static int lm_common(void* stream, const pk_lm_options& o, const float* seeds, c
   a.f64_solve = o.fp64_solve ? 1 : 0;
   PK_CHECK_ARG(o.obstacle_grid >= -1 && o.obstacle_grid <= kObsGridMax,
                "obstacle_grid must be -1 (none), 0 (default) or 1..%d cells per axis", kObsGridMax);
-  a.grid_n = obstacle_grid_option(o.obstacle_grid);
+  a.grid_n = lm_grid_option(o.obstacle_grid, Ms);
+  a.grid_auto = o.obstacle_grid == 0;
   if (int s = validate_lm(a)) return s;
   if (P == 0 || Sd == 0) return PK_OK;
   PK_CHECK_ARG(seeds && twists && parent_tf && parent_idx && act_idx && mimic_mul && mimic_off &&
@@ -2043,13 +2104,34 @@ static int launch_seed_group_body(const BatchCall& b, int body, cudaStream_t st,
     a.coll = o.enable_collision ? 1 : 0; a.coll_w = o.collision_weight; a.margin = o.collision_margin;
     if (!a.coll) a.n_self = 0;
     a.spb = spb;
-    a.grid_n = obstacle_grid_option(o.obstacle_grid);
+    a.grid_n = lm_grid_option(o.obstacle_grid, a.w.Ms);
+    a.grid_auto = o.obstacle_grid == 0;
     if (int s = validate_lm(a)) return s;
     PK_CHECK_ARG(k.seeds && k.out_cfg && k.out_err && k.target_Ts && k.lower && k.upper && k.fixed_mask,
                  "null buffer in class %d", c);
     B.cls[c] = a;
     smem = std::max(smem, lm_layout(a, tps).total);
     any = true;
+  }
+  {
+    // the fine default grid only where it keeps the blocks per SM (lm_fit_grid), over all classes
+    size_t smem_def = 0;
+    bool fine = false;
+    for (int c = 0; c < b.n_classes; ++c) {
+      if (b.cls[c].body != body) continue;
+      LmArgs d = B.cls[c];
+      if (d.grid_auto && d.grid_n > kObsGridDefault) {
+        d.grid_n = kObsGridDefault;
+        fine = true;
+      }
+      smem_def = std::max(smem_def, lm_layout(d, tps).total);
+    }
+    if (fine && lm_blocks_per_sm(smem) < lm_blocks_per_sm(smem_def)) {
+      for (int c = 0; c < b.n_classes; ++c)
+        if (b.cls[c].body == body && B.cls[c].grid_auto && B.cls[c].grid_n > kObsGridDefault)
+          B.cls[c].grid_n = kObsGridDefault;
+      smem = smem_def;
+    }
   }
   if (!any || b.n_items == 0) return PK_OK;
   PK_CHECK_CAP(smem <= 220 * 1024, "LM working set (%zu B of shared memory) too large", smem);

@@ -6,9 +6,9 @@
 // The per-seed iteration is the one of the seed-group kernel (pk_lm.cu),
 // which restates ls_ik_lm_kernel (src/pyroffi/cuda_kernels/
 // _ls_ik_cuda_kernel.cu:65-394): residual, weighted stacked Jacobian, Jacobi
-// column scaling, FP64 damped normal equations, Cholesky (step 0 on a
-// non-positive pivot), trust-region clip, 5-point line search on clamped
-// trials, accept/reject of the damping, all-time best.
+// column scaling, damped normal equations (FP64 in the reference), Cholesky
+// (step 0 on a non-positive pivot), trust-region clip, 5-point line search
+// on clamped trials, accept/reject of the damping, all-time best.
 //
 // B200 mapping: one warp owns one seed and keeps the seed's state in
 // shared memory, so no per-thread array grows with the DOF count:
@@ -18,10 +18,11 @@
 //    an actuated joint that is fixed, or moves no end effector, has an
 //    all-zero column whose damped step is exactly 0, so dropping it changes
 //    nothing but the size of the solve;
-//  * the FP64 normal equations are formed by rows (lane j computes A[i][j])
-//    and factored by the left-looking Cholesky of the seed-group kernel,
-//    parallel over the rows below the pivot with the same arithmetic per
-//    entry; the two triangular solves run column by column;
+//  * the damped system (its rows x rows dual form when the residual rows are
+//    fewer than the active columns) is formed in FP32 by packed entries,
+//    factored by a left-looking Cholesky parallel over the rows below the
+//    pivot, and solved column by column, with one FP64 refinement step when
+//    the squared pivot ratio exceeds 1e6;
 //  * the collision penalty is split over the lanes: sphere transforms by
 //    sphere, world spheres by sphere-carrying joint (bounding-sphere cull
 //    and a per-block obstacle grid, as in the seed-group kernel), other
@@ -61,7 +62,8 @@ struct WideArgs {
 // Byte offsets of the dynamic shared memory, sized for the largest class.
 struct WideLayout {
   size_t rs, rsj, rsk, pairs, ws, wc, wb, wh, cells, cell_obs, obox, warps, warp_bytes, total;
-  size_t w_cfg, w_best, w_dact, w_trial, w_dcol, w_cs, w_r, w_fw, w_pee, w_T, w_J, w_A, w_y, w_pos, w_slot;
+  size_t w_cfg, w_best, w_dact, w_trial, w_dcol, w_cs, w_r, w_fw, w_pee, w_T, w_J, w_A, w_y, w_b, w_d, w_t, w_pos,
+      w_slot;
   int max_rs, max_self, max_joints, max_act, max_rows, max_entries, nwarps;
   int grid_n;  // obstacle grid cells per axis (0: no grid)
 };
@@ -148,9 +150,12 @@ __host__ inline WideLayout wide_layout(int max_rs, int max_self, int max_joints,
   L.w_slot = q;  // per sphere-carrying joint: B, R (float4); list range, offset (int4)
   q = w_align16(q + std::max(4 * (size_t)L.max_rows * max_act, 32 * (size_t)max_joints));
   L.w_A = q;
-  L.w_y = w_align16(q + 8 * (size_t)max_act * (max_act + 1) / 2);
+  L.w_y = w_align16(q + 4 * (size_t)max_act * (max_act + 1) / 2);
+  L.w_b = L.w_y + 4 * (size_t)PK_MAX_ACT;  // the system has at most PK_MAX_ACT rows
+  L.w_d = L.w_b + 4 * (size_t)PK_MAX_ACT;
+  L.w_t = L.w_d + 4 * (size_t)PK_MAX_ACT;  // ncol or rows doubles, both <= PK_MAX_ACT
   L.w_pos = q;
-  q = w_align16(std::max(L.w_y + 8 * (size_t)PK_MAX_ACT, q + 16 * (size_t)max_rs));
+  q = w_align16(std::max(L.w_t + 8 * (size_t)PK_MAX_ACT, q + 16 * (size_t)max_rs));
   L.warp_bytes = q;
   L.warps = o;
   L.total = o + q * nwarps;
@@ -349,7 +354,8 @@ __device__ __forceinline__ void w_hinge(float d2, float rr, float& pen) {
 
 struct WideWarp {
   float *cfg, *best, *dact, *trial, *dcol, *cs, *r, *fw, *pee, *T, *J;
-  double *A, *y;
+  float *A, *y, *b, *d;  // damped system: factor, solution, right-hand side, correction
+  double* t;             // refinement scratch
   float4* pos;
   float4* slotB;  // per slot: bounding centre (world) and radius
   int4* slotL;    // per slot: first list entry, candidate count, offset in the flattened candidates, -
@@ -582,11 +588,15 @@ __device__ __noinline__ float w_direction(const WideShared& sh, int n_act, int n
   float fw2 = 0.f;
   for (int k = 0; k < rows; ++k) fw2 += W.fw[k] * W.fw[k];
 
-  // FP64 damped system, packed lower triangle: lanes take the entries
+  // FP32 damped system, packed lower triangle: lanes take the entries
   // e = i (i + 1) / 2 + j in turn.  With fewer residual rows than active
   // columns it is the dual form (Js Js^T + lam I) y = fw, p = -Js^T y (the
   // push-through identity: the same step as (Js^T Js + lam I) p = -Js^T fw,
-  // on a rows x rows system); otherwise the normal equations themselves.
+  // on a rows x rows system); otherwise the normal equations themselves,
+  // then of full column rank.  When the squared ratio of the largest to the
+  // smallest Cholesky pivot exceeds 1e6, one step of iterative refinement
+  // follows: the residual in FP64 from the FP32 entries (which FP64 holds
+  // exactly), the correction solved with the FP32 factor.
   const bool dual = rows < ncol;
   const int n = dual ? rows : ncol;
   {
@@ -594,25 +604,24 @@ __device__ __noinline__ float w_direction(const WideShared& sh, int n_act, int n
     int i = 0, j = gl;
     while (i < n && j > i) { j -= i + 1; ++i; }
     for (int e = gl; e < ne; e += G) {
-      double acc = 0.0;
+      float acc = (i == j) ? lam : 0.f;
       if (dual) {
-        for (int c = 0; c < ncol; ++c) acc += (double)W.J[c * rows + i] * (double)W.J[c * rows + j];
+        for (int c = 0; c < ncol; ++c) acc = fmaf(W.J[c * rows + i], W.J[c * rows + j], acc);
       } else {
-        for (int k = 0; k < rows; ++k) acc += (double)W.J[i * rows + k] * (double)W.J[j * rows + k];
+        for (int k = 0; k < rows; ++k) acc = fmaf(W.J[i * rows + k], W.J[j * rows + k], acc);
       }
-      if (i == j) acc += (double)lam;
       W.A[e] = acc;
       j += G;
       while (i < n && j > i) { j -= i + 1; ++i; }
     }
   }
   if (dual) {
-    for (int i = gl; i < rows; i += G) W.y[i] = (double)W.fw[i];
+    for (int i = gl; i < rows; i += G) W.b[i] = W.y[i] = W.fw[i];
   } else {
     for (int i = gl; i < ncol; i += G) {
-      double rb = 0.0;
-      for (int k = 0; k < rows; ++k) rb += (double)W.J[i * rows + k] * (double)W.fw[k];
-      W.y[i] = -rb;
+      float rb = 0.f;
+      for (int k = 0; k < rows; ++k) rb = fmaf(W.J[i * rows + k], W.fw[k], rb);
+      W.b[i] = W.y[i] = -rb;
     }
   }
   __syncwarp(gm);
@@ -620,46 +629,80 @@ __device__ __noinline__ float w_direction(const WideShared& sh, int n_act, int n
   // Cholesky A = L L^T, left-looking; a non-positive pivot zeroes the step.
   // The diagonal keeps 1 / L[k][k] (every later use multiplies by it).
   bool ok = true;
+  float pmax = 0.f, pmin = 3.4e38f;
   for (int k = 0; k < n; ++k) {
     const int kk = k * (k + 1) / 2;
-    double s2 = W.A[kk + k];
-    for (int q = 0; q < k; ++q) s2 -= W.A[kk + q] * W.A[kk + q];
-    if (!(s2 > 0.0)) ok = false;
-    const double inv = 1.0 / sqrt(ok ? s2 : 1.0);
+    float s2 = W.A[kk + k];
+    for (int q = 0; q < k; ++q) s2 = fmaf(-W.A[kk + q], W.A[kk + q], s2);
+    if (!(s2 > 0.f)) ok = false;
+    pmax = fmaxf(pmax, s2);
+    pmin = fminf(pmin, s2);
+    const float inv = 1.f / sqrtf(ok ? s2 : 1.f);
     for (int i = k + 1 + gl; i < n; i += G) {
       const int ii = i * (i + 1) / 2;
-      double tt = W.A[ii + k];
-      for (int q = 0; q < k; ++q) tt -= W.A[ii + q] * W.A[kk + q];
+      float tt = W.A[ii + k];
+      for (int q = 0; q < k; ++q) tt = fmaf(-W.A[ii + q], W.A[kk + q], tt);
       W.A[ii + k] = tt * inv;
     }
     __syncwarp(gm);
     if (gl == 0) W.A[kk + k] = inv;
     __syncwarp(gm);
   }
-  // L y = b, then L^T x = y (column by column; x overwrites y)
-  for (int i = 0; i < n; ++i) {
-    const double yi = W.y[i] * W.A[i * (i + 1) / 2 + i];
-    for (int j = i + 1 + gl; j < n; j += G) W.y[j] -= W.A[j * (j + 1) / 2 + i] * yi;
+  // L y = b, then L^T x = y (column by column; x overwrites v)
+  auto tri_solve = [&](float* v) {
+    for (int i = 0; i < n; ++i) {
+      const float yi = v[i] * W.A[i * (i + 1) / 2 + i];
+      for (int j = i + 1 + gl; j < n; j += G) v[j] = fmaf(-W.A[j * (j + 1) / 2 + i], yi, v[j]);
+      __syncwarp(gm);
+      if (gl == 0) v[i] = yi;
+      __syncwarp(gm);
+    }
+    for (int i = n - 1; i >= 0; --i) {
+      const int ii = i * (i + 1) / 2;
+      const float xi = v[i] * W.A[ii + i];
+      for (int j = gl; j < i; j += G) v[j] = fmaf(-W.A[ii + j], xi, v[j]);
+      __syncwarp(gm);
+      if (gl == 0) v[i] = xi;
+      __syncwarp(gm);
+    }
+  };
+  tri_solve(W.y);
+  if (ok && pmax > 1e6f * pmin) {
+    // the residual b - A y in FP64: t = Js y (dual: per column) or Js x
+    // (primal: per row) first, then per row of the system
+    const int nt = dual ? ncol : rows;
+    for (int c = gl; c < nt; c += G) {
+      double acc = 0.0;
+      if (dual) {
+        for (int k = 0; k < rows; ++k) acc = fma((double)W.J[c * rows + k], (double)W.y[k], acc);
+      } else {
+        for (int q = 0; q < ncol; ++q) acc = fma((double)W.J[q * rows + c], (double)W.y[q], acc);
+      }
+      W.t[c] = acc;
+    }
     __syncwarp(gm);
-    if (gl == 0) W.y[i] = yi;
+    for (int i = gl; i < n; i += G) {
+      double acc = (double)lam * (double)W.y[i];
+      if (dual) {
+        for (int c = 0; c < ncol; ++c) acc = fma((double)W.J[c * rows + i], W.t[c], acc);
+      } else {
+        for (int k = 0; k < rows; ++k) acc = fma((double)W.J[i * rows + k], W.t[k], acc);
+      }
+      W.d[i] = (float)((double)W.b[i] - acc);
+    }
     __syncwarp(gm);
-  }
-  for (int i = n - 1; i >= 0; --i) {
-    const int ii = i * (i + 1) / 2;
-    const double xi = W.y[i] * W.A[ii + i];
-    for (int j = gl; j < i; j += G) W.y[j] -= W.A[ii + j] * xi;
-    __syncwarp(gm);
-    if (gl == 0) W.y[i] = xi;
+    tri_solve(W.d);
+    for (int i = gl; i < n; i += G) W.y[i] = (float)((double)W.y[i] + (double)W.d[i]);
     __syncwarp(gm);
   }
   if (dual) {
     for (int c = gl; c < ncol; c += G) {
-      double pc = 0.0;
-      for (int k = 0; k < rows; ++k) pc += (double)W.J[c * rows + k] * W.y[k];
-      W.dcol[c] = ok ? (float)(-pc) / W.cs[c] : 0.f;
+      float pc = 0.f;
+      for (int k = 0; k < rows; ++k) pc = fmaf(W.J[c * rows + k], W.y[k], pc);
+      W.dcol[c] = ok ? -pc / W.cs[c] : 0.f;
     }
   } else {
-    for (int c = gl; c < ncol; c += G) W.dcol[c] = ok ? (float)W.y[c] / W.cs[c] : 0.f;
+    for (int c = gl; c < ncol; c += G) W.dcol[c] = ok ? W.y[c] / W.cs[c] : 0.f;
   }
   __syncwarp(gm);
   float dn2 = 0.f;
@@ -779,8 +822,11 @@ __device__ __forceinline__ WideWarp w_group_area(const WideLayout& L, unsigned c
   W.pee = reinterpret_cast<float*>(b + L.w_pee);
   W.T = reinterpret_cast<float*>(b + L.w_T);
   W.J = reinterpret_cast<float*>(b + L.w_J);
-  W.A = reinterpret_cast<double*>(b + L.w_A);
-  W.y = reinterpret_cast<double*>(b + L.w_y);
+  W.A = reinterpret_cast<float*>(b + L.w_A);
+  W.y = reinterpret_cast<float*>(b + L.w_y);
+  W.b = reinterpret_cast<float*>(b + L.w_b);
+  W.d = reinterpret_cast<float*>(b + L.w_d);
+  W.t = reinterpret_cast<double*>(b + L.w_t);
   W.pos = reinterpret_cast<float4*>(b + L.w_pos);
   W.slotB = reinterpret_cast<float4*>(b + L.w_slot);
   W.slotL = reinterpret_cast<int4*>(b + L.w_slot + 16 * (size_t)L.max_joints);

@@ -5,11 +5,12 @@
 //
 // Per seed, max_iter iterations: residual and Jacobian of every EE; exit when
 // all EEs are within (eps_pos, eps_ori); rows weighted by (pos_weight,
-// ori_weight); Jacobi column scaling; FP64 H = Js^T Js + lambda I and
-// g = Js^T f; the step's box in scaled space, ((lower - q) s, (upper - q) s)
-// (0 for fixed joints); the unconstrained Newton step by Cholesky, clamped to
-// the box; n_inner active-set re-solves (joints at a bound are held there and
-// the free ones re-solved against g + H p_bound); unscaling; the trust-region
+// ori_weight); Jacobi column scaling; H = Js^T Js + lambda I and g = Js^T f
+// (FP64 in the reference); the step's box in scaled space,
+// ((lower - q) s, (upper - q) s) (0 for fixed joints); the unconstrained
+// Newton step by Cholesky, clamped to the box; n_inner active-set re-solves
+// (joints at a bound are held there and the free ones re-solved against
+// g + H p_bound); unscaling; the trust-region
 // clip; a 5-point line search on the weighted error plus the collision
 // penalty (first minimum); accept with lambda x0.5 / reject x3; all-time
 // best tracking.
@@ -21,56 +22,17 @@
 // B200 mapping: 32 seeds of one problem per block of 128 threads, 4 lanes
 // per seed.  The lanes of a seed hold the same state and compute the same
 // step; they split the collision penalty over the obstacles (robot spheres
-// grouped by joint, with exact bounding-sphere culling at the margin).
+// grouped by joint, with exact bounding-sphere culling at the margin).  Each
+// solve of the step is FP32 with one conditional FP64 refinement step
+// (damped_step_f32: the 6 n_ee x 6 n_ee dual system for one or two EEs, the
+// normal equations for more).
+#include "pk_damped_step.cuh"
 #include "pk_seed_ik.cuh"
 
 namespace pk {
 
 constexpr int kSqpThreads = 128;
 constexpr int kSqpTps = 4;
-
-// In-place Cholesky of a packed lower triangle and solve of A x = b (x in b);
-// a non-positive pivot zeroes b and returns false.
-template <int MAXA>
-__device__ __forceinline__ bool chol_packed(double (&A)[MAXA * (MAXA + 1) / 2], double (&b)[MAXA]) {
-  bool ok = true;
-#pragma unroll
-  for (int k = 0; k < MAXA; ++k) {
-    double s2 = A[k * (k + 1) / 2 + k];
-#pragma unroll
-    for (int q = 0; q < k; ++q) s2 -= A[k * (k + 1) / 2 + q] * A[k * (k + 1) / 2 + q];
-    if (!(s2 > 0.0)) ok = false;
-    const double lkk = sqrt(ok ? s2 : 1.0);
-    const double inv = 1.0 / lkk;
-    A[k * (k + 1) / 2 + k] = lkk;
-#pragma unroll
-    for (int i = k + 1; i < MAXA; ++i) {
-      double tt = A[i * (i + 1) / 2 + k];
-#pragma unroll
-      for (int q = 0; q < k; ++q) tt -= A[i * (i + 1) / 2 + q] * A[k * (k + 1) / 2 + q];
-      A[i * (i + 1) / 2 + k] = tt * inv;
-    }
-  }
-#pragma unroll
-  for (int i = 0; i < MAXA; ++i) {
-    double s2 = b[i];
-#pragma unroll
-    for (int q = 0; q < i; ++q) s2 -= A[i * (i + 1) / 2 + q] * b[q];
-    b[i] = s2 / A[i * (i + 1) / 2 + i];
-  }
-#pragma unroll
-  for (int i = MAXA - 1; i >= 0; --i) {
-    double s2 = b[i];
-#pragma unroll
-    for (int q = i + 1; q < MAXA; ++q) s2 -= A[q * (q + 1) / 2 + i] * b[q];
-    b[i] = s2 / A[i * (i + 1) / 2 + i];
-  }
-  if (!ok) {
-#pragma unroll
-    for (int i = 0; i < MAXA; ++i) b[i] = 0.0;
-  }
-  return ok;
-}
 
 // Weighted squared error plus collision penalty at the joint poses in `ps`.
 template <int MAXEE, int TPS>
@@ -114,67 +76,34 @@ __device__ __forceinline__ void sqp_direction(const SeedIkArgs& a, const SeedIkS
   for (int k = 0; k < 6 * MAXEE; ++k)
 #pragma unroll
     for (int c = 0; c < MAXA; ++c) J[k][c] = J[k][c] / cs[c];
-  constexpr int NP = MAXA * (MAXA + 1) / 2;
-  double H[NP], g[MAXA];
-#pragma unroll
-  for (int i = 0; i < MAXA; ++i) {
-#pragma unroll
-    for (int j = 0; j <= i; ++j) {
-      double acc = 0.0;
-#pragma unroll
-      for (int k = 0; k < 6 * MAXEE; ++k) acc += (double)J[k][i] * (double)J[k][j];
-      H[i * (i + 1) / 2 + j] = acc + (i == j ? (double)lam : 0.0);
-    }
-    double gb = 0.0;
-#pragma unroll
-    for (int k = 0; k < 6 * MAXEE; ++k) gb += (double)J[k][i] * (double)fw[k];
-    g[i] = gb;
-  }
   float lb[MAXA], ub[MAXA];
+  bool fr[MAXA];
+  float zero[MAXA], xn[MAXA], x[MAXA];
 #pragma unroll
   for (int c = 0; c < MAXA; ++c) {
     const bool fx = sh.fixed[c];
     lb[c] = fx ? 0.f : (sh.lo[c] - cfg[c]) * cs[c];
     ub[c] = fx ? 0.f : (sh.hi[c] - cfg[c]) * cs[c];
+    zero[c] = 0.f;
   }
-  // unconstrained Newton step, fixed joints masked, clamped to the box
-  double A[NP], x[MAXA];
-#pragma unroll
-  for (int i = 0; i < MAXA; ++i) {
-    const bool fi = sh.fixed[i];
-#pragma unroll
-    for (int j = 0; j <= i; ++j) A[i * (i + 1) / 2 + j] = (fi || sh.fixed[j]) ? (i == j ? 1.0 : 0.0) : H[i * (i + 1) / 2 + j];
-    x[i] = fi ? 0.0 : -g[i];
-  }
-  chol_packed<MAXA>(A, x);
+  // it = -1: the unconstrained Newton step (fixed joints masked), clamped to
+  // the box; then n_inner active-set re-solves: joints at a bound stay there,
+  // the rest re-solve against g + H p_bound, i.e. with the held joints as
+  // fixed columns at p_bound.  One call site for all of them.
+  constexpr int R = 6 * MAXEE;
+  const int rows = 6 * a.n_ee;
   float p[MAXA];
-#pragma unroll
-  for (int c = 0; c < MAXA; ++c) p[c] = clampf((float)x[c], lb[c], ub[c]);
-  // active-set refinement: joints at a bound stay there, the rest re-solve
-  for (int it = 0; it < a.n_inner; ++it) {
+  for (int it = -1; it < a.n_inner; ++it) {
     bool act[MAXA];
-    float pb[MAXA];
 #pragma unroll
     for (int c = 0; c < MAXA; ++c) {
-      act[c] = p[c] <= lb[c] + 1e-8f || p[c] >= ub[c] - 1e-8f;
-      pb[c] = act[c] ? clampf(p[c], lb[c], ub[c]) : 0.f;
+      act[c] = it < 0 ? (bool)sh.fixed[c] : (p[c] <= lb[c] + 1e-8f || p[c] >= ub[c] - 1e-8f);
+      xn[c] = (it >= 0 && act[c]) ? clampf(p[c], lb[c], ub[c]) : 0.f;
+      fr[c] = !act[c];
     }
+    damped_step_f32<R, MAXA>(J, fw, rows, lam, zero, fr, xn, zero, x);
 #pragma unroll
-    for (int i = 0; i < MAXA; ++i) {
-      double adj = 0.0;
-#pragma unroll
-      for (int j = 0; j < MAXA; ++j) {
-        const double hij = j <= i ? H[i * (i + 1) / 2 + j] : H[j * (j + 1) / 2 + i];
-        adj += hij * (double)pb[j];
-      }
-      x[i] = act[i] ? 0.0 : -(g[i] + adj);
-#pragma unroll
-      for (int j = 0; j <= i; ++j)
-        A[i * (i + 1) / 2 + j] = (act[i] || act[j]) ? (i == j ? 1.0 : 0.0) : H[i * (i + 1) / 2 + j];
-    }
-    chol_packed<MAXA>(A, x);
-#pragma unroll
-    for (int c = 0; c < MAXA; ++c) p[c] = act[c] ? pb[c] : clampf((float)x[c], lb[c], ub[c]);
+    for (int c = 0; c < MAXA; ++c) p[c] = act[c] ? xn[c] : clampf(x[c], lb[c], ub[c]);
   }
   float dn2 = 0.f, max_p = 0.f, max_o = 0.f;
 #pragma unroll

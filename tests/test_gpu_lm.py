@@ -40,12 +40,13 @@ def solver_for(w, **kw):
                          self_pairs=w.self_pairs, device=DEV, **opts)
 
 
-def oracle_run(w, p, max_iter, seeds=None, lam_down=None, lam_up=None, self_pairs=True, coll=True):
+def oracle_run(w, p, max_iter, seeds=None, lam_down=None, lam_up=None, self_pairs=True, coll=True,
+               fixed_mask=None):
     m = w.model.as_dict()
     tj = w.model.link_joint(w.target_link)
     return olm.ls_ik(w.seeds[p] if seeds is None else seeds, w.target_T[p][None, None], m, [tj],
                      [w.model.ancestor_mask(w.target_link)], lower=w.model.lower, upper=w.model.upper,
-                     max_iter=max_iter, lambda_init=w.lambda_init,
+                     fixed_mask=fixed_mask, max_iter=max_iter, lambda_init=w.lambda_init,
                      lambda_down=w.lambda_down if lam_down is None else lam_down,
                      lambda_up=w.lambda_up if lam_up is None else lam_up, enable_collision=coll,
                      collision_weight=w.collision_weight, collision_margin=w.collision_margin,
@@ -113,6 +114,50 @@ def test_lm_fp32_default_success_matches_fp64_solve():
     r32 = solver_for(w).solve(tt(w.target_T), tt(w.seeds))
     n64, n32 = int(r64.success.sum()), int(r32.success.sum())
     assert n32 >= n64 - 2, (n32, n64)
+
+
+@pytest.mark.parametrize("tps", [0, 2])
+@pytest.mark.parametrize("max_iter", [2, 30])
+def test_lm_fixed_joints_seed_by_seed(tps, max_iter):
+    """Joints 0 and 5 fixed: 5 free columns against 6 residual rows, so the
+    damped step goes through the primal system (the dual one would be
+    rank-deficient); seed by seed against the FP64 oracle, and the fixed
+    joints keep their seed values."""
+    w = small_ik(P=3, Sd=40)
+    mask = np.zeros(w.model.n_act, np.int32)
+    mask[[0, 5]] = 1
+    s = solver_for(w, max_iter=max_iter, threads_per_seed=tps)
+    s.set_fixed_mask(mask)
+    cfgs, errs = s.run_lm(tt(w.target_T), tt(w.seeds))
+    cfgs, errs = cfgs.cpu().numpy(), errs.cpu().numpy()
+    np.testing.assert_array_equal(cfgs[..., [0, 5]], w.seeds[..., [0, 5]])
+    ok = 0
+    for p in range(3):
+        oc_, oe = oracle_run(w, p, max_iter, fixed_mask=mask)
+        close = (np.abs(cfgs[p] - oc_).max(axis=1) < 2e-4) & (np.abs(errs[p] - oe) <= 1e-3 * np.abs(oe) + 1e-4)
+        ok += close.sum()
+    record("IK seed disagreement with the FP64 oracle, joints 0 and 5 fixed (fraction)", 1.0 - ok / 120.0,
+           f"3 x 40 seeds, {max_iter} iterations, threads_per_seed {tps}")
+    assert ok >= 0.95 * 3 * 40, ok
+
+
+@pytest.mark.parametrize("tps", [0, 2])
+def test_lm_obstacle_grid_resolution_leaves_results_unchanged(tps):
+    """The default grid of the 100-sphere world (14 cells per axis), 8 and 10
+    cells, 16 cells (whose lists overflow their capacity here and fall back
+    to 8) and no grid give the same bits: the grid only decides which
+    obstacles take the bounding test, and each joint's hinge terms are summed
+    in increasing obstacle order."""
+    w = small_ik(P=4, Sd=64)
+    s = solver_for(w, max_iter=8, threads_per_seed=tps)
+    base = None
+    for grid in (0, 8, 10, 16, -1):
+        s.opt.obstacle_grid = grid
+        c, e = s.run_lm(tt(w.target_T), tt(w.seeds))
+        if base is None:
+            base = (c.clone(), e.clone())
+        else:
+            assert torch.equal(c, base[0]) and torch.equal(e, base[1]), grid
 
 
 def test_lm_fp64_solve_rejects_other_mappings():
