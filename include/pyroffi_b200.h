@@ -162,10 +162,10 @@ typedef struct pk_lm_options {
                               bounding sphere tests only its cell's list; 0 = default (seed-group kernels: 14
                               for up to 160 world spheres, else 8; warp-per-seed body: 8), 1..16 = that many,
                               -1 = no grid (every obstacle takes the bounding test).  A seed-group grid finer
-                              than 8 whose lists overflow their capacity falls back to 8 cells per axis.  The seed-group kernels'
-                              results do not depend on it (each joint's hinge terms are summed in increasing
-                              obstacle order); the warp-per-seed body spreads its candidates over lanes by list
-                              position, so its sums may round differently */
+                              than 8 whose lists overflow their capacity falls back to 8 cells per axis.  With one
+                              lane per seed the results do not depend on it (each joint's hinge terms are summed
+                              in increasing obstacle order); lanes sharing a seed and the warp-per-seed body take
+                              the candidates by list position, so their sums may round differently */
 } pk_lm_options;
 
 /*

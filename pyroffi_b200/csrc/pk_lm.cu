@@ -367,6 +367,7 @@ __device__ __forceinline__ void self_share(const PenaltyCtx& c, const PoseSlots&
 // does not depend on which lane took which item, and the work of a chunk is
 // spread over the warp instead of following the seed with the most
 // surviving groups.  slots_w: the pose slots of the warp's first seed.
+template <bool B4>
 __device__ __forceinline__ void self_warp(const PenaltyCtx& c, float* slots_w, int spb, bool need, float& pen,
                                           unsigned short* list, float* res) {
   const int lane = threadIdx.x & 31;
@@ -376,21 +377,37 @@ __device__ __forceinline__ void self_warp(const PenaltyCtx& c, float* slots_w, i
     const int nc = min(kSelfChunk, c.n_groups - g0);
     unsigned mine = 0u;
     int n_items = 0;
-    for (int i = 0; i < nc; ++i) {
-      bool sv = false;
-      if (need) {
+    // this lane's surviving groups of the chunk (B4: four groups' loads at a time)
+    if (need && !B4) {
+      for (int i = 0; i < nc; ++i) {
         const int2 ja = c.gjoint[g0 + i];
         const float dx = cen[(3 * ja.x) * cs] - cen[(3 * ja.y) * cs];
         const float dy = cen[(3 * ja.x + 1) * cs] - cen[(3 * ja.y + 1) * cs];
         const float dz = cen[(3 * ja.x + 2) * cs] - cen[(3 * ja.y + 2) * cs];
         const float rr = c.jb[ja.x].w + c.jb[ja.y].w + c.margin;
-        sv = dx * dx + dy * dy + dz * dz < rr * fabsf(rr);
+        if (dx * dx + dy * dy + dz * dz < rr * fabsf(rr)) mine |= 1u << i;
       }
+    } else if (need) {
+      for (int i0 = 0; i0 < nc; i0 += 4) {
+        float d2[4], rr[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int2 ja = c.gjoint[g0 + min(i0 + u, nc - 1)];
+          const float dx = cen[(3 * ja.x) * cs] - cen[(3 * ja.y) * cs];
+          const float dy = cen[(3 * ja.x + 1) * cs] - cen[(3 * ja.y + 1) * cs];
+          const float dz = cen[(3 * ja.x + 2) * cs] - cen[(3 * ja.y + 2) * cs];
+          rr[u] = c.jb[ja.x].w + c.jb[ja.y].w + c.margin;
+          d2[u] = dx * dx + dy * dy + dz * dz;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (i0 + u < nc && d2[u] < rr[u] * fabsf(rr[u])) mine |= 1u << (i0 + u);
+      }
+    }
+    for (int i = 0; i < nc; ++i) {
+      const bool sv = (mine >> i) & 1u;
       const unsigned m = __ballot_sync(0xffffffffu, sv);
-      if (sv) {
-        list[n_items + __popc(m & ((1u << lane) - 1u))] = (unsigned short)((lane << 8) | i);
-        mine |= 1u << i;
-      }
+      if (sv) list[n_items + __popc(m & ((1u << lane) - 1u))] = (unsigned short)((lane << 8) | i);
       n_items += __popc(m);
     }
     __syncwarp();
@@ -436,7 +453,11 @@ __device__ __forceinline__ void self_warp(const PenaltyCtx& c, float* slots_w, i
 // TPS == 1: every lane of the warp calls it (need == false: the lane adds
 // nothing but takes part in the warp's self-pair items, self_warp); TPS > 1:
 // the seed's lanes call it when the seed needs it.
-template <int TPS>
+//
+// B4: the grid candidates and the self-pair group culls four per step (their
+// loads in flight together); off for the 16-DOF kernels, whose register
+// state leaves no room for it.
+template <int TPS, bool B4>
 __device__ float penalty_share(const PenaltyCtx& c, const PoseSlots& ps, int t, unsigned gmask, bool need,
                                float* slots_w, int spb, unsigned short* wlist, float* wres) {
   float pen = 0.f;
@@ -474,11 +495,37 @@ __device__ float penalty_share(const PenaltyCtx& c, const PoseSlots& ps, int t, 
         // candidate slot in which any lane has a survivor
         for (int e0 = c.cell_start[cell] + t; e0 < e1; e0 += 32 * TPS) {
           unsigned mask = 0u;
-          for (int i = 0; i < 32 && e0 + i * TPS < e1; ++i) {
-            const float4 O = c.ws[c.cell_obs[e0 + i * TPS]];
-            const float rr = R + O.w;
-            const float dx = Bx - O.x, dy = By - O.y, dz = Bz - O.z;
-            if (dx * dx + dy * dy + dz * dz < rr * fabsf(rr)) mask |= 1u << i;
+          if constexpr (!B4) {
+            for (int i = 0; i < 32 && e0 + i * TPS < e1; ++i) {
+              const float4 O = c.ws[c.cell_obs[e0 + i * TPS]];
+              const float rr = R + O.w;
+              const float dx = Bx - O.x, dy = By - O.y, dz = Bz - O.z;
+              if (dx * dx + dy * dy + dz * dz < rr * fabsf(rr)) mask |= 1u << i;
+            }
+          } else {
+            // four candidates per step, their index and obstacle loads issued
+            // together (independent shared-memory loads in flight instead of
+            // one dependent pair per candidate); past the list end a step reads
+            // obstacle 0 and tests nothing
+            for (int i0 = 0; i0 < 32 && e0 + i0 * TPS < e1; i0 += 4) {
+              int idx[4];
+              bool in[4];
+#pragma unroll
+              for (int u = 0; u < 4; ++u) {
+                const int e = e0 + (i0 + u) * TPS;
+                in[u] = e < e1;
+                idx[u] = in[u] ? (int)c.cell_obs[e] : 0;
+              }
+              float4 O[4];
+#pragma unroll
+              for (int u = 0; u < 4; ++u) O[u] = c.ws[idx[u]];
+#pragma unroll
+              for (int u = 0; u < 4; ++u) {
+                const float rr = R + O[u].w;
+                const float dx = Bx - O[u].x, dy = By - O[u].y, dz = Bz - O[u].z;
+                if (in[u] && dx * dx + dy * dy + dz * dz < rr * fabsf(rr)) mask |= 1u << (i0 + u);
+              }
+            }
           }
           if (mask) {
             const Pose T = ps.load(c.jlist[j]);
@@ -492,7 +539,7 @@ __device__ float penalty_share(const PenaltyCtx& c, const PoseSlots& ps, int t, 
       } else {
         for (int ob = t; ob < c.Ms_pad; ob += 32 * TPS) {
           unsigned mask = 0u;
-  #pragma unroll
+#pragma unroll
           for (int i = 0; i < 32; ++i) {
             const float4 O = c.ws[ob + i * TPS];
             const float rr = R + O.w;
@@ -545,7 +592,7 @@ __device__ float penalty_share(const PenaltyCtx& c, const PoseSlots& ps, int t, 
 
     if (TPS > 1) self_share<TPS>(c, ps, t, pen);
   }
-  if (TPS == 1 && c.n_groups > 0) self_warp(c, slots_w, spb, need, pen, wlist, wres);
+  if (TPS == 1 && c.n_groups > 0) self_warp<B4>(c, slots_w, spb, need, pen, wlist, wres);
   __syncwarp(gmask);
   return pen;
 }
@@ -1157,7 +1204,7 @@ __device__ __forceinline__ void lm_seed_groups(const LmArgs& a, unsigned char* s
   auto penalty = [&](bool need) -> float {
     if (!use_coll) return 0.f;
     if (TPS > 1 && !need) return 0.f;
-    const float share = penalty_share<TPS>(pc, ps, t, gmask, need, slots_w, a.spb, wlist, wres);
+    const float share = penalty_share<TPS, (MAXA <= 8)>(pc, ps, t, gmask, need, slots_w, a.spb, wlist, wres);
     return a.coll_w * group_sum<TPS>(share, gmask);
   };
   // Every lane of the group computes the FK (same values); lane 0 stores it.
