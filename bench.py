@@ -46,9 +46,9 @@ L2_FLUSH_BYTES = 256 << 20
 # pyroffi_b200.profile_cases lm): DRAM bytes read + written (the ~1 MB of outputs were still in L2
 # when the launch ended), and the FP32 work the kernel executed, 2 FLOP per FFMA, 1 per FADD / FMUL,
 # twice that for the packed FFMA2 / FADD2 / FMUL2, summed over threads; the FMA pipe's active share.
-LM_DRAM_BYTES_PER_LAUNCH = 1081856 + 256
-LM_EXECUTED_FLOP_PER_LAUNCH = 29977411322
-LM_FMA_PIPE_PCT = 15.3
+LM_DRAM_BYTES_PER_LAUNCH = 1087744 + 256
+LM_EXECUTED_FLOP_PER_LAUNCH = 29031424050
+LM_FMA_PIPE_PCT = 15.5
 # The same counts for the trajectory kernel's fused forward + backward launch on the 512 x 64 x 7 workload
 # (python -m pyroffi_b200.profile_cases traj) and for the fused FK + collision kernel on the sweep robot's
 # per-link rows (python -m pyroffi_b200.profile_cases fkc5, 4,096 configurations; per configuration).

@@ -366,10 +366,10 @@ __device__ __forceinline__ void self_share(const PenaltyCtx& c, const PoseSlots&
 // each lane adds its own surviving groups' sums in group order.  The result
 // does not depend on which lane took which item, and the work of a chunk is
 // spread over the warp instead of following the seed with the most
-// surviving groups.  slots_w: the pose slots of the warp's first seed.
-template <bool B4>
-__device__ __forceinline__ void self_warp(const PenaltyCtx& c, float* slots_w, int spb, bool need, float& pen,
-                                          unsigned short* list, float* res) {
+// surviving groups.  slots_w: the pose slots of the warp's first seed; b4:
+// the culls four groups per step.
+__device__ __forceinline__ void self_warp(const PenaltyCtx& c, float* slots_w, int spb, bool need, bool b4,
+                                          float& pen, unsigned short* list, float* res) {
   const int lane = threadIdx.x & 31;
   const float* const cen = c.cen;
   const int cs = c.cs;
@@ -378,7 +378,7 @@ __device__ __forceinline__ void self_warp(const PenaltyCtx& c, float* slots_w, i
     unsigned mine = 0u;
     int n_items = 0;
     // this lane's surviving groups of the chunk (B4: four groups' loads at a time)
-    if (need && !B4) {
+    if (need && !b4) {
       for (int i = 0; i < nc; ++i) {
         const int2 ja = c.gjoint[g0 + i];
         const float dx = cen[(3 * ja.x) * cs] - cen[(3 * ja.y) * cs];
@@ -455,14 +455,16 @@ __device__ __forceinline__ void self_warp(const PenaltyCtx& c, float* slots_w, i
 // the seed's lanes call it when the seed needs it.
 //
 // B4: the grid candidates and the self-pair group culls four per step (their
-// loads in flight together); off for the 16-DOF kernels, whose register
-// state leaves no room for it.
+// loads in flight together).  The launch takes it for the one-lane 8-DOF
+// kernel on a fine grid (short lists): on the default grid's longer lists,
+// and in the 16-DOF kernels (registers), it measured slower.
 template <int TPS, bool B4>
 __device__ float penalty_share(const PenaltyCtx& c, const PoseSlots& ps, int t, unsigned gmask, bool need,
                                float* slots_w, int spb, unsigned short* wlist, float* wres) {
   float pen = 0.f;
   float* const cen = c.cen;
   const int cs = c.cs;
+  const bool b4 = B4;
   // bounding centre of joint slot j: kept per seed, or computed here
   auto centre = [&](int j) {
     if (cen) return make_float3(cen[(3 * j) * cs], cen[(3 * j + 1) * cs], cen[(3 * j + 2) * cs]);
@@ -495,7 +497,7 @@ __device__ float penalty_share(const PenaltyCtx& c, const PoseSlots& ps, int t, 
         // candidate slot in which any lane has a survivor
         for (int e0 = c.cell_start[cell] + t; e0 < e1; e0 += 32 * TPS) {
           unsigned mask = 0u;
-          if constexpr (!B4) {
+          if (!b4) {
             for (int i = 0; i < 32 && e0 + i * TPS < e1; ++i) {
               const float4 O = c.ws[c.cell_obs[e0 + i * TPS]];
               const float rr = R + O.w;
@@ -592,7 +594,7 @@ __device__ float penalty_share(const PenaltyCtx& c, const PoseSlots& ps, int t, 
 
     if (TPS > 1) self_share<TPS>(c, ps, t, pen);
   }
-  if (TPS == 1 && c.n_groups > 0) self_warp<B4>(c, slots_w, spb, need, pen, wlist, wres);
+  if (TPS == 1 && c.n_groups > 0) self_warp(c, slots_w, spb, need, b4, pen, wlist, wres);
   __syncwarp(gmask);
   return pen;
 }
@@ -1147,7 +1149,7 @@ __device__ void lm_stage(const LmArgs& a, unsigned char* smem_raw, const LmLayou
 // past `count`, which reads and writes nothing): a done seed's lanes run
 // along without changing its state, so the warp's collective steps
 // (self_warp) always see all 32 lanes.  No block-wide barrier.
-template <int MAXA, int MAXEE, int TPS, bool F64S = false>
+template <int MAXA, int MAXEE, int TPS, bool F64S = false, bool B4 = false>
 __device__ __forceinline__ void lm_seed_groups(const LmArgs& a, unsigned char* smem_raw, const LmLayout& L, int pb,
                                                int count, size_t gs_base) {
   LmShared& sh = *reinterpret_cast<LmShared*>(smem_raw);
@@ -1204,7 +1206,7 @@ __device__ __forceinline__ void lm_seed_groups(const LmArgs& a, unsigned char* s
   auto penalty = [&](bool need) -> float {
     if (!use_coll) return 0.f;
     if (TPS > 1 && !need) return 0.f;
-    const float share = penalty_share<TPS, (MAXA <= 8)>(pc, ps, t, gmask, need, slots_w, a.spb, wlist, wres);
+    const float share = penalty_share<TPS, B4>(pc, ps, t, gmask, need, slots_w, a.spb, wlist, wres);
     return a.coll_w * group_sum<TPS>(share, gmask);
   };
   // Every lane of the group computes the FK (same values); lane 0 stores it.
@@ -1327,7 +1329,7 @@ __device__ __forceinline__ void lm_seed_groups(const LmArgs& a, unsigned char* s
 // thread at 128 registers (a few hundred bytes of spills at MAXA = 8); 2
 // leaves room for the whole seed state, for launches whose shared memory
 // admits only 2 blocks per SM anyway.
-template <int MAXA, int MAXEE, int TPS, int MINB, bool F64S = false>
+template <int MAXA, int MAXEE, int TPS, int MINB, bool F64S = false, bool B4 = false>
 __global__ void __launch_bounds__(128, MINB) lm_kernel(LmArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const LmLayout L = lm_layout(a, TPS);
@@ -1335,7 +1337,7 @@ __global__ void __launch_bounds__(128, MINB) lm_kernel(LmArgs a) {
   lm_stage<MAXA>(a, smem_raw, L, pb);
   const int s_first = blockIdx.x * a.spb;
   const int count = min(a.spb, a.Sd - s_first);
-  lm_seed_groups<MAXA, MAXEE, TPS, F64S>(a, smem_raw, L, pb, count, (size_t)pb * a.Sd + s_first);
+  lm_seed_groups<MAXA, MAXEE, TPS, F64S, B4>(a, smem_raw, L, pb, count, (size_t)pb * a.Sd + s_first);
 }
 
 // Persistent seed-group kernel of pk_ik_batch: blocks take items (class,
@@ -1851,7 +1853,13 @@ static int launch_lm_t(const LmArgs& a0, cudaStream_t st) {
     int dev = 0, sms = 0;
     if (int s = cuda_status(cudaGetDevice(&dev), "cudaGetDevice")) return s;
     if (int s = cuda_status(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attribute")) return s;
-    if ((228 * 1024) / (smem + 1024) >= 3 && (long long)grid.x * grid.y > 2LL * sms) kern = lm_kernel<MAXA, MAXEE, TPS, 4, F64S>;
+    const bool four = (228 * 1024) / (smem + 1024) >= 3 && (long long)grid.x * grid.y > 2LL * sms;
+    if (four) kern = lm_kernel<MAXA, MAXEE, TPS, 4, F64S>;
+    // one lane per seed on a fine grid: the four-per-step candidate loads
+    if constexpr (TPS == 1 && !F64S) {
+      if (a.coll && a.grid_n > kObsGridDefault)
+        kern = four ? lm_kernel<MAXA, MAXEE, 1, 4, false, true> : lm_kernel<MAXA, MAXEE, 1, 2, false, true>;
+    }
   }
   if (int s = set_smem_limit((const void*)kern, smem)) return s;
   kern<<<grid, threads, smem, st>>>(a);
