@@ -291,6 +291,41 @@ def test_tree_robot_two_ees():
     np.testing.assert_allclose(res.pos_err.cpu().numpy(), pe, rtol=1e-6, atol=1e-9)
 
 
+@pytest.mark.parametrize("max_iter", [1, 3])
+def test_tree_robot_two_ees_fixed_joints(max_iter):
+    """15-DOF bimanual tree, two EE targets, five joints fixed: 10 free
+    columns against 12 residual rows, so the 16-DOF kernel solves the primal
+    system (out of line) instead of its usual dual one; seed by seed against
+    the FP64 oracle with the same fixed joints."""
+    rng = np.random.default_rng(23)
+    model = R.bimanual_tree(rng)
+    links = (10, 16)
+    P, Sd = 3, 32
+    tcfg = model.random_cfgs(rng, P)
+    m = model.as_dict()
+    Tj = okin.fk_joints(tcfg, m["twists"], m["parent_tf"], m["parent_idx"], m["act_idx"], m["mimic_mul"],
+                        m["mimic_off"], m["mimic_act_idx"], m["topo_inv"])
+    tj = [model.link_joint(l) for l in links]
+    target = Tj[:, tj].astype(np.float32)
+    seeds = model.random_cfgs(rng, P * Sd).reshape(P, Sd, -1).astype(np.float32)
+    mask = np.zeros(model.n_act, np.int32)
+    mask[[0, 3, 6, 9, 12]] = 1
+    s = BatchIkSolver(model, links, max_iter=max_iter, lambda_init=1e-2, lambda_down=0.1, lambda_up=10.0,
+                      device=DEV)
+    s.set_fixed_mask(mask)
+    cfgs, errs = s.run_lm(tt(target), tt(seeds))
+    cfgs, errs = cfgs.cpu().numpy(), errs.cpu().numpy()
+    np.testing.assert_array_equal(cfgs[..., mask == 1], seeds[..., mask == 1])
+    anc = [model.ancestor_mask(l) for l in links]
+    ok = 0
+    for p in range(P):
+        oc_, oe = olm.ls_ik(seeds[p], target[p][None], m, tj, anc, lower=model.lower, upper=model.upper,
+                            fixed_mask=mask, max_iter=max_iter, lambda_init=1e-2, lambda_down=0.1,
+                            lambda_up=10.0)
+        ok += ((np.abs(cfgs[p] - oc_).max(axis=1) < 2e-4) & (np.abs(errs[p] - oe) <= 1e-3 * np.abs(oe) + 1e-4)).sum()
+    assert ok >= 0.95 * P * Sd, ok
+
+
 def test_lm_ragged_seed_counts():
     """Seeds per problem not a multiple of the block's seed count."""
     w = small_ik(P=2, Sd=37)
