@@ -78,7 +78,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--cpu-sample", type=int, default=8, help="problems per CPU-baseline sample")
+    ap.add_argument("--cpu-sample", type=int, default=64, help="problems per CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true", help="skip the configs 1, 3, 4, 5 measurements")
     return ap.parse_args()
