@@ -34,6 +34,7 @@ struct SeedIkArgs {
   int n_inner;                 // SQP: active-set re-solves per step
   float pos_weight, ori_weight;  // SQP: fixed row weights
   int grid_entries;            // capacity of the sphere-obstacle grid's lists (0: no grid)
+  int grid_n;                  // cells per axis the grid is allocated for
 };
 
 struct SeedIkShared {
@@ -45,6 +46,7 @@ struct SeedIkShared {
   int fixed[PK_MAX_ACT];              // fixed or padding
   int n_groups;                       // joint groups of the robot spheres
   int grid_on;                        // the sphere-obstacle grid is built
+  int grid_n;                         // its cells per axis
   float3 glo, ginv;                   // its origin and inverse cell size
 };
 
@@ -62,6 +64,7 @@ struct RobotSpheresS {
   const int* cell_start;            // obstacle grid (null: scan every world sphere)
   const unsigned short* cell_obs;
   float3 glo, ginv;
+  int gn;                           // cells per axis
 };
 
 __host__ __device__ __forceinline__ size_t seed_ik_spheres_bytes(int n_rs, int nj) {
@@ -79,7 +82,7 @@ __host__ __device__ inline size_t seed_ik_grid_offset(const SeedIkArgs& a) {
 }
 __host__ __device__ inline size_t seed_ik_grid_bytes(const SeedIkArgs& a) {
   if (!a.grid_entries) return 0;
-  return seed_ik_align16(sizeof(int) * (obstacle_grid_cells(kObsGridDefault) + 1)) + seed_ik_align16(2 * (size_t)a.grid_entries) +
+  return seed_ik_align16(sizeof(int) * (obstacle_grid_cells(a.grid_n) + 1)) + seed_ik_align16(2 * (size_t)a.grid_entries) +
          seed_ik_align16(sizeof(int) * (size_t)a.w.Ms);
 }
 __host__ __device__ inline size_t seed_ik_slots_offset(const SeedIkArgs& a) {
@@ -186,24 +189,38 @@ __device__ inline void seed_ik_stage(const SeedIkArgs& a, SeedIkShared& sh, Robo
     unsigned char* g = reinterpret_cast<unsigned char*>(world_dst) + (seed_ik_grid_offset(a) - seed_ik_world_offset(a));
     int* cell_start = reinterpret_cast<int*>(g);
     unsigned short* cell_obs =
-        reinterpret_cast<unsigned short*>(g + seed_ik_align16(sizeof(int) * (obstacle_grid_cells(kObsGridDefault) + 1)));
+        reinterpret_cast<unsigned short*>(g + seed_ik_align16(sizeof(int) * (obstacle_grid_cells(a.grid_n) + 1)));
     int* obox = reinterpret_cast<int*>(reinterpret_cast<unsigned char*>(cell_obs) +
                                        seed_ik_align16(2 * (size_t)a.grid_entries));
     float reach = 0.f;
     for (int k = 0; k < R.ng; ++k) reach = fmaxf(reach, R.bound[k].w);
     reach += a.collision_margin;
     if (tid == 0) {
-      obstacle_grid_bounds(ob.sph, ob.Ms, reach, kObsGridDefault, sh.glo, sh.ginv);
+      sh.grid_n = a.grid_n;
+      obstacle_grid_bounds(ob.sph, ob.Ms, reach, sh.grid_n, sh.glo, sh.ginv);
       sh.grid_on = 1;
     }
     __syncthreads();
-    obstacle_grid_build(ob.sph, ob.Ms, reach, kObsGridDefault, sh.glo, sh.ginv, obox, cell_start, cell_obs, a.grid_entries,
+    obstacle_grid_build(ob.sph, ob.Ms, reach, sh.grid_n, sh.glo, sh.ginv, obox, cell_start, cell_obs, a.grid_entries,
                         sh.grid_on);
+    // a fine grid whose lists overflow the capacity falls back to the default resolution
+    if (!sh.grid_on && sh.grid_n > kObsGridDefault) {
+      __syncthreads();
+      if (tid == 0) {
+        sh.grid_n = kObsGridDefault;
+        obstacle_grid_bounds(ob.sph, ob.Ms, reach, sh.grid_n, sh.glo, sh.ginv);
+        sh.grid_on = 1;
+      }
+      __syncthreads();
+      obstacle_grid_build(ob.sph, ob.Ms, reach, sh.grid_n, sh.glo, sh.ginv, obox, cell_start, cell_obs,
+                          a.grid_entries, sh.grid_on);
+    }
     if (sh.grid_on) {
       R.cell_start = cell_start;
       R.cell_obs = cell_obs;
       R.glo = sh.glo;
       R.ginv = sh.ginv;
+      R.gn = sh.grid_n;
     }
   }
 }
@@ -329,7 +346,7 @@ __device__ __forceinline__ float seed_ik_penalty(const SeedIkArgs& a, const Pose
       }
     };
     if (R.cell_start) {
-      const int cell = obstacle_grid_cell(R.glo, R.ginv, kObsGridDefault, B);
+      const int cell = obstacle_grid_cell(R.glo, R.ginv, R.gn, B);
       if (cell >= 0) {
         const int e1 = R.cell_start[cell + 1];
         for (int e = R.cell_start[cell] + gl; e < e1; e += TPS) {
@@ -374,7 +391,9 @@ static inline int seed_ik_common(SeedIkArgs& a, int n_act, int n_joints, int n_e
   PK_CHECK_ARG(a.iters >= 0, "negative iteration count");
   a.stage_world = a.w.smem_floats() * sizeof(float) <= 48 * 1024;
   const bool want_grid = grid && a.enable_collision && a.stage_world && a.w.Ms >= 32 && a.w.Ms <= 65535;
-  a.grid_entries = want_grid ? std::min(std::max(16 * a.w.Ms, 1024), 8192) : 0;
+  // the LM kernels' default resolution (lm_grid_option) and list capacity
+  a.grid_n = want_grid ? lm_grid_option(0, a.w.Ms) : 0;
+  a.grid_entries = want_grid ? std::min(std::max((a.grid_n > kObsGridDefault ? 80 : 48) * a.w.Ms, 1024), 16384) : 0;
   size_t smem = seed_ik_smem(a, nth);
   if (smem > 200 * 1024 && a.grid_entries) {
     a.grid_entries = 0;
