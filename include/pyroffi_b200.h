@@ -159,10 +159,11 @@ typedef struct pk_lm_options {
                               the FP32 form */
   int32_t obstacle_grid;    /* the LM kernels' obstacle tile: the world spheres are binned into a uniform grid of
                               this many cells per axis, built per block in shared memory, and each joint's
-                              bounding sphere tests only its cell's list; 0 = default (seed-group kernels: 14
-                              for up to 160 world spheres, else 8; warp-per-seed body: 8), 1..16 = that many,
-                              -1 = no grid (every obstacle takes the bounding test).  A seed-group grid finer
-                              than 8 whose lists overflow their capacity falls back to 8 cells per axis.  With one
+                              bounding sphere tests only its cell's list; 0 = default (14 for up to 160 world
+                              spheres, 12 for up to 1024, else 8; the launch keeps 8 where the finer grid's
+                              shared memory would lower the blocks or seeds resident per SM), 1..16 = that many,
+                              -1 = no grid (every obstacle takes the bounding test).  A grid finer than 8 whose
+                              lists overflow their capacity falls back to 8 cells per axis.  With one
                               lane per seed the results do not depend on it (each joint's hinge terms are summed
                               in increasing obstacle order); lanes sharing a seed and the warp-per-seed body take
                               the candidates by list position, so their sums may round differently */

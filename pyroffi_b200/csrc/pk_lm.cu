@@ -161,7 +161,7 @@ __host__ __device__ inline LmLayout lm_layout(const LmArgs& a, int tps, int thre
   }
   L.grid = (a.grid_n > 0 && a.coll && a.w.Ms >= 32 && a.w.Ms <= 65535 && a.w.Ms <= L.scratch_ints) ? 1 : 0;
   // list capacity: a finer grid lists each obstacle in more cells
-  L.max_entries = L.grid ? min(max((a.grid_n > kObsGridDefault ? 80 : 48) * a.w.Ms, 1024), 16384) : 0;
+  L.max_entries = L.grid ? obstacle_grid_capacity(a.grid_n, a.w.Ms) : 0;
   L.rs = o; o = lm_align16(o + 16 * (size_t)n_rs);
   L.rsp = o; o = lm_align16(o + (threads == 0 ? 16 * (size_t)(n_rs + a.m.n_joints) : 0));
   // the world, in stage_world's layout: spheres in ms_pad float4 slots, then

@@ -82,6 +82,7 @@ struct WideLaunch {
   int* queue;         // persistent: item counter; null: grid launch (problem blockIdx.y, seed block blockIdx.x)
   int grid_chunk;     // grid launch: seeds per block
   int grid_n;         // obstacle grid cells per axis (0: no grid)
+  int grid_auto;      // grid_n is the default resolution (the launch may coarsen it)
   WideLayout L;
 };
 
@@ -105,6 +106,7 @@ struct WideShared {
   float4 jb[PK_MAX_JOINTS];        // bounding sphere per slot (joint frame)
   int n_rs, n_pairs;
   int grid_on;
+  int grid_n;                      // cells per axis of the grid in use
   float3 glo, ginv;
   float rmax;
 };
@@ -117,7 +119,7 @@ __host__ inline WideLayout wide_layout(int max_rs, int max_self, int max_joints,
   L.max_rs = max_rs; L.max_self = max_self; L.max_joints = max_joints; L.max_act = max_act;
   L.max_rows = 6 * max_ee; L.nwarps = nwarps;
   L.grid_n = grid_n;
-  L.max_entries = (grid_n > 0 && w.Ms >= 32 && w.Ms <= 65535) ? std::min(std::max(16 * w.Ms, 1024), 8192) : 0;
+  L.max_entries = (grid_n > 0 && w.Ms >= 32 && w.Ms <= 65535) ? obstacle_grid_capacity(grid_n, w.Ms) : 0;
   size_t o = w_align16(sizeof(WideShared));
   L.rs = o; o = w_align16(o + 16 * (size_t)max_rs);
   L.rsj = o; o = w_align16(o + 4 * (size_t)max_rs);
@@ -314,16 +316,30 @@ __device__ void wide_stage_class(const WideLaunch& P, const WideArgs& A, unsigne
     sh.n_pairs = n_pairs;
     // obstacle-grid bounds (world radii already carry the margin)
     sh.grid_on = 0;
+    sh.grid_n = L.grid_n;
     if (L.max_entries > 0 && n_js > 0 && P.coll) {
-      obstacle_grid_bounds(ws4, w.Ms, rmax, L.grid_n, sh.glo, sh.ginv);
+      obstacle_grid_bounds(ws4, w.Ms, rmax, sh.grid_n, sh.glo, sh.ginv);
       sh.grid_on = 1;
     }
   }
   __syncthreads();
 
-  if (sh.grid_on)
-    obstacle_grid_build(ws4, w.Ms, sh.rmax, L.grid_n, sh.glo, sh.ginv, obox, cell_start, cell_obs, L.max_entries,
+  if (sh.grid_on) {
+    obstacle_grid_build(ws4, w.Ms, sh.rmax, sh.grid_n, sh.glo, sh.ginv, obox, cell_start, cell_obs, L.max_entries,
                         sh.grid_on);
+    // a fine grid whose lists overflow the capacity falls back to the default resolution
+    if (!sh.grid_on && sh.grid_n > kObsGridDefault) {
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        sh.grid_n = kObsGridDefault;
+        obstacle_grid_bounds(ws4, w.Ms, sh.rmax, sh.grid_n, sh.glo, sh.ginv);
+        sh.grid_on = 1;
+      }
+      __syncthreads();
+      obstacle_grid_build(ws4, w.Ms, sh.rmax, sh.grid_n, sh.glo, sh.ginv, obox, cell_start, cell_obs,
+                          L.max_entries, sh.grid_on);
+    }
+  }
 }
 
 // Targets of problem pb (threads < n_ee); the caller synchronises.
@@ -451,7 +467,7 @@ __device__ __noinline__ float w_penalty(const WideLaunch& P, const WideShared& s
       const float3 B = pose_apply(w_load(W.T, sh.js_joint[j]), make_float3(bl.x, bl.y, bl.z));
       int e0 = 0, n = Ms;
       if (sh.grid_on) {
-        const int cell = obstacle_grid_cell(sh.glo, sh.ginv, P.L.grid_n, B);
+        const int cell = obstacle_grid_cell(sh.glo, sh.ginv, sh.grid_n, B);
         // outside the grid no obstacle is within reach of this joint
         if (cell < 0) {
           n = 0;
@@ -913,7 +929,8 @@ static void wide_options(WideLaunch& P, const pk_lm_options& o) {
   P.max_iter = o.max_iter; P.pos_w = o.pos_weight; P.ori_w = o.ori_weight; P.lam0 = o.lambda_init;
   P.lam_down = o.lambda_down; P.lam_up = o.lambda_up; P.eps_pos = o.eps_pos; P.eps_ori = o.eps_ori;
   P.coll = o.enable_collision ? 1 : 0; P.coll_w = o.collision_weight; P.margin = o.collision_margin;
-  P.grid_n = obstacle_grid_option(o.obstacle_grid);
+  P.grid_n = lm_grid_option(o.obstacle_grid, P.w.Ms);
+  P.grid_auto = o.obstacle_grid == 0;
 }
 
 static int wide_group(const pk_lm_options& o) { return o.lanes_per_wide_seed == 32 ? 32 : 16; }
@@ -951,15 +968,22 @@ static int run_warp_t(WideLaunch& P, const WideMax& mx, int grid_seeds, int grid
   if (int s = cuda_status(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attribute")) return s;
   int best_threads = 0, best_per_sm = 0, best_groups = -1;
   WideLayout best{};
-  for (int threads = 256; threads >= 64 && threads >= G; threads >>= 1) {
-    const WideLayout L = wide_layout(mx.rs, mx.self, mx.joints, mx.act, mx.ee, P.w, threads / G, P.grid_n);
-    if (L.total > (size_t)max_smem) continue;
-    if (int s = set_smem_limit((const void*)kern, L.total)) return s;
-    int per_sm = 0;
-    if (int s = cuda_status(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, L.total), "occupancy"))
-      return s;
-    const int groups = per_sm * (threads / G);
-    if (groups > best_groups) { best_groups = groups; best_threads = threads; best_per_sm = per_sm; best = L; }
+  // the default grid resolution, and the coarser 8 cells when it keeps more
+  // seeds resident (its lists and cells take less shared memory)
+  const int grids[2] = {P.grid_n, (P.grid_auto && P.grid_n > kObsGridDefault) ? kObsGridDefault : -1};
+  for (int gi = 0; gi < 2; ++gi) {
+    if (grids[gi] < 0) continue;
+    for (int threads = 256; threads >= 64 && threads >= G; threads >>= 1) {
+      const WideLayout L = wide_layout(mx.rs, mx.self, mx.joints, mx.act, mx.ee, P.w, threads / G, grids[gi]);
+      if (L.total > (size_t)max_smem) continue;
+      if (int s = set_smem_limit((const void*)kern, L.total)) return s;
+      int per_sm = 0;
+      if (int s = cuda_status(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, L.total),
+                              "occupancy"))
+        return s;
+      const int groups = per_sm * (threads / G);
+      if (groups > best_groups) { best_groups = groups; best_threads = threads; best_per_sm = per_sm; best = L; }
+    }
   }
   PK_CHECK_CAP(best_threads > 0 && best_per_sm > 0,
                "warp-body LM working set does not fit in %d B of shared memory even for one seed group per block",

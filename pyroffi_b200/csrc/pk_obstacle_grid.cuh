@@ -21,15 +21,27 @@ constexpr int kObsGridMax = 16;
 __host__ __device__ __forceinline__ int obstacle_grid_cells(int G) { return G * G * G; }
 // pk_lm_options.obstacle_grid -> cells per axis: 0 the default, -1 no grid (0 here)
 __host__ __device__ __forceinline__ int obstacle_grid_option(int v) { return v == 0 ? kObsGridDefault : (v < 0 ? 0 : v); }
-// The seed-group LM kernels' default: 14 cells per axis for up to 160
-// obstacle spheres, 8 above.  On the 100-sphere IK benchmark world the finer
-// grid lists 34 candidates per query against 57 (the same 5.5 survive the
-// bounding test), for 2.6x the list entries.
+// The IK kernels' default: 14 cells per axis for up to 160 obstacle
+// spheres, 12 for up to 1024, 8 above, with lists of up to 80 entries per
+// sphere (16384 in all) for the finer grids; a grid whose lists overflow
+// falls back to 8 cells (obstacle_grid_capacity).  On the 100-sphere IK
+// benchmark world the 14-cell grid lists 34 candidates per query against 57
+// at 8 (the same 5.5 survive the bounding test); on the 500-sphere mixed
+// batch world 12 cells list 47-92 candidates per evaluation against 122-150.
 constexpr int kObsGridFine = 14;
 constexpr int kObsGridFineMaxSpheres = 160;
+constexpr int kObsGridMid = 12;
+constexpr int kObsGridMidMaxSpheres = 1024;
 __host__ __device__ __forceinline__ int lm_grid_option(int v, int Ms) {
-  if (v == 0) return Ms <= kObsGridFineMaxSpheres ? kObsGridFine : kObsGridDefault;
+  if (v == 0)
+    return Ms <= kObsGridFineMaxSpheres ? kObsGridFine : (Ms <= kObsGridMidMaxSpheres ? kObsGridMid : kObsGridDefault);
   return obstacle_grid_option(v);
+}
+// List capacity of a grid of G cells per axis over Ms spheres.
+__host__ __device__ __forceinline__ int obstacle_grid_capacity(int G, int Ms) {
+  const int per = G > kObsGridDefault ? 80 : 48;
+  const int c = per * Ms;
+  return c < 1024 ? 1024 : (c > 16384 ? 16384 : c);
 }
 
 // Origin and inverse cell size of the grid (one thread).

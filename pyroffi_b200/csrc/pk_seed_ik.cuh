@@ -393,7 +393,7 @@ static inline int seed_ik_common(SeedIkArgs& a, int n_act, int n_joints, int n_e
   const bool want_grid = grid && a.enable_collision && a.stage_world && a.w.Ms >= 32 && a.w.Ms <= 65535;
   // the LM kernels' default resolution (lm_grid_option) and list capacity
   a.grid_n = want_grid ? lm_grid_option(0, a.w.Ms) : 0;
-  a.grid_entries = want_grid ? std::min(std::max((a.grid_n > kObsGridDefault ? 80 : 48) * a.w.Ms, 1024), 16384) : 0;
+  a.grid_entries = want_grid ? obstacle_grid_capacity(a.grid_n, a.w.Ms) : 0;
   size_t smem = seed_ik_smem(a, nth);
   if (smem > 200 * 1024 && a.grid_entries) {
     a.grid_entries = 0;
