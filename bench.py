@@ -165,18 +165,38 @@ class ClockSampler:
         self.proc = None
         self.file = None
 
+    def _lines(self) -> int:
+        try:
+            return sum(1 for r in Path(self.file.name).read_text().splitlines() if r.strip())
+        except Exception:
+            return 0
+
     def __enter__(self):
+        self.n0 = 0
+        self.after = False
         try:
             self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                  "-lms", "100"], stdout=self.file, stderr=subprocess.DEVNULL)
+            # the sampler is up (its first line written) before the timed region starts
+            t0 = time.time()
+            while self._lines() == 0 and time.time() - t0 < 3.0:
+                time.sleep(0.01)
+            self.n0 = self._lines()
         except Exception:
             self.proc = None
         return self
 
     def __exit__(self, *exc):
         if self.proc is not None:
+            # a timed region shorter than the 100 ms period may hold no sample:
+            # then the first sample after it (clocks still at their load values)
+            if self._lines() <= self.n0:
+                self.after = True
+                t0 = time.time()
+                while self._lines() <= self.n0 and time.time() - t0 < 1.0:
+                    time.sleep(0.005)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -188,6 +208,7 @@ class ClockSampler:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.file.flush()
         rows = [r.split(",") for r in Path(self.file.name).read_text().strip().splitlines() if r.strip()]
+        rows = rows[self.n0:]                      # samples from the timed region on
         sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
         smax = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
         reasons = set()
@@ -198,8 +219,11 @@ class ClockSampler:
             for name, v in zip(names, r[5:9]):
                 if v.strip().lower() == "active":
                     reasons.add(name)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        out = {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+               "reasons": sorted(reasons), "samples": len(sm)}
+        if self.after:
+            out["window"] = "first sample after the timed region (the region is shorter than the 100 ms period)"
+        return out
 
 
 def fp32_peak_tflops(torch, lib_call, stream_ptr):

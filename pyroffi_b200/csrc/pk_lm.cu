@@ -456,8 +456,11 @@ __device__ __forceinline__ void self_warp(const PenaltyCtx& c, float* slots_w, i
 //
 // B4: the grid candidates and the self-pair group culls four per step (their
 // loads in flight together).  The launch takes it for the one-lane 8-DOF
-// kernel on a fine grid (short lists): on the default grid's longer lists,
-// and in the 16-DOF kernels (registers), it measured slower.
+// kernel on a grid of 14 or more cells per axis (short lists): on longer
+// lists, and in the 16-DOF kernels (registers), it measured slower.  The
+// survivors are the same, but the compiler may contract a distance or a
+// hinge sum differently in the two forms (one ulp in about 1 of 2,000
+// outputs was seen).
 template <int TPS, bool B4>
 __device__ float penalty_share(const PenaltyCtx& c, const PoseSlots& ps, int t, unsigned gmask, bool need,
                                float* slots_w, int spb, unsigned short* wlist, float* wres) {
@@ -1855,9 +1858,10 @@ static int launch_lm_t(const LmArgs& a0, cudaStream_t st) {
     if (int s = cuda_status(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attribute")) return s;
     const bool four = (228 * 1024) / (smem + 1024) >= 3 && (long long)grid.x * grid.y > 2LL * sms;
     if (four) kern = lm_kernel<MAXA, MAXEE, TPS, 4, F64S>;
-    // one lane per seed on a fine grid: the four-per-step candidate loads
+    // one lane per seed on the finest default grid (short lists): the
+    // four-per-step candidate loads
     if constexpr (TPS == 1 && !F64S) {
-      if (a.coll && a.grid_n > kObsGridDefault)
+      if (a.coll && a.grid_n >= kObsGridFine)
         kern = four ? lm_kernel<MAXA, MAXEE, 1, 4, false, true> : lm_kernel<MAXA, MAXEE, 1, 2, false, true>;
     }
   }
