@@ -91,11 +91,12 @@ def per_class_reference(w, b):
         if b.counts[c] == 0:
             out.append(None)
             continue
-        # the same kernels as the batch's bodies: 2 lanes x 64 seeds (body 0: lanes per seed change only the
-        # lane that sums each penalty term, the sum order is fixed), one lane per seed (body 2), warp body (1)
-        tps = {BODY_SEED_GROUP: 2, BODY_SEED_GROUP16: 0, BODY_WARP: 16}[b.bodies[c]]
+        # the same mappings as the batch's bodies: one lane per seed (bodies 0 and 2), the warp body (1)
+        tps = {BODY_SEED_GROUP: 1, BODY_SEED_GROUP16: 0, BODY_WARP: 16}[b.bodies[c]]
         s = BatchIkSolver(cl.model, cl.target_links, spheres=cl.spheres, world=w.world, device=DEV,
-                          **opts(w, threads_per_seed=tps, seeds_per_block=64 if tps == 2 else 0))
+                          **opts(w, threads_per_seed=tps))
+        # the batch's grid resolution, named (the default one is fitted to each launch's shared memory)
+        s.opt.obstacle_grid = b.opt.obstacle_grid
         out.append(s.run_lm(b.targets[c], b.seeds[c]))
     return out
 
@@ -117,6 +118,7 @@ def make_batch(w, **kw):
 def test_batch_equals_per_class_launches(mixed):
     w = mixed
     b = make_batch(w)
+    b.opt.obstacle_grid = 12
     assert b.bodies == [BODY_SEED_GROUP, BODY_SEED_GROUP, BODY_SEED_GROUP16, BODY_WARP]
     b.run_lm()
     ref = per_class_reference(w, b)
