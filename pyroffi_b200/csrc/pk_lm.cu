@@ -5,17 +5,20 @@
 // (src/pyroffi/cuda_kernels/_ls_ik_cuda_kernel.cu:65-529).  The iteration is
 // the reference's: residual = world position difference + rotation vector of
 // q_ee * conj(q_tgt); stacked geometric Jacobian; row weights; Jacobi column
-// scaling; FP64 damped normal equations with fixed-joint masking and a
-// Cholesky solve; trust-region clip; 5-point line search on clamped trials;
-// accept/reject of the damping step; all-time best tracking.
+// scaling; damped normal equations with fixed-joint masking and a Cholesky
+// solve (FP64 in the reference; here the FP32 dual system with one
+// conditional FP64 refinement, lm_solve_f32); trust-region clip; 5-point
+// line search on clamped trials; accept/reject of the damping step;
+// all-time best tracking.
 //
 // B200 mapping:
-//  * a group of TPS adjacent lanes owns one seed.  Every lane of the group
-//    runs the (cheap) FK / Jacobian / normal-equation math redundantly, so
-//    the group's decisions are bit-identical without broadcasts, and the
-//    (dominant) collision penalty is split: lane t transforms robot spheres
-//    t, t+TPS, ... and tests them against every obstacle; partial sums meet
-//    in a butterfly shuffle.
+//  * a group of TPS adjacent lanes owns one seed (TPS = 1 by default: one
+//    lane per seed, 128 seeds per block).  Every lane of a group runs the
+//    (cheap) FK / Jacobian / damped-step math redundantly, so the group's
+//    decisions are bit-identical without broadcasts; with TPS > 1 the
+//    (dominant) collision penalty is split over the group's lanes and the
+//    partial sums meet in a butterfly shuffle; with one lane per seed the
+//    self pairs are drained by the whole warp (self_warp).
 //  * robot description, obstacle set, sphere list, limits and this block's
 //    targets are staged once per block in shared memory; joint poses of
 //    each lane live in a bank-strided shared slot array; configuration,
